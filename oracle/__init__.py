@@ -1,0 +1,348 @@
+"""ORACLE — test infrastructure, not product code.
+
+A CPU restatement of PyMatting's closed-form alpha path. Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline / reference legs of
+``bench.py`` import it, and only as the checker or the timed CPU baseline;
+the product package ``pymatting_b200`` never imports it.
+
+Pieces and the reference code each restates (paths inside PyMatting 1.1.15):
+
+* ``cf_laplacian``       pymatting/laplacian/cf_laplacian.py:5-177 (C, bit-exact)
+* ``make_linear_system`` pymatting/laplacian/laplacian.py:5-60
+* ``trimap_split``       pymatting/util/util.py:439-525
+* ``cg``                 pymatting/solver/cg.py:4-117
+* ``jacobi``             pymatting/preconditioner/jacobi.py:1-31
+* ``make_P`` / ``vcycle`` pymatting/preconditioner/vcycle.py:6-153
+* ``ichol``              pymatting/preconditioner/ichol.py:6-301 (C)
+* ``estimate_alpha_cf``  pymatting/alpha/estimate_alpha_cf.py:8-78
+
+Parity of this restatement with the reference itself is pinned by
+``tests/test_oracle.py`` against the fixtures in ``tests/golden/`` that
+``tests/golden/make_golden.py`` produced by running the reference.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+import scipy.sparse
+import scipy.sparse.linalg
+
+from . import build as _build
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        lib = ctypes.CDLL(path)
+        i64 = ctypes.c_int64
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int64)
+        up = ctypes.POINTER(ctypes.c_uint8)
+        lib.oracle_cf_laplacian.argtypes = [dp, i64, i64, ctypes.c_double, i64,
+                                            up, dp, ip, ip]
+        lib.oracle_cf_laplacian.restype = ctypes.c_int
+        lib.oracle_ichol.argtypes = [i64, dp, ip, ip, dp, ip, ip, ctypes.c_double,
+                                     ctypes.c_double, i64, ctypes.c_double,
+                                     ctypes.c_int]
+        lib.oracle_ichol.restype = i64
+        lib.oracle_backsub_L.argtypes = [dp, ip, ip, dp, i64]
+        lib.oracle_backsub_LT.argtypes = [dp, ip, ip, dp, i64]
+        _lib = lib
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+# --------------------------------------------------------------------------
+# Laplacian and linear system
+# --------------------------------------------------------------------------
+
+def cf_laplacian_arrays(image, epsilon=1e-7, radius=1, is_known=None):
+    """Return ``(values, indices, indptr)`` exactly as the reference fills them."""
+    lib = _load()
+    image = np.ascontiguousarray(image, dtype=np.float64)
+    h, w, d = image.shape
+    assert d == 3
+    n = h * w
+    if is_known is None:
+        is_known = np.zeros((h, w), dtype=np.bool_)
+    known = np.ascontiguousarray(np.asarray(is_known).reshape(h, w), dtype=np.uint8)
+    slots = (4 * radius + 1) ** 2
+    values = np.zeros(n * slots, dtype=np.float64)
+    indices = np.zeros(n * slots, dtype=np.int64)
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    rc = lib.oracle_cf_laplacian(_p(image, ctypes.c_double), h, w, float(epsilon),
+                                 int(radius), _p(known, ctypes.c_uint8),
+                                 _p(values, ctypes.c_double),
+                                 _p(indices, ctypes.c_int64),
+                                 _p(indptr, ctypes.c_int64))
+    if rc != 0:
+        raise MemoryError("oracle_cf_laplacian failed")
+    return values, indices, indptr
+
+
+def cf_laplacian(image, epsilon=1e-7, radius=1, is_known=None):
+    h, w, _ = image.shape
+    n = h * w
+    values, indices, indptr = cf_laplacian_arrays(image, epsilon, radius, is_known)
+    return scipy.sparse.csr_matrix((values, indices, indptr), (n, n))
+
+
+def trimap_split(trimap, flatten=True, bg_threshold=0.1, fg_threshold=0.9):
+    if flatten:
+        trimap = trimap.flatten()
+    is_fg = trimap >= fg_threshold
+    is_bg = trimap <= bg_threshold
+    if is_bg.sum() == 0:
+        raise ValueError(
+            "Trimap did not contain background values (values <= %f)" % bg_threshold)
+    if is_fg.sum() == 0:
+        raise ValueError(
+            "Trimap did not contain foreground values (values >= %f)" % fg_threshold)
+    is_known = is_fg | is_bg
+    return is_fg, is_bg, is_known, ~is_known
+
+
+def make_linear_system(L, trimap, lambda_value=100.0, return_c=False):
+    is_fg, _bg, is_known, _unk = trimap_split(trimap)
+    c = lambda_value * is_known
+    b = lambda_value * is_fg
+    A = (L + scipy.sparse.diags(c)).tocsr()
+    A.sum_duplicates()
+    if return_c:
+        return A, b, c
+    return A, b
+
+
+# --------------------------------------------------------------------------
+# Solver and preconditioners
+# --------------------------------------------------------------------------
+
+def cg(A, b, x0=None, atol=0.0, rtol=1e-7, maxiter=10000, callback=None, M=None,
+       reorthogonalize=False):
+    """Preconditioned CG with the reference's update order and exit tests."""
+    if M is None:
+        def precondition(v):
+            return v
+    elif callable(M):
+        precondition = M
+    else:
+        def precondition(v):
+            return M.dot(v)
+    apply = A if callable(A) else A.dot
+
+    x = np.zeros_like(b) if x0 is None else x0.copy()
+    norm_b = np.linalg.norm(b)
+    r = b - apply(x)
+    norm_r = np.linalg.norm(r)
+    if norm_r < atol or norm_r < rtol * norm_b:
+        return x
+    z = precondition(r)
+    p = z.copy()
+    rz = np.inner(r, z)
+    for _ in range(maxiter):
+        r_old = r.copy()
+        Ap = apply(p)
+        alpha = rz / np.inner(p, Ap)
+        x += alpha * p
+        r -= alpha * Ap
+        norm_r = np.linalg.norm(r)
+        if callback is not None:
+            callback(A, x, b, norm_b, r, norm_r)
+        if norm_r < atol or norm_r < rtol * norm_b:
+            return x
+        z = precondition(r)
+        if reorthogonalize:
+            beta = np.inner(r - r_old, z) / rz
+            rz = np.inner(r, z)
+        else:
+            beta = 1.0 / rz
+            rz = np.inner(r, z)
+            beta *= rz
+        p *= beta
+        p += z
+    raise ValueError(
+        "Conjugate gradient descent did not converge within %d iterations" % maxiter)
+
+
+class CounterCallback:
+    def __init__(self):
+        self.n = 0
+
+    def __call__(self, A, x, b, norm_b, r, norm_r):
+        self.n += 1
+
+
+def jacobi(A):
+    inverse_diagonal = 1.0 / A.diagonal()
+    return lambda v: v * inverse_diagonal
+
+
+def make_P(shape):
+    """Full-weighting prolongation/restriction pair (upsample, downsample)."""
+    h, w = shape
+    h2, w2 = h // 2, w // 2
+    n, n2 = h * w, h2 * w2
+    wts = np.float64([1, 2, 1, 2, 4, 2, 1, 2, 1]) / 16
+    cy, cx = np.divmod(np.arange(n2), w2)
+    oy = np.array([-1, -1, -1, 0, 0, 0, 1, 1, 1])
+    ox = np.array([-1, 0, 1, -1, 0, 1, -1, 0, 1])
+    fx = (2 * cx)[:, None] + ox[None, :]
+    fy = (2 * cy)[:, None] + oy[None, :]
+    keep = (fx >= 0) & (fx < w) & (fy >= 0) & (fy <= h)
+    rows = np.broadcast_to(np.arange(n2)[:, None], keep.shape)[keep]
+    cols = (fx + fy * w)[keep]
+    vals = np.broadcast_to(wts[None, :], keep.shape)[keep]
+    down = scipy.sparse.csr_matrix((vals, (rows, cols)), (n2, n))
+    return down.T, down
+
+
+def _jacobi_sweeps(A, diag, b, x, count, omega):
+    if x is None:
+        if count > 0:
+            x = omega * b / diag
+            count -= 1
+        else:
+            x = np.zeros_like(b)
+    for _ in range(count):
+        x = x + omega * (b - A.dot(x)) / diag
+    return x
+
+
+def _vcycle(A, b, shape, cache, pre, post, omega, direct):
+    h, w = shape
+    if h * w <= direct:
+        return scipy.sparse.linalg.spsolve(A, b)
+    if shape not in cache:
+        up, down = make_P(shape)
+        cache[shape] = (up, down, down.dot(A).dot(up), A.diagonal())
+    up, down, coarse_A, diag = cache[shape]
+    x = _jacobi_sweeps(A, diag, b, None, pre, omega)
+    coarse_b = down.dot(b - A.dot(x))
+    x += up.dot(_vcycle(coarse_A, coarse_b, (h // 2, w // 2), cache, pre, post,
+                        omega, direct))
+    return _jacobi_sweeps(A, diag, b, x, post, omega)
+
+
+def vcycle(A, shape, num_pre_iter=1, num_post_iter=1, omega=0.8,
+           direct_solve_size=64, cache=None):
+    if cache is None:
+        cache = {}
+    return lambda r: _vcycle(A, r, shape, cache, num_pre_iter, num_post_iter,
+                             omega, direct_solve_size)
+
+
+class CholeskyDecomposition:
+    def __init__(self, Ltuple):
+        self.Ltuple = Ltuple
+
+    @property
+    def L(self):
+        Lv, Lr, Lp = self.Ltuple
+        n = len(Lp) - 1
+        return scipy.sparse.csc_matrix(self.Ltuple, (n, n))
+
+    def __call__(self, b):
+        lib = _load()
+        Lv, Lr, Lp = self.Ltuple
+        x = np.array(b, dtype=np.float64, copy=True)
+        n = len(x)
+        lib.oracle_backsub_L(_p(Lv, ctypes.c_double), _p(Lr, ctypes.c_int64),
+                             _p(Lp, ctypes.c_int64), _p(x, ctypes.c_double), n)
+        lib.oracle_backsub_LT(_p(Lv, ctypes.c_double), _p(Lr, ctypes.c_int64),
+                              _p(Lp, ctypes.c_int64), _p(x, ctypes.c_double), n)
+        return x
+
+
+ICHOL_SHIFTS = [0.0, 1e-4, 1e-3, 1e-2, 0.1, 0.5, 1.0, 10.0, 100, 1e3, 1e4, 1e5]
+
+
+def ichol(A, discard_threshold=1e-4, shifts=ICHOL_SHIFTS, max_nnz=int(4e9 / 16),
+          relative_discard_threshold=0.0, diag_keep_discarded=True):
+    lib = _load()
+    if isinstance(A, scipy.sparse.csr_matrix):
+        A = A.T
+    if not isinstance(A, scipy.sparse.csc_matrix):
+        raise ValueError("Matrix A must be a scipy.sparse.csc_matrix")
+    if not A.has_canonical_format:
+        A.sum_duplicates()
+    m, n = A.shape
+    assert m == n
+    Av = np.ascontiguousarray(A.data, dtype=np.float64)
+    Ar = np.ascontiguousarray(A.indices, dtype=np.int64)
+    Ap = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    # Fill stays inside the row envelope of A (row i spans columns
+    # first_col[i]..i), so that envelope bounds the factor; sizing by it
+    # instead of max_nnz keeps memory small. The max_nnz test stays exact.
+    first_col = np.arange(n, dtype=np.int64)
+    if A.nnz:
+        cols = np.repeat(np.arange(n, dtype=np.int64), np.diff(Ap))
+        np.minimum.at(first_col, Ar, cols)
+    envelope = int(np.sum(np.arange(n, dtype=np.int64) - np.minimum(first_col, np.arange(n)) + 1))
+    cap = int(max(min(max_nnz, envelope), 1))
+    Lv = np.empty(cap, dtype=np.float64)
+    Lr = np.empty(cap, dtype=np.int64)
+    Lp = np.zeros(n + 1, dtype=np.int64)
+    nnz = -1
+    for shift in shifts:
+        nnz = lib.oracle_ichol(n, _p(Av, ctypes.c_double), _p(Ar, ctypes.c_int64),
+                               _p(Ap, ctypes.c_int64), _p(Lv, ctypes.c_double),
+                               _p(Lr, ctypes.c_int64), _p(Lp, ctypes.c_int64),
+                               float(discard_threshold), float(shift), int(max_nnz),
+                               float(relative_discard_threshold),
+                               int(bool(diag_keep_discarded)))
+        if nnz >= 0:
+            break
+        if nnz == -2 or (nnz == -3):
+            raise ValueError(
+                "Thresholded incomplete Cholesky decomposition failed because more "
+                "than max_nnz non-zero elements were created. Try increasing max_nnz "
+                "or discard_threshold.")
+    if nnz < 0:
+        raise ValueError(
+            "Thresholded incomplete Cholesky decomposition failed due to insufficient "
+            "positive-definiteness of matrix A and diagonal shifts did not help.")
+    return CholeskyDecomposition((Lv[:nnz].copy(), Lr[:nnz].copy(), Lp))
+
+
+# --------------------------------------------------------------------------
+# Alpha estimation
+# --------------------------------------------------------------------------
+
+def estimate_alpha_cf(image, trimap, preconditioner=None, laplacian_kwargs={},
+                      cg_kwargs={}):
+    if preconditioner is None:
+        preconditioner = ichol
+    is_fg, _bg, is_known, is_unknown = trimap_split(trimap)
+    L = cf_laplacian(image, **laplacian_kwargs, is_known=is_known)
+    L_U = L[is_unknown, :][:, is_unknown]
+    R = L[is_unknown, :][:, is_known]
+    m = is_fg[is_known]
+    x = trimap.copy().ravel()
+    x[is_unknown] = cg(L_U, -R.dot(m), M=preconditioner(L_U), **cg_kwargs)
+    return np.clip(x, 0, 1).reshape(trimap.shape)
+
+
+def solve_soft(image, trimap, preconditioner="vcycle", rtol=1e-7, atol=0.0,
+               lambda_value=100.0, maxiter=10000, epsilon=1e-7):
+    """Soft-constraint full-grid solve: returns ``(x, iterations)``."""
+    h, w = trimap.shape
+    A, b = make_linear_system(cf_laplacian(image, epsilon=epsilon), trimap,
+                              lambda_value)
+    if preconditioner == "vcycle":
+        M = vcycle(A, (h, w))
+    elif preconditioner == "jacobi":
+        M = jacobi(A)
+    elif preconditioner == "ichol":
+        M = ichol(A)
+    else:
+        M = None
+    cb = CounterCallback()
+    x = cg(A, b, M=M, rtol=rtol, atol=atol, maxiter=maxiter, callback=cb)
+    return x, cb.n

@@ -1,0 +1,247 @@
+"""Generate the golden fixtures in this folder by running PyMatting itself.
+
+Run in a container where the reference source tree is available:
+
+    python tests/golden/make_golden.py /path/to/pymatting-checkout
+
+The reference is imported in place. Its package ``__init__`` asks
+``importlib.metadata`` for its own version, which fails for a source tree
+that is not pip-installed, so the lookup is answered with "1.1.15" for that
+one name. Outputs are small ``.npz`` files; the tests read only those, never
+the reference tree.
+"""
+
+import importlib.metadata
+import os
+import sys
+
+import numpy as np
+import scipy.sparse
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+
+def import_reference(root):
+    real_version = importlib.metadata.version
+
+    def version(name):
+        if name.lower() == "pymatting":
+            return "1.1.15"
+        return real_version(name)
+
+    importlib.metadata.version = version
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
+    sys.path.insert(0, root)
+    import pymatting  # noqa: E402
+    return pymatting
+
+
+def small_image(rng, h, w):
+    base = rng.uniform(0.1, 0.9, size=(1, 1, 3))
+    img = base + 0.15 * rng.standard_normal((h, w, 3))
+    # A few flat clipped patches exercise the near-singular covariance case.
+    img[: max(h // 3, 1), : max(w // 3, 1), :] = 1.0
+    return np.clip(img, 0.0, 1.0)
+
+
+def gen_cf(pm, rng):
+    cases = [(1, 1, 1, False), (2, 5, 1, False), (3, 3, 1, False), (5, 5, 1, True),
+             (7, 9, 1, False), (16, 13, 1, True), (24, 20, 1, False),
+             (11, 17, 2, False), (9, 8, 2, True)]
+    out = {}
+    for k, (h, w, r, with_known) in enumerate(cases):
+        img = small_image(rng, h, w)
+        if with_known:
+            known = rng.uniform(size=(h, w)) < 0.6
+        else:
+            known = np.zeros((h, w), dtype=bool)
+        eps = 1e-7 if k % 3 else 1e-5
+        L = pm.cf_laplacian(img, epsilon=eps, radius=r, is_known=known)
+        out[f"c{k}_image"] = img
+        out[f"c{k}_known"] = known
+        out[f"c{k}_meta"] = np.array([h, w, r], dtype=np.int64)
+        out[f"c{k}_eps"] = np.array([eps])
+        out[f"c{k}_values"] = L.data
+        out[f"c{k}_indices"] = L.indices.astype(np.int64)
+        out[f"c{k}_indptr"] = L.indptr.astype(np.int64)
+    out["count"] = np.array([len(cases)])
+    np.savez_compressed(os.path.join(HERE, "cf_laplacian_small.npz"), **out)
+
+
+def gen_cg(pm):
+    """The reference's own CG test matrices, with the reference's answers."""
+    np.random.seed(0)
+    out = {}
+    k = 0
+    for n in [1, 5, 10]:
+        x_true = np.random.rand(n)
+        A = np.random.rand(n, n)
+        A += A.T + n * np.eye(n)
+        b = A.dot(x_true)
+        M_jacobi = np.diag(1.0 / np.diag(A))
+        for x0 in [None, np.random.rand(n)]:
+            for mk in ["none", "matrix", "callable"]:
+                M = {"none": None, "matrix": M_jacobi,
+                     "callable": (lambda v, M_=M_jacobi: M_.dot(v))}[mk]
+                cb = pm.CounterCallback()
+                x = pm.cg(A, b, x0=x0, M=M, rtol=0, atol=1e-10, callback=cb)
+                out[f"k{k}_A"] = A
+                out[f"k{k}_b"] = b
+                out[f"k{k}_x0"] = np.zeros(0) if x0 is None else x0
+                out[f"k{k}_M"] = np.array([["none", "matrix", "callable"].index(mk)])
+                out[f"k{k}_x"] = x
+                out[f"k{k}_iters"] = np.array([cb.n])
+                k += 1
+    out["count"] = np.array([k])
+    # Docstring examples of cg / jacobi / vcycle / ichol.
+    A = np.array([[3.0, 1.0], [1.0, 2.0]])
+    out["doc_cg"] = pm.cg(A, np.array([4.0, 3.0]), M=pm.jacobi(A))
+    out["doc_jacobi"] = pm.jacobi(np.array([[2, 3], [3, 5]]))(np.array([1, 2]))
+    out["doc_vcycle"] = pm.vcycle(np.array([[2, 3], [3, 5]]), (2, 2))(np.array([1, 2]))
+    out["doc_ichol"] = pm.ichol(scipy.sparse.csc_matrix(np.array([[2.0, 3.0], [3.0, 5.0]])))(
+        np.array([1.0, 2.0]))
+    np.savez_compressed(os.path.join(HERE, "cg_small.npz"), **out)
+
+
+def _store_csc(out, k, A):
+    A = scipy.sparse.csc_matrix(A)
+    A.sum_duplicates()
+    out[f"k{k}_A_data"] = A.data
+    out[f"k{k}_A_indices"] = A.indices.astype(np.int64)
+    out[f"k{k}_A_indptr"] = A.indptr.astype(np.int64)
+
+
+def gen_ichol(pm, rng):
+    """Reference factors: the test_ichol matrices plus thresholded CF systems."""
+    out = {}
+    np.random.seed(0)
+    k = 0
+    for _ in range(4):
+        n = 50
+        A = np.random.rand(n, n)
+        A[np.random.rand(n, n) < 0.8] = 0
+        A += A.T + n * np.eye(n)
+        Ac = scipy.sparse.csc_matrix(A)
+        dec = pm.ichol(Ac, discard_threshold=0.0, max_nnz=100000)
+        Lv, Lr, Lp = dec.Ltuple
+        _store_csc(out, k, Ac)
+        out[f"k{k}_params"] = np.array([0.0, 0.0, 1.0])
+        out[f"k{k}_Lv"], out[f"k{k}_Lr"], out[f"k{k}_Lp"] = Lv, Lr, Lp
+        k += 1
+    # Hard-constraint CF system L_U of a small synthetic problem, with the
+    # default and stronger thresholds (both the absolute and relative paths).
+    from pymatting_b200.synthetic import make_matting_problem
+    img, tri, _, _ = make_matting_problem(30, 40, 11, sigma=2.0, band=3,
+                                          unknown_fraction=0.3)
+    is_fg, is_bg, is_known, is_unknown = pm.trimap_split(tri)
+    L = pm.cf_laplacian(img, is_known=is_known)
+    L_U = L[is_unknown, :][:, is_unknown]
+    for params in [(1e-4, 0.0, 1.0), (1e-2, 0.0, 1.0), (1e-4, 0.05, 1.0),
+                   (1e-3, 0.0, 0.0)]:
+        thr, rel, keep = params
+        dec = pm.ichol(L_U.copy(), discard_threshold=thr,
+                       relative_discard_threshold=rel,
+                       diag_keep_discarded=bool(keep))
+        Lv, Lr, Lp = dec.Ltuple
+        # ichol factors the CSC view of L_U's transpose (a CSR input is
+        # transposed first), whose bits differ from L_U's own columns.
+        _store_csc(out, k, L_U.T)
+        out[f"k{k}_params"] = np.array(params)
+        out[f"k{k}_Lv"], out[f"k{k}_Lr"], out[f"k{k}_Lp"] = Lv, Lr, Lp
+        k += 1
+    out["count"] = np.array([k])
+    np.savez_compressed(os.path.join(HERE, "ichol_small.npz"), **out)
+
+
+def gen_soft(pm):
+    """Soft-constraint system of a small synthetic image: vcycle output and
+    CG results for every preconditioner."""
+    from pymatting_b200.synthetic import make_matting_problem
+    out = {}
+    for k, (h, w, seed) in enumerate([(30, 40, 3), (37, 29, 4)]):
+        img, tri, _, _ = make_matting_problem(h, w, seed, sigma=2.0, band=3,
+                                              unknown_fraction=0.25)
+        A, b = pm.make_linear_system(pm.cf_laplacian(img), tri)
+        rng = np.random.default_rng(seed)
+        v = rng.standard_normal(h * w)
+        out[f"k{k}_image"], out[f"k{k}_trimap"] = img, tri
+        out[f"k{k}_b"] = b
+        out[f"k{k}_A_data"] = A.data
+        out[f"k{k}_A_indices"] = A.indices.astype(np.int64)
+        out[f"k{k}_A_indptr"] = A.indptr.astype(np.int64)
+        out[f"k{k}_v"] = v
+        out[f"k{k}_vcycle_v"] = pm.vcycle(A, (h, w))(v)
+        out[f"k{k}_vcycle_v_2_3"] = pm.vcycle(A, (h, w), num_pre_iter=2,
+                                              num_post_iter=3, omega=0.7)(v)
+        for name, fac in [("none", lambda A: None), ("jacobi", pm.jacobi),
+                          ("vcycle", lambda A: pm.vcycle(A, (h, w))),
+                          ("ichol", pm.ichol)]:
+            cb = pm.CounterCallback()
+            x = pm.cg(A, b, M=fac(A), rtol=1e-7, callback=cb)
+            out[f"k{k}_x_{name}"] = x
+            out[f"k{k}_it_{name}"] = np.array([cb.n])
+    out["count"] = np.array([2])
+    np.savez_compressed(os.path.join(HERE, "soft_small.npz"), **out)
+
+
+def gen_lemur(pm, root):
+    """The reference tests' lemur inputs and the values they pin."""
+    cwd = os.getcwd()
+    os.chdir(root)
+    try:
+        out = {}
+        image = pm.load_image("data/lemur/lemur.png", "rgb", 0.125, "bilinear")
+        trimap = pm.load_image("data/lemur/lemur_trimap.png", "gray", 0.125, "nearest")
+        out["s0125_image"], out["s0125_trimap"] = image, trimap
+        A, b = pm.make_linear_system(pm.cf_laplacian(image), trimap)
+        for name, fac in [("none", lambda A: None), ("jacobi", pm.jacobi),
+                          ("icholt", lambda A: pm.ichol(A, max_nnz=500000)),
+                          ("vcycle", lambda A: pm.vcycle(A, trimap.shape))]:
+            cb = pm.CounterCallback()
+            x = pm.cg(A, b, M=fac(A), atol=1e-6, rtol=0, maxiter=10000, callback=cb)
+            out[f"s0125_it_{name}"] = np.array([cb.n])
+            out[f"s0125_x_{name}"] = x
+
+        image = pm.load_image("data/lemur/lemur.png", "rgb", 0.1, "bilinear")
+        trimap = pm.load_image("data/lemur/lemur_trimap.png", "gray", 0.1, "nearest")
+        good = pm.load_image("data/lemur/lemur_alpha_fba.png", "gray", 0.1, "bilinear")
+        out["s01_image"], out["s01_trimap"], out["s01_good"] = image, trimap, good
+        out["s01_alpha_cf"] = pm.estimate_alpha_cf(image, trimap)
+        A, b = pm.make_linear_system(pm.cf_laplacian(image), trimap)
+        import scipy.sparse.linalg
+        out["s01_x_soft_direct"] = scipy.sparse.linalg.spsolve(A, b)
+        np.savez_compressed(os.path.join(HERE, "lemur.npz"), **out)
+    finally:
+        os.chdir(cwd)
+
+
+def gen_c1(pm):
+    """estimate_alpha_cf on the 320x240 synthetic workload (default ichol)."""
+    from pymatting_b200.synthetic import make_matting_problem
+    img, tri, _, frac = make_matting_problem(240, 320, 1, sigma=2.0, band=7,
+                                             unknown_fraction=0.12)
+    alpha = pm.estimate_alpha_cf(img, tri)
+    unknown = (tri > 0.1) & (tri < 0.9)
+    np.savez_compressed(os.path.join(HERE, "synthetic_320x240.npz"),
+                        image_sum=np.array([img.sum(), tri.sum()]),
+                        alpha_unknown=alpha[unknown], frac=np.array([frac]))
+
+
+def main():
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    pm = import_reference(root)
+    rng = np.random.default_rng(2024)
+    only = sys.argv[2:]
+    for name, fn in [("cf", lambda: gen_cf(pm, rng)), ("cg", lambda: gen_cg(pm)),
+                     ("ichol", lambda: gen_ichol(pm, rng)), ("soft", lambda: gen_soft(pm)),
+                     ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm))]:
+        if not only or name in only:
+            fn()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,132 @@
+"""Pin the oracle (CPU restatement) against the reference's own outputs.
+
+The fixtures in tests/golden were produced by running PyMatting itself
+(tests/golden/make_golden.py). Here the oracle must reproduce them: the
+Laplacian bit for bit, the solver and preconditioners within rounding.
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse
+
+import oracle
+from tests.conftest import golden
+
+
+def test_cf_laplacian_bit_exact():
+    g = golden("cf_laplacian_small.npz")
+    for k in range(int(g["count"][0])):
+        h, w, r = (int(v) for v in g[f"c{k}_meta"])
+        values, indices, indptr = oracle.cf_laplacian_arrays(
+            g[f"c{k}_image"], float(g[f"c{k}_eps"][0]), r, g[f"c{k}_known"])
+        np.testing.assert_array_equal(indices, g[f"c{k}_indices"])
+        np.testing.assert_array_equal(indptr, g[f"c{k}_indptr"])
+        # Same IEEE operation order as the reference: identical bits.
+        np.testing.assert_array_equal(values, g[f"c{k}_values"])
+
+
+def test_cg_reference_cases():
+    g = golden("cg_small.npz")
+    for k in range(int(g["count"][0])):
+        A, b = g[f"k{k}_A"], g[f"k{k}_b"]
+        x0 = g[f"k{k}_x0"]
+        x0 = None if x0.size == 0 else x0
+        mk = int(g[f"k{k}_M"][0])
+        Mj = np.diag(1.0 / np.diag(A))
+        M = [None, Mj, lambda v: Mj.dot(v)][mk]
+        cb = oracle.CounterCallback()
+        x = oracle.cg(A, b, x0=x0, M=M, rtol=0, atol=1e-10, callback=cb)
+        assert cb.n == int(g[f"k{k}_iters"][0])
+        np.testing.assert_allclose(x, g[f"k{k}_x"], rtol=0, atol=1e-12)
+        assert np.linalg.norm(A.dot(x) - b) < 1e-10
+
+
+def test_docstring_examples():
+    g = golden("cg_small.npz")
+    A = np.array([[3.0, 1.0], [1.0, 2.0]])
+    np.testing.assert_allclose(oracle.cg(A, np.array([4.0, 3.0]), M=oracle.jacobi(A)),
+                               g["doc_cg"], atol=1e-12)
+    np.testing.assert_allclose(
+        oracle.jacobi(np.array([[2, 3], [3, 5]]))(np.array([1, 2])), g["doc_jacobi"])
+    np.testing.assert_allclose(
+        oracle.vcycle(np.array([[2, 3], [3, 5]]), (2, 2))(np.array([1, 2])),
+        g["doc_vcycle"], atol=1e-12)
+    d = oracle.ichol(scipy.sparse.csc_matrix(np.array([[2.0, 3.0], [3.0, 5.0]])))
+    np.testing.assert_allclose(d(np.array([1.0, 2.0])), g["doc_ichol"], atol=1e-12)
+
+
+def _csc(g, k):
+    n = len(g[f"k{k}_A_indptr"]) - 1
+    return scipy.sparse.csc_matrix(
+        (g[f"k{k}_A_data"], g[f"k{k}_A_indices"], g[f"k{k}_A_indptr"]), (n, n))
+
+
+def test_ichol_factors_match_reference():
+    g = golden("ichol_small.npz")
+    for k in range(int(g["count"][0])):
+        A = _csc(g, k)
+        thr, rel, keep = (float(v) for v in g[f"k{k}_params"])
+        d = oracle.ichol(A, discard_threshold=thr, relative_discard_threshold=rel,
+                         diag_keep_discarded=bool(keep),
+                         max_nnz=100000 if thr == 0.0 else int(4e9 / 16))
+        Lv, Lr, Lp = d.Ltuple
+        np.testing.assert_array_equal(Lp, g[f"k{k}_Lp"])
+        np.testing.assert_array_equal(Lr, g[f"k{k}_Lr"])
+        np.testing.assert_array_equal(Lv, g[f"k{k}_Lv"])
+
+
+def test_soft_system_and_vcycle():
+    g = golden("soft_small.npz")
+    for k in range(int(g["count"][0])):
+        img, tri = g[f"k{k}_image"], g[f"k{k}_trimap"]
+        h, w = tri.shape
+        A, b = oracle.make_linear_system(oracle.cf_laplacian(img), tri)
+        np.testing.assert_array_equal(A.indptr, g[f"k{k}_A_indptr"])
+        np.testing.assert_array_equal(A.indices, g[f"k{k}_A_indices"])
+        np.testing.assert_array_equal(A.data, g[f"k{k}_A_data"])
+        np.testing.assert_array_equal(b, g[f"k{k}_b"])
+        v = g[f"k{k}_v"]
+        np.testing.assert_allclose(oracle.vcycle(A, (h, w))(v), g[f"k{k}_vcycle_v"],
+                                   rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(
+            oracle.vcycle(A, (h, w), num_pre_iter=2, num_post_iter=3, omega=0.7)(v),
+            g[f"k{k}_vcycle_v_2_3"], rtol=1e-10, atol=1e-12)
+        for name in ["none", "jacobi", "vcycle", "ichol"]:
+            M = {"none": None, "jacobi": oracle.jacobi(A),
+                 "vcycle": oracle.vcycle(A, (h, w)), "ichol": oracle.ichol(A)}[name]
+            cb = oracle.CounterCallback()
+            x = oracle.cg(A, b, M=M, rtol=1e-7, callback=cb)
+            assert abs(cb.n - int(g[f"k{k}_it_{name}"][0])) <= 1
+            np.testing.assert_allclose(x, g[f"k{k}_x_{name}"], rtol=0, atol=1e-6)
+
+
+def test_lemur_pins():
+    """The reference tests' iteration caps and the Laplacian error pin."""
+    g = golden("lemur.npz")
+    image, trimap = g["s0125_image"], g["s0125_trimap"]
+    A, b = oracle.make_linear_system(oracle.cf_laplacian(image), trimap)
+    caps = {"none": 378, "jacobi": 197, "icholt": 3, "vcycle": 48}
+    for name, fac in [("none", lambda A: None), ("jacobi", oracle.jacobi),
+                      ("icholt", lambda A: oracle.ichol(A, max_nnz=500000)),
+                      ("vcycle", lambda A: oracle.vcycle(A, trimap.shape))]:
+        cb = oracle.CounterCallback()
+        x = oracle.cg(A, b, M=fac(A), atol=1e-6, rtol=0, callback=cb)
+        assert np.linalg.norm(b - A.dot(x)) <= 1e-6
+        assert cb.n <= caps[name]
+        assert cb.n == int(g[f"s0125_it_{name}"][0])
+    image, trimap, good = g["s01_image"], g["s01_trimap"], g["s01_good"]
+    alpha = oracle.estimate_alpha_cf(image, trimap)
+    np.testing.assert_allclose(alpha, g["s01_alpha_cf"], rtol=0, atol=1e-9)
+    assert np.linalg.norm(alpha - good) < 1.68
+
+
+def test_synthetic_320x240_estimate_alpha_cf():
+    """The first workload: estimate_alpha_cf (ichol default) on 320x240."""
+    from pymatting_b200.synthetic import make_matting_problem
+    g = golden("synthetic_320x240.npz")
+    img, tri, _, frac = make_matting_problem(240, 320, 1, sigma=2.0, band=7,
+                                             unknown_fraction=0.12)
+    np.testing.assert_allclose([img.sum(), tri.sum()], g["image_sum"], rtol=1e-12)
+    alpha = oracle.estimate_alpha_cf(img, tri)
+    unknown = (tri > 0.1) & (tri < 0.9)
+    np.testing.assert_allclose(alpha[unknown], g["alpha_unknown"], rtol=0, atol=1e-9)
