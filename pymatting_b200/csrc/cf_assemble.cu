@@ -1,0 +1,496 @@
+// Closed-form matting Laplacian assembly on the device.
+//
+// Restates pymatting/laplacian/cf_laplacian.py:5-129 (_cf_laplacian) without
+// its serial scatter: every thread owns one pixel i and gathers the entries
+// of row i from the (2r+1)^2 windows that contain it. A CTA first computes
+// the coefficients of every window touching its tile (colour mean and the
+// inverse of the epsilon-regularised covariance, :38-92) into shared memory,
+// then each thread walks its windows in raster order and adds
+//     delta_ij - (1 + c_i' M c_j) / |w|                         (:95-129)
+// to slot (j - i). Windows fully inside the known region are skipped (:34).
+//
+// This translation unit is compiled with -fmad=false and every expression
+// keeps the reference's operation order, so each slot receives the same
+// rounded terms in the same order as the reference loop: the values are
+// bitwise identical to PyMatting's CSR data.
+#include "pm_common.cuh"
+
+namespace pmb {
+
+enum { kModeEll = 0, kModeHalf = 1, kModeHard = 2 };
+
+constexpr int kAT = 16;  // assembly tile (kAT x kAT pixels, one per thread)
+
+struct AssembleArgs {
+    const double* image;      // h*w*3, interleaved RGB
+    const uint8_t* known;     // h*w (may be null: nothing known)
+    int h, w;
+    double epsilon;
+    // kModeEll
+    double* values;           // n * (4r+1)^2
+    int64_t* indices;         // n * (4r+1)^2
+    int64_t* indptr;          // n + 1
+    // kModeHalf / kModeHard
+    double* planes;           // kNH planes of h*pitch
+    int pitch;
+    const uint8_t* diag_mask; // kModeHalf: centre += diag_value where mask
+    double diag_value;
+    const uint8_t* fg;        // kModeHard: foreground mask (1 where trimap >= 0.9)
+    double* rhs;              // kModeHard: pitched right-hand side -R m
+};
+
+template <int R, int MODE>
+__global__ void __launch_bounds__(kAT * kAT)
+cf_assemble_kernel(AssembleArgs a) {
+    constexpr int SZ = 2 * R + 1;          // window side
+    constexpr int WA = SZ * SZ;            // window area
+    constexpr int S = 4 * R + 1;           // stencil side
+    constexpr int NS = S * S;              // slots per row
+    constexpr int IW = kAT + 4 * R;        // image tile side (halo 2R)
+    constexpr int WW = kAT + 2 * R;        // window tile side (halo R)
+
+    __shared__ double s_img[IW * IW * 3];
+    __shared__ uint8_t s_known[IW * IW];
+    __shared__ double s_mean[WW * WW * 3];
+    __shared__ double s_m[WW * WW * 6];
+    __shared__ uint8_t s_act[WW * WW];
+
+    const int h = a.h, w = a.w;
+    const int x0 = blockIdx.x * kAT, y0 = blockIdx.y * kAT;
+    const int tid = threadIdx.x;
+
+    for (int q = tid; q < IW * IW; q += blockDim.x) {
+        int ly = q / IW, lx = q % IW;
+        int y = y0 - 2 * R + ly, x = x0 - 2 * R + lx;
+        bool in = (y >= 0 && y < h && x >= 0 && x < w);
+        int64_t gi = (int64_t)y * w + x;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s_img[q * 3 + c] = in ? a.image[gi * 3 + c] : 0.0;
+        s_known[q] = in ? (a.known ? a.known[gi] : 0) : 1;
+    }
+    __syncthreads();
+
+    const double wa = (double)WA;
+    for (int q = tid; q < WW * WW; q += blockDim.x) {
+        int ly = q / WW, lx = q % WW;
+        int ky = y0 - R + ly, kx = x0 - R + lx;
+        bool act = (ky >= R && ky < h - R && kx >= R && kx < w - R);
+        if (act) {
+            bool all_known = true;
+            for (int dy = 0; dy < SZ; ++dy)
+                for (int dx = 0; dx < SZ; ++dx)
+                    all_known = all_known && s_known[(ly + dy) * IW + (lx + dx)];
+            act = !all_known;
+        }
+        s_act[q] = act;
+        if (!act) continue;
+        double mean[3];
+        for (int c = 0; c < 3; ++c) {
+            double s = 0.0;
+            for (int dy = 0; dy < SZ; ++dy)
+                for (int dx = 0; dx < SZ; ++dx)
+                    s += s_img[((ly + dy) * IW + (lx + dx)) * 3 + c];
+            mean[c] = s / wa;
+            s_mean[q * 3 + c] = mean[c];
+        }
+        double a00 = a.epsilon, a01 = 0.0, a02 = 0.0;
+        double a11 = a.epsilon, a12 = 0.0, a22 = a.epsilon;
+        for (int dy = 0; dy < SZ; ++dy) {
+            for (int dx = 0; dx < SZ; ++dx) {
+                const double* p = s_img + ((ly + dy) * IW + (lx + dx)) * 3;
+                double c0 = p[0] - mean[0], c1 = p[1] - mean[1], c2 = p[2] - mean[2];
+                a00 += c0 * c0;
+                a01 += c0 * c1;
+                a02 += c0 * c2;
+                a11 += c1 * c1;
+                a12 += c1 * c2;
+                a22 += c2 * c2;
+            }
+        }
+        a00 /= wa; a01 /= wa; a02 /= wa;
+        a11 /= wa; a12 /= wa; a22 /= wa;
+        double det = a00 * a12 * a12 + a01 * a01 * a22 + a02 * a02 * a11
+                     - a00 * a11 * a22 - 2 * a01 * a02 * a12;
+        double inv_det = 1.0 / det;
+        s_m[q * 6 + 0] = (a12 * a12 - a11 * a22) * inv_det;
+        s_m[q * 6 + 1] = (a01 * a22 - a02 * a12) * inv_det;
+        s_m[q * 6 + 2] = (a02 * a11 - a01 * a12) * inv_det;
+        s_m[q * 6 + 3] = (a02 * a02 - a00 * a22) * inv_det;
+        s_m[q * 6 + 4] = (a00 * a12 - a01 * a02) * inv_det;
+        s_m[q * 6 + 5] = (a01 * a01 - a00 * a11) * inv_det;
+    }
+    __syncthreads();
+
+    const int tx = tid % kAT, ty = tid / kAT;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= w || y >= h) return;
+    const int64_t i = (int64_t)y * w + x;
+
+    // Row accumulators. In the half mode only forward slots are needed.
+    double acc[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) acc[q] = 0.0;
+
+    const double* Ii = s_img + ((ty + 2 * R) * IW + (tx + 2 * R)) * 3;
+#pragma unroll
+    for (int wy = 0; wy < SZ; ++wy) {          // window centre ky = y - R + wy
+#pragma unroll
+        for (int wx = 0; wx < SZ; ++wx) {      // window centre kx = x - R + wx
+            const int q = (ty + wy) * WW + (tx + wx);
+            if (!s_act[q]) continue;
+            const double* mu = s_mean + q * 3;
+            const double* m = s_m + q * 6;
+            double s = Ii[0] - mu[0], t = Ii[1] - mu[1], u = Ii[2] - mu[2];
+            double c0 = m[0] * s + m[1] * t + m[2] * u;
+            double c1 = m[1] * s + m[3] * t + m[4] * u;
+            double c2 = m[2] * s + m[4] * t + m[5] * u;
+            // Window (wy, wx) covers rows y-2R+wy .. y+wy and columns
+            // x-2R+wx .. x+wx; (jy, jx) walks them in raster order.
+#pragma unroll
+            for (int jy = 0; jy < SZ; ++jy) {
+#pragma unroll
+                for (int jx = 0; jx < SZ; ++jx) {
+                    const int ddy = wy - 2 * R + jy;   // (yj - yi)
+                    const int ddx = wx - 2 * R + jx;   // (xj - xi)
+                    if (MODE == kModeHalf && half_index(ddy, ddx) < 0) continue;
+                    const double* Ij = s_img + ((ty + 2 * R + ddy) * IW + (tx + 2 * R + ddx)) * 3;
+                    double cj0 = Ij[0] - mu[0], cj1 = Ij[1] - mu[1], cj2 = Ij[2] - mu[2];
+                    double temp = c0 * cj0 + c1 * cj1 + c2 * cj2;
+                    double value = ((ddy == 0 && ddx == 0) ? 1.0 : 0.0) - (1 + temp) / wa;
+                    acc[(ddy + 2 * R) * S + (ddx + 2 * R)] += value;
+                }
+            }
+        }
+    }
+
+    if (MODE == kModeEll) {
+        const int64_t base = i * NS;
+#pragma unroll
+        for (int dy = -2 * R; dy <= 2 * R; ++dy) {
+#pragma unroll
+            for (int dx = -2 * R; dx <= 2 * R; ++dx) {
+                const int slot = (dy + 2 * R) * S + (dx + 2 * R);
+                const int yj = y + dy, xj = x + dx;
+                const bool in = (yj >= 0 && yj < h && xj >= 0 && xj < w);
+                double v = acc[slot];
+                if (dy == 0 && dx == 0 && a.diag_mask && a.diag_mask[i]) v = v + a.diag_value;
+                a.values[base + slot] = v;
+                a.indices[base + slot] = in ? ((int64_t)yj * w + xj) : 0;
+            }
+        }
+        a.indptr[i + 1] = base + NS;
+        if (i == 0) a.indptr[0] = 0;
+    } else {
+        const int64_t pstride = (int64_t)h * a.pitch;
+        const int64_t pi = (int64_t)y * a.pitch + x;
+        const bool ki = a.known ? a.known[i] != 0 : false;
+#pragma unroll
+        for (int p = 0; p < kNH; ++p) {
+            const int dy = half_dy(p), dx = half_dx(p);
+            const int slot = (dy + 2) * S + (dx + 2);
+            const int yj = y + dy, xj = x + dx;
+            const bool in = (yj >= 0 && yj < h && xj >= 0 && xj < w);
+            double v = in ? acc[slot] : 0.0;
+            if (MODE == kModeHalf) {
+                if (p == 0 && a.diag_mask && a.diag_mask[i]) v = v + a.diag_value;
+            } else {
+                // Hard constraints: keep only unknown-unknown couplings; a
+                // known pixel's row becomes the identity.
+                if (p == 0) {
+                    v = ki ? 1.0 : v;
+                } else {
+                    const bool kj = in ? a.known[(int64_t)yj * w + xj] != 0 : true;
+                    v = (ki || kj) ? 0.0 : v;
+                }
+            }
+            a.planes[p * pstride + pi] = v;
+        }
+        if (MODE == kModeHard) {
+            // -R m with m = is_fg on the known columns, summed in column order
+            // as scipy's CSR product does (estimate_alpha_cf.py:66-74).
+            double sum = 0.0;
+            if (!ki) {
+#pragma unroll
+                for (int dy = -2; dy <= 2; ++dy) {
+#pragma unroll
+                    for (int dx = -2; dx <= 2; ++dx) {
+                        const int yj = y + dy, xj = x + dx;
+                        if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
+                        const int64_t j = (int64_t)yj * w + xj;
+                        if (!a.known[j]) continue;
+                        const double m = a.fg[j] ? 1.0 : 0.0;
+                        sum += acc[(dy + 2) * S + (dx + 2)] * m;
+                    }
+                }
+            }
+            a.rhs[pi] = ki ? 0.0 : -sum;
+        }
+    }
+}
+
+}  // namespace pmb
+
+using namespace pmb;
+
+// Launchers (called from the C-ABI layer in engine.cu).
+int pmb_launch_cf_ell(const double* image, const uint8_t* known, int h, int w, int r,
+                      double eps, const uint8_t* diag_mask, double diag_value, double* values,
+                      int64_t* indices, int64_t* indptr, cudaStream_t s) {
+    AssembleArgs a = {};
+    a.image = image; a.known = known; a.h = h; a.w = w; a.epsilon = eps;
+    a.values = values; a.indices = indices; a.indptr = indptr;
+    a.diag_mask = diag_mask; a.diag_value = diag_value;
+    dim3 grid((w + kAT - 1) / kAT, (h + kAT - 1) / kAT);
+    if (r == 1) cf_assemble_kernel<1, kModeEll><<<grid, kAT * kAT, 0, s>>>(a);
+    else if (r == 2) cf_assemble_kernel<2, kModeEll><<<grid, kAT * kAT, 0, s>>>(a);
+    else return -1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_cf_half(const double* image, const uint8_t* known, int h, int w, double eps,
+                       double* planes, int pitch, const uint8_t* diag_mask, double diag_value,
+                       cudaStream_t s) {
+    AssembleArgs a = {};
+    a.image = image; a.known = known; a.h = h; a.w = w; a.epsilon = eps;
+    a.planes = planes; a.pitch = pitch; a.diag_mask = diag_mask; a.diag_value = diag_value;
+    dim3 grid((w + kAT - 1) / kAT, (h + kAT - 1) / kAT);
+    cf_assemble_kernel<1, kModeHalf><<<grid, kAT * kAT, 0, s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_cf_hard(const double* image, const uint8_t* known, const uint8_t* fg, int h,
+                       int w, double eps, double* planes, int pitch, double* rhs,
+                       cudaStream_t s) {
+    AssembleArgs a = {};
+    a.image = image; a.known = known; a.h = h; a.w = w; a.epsilon = eps;
+    a.planes = planes; a.pitch = pitch; a.fg = fg; a.rhs = rhs;
+    dim3 grid((w + kAT - 1) / kAT, (h + kAT - 1) / kAT);
+    cf_assemble_kernel<1, kModeHard><<<grid, kAT * kAT, 0, s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// --------------------------------------------------------------------------
+// Sparse-format conversions of the assembled rows
+// --------------------------------------------------------------------------
+
+namespace pmb {
+
+// Exclusive scan of n int64 counts in place, one 1024-thread block per chunk
+// of 1024 elements plus a sequential pass over the chunk totals.
+__global__ void k_scan_chunks(int64_t* v, int64_t n, int64_t* chunk_sum) {
+    __shared__ int64_t s[1024];
+    const int64_t i = blockIdx.x * 1024ll + threadIdx.x;
+    int64_t x = i < n ? v[i] : 0;
+    s[threadIdx.x] = x;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int64_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    if (i < n) v[i] = s[threadIdx.x] - x;
+    if (threadIdx.x == 1023) chunk_sum[blockIdx.x] = s[1023];
+}
+
+__global__ void k_scan_totals(int64_t* chunk_sum, int64_t nchunks, int64_t* total) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int64_t run = 0;
+    for (int64_t c = 0; c < nchunks; ++c) {
+        const int64_t t = chunk_sum[c];
+        chunk_sum[c] = run;
+        run += t;
+    }
+    *total = run;
+}
+
+__global__ void k_scan_add(int64_t* v, int64_t n, const int64_t* chunk_sum) {
+    const int64_t i = blockIdx.x * 1024ll + threadIdx.x;
+    if (i < n) v[i] += chunk_sum[blockIdx.x];
+}
+
+// Row counts for the canonical CSR of an assembled ELL: in-image slots with
+// a non-zero value (scipy drops explicit zeros when forming L + C,
+// pymatting/laplacian/laplacian.py:50-55).
+__global__ void k_ell_count(const double* __restrict__ values, int h, int w, int r,
+                            int64_t* counts) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)h * w) return;
+    const int S = 4 * r + 1, y = (int)(i / w), x = (int)(i % w);
+    int64_t c = 0;
+    for (int dy = -2 * r; dy <= 2 * r; ++dy)
+        for (int dx = -2 * r; dx <= 2 * r; ++dx) {
+            const int yj = y + dy, xj = x + dx;
+            if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
+            if (values[i * S * S + (dy + 2 * r) * S + (dx + 2 * r)] != 0.0) ++c;
+        }
+    counts[i] = c;
+}
+
+__global__ void k_ell_fill(const double* __restrict__ values, int h, int w, int r,
+                           const int64_t* __restrict__ rowptr, int64_t* indices, double* data) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)h * w) return;
+    const int S = 4 * r + 1, y = (int)(i / w), x = (int)(i % w);
+    int64_t k = rowptr[i];
+    for (int dy = -2 * r; dy <= 2 * r; ++dy)
+        for (int dx = -2 * r; dx <= 2 * r; ++dx) {
+            const int yj = y + dy, xj = x + dx;
+            if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
+            const double v = values[i * S * S + (dy + 2 * r) * S + (dx + 2 * r)];
+            if (v == 0.0) continue;
+            indices[k] = (int64_t)yj * w + xj;
+            data[k] = v;
+            ++k;
+        }
+}
+
+// Unknown-pixel compaction for the hard-constraint system.
+__global__ void k_flag_unknown(const uint8_t* __restrict__ known, int64_t n, int64_t* flag) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = known[i] ? 0 : 1;
+}
+
+// Row counts of L_U = L[U, :][:, U] (estimate_alpha_cf.py:66): in-image
+// slots whose column is unknown. cidx holds the compact index of every
+// pixel (exclusive scan of the unknown flags).
+__global__ void k_lu_count(const uint8_t* __restrict__ known, int h, int w, int64_t* counts_u,
+                           const int64_t* __restrict__ cidx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)h * w || known[i]) return;
+    const int y = (int)(i / w), x = (int)(i % w);
+    int64_t c = 0;
+    for (int dy = -2; dy <= 2; ++dy)
+        for (int dx = -2; dx <= 2; ++dx) {
+            const int yj = y + dy, xj = x + dx;
+            if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
+            if (!known[(int64_t)yj * w + xj]) ++c;
+        }
+    counts_u[cidx[i]] = c;
+}
+
+// Fill L_U (CSR, compact indices) and b_U = -R m with m = is_fg on the known
+// columns, summed in column order (estimate_alpha_cf.py:66-74).
+__global__ void k_lu_fill(const double* __restrict__ values, const uint8_t* __restrict__ known,
+                          const uint8_t* __restrict__ fg, int h, int w,
+                          const int64_t* __restrict__ cidx, const int64_t* __restrict__ rowptr,
+                          int64_t* indices, double* data, double* rhs) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)h * w || known[i]) return;
+    const int y = (int)(i / w), x = (int)(i % w);
+    const int64_t ci = cidx[i];
+    int64_t k = rowptr[ci];
+    double sum = 0.0;
+    for (int dy = -2; dy <= 2; ++dy)
+        for (int dx = -2; dx <= 2; ++dx) {
+            const int yj = y + dy, xj = x + dx;
+            if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
+            const int64_t j = (int64_t)yj * w + xj;
+            const double v = values[i * 25 + (dy + 2) * 5 + (dx + 2)];
+            if (known[j]) {
+                sum += v * (fg[j] ? 1.0 : 0.0);
+            } else {
+                indices[k] = cidx[j];
+                data[k] = v;
+                ++k;
+            }
+        }
+    rhs[ci] = -sum;
+}
+
+// alpha = clip(x, 0, 1) with x = trimap on known pixels and the solution
+// on unknown ones (estimate_alpha_cf.py:72-76).
+__global__ void k_alpha_compose(const double* __restrict__ trimap, const uint8_t* __restrict__ known,
+                                const int64_t* __restrict__ cidx, const double* __restrict__ xu,
+                                int64_t n, double* alpha) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = known[i] ? trimap[i] : xu[cidx[i]];
+    v = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+    alpha[i] = v;
+}
+
+// Trimap split (pymatting/util/util.py:510-525): fg = t >= fg_thr,
+// bg = t <= bg_thr, known = fg | bg; counts[0] = #fg, counts[1] = #bg.
+__global__ void k_trimap_masks(const double* __restrict__ trimap, int64_t n, double fg_thr,
+                               double bg_thr, uint8_t* is_fg, uint8_t* is_known,
+                               unsigned long long* counts) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool f = false, b = false;
+    if (i < n) {
+        const double t = trimap[i];
+        f = t >= fg_thr;
+        b = t <= bg_thr;
+        is_fg[i] = f;
+        is_known[i] = f || b;
+    }
+    const unsigned nf = __popc(__ballot_sync(0xffffffffu, f));
+    const unsigned nb = __popc(__ballot_sync(0xffffffffu, b));
+    if ((threadIdx.x & 31) == 0) {
+        if (nf) atomicAdd(counts, (unsigned long long)nf);
+        if (nb) atomicAdd(counts + 1, (unsigned long long)nb);
+    }
+}
+
+}  // namespace pmb
+
+int pmb_scan_exclusive(int64_t* v, int64_t n, int64_t* chunk_scratch, int64_t* total,
+                       cudaStream_t s) {
+    const int64_t nchunks = (n + 1023) / 1024;
+    if (n <= 0) {
+        return cudaMemsetAsync(total, 0, sizeof(int64_t), s) == cudaSuccess ? 0 : -2;
+    }
+    k_scan_chunks<<<(unsigned)nchunks, 1024, 0, s>>>(v, n, chunk_scratch);
+    k_scan_totals<<<1, 32, 0, s>>>(chunk_scratch, nchunks, total);
+    k_scan_add<<<(unsigned)nchunks, 1024, 0, s>>>(v, n, chunk_scratch);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_ell_count(const double* values, int h, int w, int r, int64_t* counts, cudaStream_t s) {
+    const int64_t n = (int64_t)h * w;
+    k_ell_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, h, w, r, counts);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_ell_fill(const double* values, int h, int w, int r, const int64_t* rowptr,
+                        int64_t* indices, double* data, cudaStream_t s) {
+    const int64_t n = (int64_t)h * w;
+    k_ell_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, h, w, r, rowptr, indices, data);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_flag_unknown(const uint8_t* known, int64_t n, int64_t* flag, cudaStream_t s) {
+    k_flag_unknown<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(known, n, flag);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_lu_count(const uint8_t* known, int h, int w, int64_t* counts_u, const int64_t* cidx,
+                        cudaStream_t s) {
+    const int64_t n = (int64_t)h * w;
+    k_lu_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(known, h, w, counts_u, cidx);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_lu_fill(const double* values, const uint8_t* known, const uint8_t* fg, int h, int w,
+                       const int64_t* cidx, const int64_t* rowptr, int64_t* indices, double* data,
+                       double* rhs, cudaStream_t s) {
+    const int64_t n = (int64_t)h * w;
+    k_lu_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, known, fg, h, w, cidx, rowptr,
+                                                          indices, data, rhs);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_alpha_compose(const double* trimap, const uint8_t* known, const int64_t* cidx,
+                             const double* xu, int64_t n, double* alpha, cudaStream_t s) {
+    k_alpha_compose<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(trimap, known, cidx, xu, n, alpha);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int pmb_launch_trimap_masks(const double* trimap, int64_t n, double fg_thr, double bg_thr,
+                            uint8_t* is_fg, uint8_t* is_known, unsigned long long* counts,
+                            cudaStream_t s) {
+    if (cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess) return -2;
+    k_trimap_masks<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(trimap, n, fg_thr, bg_thr, is_fg,
+                                                               is_known, counts);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}

@@ -1,0 +1,390 @@
+// Thresholded incomplete Cholesky factorisation and its triangular solves.
+//
+// Restates pymatting/preconditioner/ichol.py:
+//   _ichol :6-113           column-by-column factorisation with absolute and
+//                           relative discard thresholds, diagonal compensation
+//                           of discarded entries, failure codes -1 (not
+//                           positive definite) / -2 (more than max_nnz);
+//   _backsub_L_csc_inplace  :116-129  and  _backsub_LT_csc_inplace :132-145.
+//
+// The factorisation is inherently sequential over columns (column j needs
+// every column k < j that has a kept entry in row j). Instead of the
+// reference's left-looking linked lists, one CTA runs it right-looking over
+// a dense band "front": when column k is final, its kept entries update the
+// pending columns k+1 .. k+B directly (B = bandwidth of A; fill never leaves
+// the envelope). Each column then costs a handful of block-wide steps, all
+// of them parallel across the column's entries and entry pairs. Diagonal
+// updates happen in the same column order as the reference; the off-
+// diagonal accumulations differ only in summation order.
+//
+// The factor's dependency levels (level[i] = 1 + max level of the columns
+// that update row i) fall out of the factorisation for free and drive the
+// level-scheduled triangular solves: one thread per row inside a level,
+// rows subtract their terms in the reference's order, levels separated by
+// block barriers (single CTA: the systems this preconditioner is used on
+// are the compressed unknown regions, tens of thousands of rows).
+#include "pm_common.cuh"
+#include "ichol.cuh"
+
+namespace pmb {
+
+constexpr int kIcholThreads = 1024;
+
+// Per-column statistics of A (lower part, CSC): diagonal (+ shift), sum of
+// |A[j:, j]| for the relative threshold, and the largest i - j.
+__global__ void k_ichol_init(int64_t n, const int64_t* __restrict__ Ap,
+                             const int64_t* __restrict__ Ar, const double* __restrict__ Av,
+                             double shift, double* d, double* rsum, int* level,
+                             unsigned long long* band) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double dj = shift, rj = 0.0;
+    int64_t bmax = 0;
+    for (int64_t k = Ap[j]; k < Ap[j + 1]; ++k) {
+        const int64_t i = Ar[k];
+        if (i == j) dj += Av[k];
+        if (i >= j) rj += fabs(Av[k]);
+        if (i > j && Av[k] != 0.0 && i - j > bmax) bmax = i - j;
+    }
+    d[j] = dj;
+    rsum[j] = rj;
+    level[j] = 0;
+    if (bmax > 0) atomicMax(band, (unsigned long long)bmax);
+}
+
+// Load column j of A (entries below the diagonal with non-zero value) into
+// its front slot. The slot was cleared beforehand.
+__device__ __forceinline__ void load_column(int64_t j, int64_t W, const int64_t* __restrict__ Ap,
+                                            const int64_t* __restrict__ Ar,
+                                            const double* __restrict__ Av, double* F,
+                                            uint8_t* pat) {
+    const int64_t slot = (j % W) * W;
+    for (int64_t k = Ap[j] + threadIdx.x; k < Ap[j + 1]; k += blockDim.x) {
+        const int64_t i = Ar[k];
+        const double v = Av[k];
+        if (i > j && v != 0.0) {
+            // Canonical input has one entry per (i, j): no two threads
+            // write the same offset.
+            F[slot + (i - j)] += v;
+            pat[slot + (i - j)] = 1;
+        }
+    }
+}
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int y = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        s_warp[lane] = y;
+    }
+    __syncthreads();
+    const int base = warp > 0 ? s_warp[warp - 1] : 0;
+    if (total) *total = s_warp[(blockDim.x >> 5) - 1];
+    const int r = base + x - v;
+    __syncthreads();
+    return r;
+}
+
+// The factorisation. One CTA. Front F / pat: W x W (W = B + 1), slot of
+// column j = j % W, entry (i, j) at offset i - j. cand / kept: scratch of
+// at least W entries each.
+__global__ void __launch_bounds__(kIcholThreads)
+k_ichol_factor(int64_t n, int64_t W, const int64_t* __restrict__ Ap,
+               const int64_t* __restrict__ Ar, const double* __restrict__ Av, double* d,
+               const double* __restrict__ rsum, int* level, double* F, uint8_t* pat, int* cand,
+               double* keptv, int64_t* kepti, int64_t* Lp, int64_t* Lr, double* Lv,
+               int64_t cap, double discard, int64_t max_nnz, double rel_discard, int diag_keep,
+               int64_t* result) {
+    __shared__ int s_warp[32];
+    __shared__ int64_t s_nnz;
+    __shared__ int s_cn, s_m, s_fail;
+    __shared__ double s_dj;
+
+    // Initial front: columns 0 .. W-1.
+    for (int64_t j = 0; j < W && j < n; ++j) load_column(j, W, Ap, Ar, Av, F, pat);
+    if (threadIdx.x == 0) {
+        s_nnz = 0;
+        s_fail = 0;
+        Lp[0] = 0;
+    }
+    __syncthreads();
+
+    for (int64_t j = 0; j < n; ++j) {
+        const int64_t slot = (j % W) * W;
+        // Candidate rows of column j, ascending (the reference sorts them,
+        // ichol.py:87-89).
+        int cn_total = 0;
+        int written = 0;
+        for (int64_t base = 1; base < W; base += blockDim.x) {
+            const int64_t o = base + threadIdx.x;
+            const int flag = (o < W && j + o < n && pat[slot + o]) ? 1 : 0;
+            int chunk_total;
+            const int pos = block_exclusive_scan(flag, s_warp, &chunk_total);
+            if (flag) cand[written + pos] = (int)o;
+            written += chunk_total;
+            cn_total += chunk_total;
+        }
+        if (threadIdx.x == 0) {
+            s_cn = cn_total;
+            const double dj = d[j];
+            if (!(dj > 0.0)) {
+                s_fail = -1;               // ichol.py:80-81
+            } else if (s_nnz + 1 + cn_total > max_nnz || s_nnz + 1 + cn_total > cap) {
+                s_fail = -2;               // ichol.py:82-83
+            } else {
+                const double sj = sqrt(dj);
+                d[j] = sj;
+                s_dj = sj;
+                Lv[s_nnz] = sj;
+                Lr[s_nnz] = j;
+                s_nnz += 1;
+            }
+        }
+        __syncthreads();
+        if (s_fail) break;
+        const int cn = s_cn;
+        const double dj = s_dj;
+        const int64_t nnz0 = s_nnz;
+        const double rel = rel_discard * rsum[j];
+        // Scale, threshold, diagonal updates; compact the kept entries.
+        int kept_total = 0;
+        for (int base = 0; base < cn; base += blockDim.x) {
+            const int q = base + threadIdx.x;
+            int keep = 0;
+            double L = 0.0;
+            int64_t i = 0;
+            if (q < cn) {
+                const int o = cand[q];
+                i = j + o;
+                const double a = F[slot + o];
+                L = a / dj;
+                if (diag_keep) d[i] -= L * L;
+                keep = (fabs(L) > discard && fabs(a) > rel) ? 1 : 0;
+                if (keep && !diag_keep) d[i] -= L * L;
+            }
+            int chunk_total;
+            const int pos = block_exclusive_scan(keep, s_warp, &chunk_total);
+            if (keep) {
+                const int64_t at = nnz0 + kept_total + pos;
+                Lv[at] = L;
+                Lr[at] = i;
+                keptv[kept_total + pos] = L;
+                kepti[kept_total + pos] = i;
+            }
+            kept_total += chunk_total;
+        }
+        if (threadIdx.x == 0) {
+            s_m = kept_total;
+            s_nnz = nnz0 + kept_total;
+            Lp[j + 1] = nnz0 + kept_total;
+        }
+        __syncthreads();
+        const int m = s_m;
+        // Levels of the rows this column feeds.
+        const int lj = level[j] + 1;
+        for (int q = threadIdx.x; q < m; q += blockDim.x) {
+            const int64_t i = kepti[q];
+            if (level[i] < lj) level[i] = lj;
+        }
+        // Right-looking update of the pending columns: for kept rows
+        // ia > ib, F[ib][ia - ib] -= L_ia L_ib.
+        const int64_t pairs = (int64_t)m * (m - 1) / 2;
+        for (int64_t p = threadIdx.x; p < pairs; p += blockDim.x) {
+            // Invert p = a (a - 1) / 2 + b with 0 <= b < a.
+            int64_t a = (int64_t)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+            while (a * (a - 1) / 2 > p) --a;
+            while ((a + 1) * a / 2 <= p) ++a;
+            const int64_t b = p - a * (a - 1) / 2;
+            const int64_t ia = kepti[a], ib = kepti[b];
+            const int64_t off = ((ib % W) * W) + (ia - ib);
+            F[off] -= keptv[a] * keptv[b];
+            pat[off] = 1;
+        }
+        __syncthreads();
+        // Recycle the slot for column j + W.
+        for (int64_t o = threadIdx.x; o < W; o += blockDim.x) {
+            F[slot + o] = 0.0;
+            pat[slot + o] = 0;
+        }
+        __syncthreads();
+        if (j + W < n) load_column(j + W, W, Ap, Ar, Av, F, pat);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *result = s_fail ? (int64_t)s_fail : s_nnz;
+}
+
+// Level histogram / order of rows, and the row (CSR) view of L used by the
+// forward solve. All small single-purpose kernels.
+__global__ void k_level_count(int64_t n, const int* __restrict__ level, int64_t* cnt,
+                              int* maxlevel) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    atomicAdd((unsigned long long*)&cnt[level[i]], 1ull);
+    atomicMax(maxlevel, level[i]);
+}
+
+__global__ void k_level_scatter(int64_t n, const int* __restrict__ level, int64_t* fill,
+                                int* order) {
+    // Sequential within one thread per level bucket would be slow; rows are
+    // placed with atomics, then each level segment is sorted by row.
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long at = atomicAdd((unsigned long long*)&fill[level[i]], 1ull);
+    order[at] = (int)i;
+}
+
+// Insertion-sort each level segment so the schedule is deterministic.
+__global__ void k_level_sort(const int64_t* __restrict__ lptr, int nlevels, int* order) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlevels) return;
+    const int64_t a = lptr[l], b = lptr[l + 1];
+    for (int64_t k = a + 1; k < b; ++k) {
+        const int v = order[k];
+        int64_t q = k - 1;
+        while (q >= a && order[q] > v) {
+            order[q + 1] = order[q];
+            --q;
+        }
+        order[q + 1] = v;
+    }
+}
+
+__global__ void k_row_count(int64_t n, const int64_t* __restrict__ Lp, const int64_t* __restrict__ Lr,
+                            int64_t* rcnt) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int64_t k = Lp[j] + 1; k < Lp[j + 1]; ++k)
+        atomicAdd((unsigned long long*)&rcnt[Lr[k]], 1ull);
+}
+
+// Row view entries in ascending column order: column j writes its entry
+// of row i at the slot given by the number of columns < j with an entry in
+// row i — computed by walking columns in order within one thread per row
+// would be quadratic, so entries are appended with atomics and each row is
+// sorted afterwards.
+__global__ void k_row_fill(int64_t n, const int64_t* __restrict__ Lp, const int64_t* __restrict__ Lr,
+                           const double* __restrict__ Lv, int64_t* rfill, int64_t* Rc, double* Rv) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int64_t k = Lp[j] + 1; k < Lp[j + 1]; ++k) {
+        const int64_t i = Lr[k];
+        const unsigned long long at = atomicAdd((unsigned long long*)&rfill[i], 1ull);
+        Rc[at] = j;
+        Rv[at] = Lv[k];
+    }
+}
+
+__global__ void k_row_sort(int64_t n, const int64_t* __restrict__ Rp, int64_t* Rc, double* Rv) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int64_t k = Rp[i] + 1; k < Rp[i + 1]; ++k) {
+        const int64_t c = Rc[k];
+        const double v = Rv[k];
+        int64_t q = k - 1;
+        while (q >= Rp[i] && Rc[q] > c) {
+            Rc[q + 1] = Rc[q];
+            Rv[q + 1] = Rv[q];
+            --q;
+        }
+        Rc[q + 1] = c;
+        Rv[q + 1] = v;
+    }
+}
+
+// x = L^-T L^-1 b. Forward: y_i = (b_i - sum_{j<i} L_ij y_j) / L_ii with
+// the subtractions in ascending j (the column sweep of
+// _backsub_L_csc_inplace applies them in that order); backward: x_i =
+// (y_i - sum_{k>i} L_ki x_k) / L_ii over column i in ascending k
+// (_backsub_LT_csc_inplace). Levels run forward, then in reverse.
+__global__ void __launch_bounds__(kIcholThreads)
+k_ichol_solve(int64_t n, int nlevels, const int64_t* __restrict__ lptr, const int* __restrict__ order,
+              const int64_t* __restrict__ Lp, const int64_t* __restrict__ Lr,
+              const double* __restrict__ Lv, const int64_t* __restrict__ Rp,
+              const int64_t* __restrict__ Rc, const double* __restrict__ Rv,
+              const double* __restrict__ b, double* x, const InstState* st) {
+    if (st && st->status != kRunning) return;
+    for (int l = 0; l < nlevels; ++l) {
+        for (int64_t q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
+            const int64_t i = order[q];
+            double s = b[i];
+            for (int64_t k = Rp[i]; k < Rp[i + 1]; ++k) s -= Rv[k] * x[Rc[k]];
+            x[i] = s / Lv[Lp[i]];
+        }
+        __syncthreads();
+    }
+    for (int l = nlevels - 1; l >= 0; --l) {
+        for (int64_t q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
+            const int64_t i = order[q];
+            double s = x[i];
+            for (int64_t k = Lp[i] + 1; k < Lp[i + 1]; ++k) s -= Lv[k] * x[Lr[k]];
+            x[i] = s / Lv[Lp[i]];
+        }
+        __syncthreads();
+    }
+}
+
+// The forward sweep above overwrites x in place: y lives in x. For the
+// forward pass to read y_j of earlier levels and b_i of its own row, b and
+// x may alias (the reference also works in place on a copy of b).
+
+void ichol_launch_init(int64_t n, const int64_t* Ap, const int64_t* Ar, const double* Av,
+                       double shift, double* d, double* rsum, int* level, unsigned long long* band,
+                       cudaStream_t s) {
+    if (n > 0) k_ichol_init<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Ap, Ar, Av, shift, d, rsum, level, band);
+}
+
+void ichol_launch_factor(int64_t n, int64_t W, const int64_t* Ap, const int64_t* Ar,
+                         const double* Av, double* d, const double* rsum, int* level, double* F,
+                         uint8_t* pat, int* cand, double* keptv, int64_t* kepti, int64_t* Lp,
+                         int64_t* Lr, double* Lv, int64_t cap, double discard, int64_t max_nnz,
+                         double rel, int diag_keep, int64_t* result, cudaStream_t s) {
+    k_ichol_factor<<<1, kIcholThreads, 0, s>>>(n, W, Ap, Ar, Av, d, rsum, level, F, pat, cand, keptv,
+                                               kepti, Lp, Lr, Lv, cap, discard, max_nnz, rel,
+                                               diag_keep, result);
+}
+
+void ichol_launch_levels(int64_t n, const int* level, int64_t* cnt, int* maxlevel, cudaStream_t s) {
+    if (n > 0) k_level_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, level, cnt, maxlevel);
+}
+
+void ichol_launch_level_scatter(int64_t n, const int* level, int64_t* fill, int* order,
+                                const int64_t* lptr, int nlevels, cudaStream_t s) {
+    if (n > 0) k_level_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, level, fill, order);
+    if (nlevels > 0) k_level_sort<<<(nlevels + 127) / 128, 128, 0, s>>>(lptr, nlevels, order);
+}
+
+void ichol_launch_rows(int64_t n, const int64_t* Lp, const int64_t* Lr, const double* Lv,
+                       int64_t* rcnt, cudaStream_t s) {
+    if (n > 0) k_row_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Lp, Lr, rcnt);
+}
+
+void ichol_launch_row_fill(int64_t n, const int64_t* Lp, const int64_t* Lr, const double* Lv,
+                           int64_t* rfill, int64_t* Rc, double* Rv, const int64_t* Rp,
+                           cudaStream_t s) {
+    if (n > 0) {
+        k_row_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Lp, Lr, Lv, rfill, Rc, Rv);
+        k_row_sort<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Rp, Rc, Rv);
+    }
+}
+
+void ichol_launch_solve(int64_t n, int nlevels, const int64_t* lptr, const int* order,
+                        const int64_t* Lp, const int64_t* Lr, const double* Lv, const int64_t* Rp,
+                        const int64_t* Rc, const double* Rv, const double* b, double* x,
+                        const InstState* st, cudaStream_t s) {
+    k_ichol_solve<<<1, kIcholThreads, 0, s>>>(n, nlevels, lptr, order, Lp, Lr, Lv, Rp, Rc, Rv, b, x, st);
+}
+
+}  // namespace pmb

@@ -1,0 +1,149 @@
+// Shared definitions for the sm_100a kernels of the closed-form alpha path.
+//
+// Operator layout ("half stencil"). The radius-1 matting Laplacian couples
+// pixels at most two apart (pymatting/laplacian/cf_laplacian.py:15-23 writes
+// a 5x5 block per row), and so do its Galerkin coarse operators. The matrix
+// is symmetric, so only the centre and the 12 "forward" offsets are stored:
+// plane p holds A[i, i + d_p] for d_p = (dy, dx) with dy > 0, or dy == 0 and
+// dx >= 0. The backward entry A[i, i - d_p] is plane p read at pixel i - d_p.
+// Planes are row-pitched 2D arrays, one after the other, so one apply reads
+// 13 planes plus x and writes y: 15 values per pixel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pmb {
+
+constexpr int kRS = 2;       // stencil radius of the stored operator
+constexpr int kNH = 13;      // stored planes (centre + 12 forward offsets)
+constexpr int kTX = 32;      // fine tile width  (one thread per pixel)
+constexpr int kTY = 8;       // fine tile height
+constexpr int kCX = 16;      // coarse tile width used by the restriction
+constexpr int kCY = 8;       // coarse tile height
+constexpr int kThreads = kTX * kTY;
+
+__host__ __device__ constexpr int half_dy(int p) { return p < 3 ? 0 : (p < 8 ? 1 : 2); }
+__host__ __device__ constexpr int half_dx(int p) { return p < 3 ? p : (p < 8 ? p - 5 : p - 10); }
+// Plane index of forward offset (dy, dx); -1 if (dy, dx) is not forward.
+__host__ __device__ constexpr int half_index(int dy, int dx) {
+    return (dy == 0 && dx >= 0 && dx <= 2) ? dx
+         : (dy == 1 && dx >= -2 && dx <= 2) ? 5 + dx
+         : (dy == 2 && dx >= -2 && dx <= 2) ? 10 + dx : -1;
+}
+
+// One grid (an image, or one multigrid level of an image) inside a batch.
+struct GridDesc {
+    int h, w, pitch, inst;  // inst: index of the image in the batch
+    int64_t voff;           // offset of element (0, 0) in the level's vectors
+    int64_t poff;           // offset of plane 0 in the level's plane buffer
+    int64_t pstride;        // elements between consecutive planes (h * pitch)
+};
+
+// Tiles of one tile shape over the grids of one level. Grid g owns the global
+// tiles [tile_start[g], tile_start[g + 1]).
+struct WorkList {
+    const GridDesc* grids;
+    const int* tile_start;
+    int ngrids;
+    int total;
+};
+
+// Per-image solver state, kept on the device so a whole iteration can be
+// replayed from a CUDA graph without the host.
+struct InstState {
+    double rz;        // r . z of the current iterate
+    double alpha;     // step length of the current iteration
+    double beta;      // p <- z + beta p
+    double norm_b;
+    double norm_r;
+    double tol;       // converged when norm_r < tol (tol = max(atol, rtol*|b|))
+    double pap;       // p . Ap
+    double aux;       // spare slot (outer residual of the refinement loop)
+    int iters;        // completed iterations
+    int status;       // kRunning / kConverged / kMaxIter / kNonFinite
+    int maxiter;
+    int flags;        // kFirst: p = z on the next apply
+    unsigned int counter;  // tiles finished in the current reduction
+    int pad[3];
+};
+
+enum : int { kRunning = 0, kConverged = 1, kMaxIter = 2, kNonFinite = 3, kSkip = 4 };
+enum : int { kFirst = 1 };
+
+__device__ __forceinline__ int find_grid(const WorkList& wl, int tile) {
+    int lo = 0, hi = wl.ngrids - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (wl.tile_start[mid] <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename T> struct Acc { typedef double type; };
+
+// Block-wide sum of up to 3 doubles; result valid in thread 0. Fixed tree
+// order, so results are reproducible run to run.
+template <int NQ>
+__device__ __forceinline__ void block_sum(double (&v)[NQ], double* smem /* NQ*32 */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    }
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) smem[q * 32 + warp] = v[q];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = lane < nwarps ? smem[q * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            v[q] = t;
+        }
+    }
+}
+
+// Deterministic two-stage reduction across the tiles of one image.
+// Each tile stores its partial sums; the block that finishes the image's last
+// tile adds all partials in tile order and runs `fin` (thread 0 only).
+// Returns true in the block that ran the finaliser.
+template <int NQ, typename Fin>
+__device__ __forceinline__ bool tile_reduce(double (&v)[NQ], double* partials, int total,
+                                            int tile, int t0, int t1, InstState* st,
+                                            double* smem, Fin fin) {
+    block_sum<NQ>(v, smem);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) partials[(int64_t)q * total + tile] = v[q];
+        __threadfence();
+        unsigned int done = atomicAdd(&st->counter, 1u);
+        last = (done == (unsigned int)(t1 - t0 - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double s[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        s[q] = 0.0;
+        for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x)
+            s[q] += __ldcg(partials + (int64_t)q * total + t);
+    }
+    block_sum<NQ>(s, smem);
+    if (threadIdx.x == 0) {
+        st->counter = 0u;
+        fin(s);
+    }
+    __syncthreads();
+    return true;
+}
+
+}  // namespace pmb

@@ -1,0 +1,978 @@
+// Matrix-free half-stencil kernels: the soft-constraint system A = L + lambda D,
+// the fused preconditioned conjugate-gradient steps, and the geometric
+// multigrid V-cycle used as its preconditioner.
+//
+// Every kernel walks a WorkList of tiles over a batch of grids (images of
+// different sizes, or the same multigrid level of several images) with a
+// grid-stride loop, so one launch serves the whole batch. Per-image scalars
+// (alpha, beta, norms, convergence status) live in InstState on the device;
+// an image whose status is no longer "running" is skipped tile by tile.
+//
+// Reference algorithms restated here:
+//   cg          pymatting/solver/cg.py:64-117
+//   jacobi      pymatting/preconditioner/jacobi.py:24-31
+//   V-cycle     pymatting/preconditioner/vcycle.py:6-100 (make_P weights
+//               and border mask, jacobi_step, _vcycle_step)
+#include "pm_common.cuh"
+#include "stencil.cuh"
+
+namespace pmb {
+
+// --------------------------------------------------------------------------
+// Tile helpers
+// --------------------------------------------------------------------------
+
+// Stage v over [y0-2, y0+H+1] x [x0-2, x0+W+1] (zero outside the grid).
+template <typename T, int H, int W>
+__device__ __forceinline__ void stage_halo(T* s, const T* __restrict__ v, const GridDesc& g,
+                                           int y0, int x0) {
+    constexpr int SW = W + 4, SH = H + 4;
+    for (int q = threadIdx.x; q < SW * SH; q += blockDim.x) {
+        const int ly = q / SW, lx = q - ly * SW;
+        const int y = y0 - 2 + ly, x = x0 - 2 + lx;
+        T val = T(0);
+        if (y >= 0 && y < g.h && x >= 0 && x < g.w) val = v[g.voff + (int64_t)y * g.pitch + x];
+        s[q] = val;
+    }
+}
+
+// (A x)_i at pixel (y, x) with x staged in shared memory: s is the staged
+// tile, (ly, lx) the pixel's position in it and sw its row stride.
+template <typename T>
+__device__ __forceinline__ T apply_at(const T* __restrict__ P, const GridDesc& g, int y, int x,
+                                      const T* s, int ly, int lx, int sw) {
+    const int64_t i = (int64_t)y * g.pitch + x;
+    const T* Pg = P + g.poff;
+    T acc = __ldg(Pg + i) * s[ly * sw + lx];
+#pragma unroll
+    for (int p = 1; p < kNH; ++p) {
+        const int dy = half_dy(p), dx = half_dx(p);
+        const T* Pp = Pg + p * g.pstride;
+        acc += __ldg(Pp + i) * s[(ly + dy) * sw + lx + dx];
+        const int yy = y - dy, xx = x - dx;
+        if (yy >= 0 && xx >= 0 && xx < g.w)
+            acc += __ldg(Pp + i - (int64_t)dy * g.pitch - dx) * s[(ly - dy) * sw + lx - dx];
+    }
+    return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ T diag_at(const T* __restrict__ P, const GridDesc& g, int y, int x) {
+    return __ldg(P + g.poff + (int64_t)y * g.pitch + x);
+}
+
+struct TileCoord { int g, y0, x0; };
+
+template <int H, int W>
+__device__ __forceinline__ TileCoord tile_coord(const WorkList& wl, int t) {
+    TileCoord c;
+    c.g = find_grid(wl, t);
+    const int local = t - wl.tile_start[c.g];
+    const int tiles_x = (wl.grids[c.g].w + W - 1) / W;
+    const int ty = local / tiles_x;
+    c.y0 = ty * H;
+    c.x0 = (local - ty * tiles_x) * W;
+    return c;
+}
+
+// --------------------------------------------------------------------------
+// Conjugate gradient steps (cg.py:64-117)
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ void finish_beta(InstState* st, double rz_new) {
+    // First pass after the initial residual: only record r.z (cg.py:78-80).
+    if (st->flags & kFirst) {
+        st->rz = rz_new;
+        return;
+    }
+    // beta = (1 / rz) * r.z  (cg.py:105-108)
+    double beta = 1.0 / st->rz;
+    beta *= rz_new;
+    st->beta = beta;
+    st->rz = rz_new;
+}
+
+// beta = ((r - r_old) . z) / rz when reorthogonalising (cg.py:102-104).
+__device__ __forceinline__ void finish_beta_reorth(InstState* st, double rz_new, double dz) {
+    if (st->flags & kFirst) {
+        st->rz = rz_new;
+        return;
+    }
+    st->beta = dz / st->rz;
+    st->rz = rz_new;
+}
+
+// r = b - A x0 (or r = b), |b|, |r|, and for Jacobi / no preconditioner also
+// z and r.z. Finaliser sets norm_b, tol, status (cg.py:64-80).
+template <typename T, int PREC>
+__global__ void __launch_bounds__(kThreads)
+k_cg_init(WorkList wl, const T* __restrict__ P, const T* __restrict__ b, T* x,
+          const T* __restrict__ x0, T* r, T* z, InstState* st, double* partials,
+          double atol, double rtol, int maxiter) {
+    __shared__ T s_x[(kTY + 4) * (kTX + 4)];
+    __shared__ double s_red[3 * 32];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        InstState* s = st + g.inst;
+        if (x0) {
+            __syncthreads();
+            stage_halo<T, kTY, kTX>(s_x, x0, g, c.y0, c.x0);
+            __syncthreads();
+        }
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, xx = c.x0 + lx;
+        double v[3] = {0.0, 0.0, 0.0};
+        if (y < g.h && xx < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+            const T bi = b[i];
+            T ri = bi;
+            if (x0) {
+                ri = bi - apply_at<T>(P, g, y, xx, s_x, ly + 2, lx + 2, kTX + 4);
+                x[i] = s_x[(ly + 2) * (kTX + 4) + lx + 2];
+            } else {
+                x[i] = T(0);
+            }
+            r[i] = ri;
+            v[0] = (double)bi * (double)bi;
+            v[1] = (double)ri * (double)ri;
+            if (PREC == kPrecJacobi) {
+                const T inv = T(1) / diag_at<T>(P, g, y, xx);
+                const T zi = ri * inv;
+                z[i] = zi;
+                v[2] = (double)ri * (double)zi;
+            } else if (PREC == kPrecNone) {
+                v[2] = v[1];
+            }
+        }
+        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        tile_reduce<3>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+            s->norm_b = sqrt(sum[0]);
+            s->norm_r = sqrt(sum[1]);
+            s->tol = fmax(atol, rtol * s->norm_b);
+            s->iters = 0;
+            s->maxiter = maxiter;
+            s->flags = kFirst;
+            s->beta = 0.0;
+            s->alpha = 0.0;
+            if (s->norm_r < atol || s->norm_r < rtol * s->norm_b) s->status = kConverged;
+            else if (maxiter <= 0) s->status = kMaxIter;
+            else s->status = kRunning;
+            if (PREC != kPrecVcycle && PREC != kPrecExternal) s->rz = sum[2];
+        });
+    }
+}
+
+// p_new = z + beta p_old (p_new = z on the first pass), Ap = A p_new and
+// p_new . Ap; finaliser: alpha = rz / (p . Ap)   (cg.py:85-90, 111-113).
+// p is double-buffered by iteration parity: neighbouring tiles still read
+// p_old while this tile writes p_new.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_cg_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ z, T* p0, T* p1,
+           T* Ap, InstState* st, double* partials) {
+    __shared__ T s_p[(kTY + 4) * (kTX + 4)];
+    __shared__ double s_red[32];
+    constexpr int SW = kTX + 4, SH = kTY + 4;
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        InstState* s = st + g.inst;
+        if (s->status != kRunning) continue;
+        const bool first = (s->flags & kFirst) != 0;
+        const T beta = (T)s->beta;
+        const int par = s->iters & 1;
+        const T* pold = par ? p1 : p0;
+        T* pnew = par ? p0 : p1;
+        __syncthreads();
+        for (int q = threadIdx.x; q < SW * SH; q += blockDim.x) {
+            const int ly = q / SW, lx = q - ly * SW;
+            const int y = c.y0 - 2 + ly, x = c.x0 - 2 + lx;
+            T val = T(0);
+            if (y >= 0 && y < g.h && x >= 0 && x < g.w) {
+                const int64_t i = g.voff + (int64_t)y * g.pitch + x;
+                val = first ? z[i] : (T)(z[i] + beta * pold[i]);
+            }
+            s_p[q] = val;
+        }
+        __syncthreads();
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, x = c.x0 + lx;
+        double v[1] = {0.0};
+        if (y < g.h && x < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + x;
+            const T pi = s_p[(ly + 2) * SW + lx + 2];
+            const T api = apply_at<T>(P, g, y, x, s_p, ly + 2, lx + 2, SW);
+            pnew[i] = pi;
+            Ap[i] = api;
+            v[0] = (double)pi * (double)api;
+        }
+        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        tile_reduce<1>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+            s->pap = sum[0];
+            s->alpha = s->rz / sum[0];
+            s->flags &= ~kFirst;
+        });
+    }
+}
+
+// x += alpha p; r -= alpha Ap; |r|; convergence test (cg.py:89-99). For the
+// Jacobi / identity preconditioners also z = M r and beta (cg.py:101-113).
+// With reorthogonalisation the change r - r_old is kept in `dr` (or reduced
+// directly against z for Jacobi).
+template <typename T, int PREC>
+__global__ void __launch_bounds__(kThreads)
+k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0, const T* p1,
+            const T* __restrict__ Ap, T* dr, int reorth, InstState* st, double* partials) {
+    __shared__ double s_red[3 * 32];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        InstState* s = st + g.inst;
+        if (s->status != kRunning) continue;
+        const double alpha = s->alpha;
+        const T* p = (s->iters & 1) ? p0 : p1;   // the buffer k_cg_apply wrote
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, xx = c.x0 + lx;
+        double v[3] = {0.0, 0.0, 0.0};
+        if (y < g.h && xx < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+            const T a = (T)alpha;
+            const T rold = r[i];
+            x[i] = x[i] + a * p[i];
+            const T ri = rold - a * Ap[i];
+            r[i] = ri;
+            v[0] = (double)ri * (double)ri;
+            if (PREC == kPrecJacobi) {
+                const T inv = T(1) / diag_at<T>(P, g, y, xx);
+                const T zi = ri * inv;
+                z[i] = zi;
+                v[1] = (double)ri * (double)zi;
+                if (reorth) v[2] = (double)(ri - rold) * (double)zi;
+            } else if (PREC == kPrecNone) {
+                v[1] = v[0];
+                if (reorth) v[2] = (double)(ri - rold) * (double)ri;
+            } else if (reorth) {
+                dr[i] = ri - rold;
+            }
+        }
+        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        tile_reduce<3>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+            const double nr = sqrt(sum[0]);
+            s->norm_r = nr;
+            s->iters += 1;
+            if (!isfinite(nr)) s->status = kNonFinite;
+            else if (nr < s->tol) s->status = kConverged;
+            else if (s->iters >= s->maxiter) s->status = kMaxIter;
+            if (s->status == kRunning && (PREC == kPrecJacobi || PREC == kPrecNone)) {
+                if (reorth) finish_beta_reorth(s, sum[1], sum[2]);
+                else finish_beta(s, sum[1]);
+            }
+        });
+    }
+}
+
+// r . z (and (r - r_old) . z) for preconditioners applied outside the fused
+// kernels; finaliser computes beta.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_cg_rz(WorkList wl, const T* __restrict__ r, const T* __restrict__ z, const T* __restrict__ dr,
+        int reorth, InstState* st, double* partials) {
+    __shared__ double s_red[2 * 32];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        InstState* s = st + g.inst;
+        if (s->status != kRunning) continue;
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, xx = c.x0 + lx;
+        double v[2] = {0.0, 0.0};
+        if (y < g.h && xx < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+            v[0] = (double)r[i] * (double)z[i];
+            if (reorth) v[1] = (double)dr[i] * (double)z[i];
+        }
+        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        tile_reduce<2>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+            if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
+            else finish_beta(s, sum[0]);
+        });
+    }
+}
+
+// --------------------------------------------------------------------------
+// V-cycle (vcycle.py:46-100)
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ double pw(int a) { return a == 0 ? 2.0 : 1.0; }
+
+// Restriction of the pre-smoothed residual. One CTA per coarse tile:
+//   x1 = omega b / d         (first Jacobi sweep from zero, vcycle.py:33-36)
+//        or x1 = 0 (no pre-smoothing) or x1 = xs (explicit sweeps);
+//   res = b - A x1 on the fine pixels under the tile (vcycle.py:77);
+//   b_coarse = R res with full-weighting [1 2 1]^2 / 16 (vcycle.py:12-26, 80).
+// Status of the image is checked through `st` when st != null.
+template <typename T, int PRE>
+__global__ void __launch_bounds__(kThreads)
+k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const T* __restrict__ P,
+          const T* __restrict__ b, const T* __restrict__ xs, T* bc, double omega,
+          const InstState* st) {
+    constexpr int RW = 2 * kCX + 1, RH = 2 * kCY + 1;   // residual region
+    constexpr int XW = RW + 4, XH = RH + 4;             // x1 region
+    __shared__ T s_x[XH * XW];
+    __shared__ T s_r[RH * RW];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kCY, kCX>(wl, t);
+        const GridDesc gc = wl.grids[c.g];
+        const GridDesc gf = fine[c.g];
+        if (st && st[gc.inst].status != kRunning) continue;
+        const int fy0 = 2 * c.y0 - 1, fx0 = 2 * c.x0 - 1;   // residual region origin
+        __syncthreads();
+        if (PRE != 0) {
+            for (int q = threadIdx.x; q < XW * XH; q += blockDim.x) {
+                const int ly = q / XW, lx = q - ly * XW;
+                const int y = fy0 - 2 + ly, x = fx0 - 2 + lx;
+                T val = T(0);
+                if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
+                    const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
+                    if (PRE == 1) val = (T)omega * b[i] / diag_at<T>(P, gf, y, x);
+                    else val = xs[i];
+                }
+                s_x[q] = val;
+            }
+            __syncthreads();
+        }
+        for (int q = threadIdx.x; q < RW * RH; q += blockDim.x) {
+            const int ly = q / RW, lx = q - ly * RW;
+            const int y = fy0 + ly, x = fx0 + lx;
+            T val = T(0);
+            if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
+                const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
+                val = b[i];
+                if (PRE != 0) val = val - apply_at<T>(P, gf, y, x, s_x, ly + 2, lx + 2, XW);
+            }
+            s_r[q] = val;
+        }
+        __syncthreads();
+        const int lx = threadIdx.x % kCX, ly = threadIdx.x / kCX;
+        if (ly < kCY) {
+            const int Y = c.y0 + ly, X = c.x0 + lx;
+            if (Y < gc.h && X < gc.w) {
+                T sum = T(0);
+#pragma unroll
+                for (int ay = -1; ay <= 1; ++ay)
+#pragma unroll
+                    for (int ax = -1; ax <= 1; ++ax)
+                        sum += (T)(pw(ax) * pw(ay) / 16.0) *
+                               s_r[(2 * ly + 1 + ay) * RW + (2 * lx + 1 + ax)];
+                bc[gc.voff + (int64_t)Y * gc.pitch + X] = sum;
+            }
+        }
+    }
+}
+
+// Prolongation of the coarse correction and the first post-smoothing sweep:
+//   x2 = x1 + P xc           (vcycle.py:95; P = R^T)
+//   x3 = x2 + omega (b - A x2) / d    (vcycle.py:98, one sweep; POST = 0
+//                                       stores x2 unchanged)
+// At level 0 (rz != 0) the block also accumulates r . z with r = b, and
+// (r - r_old) . z when reorthogonalising, finishing beta.
+template <typename T, int PRE, int POST>
+__global__ void __launch_bounds__(kThreads)
+k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const T* __restrict__ P,
+        const T* __restrict__ b, const T* __restrict__ xs, const T* __restrict__ xc, T* xout,
+        double omega, InstState* st, int level0, const T* __restrict__ dr, int reorth,
+        double* partials) {
+    constexpr int SW = kTX + 4, SH = kTY + 4;
+    constexpr int CW = (kTX + 5) / 2 + 3, CH = (kTY + 5) / 2 + 3;
+    __shared__ T s_x[SH * SW];
+    __shared__ T s_c[CH * CW];
+    __shared__ double s_red[2 * 32];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc gf = wl.grids[c.g];
+        const GridDesc gc = coarse[c.g];
+        InstState* s = st ? st + gf.inst : nullptr;
+        if (s && s->status != kRunning) continue;
+        const int cy0 = (c.y0 - 3) >> 1, cx0 = (c.x0 - 3) >> 1;
+        __syncthreads();
+        for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
+            const int ly = q / CW, lx = q - ly * CW;
+            const int Y = cy0 + ly, X = cx0 + lx;
+            T val = T(0);
+            if (Y >= 0 && Y < gc.h && X >= 0 && X < gc.w) val = xc[gc.voff + (int64_t)Y * gc.pitch + X];
+            s_c[q] = val;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < SW * SH; q += blockDim.x) {
+            const int ly = q / SW, lx = q - ly * SW;
+            const int y = c.y0 - 2 + ly, x = c.x0 - 2 + lx;
+            T val = T(0);
+            if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
+                const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
+                T x1 = T(0);
+                if (PRE == 1) x1 = (T)omega * b[i] / diag_at<T>(P, gf, y, x);
+                else if (PRE > 1) x1 = xs[i];
+                // Coarse pixels whose 3x3 support contains (y, x), in raster
+                // order of the coarse grid: |y - 2Y| <= 1 and |x - 2X| <= 1.
+                T sum = T(0);
+                const int Yhi = min((y + 1) >> 1, gc.h - 1);
+                const int Xhi = min((x + 1) >> 1, gc.w - 1);
+                for (int Y = y >> 1; Y <= Yhi; ++Y) {
+                    const int ay = y - 2 * Y;
+                    for (int X = x >> 1; X <= Xhi; ++X) {
+                        const int ax = x - 2 * X;
+                        sum += (T)(pw(ax) * pw(ay) / 16.0) * s_c[(Y - cy0) * CW + (X - cx0)];
+                    }
+                }
+                val = x1 + sum;
+            }
+            s_x[q] = val;
+        }
+        __syncthreads();
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, x = c.x0 + lx;
+        double v[2] = {0.0, 0.0};
+        if (y < gf.h && x < gf.w) {
+            const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
+            T x3 = s_x[(ly + 2) * SW + lx + 2];
+            if (POST > 0) {
+                const T bi = b[i];
+                const T ax = apply_at<T>(P, gf, y, x, s_x, ly + 2, lx + 2, SW);
+                x3 = x3 + (T)omega * (bi - ax) / diag_at<T>(P, gf, y, x);
+            }
+            xout[i] = x3;
+            if (level0) {
+                v[0] = (double)b[i] * (double)x3;
+                if (reorth) v[1] = (double)dr[i] * (double)x3;
+            }
+        }
+        if (level0 && s) {
+            const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+            tile_reduce<2>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+                if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
+                else finish_beta(s, sum[0]);
+            });
+        }
+    }
+}
+
+// One weighted Jacobi sweep xout = xin + omega (b - A xin) / d, or the first
+// sweep from zero xout = omega b / d when xin == null (vcycle.py:32-43).
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_vc_smooth(WorkList wl, const T* __restrict__ P, const T* __restrict__ b,
+            const T* __restrict__ xin, T* xout, double omega, const InstState* st) {
+    __shared__ T s_x[(kTY + 4) * (kTX + 4)];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        if (st && st[g.inst].status != kRunning) continue;
+        if (xin) {
+            __syncthreads();
+            stage_halo<T, kTY, kTX>(s_x, xin, g, c.y0, c.x0);
+            __syncthreads();
+        }
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, x = c.x0 + lx;
+        if (y < g.h && x < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + x;
+            const T d = diag_at<T>(P, g, y, x);
+            T out;
+            if (xin) {
+                const T ax = apply_at<T>(P, g, y, x, s_x, ly + 2, lx + 2, kTX + 4);
+                out = s_x[(ly + 2) * (kTX + 4) + lx + 2] + (T)omega * (b[i] - ax) / d;
+            } else {
+                out = (T)omega * b[i] / d;
+            }
+            xout[i] = out;
+        }
+    }
+}
+
+// Coarsest level: x = A^{-1} b with the inverse precomputed per image
+// (replaces scipy.sparse.linalg.spsolve at vcycle.py:59-60). One CTA per
+// image; the rz reduction runs when the coarsest level is level 0.
+template <typename T>
+__global__ void k_vc_direct(const DirectDesc* dd, int count, const T* __restrict__ b, T* x,
+                            InstState* st, int rz_level0) {
+    if ((int)blockIdx.x >= count) return;
+    const DirectDesc d = dd[blockIdx.x];
+    InstState* s = st ? st + d.g.inst : nullptr;
+    if (s && s->status != kRunning) return;
+    const int n = d.g.h * d.g.w;
+    __shared__ double s_b[kMaxDirect];
+    __shared__ double s_red[32];
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const int yy = q / d.g.w, xx = q - yy * d.g.w;
+        s_b[q] = (double)b[d.g.voff + (int64_t)yy * d.g.pitch + xx];
+    }
+    __syncthreads();
+    double v[1] = {0.0};
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const double* row = d.inv + (int64_t)q * n;
+        double acc = 0.0;
+        for (int j = 0; j < n; ++j) acc += row[j] * s_b[j];
+        const int yy = q / d.g.w, xx = q - yy * d.g.w;
+        x[d.g.voff + (int64_t)yy * d.g.pitch + xx] = (T)acc;
+        if (rz_level0) v[0] += s_b[q] * (double)(T)acc;
+    }
+    if (rz_level0 && s) {
+        block_sum<1>(v, s_red);
+        if (threadIdx.x == 0) finish_beta(s, v[0]);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Setup: Galerkin coarse operator, dense coarsest inverse, precision copies
+// --------------------------------------------------------------------------
+
+// Entry A[i, i + e] of a half-stencil operator for any |e| <= 2.
+__device__ __forceinline__ double half_entry(const double* Pg, const GridDesc& g, int y, int x,
+                                             int ey, int ex) {
+    const int yj = y + ey, xj = x + ex;
+    if (yj < 0 || yj >= g.h || xj < 0 || xj >= g.w) return 0.0;
+    int p = half_index(ey, ex);
+    if (p >= 0) return Pg[p * g.pstride + (int64_t)y * g.pitch + x];
+    p = half_index(-ey, -ex);
+    return Pg[p * g.pstride + (int64_t)yj * g.pitch + xj];
+}
+
+// Coarse operator R A P (vcycle.py:65) for one coarse pixel and forward
+// offset D: sum over the 3x3 restriction support a of I and b of I + D of
+// w_a w_b A[fa, fb]. One thread per (coarse pixel, forward offset).
+__global__ void k_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrids,
+                           const double* __restrict__ Pf, double* Pc, int64_t total) {
+    int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    // Locate the grid: coarse pixel counts are prefix-summed on the fly
+    // (ngrids is small).
+    int g = 0;
+    int64_t base = 0;
+    for (; g < ngrids; ++g) {
+        const int64_t cnt = (int64_t)coarse_g[g].h * coarse_g[g].w * kNH;
+        if (idx < base + cnt) break;
+        base += cnt;
+    }
+    const GridDesc gf = fine_g[g], gc = coarse_g[g];
+    const int64_t local = idx - base;
+    const int p = (int)(local % kNH);
+    const int64_t pix = local / kNH;
+    const int Y = (int)(pix / gc.w), X = (int)(pix % gc.w);
+    const int DY = half_dy(p), DX = half_dx(p);
+    double acc = 0.0;
+    const int Y2 = Y + DY, X2 = X + DX;
+    if (Y2 >= 0 && Y2 < gc.h && X2 >= 0 && X2 < gc.w) {
+        const double* Pg = Pf + gf.poff;
+        for (int ay = -1; ay <= 1; ++ay) {
+            for (int ax = -1; ax <= 1; ++ax) {
+                const int fy = 2 * Y + ay, fx = 2 * X + ax;
+                if (fy < 0 || fy >= gf.h || fx < 0 || fx >= gf.w) continue;
+                const double wa = pw(ax) * pw(ay) / 16.0;
+                for (int by = -1; by <= 1; ++by) {
+                    for (int bx = -1; bx <= 1; ++bx) {
+                        const int gy = 2 * Y2 + by, gx = 2 * X2 + bx;
+                        if (gy < 0 || gy >= gf.h || gx < 0 || gx >= gf.w) continue;
+                        const int ey = gy - fy, ex = gx - fx;
+                        if (ey < -2 || ey > 2 || ex < -2 || ex > 2) continue;
+                        const double wb = pw(bx) * pw(by) / 16.0;
+                        acc += wa * half_entry(Pg, gf, fy, fx, ey, ex) * wb;
+                    }
+                }
+            }
+        }
+    }
+    Pc[gc.poff + p * gc.pstride + (int64_t)Y * gc.pitch + X] = acc;
+}
+
+// Dense inverse of the coarsest operator by Gauss-Jordan elimination with
+// partial pivoting. One CTA per image; n <= kMaxDirect.
+__global__ void k_dense_inverse(const DirectDesc* dd, int count, const double* __restrict__ Pc,
+                                double* work, int* status) {
+    if (blockIdx.x >= count) return;
+    const DirectDesc d = dd[blockIdx.x];
+    const GridDesc g = d.g;
+    const int n = g.h * g.w;
+    double* A = work + d.work_off;           // n x n
+    double* Inv = d.inv;                      // n x n
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        const int yi = i / g.w, xi = i - yi * g.w, yj = j / g.w, xj = j - yj * g.w;
+        const int ey = yj - yi, ex = xj - xi;
+        double v = 0.0;
+        if (ey >= -2 && ey <= 2 && ex >= -2 && ex <= 2) v = half_entry(Pc + g.poff, g, yi, xi, ey, ex);
+        A[q] = v;
+        Inv[q] = (i == j) ? 1.0 : 0.0;
+    }
+    __shared__ int s_piv;
+    __shared__ double s_pval;
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        if (threadIdx.x == 0) {
+            int best = k;
+            double bv = fabs(A[(int64_t)k * n + k]);
+            for (int i = k + 1; i < n; ++i) {
+                const double v = fabs(A[(int64_t)i * n + k]);
+                if (v > bv) { bv = v; best = i; }
+            }
+            s_piv = best;
+            s_pval = A[(int64_t)best * n + k];
+            if (bv == 0.0 || !isfinite(bv)) atomicExch(status, 1);
+        }
+        __syncthreads();
+        const int pr = s_piv;
+        if (pr != k) {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                double t = A[(int64_t)k * n + j]; A[(int64_t)k * n + j] = A[(int64_t)pr * n + j]; A[(int64_t)pr * n + j] = t;
+                t = Inv[(int64_t)k * n + j]; Inv[(int64_t)k * n + j] = Inv[(int64_t)pr * n + j]; Inv[(int64_t)pr * n + j] = t;
+            }
+        }
+        __syncthreads();
+        const double piv = s_pval;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            A[(int64_t)k * n + j] /= piv;
+            Inv[(int64_t)k * n + j] /= piv;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+            const int i = q / n, j = q - i * n;
+            if (i == k) continue;
+            const double f = A[(int64_t)i * n + k];
+            if (j == k) continue;
+            A[q] -= f * A[(int64_t)k * n + j];
+            Inv[q] -= f * Inv[(int64_t)k * n + j];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            if (i == k) continue;
+            const double f = A[(int64_t)i * n + k];
+            Inv[(int64_t)i * n + k] -= f * Inv[(int64_t)k * n + k];
+            A[(int64_t)i * n + k] = 0.0;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_convert_f32(const double* __restrict__ src, float* dst, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i < n; i += (int64_t)gridDim.x * blockDim.x) dst[i] = (float)src[i];
+}
+
+// --------------------------------------------------------------------------
+// Packing between user layout (contiguous h*w per image) and pitched grids
+// --------------------------------------------------------------------------
+
+template <typename TS, typename TD>
+__global__ void k_pack(const GridDesc* grids, int ngrids, const int64_t* user_off,
+                       const TS* __restrict__ src, TD* dst, int64_t total) {
+    int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        int g = 0;
+        while (g + 1 < ngrids && user_off[g + 1] <= idx) ++g;
+        const GridDesc d = grids[g];
+        const int64_t local = idx - user_off[g];
+        const int y = (int)(local / d.w), x = (int)(local % d.w);
+        dst[d.voff + (int64_t)y * d.pitch + x] = (TD)src[idx];
+    }
+}
+
+template <typename TS, typename TD>
+__global__ void k_unpack(const GridDesc* grids, int ngrids, const int64_t* user_off,
+                         const TS* __restrict__ src, TD* dst, int64_t total) {
+    int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        int g = 0;
+        while (g + 1 < ngrids && user_off[g + 1] <= idx) ++g;
+        const GridDesc d = grids[g];
+        const int64_t local = idx - user_off[g];
+        const int y = (int)(local / d.w), x = (int)(local % d.w);
+        dst[idx] = (TD)src[d.voff + (int64_t)y * d.pitch + x];
+    }
+}
+
+// y = A x on pitched vectors (no reductions): used by A.dot(x).
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ x, T* y) {
+    __shared__ T s_x[(kTY + 4) * (kTX + 4)];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        __syncthreads();
+        stage_halo<T, kTY, kTX>(s_x, x, g, c.y0, c.x0);
+        __syncthreads();
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int yy = c.y0 + ly, xx = c.x0 + lx;
+        if (yy < g.h && xx < g.w)
+            y[g.voff + (int64_t)yy * g.pitch + xx] = apply_at<T>(P, g, yy, xx, s_x, ly + 2, lx + 2, kTX + 4);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Iterative refinement around the FP32 inner solve
+// --------------------------------------------------------------------------
+
+// r64 = b - A64 x64 in FP64; finaliser runs the outer convergence test and
+// (re)starts the inner FP32 solve on r32 = (float) r64 with x32 = 0.
+template <int PREC>
+__global__ void __launch_bounds__(kThreads)
+k_refine_residual(WorkList wl, const double* __restrict__ P64, const float* __restrict__ P32,
+                  const double* __restrict__ b, const double* __restrict__ x64, float* r32,
+                  float* x32, float* z32, InstState* outer, InstState* inner, double* partials,
+                  double atol, double rtol, double inner_rtol, int maxiter, int max_outer) {
+    __shared__ double s_x[(kTY + 4) * (kTX + 4)];
+    __shared__ double s_red[3 * 32];
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        InstState* so = outer + g.inst;
+        InstState* si = inner + g.inst;
+        if (so->status != kRunning) continue;
+        __syncthreads();
+        stage_halo<double, kTY, kTX>(s_x, x64, g, c.y0, c.x0);
+        __syncthreads();
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, xx = c.x0 + lx;
+        double v[3] = {0.0, 0.0, 0.0};
+        if (y < g.h && xx < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+            const double bi = b[i];
+            const double ri = bi - apply_at<double>(P64, g, y, xx, s_x, ly + 2, lx + 2, kTX + 4);
+            const float rf = (float)ri;
+            r32[i] = rf;
+            x32[i] = 0.0f;
+            v[0] = bi * bi;
+            v[1] = ri * ri;
+            if (PREC == kPrecJacobi) {
+                const float zi = rf * (1.0f / diag_at<float>(P32, g, y, xx));
+                z32[i] = zi;
+                v[2] = (double)rf * (double)zi;
+            } else if (PREC == kPrecNone) {
+                v[2] = (double)rf * (double)rf;
+            }
+        }
+        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        tile_reduce<3>(v, partials, wl.total, t, t0, t1, so, s_red, [&](double* sum) {
+            const double nb = sqrt(sum[0]);
+            const double nr = sqrt(sum[1]);
+            if (so->iters == 0) {
+                so->norm_b = nb;
+                so->tol = fmax(atol, rtol * nb);
+            }
+            so->norm_r = nr;
+            if (!isfinite(nr)) so->status = kNonFinite;
+            else if (nr < atol || nr < rtol * so->norm_b) so->status = kConverged;
+            else if (so->iters >= max_outer) so->status = kMaxIter;
+            if (so->status == kRunning) {
+                si->norm_b = nr;
+                si->norm_r = nr;
+                si->tol = inner_rtol * nr;
+                si->iters = 0;
+                si->maxiter = maxiter;
+                si->flags = kFirst;
+                si->beta = 0.0;
+                si->status = kRunning;
+                if (PREC != kPrecVcycle) si->rz = sum[2];
+            } else {
+                si->status = kSkip;
+            }
+        });
+    }
+}
+
+// x64 += x32 for images whose inner solve ran; counts outer iterations.
+__global__ void __launch_bounds__(kThreads)
+k_refine_correct(WorkList wl, double* x64, const float* __restrict__ x32, InstState* outer,
+                 const InstState* inner) {
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        if (outer[g.inst].status != kRunning) continue;
+        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+        const int y = c.y0 + ly, xx = c.x0 + lx;
+        if (y < g.h && xx < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+            x64[i] += (double)x32[i];
+        }
+    }
+}
+
+__global__ void k_refine_count(InstState* outer, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && outer[i].status == kRunning) outer[i].iters += 1;
+}
+
+// --------------------------------------------------------------------------
+// Explicit instantiation helpers used by the engine
+// --------------------------------------------------------------------------
+
+template <typename T>
+void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, const T* b,
+                    T* x, const T* x0, T* r, T* z, InstState* st, double* part, double atol,
+                    double rtol, int maxiter, cudaStream_t s) {
+    switch (prec) {
+    case kPrecNone: k_cg_init<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
+    case kPrecJacobi: k_cg_init<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
+    case kPrecVcycle: k_cg_init<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
+    default: k_cg_init<T, kPrecExternal><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
+    }
+}
+
+template <typename T>
+void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const T* P, const T* z, T* p0, T* p1,
+                     T* Ap, InstState* st, double* part, cudaStream_t s) {
+    k_cg_apply<T><<<L.grid, kThreads, 0, s>>>(wl, P, z, p0, p1, Ap, st, part);
+}
+
+template <typename T>
+void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
+                      T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth,
+                      InstState* st, double* part, cudaStream_t s) {
+    switch (prec) {
+    case kPrecNone: k_cg_update<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, st, part); break;
+    case kPrecJacobi: k_cg_update<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, st, part); break;
+    default: k_cg_update<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, st, part); break;
+    }
+}
+
+template <typename T>
+void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z, const T* dr,
+                  int reorth, InstState* st, double* part, cudaStream_t s) {
+    k_cg_rz<T><<<L.grid, kThreads, 0, s>>>(wl, r, z, dr, reorth, st, part);
+}
+
+template <typename T>
+void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridDesc* fine,
+                    const T* P, const T* b, const T* xs, T* bc, double omega,
+                    const InstState* st, cudaStream_t s) {
+    if (pre == 0) k_vc_down<T, 0><<<L.grid, kThreads, 0, s>>>(wl, fine, P, b, xs, bc, omega, st);
+    else if (pre == 1) k_vc_down<T, 1><<<L.grid, kThreads, 0, s>>>(wl, fine, P, b, xs, bc, omega, st);
+    else k_vc_down<T, 2><<<L.grid, kThreads, 0, s>>>(wl, fine, P, b, xs, bc, omega, st);
+}
+
+template <typename T>
+void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
+                  const T* P, const T* b, const T* xs, const T* xc, T* xout, double omega,
+                  InstState* st, int level0, const T* dr, int reorth, double* part,
+                  cudaStream_t s) {
+    const int pk = pre > 1 ? 2 : pre;
+    const int qk = post > 0 ? 1 : 0;
+#define PMB_UP(PK, QK) k_vc_up<T, PK, QK><<<L.grid, kThreads, 0, s>>>(wl, coarse, P, b, xs, xc, xout, omega, st, level0, dr, reorth, part)
+    if (pk == 0 && qk == 0) PMB_UP(0, 0);
+    else if (pk == 0) PMB_UP(0, 1);
+    else if (pk == 1 && qk == 0) PMB_UP(1, 0);
+    else if (pk == 1) PMB_UP(1, 1);
+    else if (qk == 0) PMB_UP(2, 0);
+    else PMB_UP(2, 1);
+#undef PMB_UP
+}
+
+template <typename T>
+void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const T* P, const T* b, const T* xin,
+                      T* xout, double omega, const InstState* st, cudaStream_t s) {
+    k_vc_smooth<T><<<L.grid, kThreads, 0, s>>>(wl, P, b, xin, xout, omega, st);
+}
+
+template <typename T>
+void launch_vc_direct(const DirectDesc* dd, int count, const T* b, T* x, InstState* st,
+                      int rz_level0, cudaStream_t s) {
+    if (count > 0) k_vc_direct<T><<<count, 256, 0, s>>>(dd, count, b, x, st, rz_level0);
+}
+
+template <typename T>
+void launch_apply(const LaunchCfg& L, const WorkList& wl, const T* P, const T* x, T* y,
+                  cudaStream_t s) {
+    k_apply<T><<<L.grid, kThreads, 0, s>>>(wl, P, x, y);
+}
+
+template <typename TS, typename TD>
+void launch_pack(const GridDesc* grids, int ngrids, const int64_t* uoff, const TS* src, TD* dst,
+                 int64_t total, cudaStream_t s) {
+    if (total <= 0) return;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_pack<TS, TD><<<blocks, 256, 0, s>>>(grids, ngrids, uoff, src, dst, total);
+}
+
+template <typename TS, typename TD>
+void launch_unpack(const GridDesc* grids, int ngrids, const int64_t* uoff, const TS* src, TD* dst,
+                   int64_t total, cudaStream_t s) {
+    if (total <= 0) return;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_unpack<TS, TD><<<blocks, 256, 0, s>>>(grids, ngrids, uoff, src, dst, total);
+}
+
+void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrids, const double* Pf,
+                     double* Pc, int64_t total, cudaStream_t s) {
+    if (total <= 0) return;
+    k_galerkin<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(fine_g, coarse_g, ngrids, Pf, Pc, total);
+}
+
+void launch_dense_inverse(const DirectDesc* dd, int count, const double* Pc, double* work,
+                          int* status, cudaStream_t s) {
+    if (count > 0) k_dense_inverse<<<count, 256, 0, s>>>(dd, count, Pc, work, status);
+}
+
+void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_convert_f32<<<blocks, 256, 0, s>>>(src, dst, n);
+}
+
+void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl, const double* P64,
+                            const float* P32, const double* b, const double* x64, float* r32,
+                            float* x32, float* z32, InstState* outer, InstState* inner,
+                            double* part, double atol, double rtol, double inner_rtol,
+                            int maxiter, int max_outer, cudaStream_t s) {
+#define PMB_RR(PK) k_refine_residual<PK><<<L.grid, kThreads, 0, s>>>(wl, P64, P32, b, x64, r32, x32, z32, outer, inner, part, atol, rtol, inner_rtol, maxiter, max_outer)
+    if (prec == kPrecNone) PMB_RR(kPrecNone);
+    else if (prec == kPrecJacobi) PMB_RR(kPrecJacobi);
+    else PMB_RR(kPrecVcycle);
+#undef PMB_RR
+}
+
+void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, const float* x32,
+                           InstState* outer, const InstState* inner, int ninst, cudaStream_t s) {
+    k_refine_correct<<<L.grid, kThreads, 0, s>>>(wl, x64, x32, outer, inner);
+    k_refine_count<<<(ninst + 127) / 128, 128, 0, s>>>(outer, ninst);
+}
+
+#define PMB_INST(T)                                                                          \
+    template void launch_cg_init<T>(int, const LaunchCfg&, const WorkList&, const T*, const T*, \
+                                    T*, const T*, T*, T*, InstState*, double*, double, double, \
+                                    int, cudaStream_t);                                      \
+    template void launch_cg_apply<T>(const LaunchCfg&, const WorkList&, const T*, const T*, T*, \
+                                     T*, T*, InstState*, double*, cudaStream_t);             \
+    template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*, \
+                                      T*, const T*, const T*, const T*, T*, int, InstState*,  \
+                                      double*, cudaStream_t);                                \
+    template void launch_cg_rz<T>(const LaunchCfg&, const WorkList&, const T*, const T*,      \
+                                  const T*, int, InstState*, double*, cudaStream_t);         \
+    template void launch_vc_down<T>(int, const LaunchCfg&, const WorkList&, const GridDesc*,  \
+                                    const T*, const T*, const T*, T*, double,                \
+                                    const InstState*, cudaStream_t);                         \
+    template void launch_vc_up<T>(int, int, const LaunchCfg&, const WorkList&,                \
+                                  const GridDesc*, const T*, const T*, const T*, const T*, T*, \
+                                  double, InstState*, int, const T*, int, double*,           \
+                                  cudaStream_t);                                             \
+    template void launch_vc_smooth<T>(const LaunchCfg&, const WorkList&, const T*, const T*,  \
+                                      const T*, T*, double, const InstState*, cudaStream_t); \
+    template void launch_vc_direct<T>(const DirectDesc*, int, const T*, T*, InstState*, int,  \
+                                      cudaStream_t);                                         \
+    template void launch_apply<T>(const LaunchCfg&, const WorkList&, const T*, const T*, T*,  \
+                                  cudaStream_t);
+
+PMB_INST(double)
+PMB_INST(float)
+#undef PMB_INST
+
+template void launch_pack<double, double>(const GridDesc*, int, const int64_t*, const double*, double*, int64_t, cudaStream_t);
+template void launch_pack<double, float>(const GridDesc*, int, const int64_t*, const double*, float*, int64_t, cudaStream_t);
+template void launch_pack<float, double>(const GridDesc*, int, const int64_t*, const float*, double*, int64_t, cudaStream_t);
+template void launch_unpack<double, double>(const GridDesc*, int, const int64_t*, const double*, double*, int64_t, cudaStream_t);
+template void launch_unpack<float, double>(const GridDesc*, int, const int64_t*, const float*, double*, int64_t, cudaStream_t);
+template void launch_unpack<double, float>(const GridDesc*, int, const int64_t*, const double*, float*, int64_t, cudaStream_t);
+
+}  // namespace pmb

@@ -1,0 +1,255 @@
+"""Closed-form matting Laplacian and the soft-constraint linear system.
+
+Drop-in for ``pymatting.laplacian.cf_laplacian`` (cf_laplacian.py:132-177)
+and ``pymatting.laplacian.make_linear_system`` (laplacian.py:5-60).
+
+Both return ``scipy.sparse.csr_matrix`` objects, as the reference does, but
+the matrix is assembled on the GPU and stays there: the returned object is a
+``DeviceCSRMatrix`` (a ``csr_matrix`` subclass) whose ``data`` / ``indices``
+/ ``indptr`` arrays are only copied to the host the first time host code
+touches them. Solvers of this package recognise a matrix whose host arrays
+were never exposed and use its device form directly (the 13-plane half
+stencil for the solve, the exact CSR arrays for everything else). Once the
+host arrays exist the matrix is treated like any other scipy matrix, so
+in-place edits are always honoured.
+"""
+
+import numpy as np
+import scipy.sparse
+import torch
+
+from . import _device as dev
+from . import _ffi
+from .util import trimap_split
+
+__all__ = ["cf_laplacian", "make_linear_system", "DeviceCSRMatrix", "CFSource",
+           "device_source", "device_csr_arrays"]
+
+
+class CFSource:
+    """Device-side description of a closed-form Laplacian system.
+
+    Holds the image and masks on the device and assembles, on demand, the
+    forms the solvers need: the half-stencil planes (radius 1), the
+    reference's CSR arrays (exactly as ``cf_laplacian`` builds them) and
+    the canonical CSR of ``L + diag(diag_value * diag_mask)``.
+    """
+
+    def __init__(self, image_t, known_t, h, w, epsilon, radius, diag_mask_t=None,
+                 diag_value=0.0):
+        self.image = image_t
+        self.known = known_t
+        self.h, self.w = int(h), int(w)
+        self.epsilon = float(epsilon)
+        self.radius = int(radius)
+        self.diag_mask = diag_mask_t
+        self.diag_value = float(diag_value)
+        self._planes = None
+        self._csr = None
+
+    @property
+    def n(self):
+        return self.h * self.w
+
+    @property
+    def pitch(self):
+        return int(_ffi.lib().pmb_grid_pitch(self.w))
+
+    @property
+    def plane_elems(self):
+        return 13 * self.h * self.pitch
+
+    def with_diag(self, mask_t, value):
+        return CFSource(self.image, self.known, self.h, self.w, self.epsilon, self.radius,
+                        mask_t, value)
+
+    def assemble_planes(self, out):
+        """Write the 13 half-stencil planes into device tensor ``out``."""
+        if self.radius != 1:
+            raise NotImplementedError("the stencil solver supports radius=1 Laplacians")
+        _ffi.check(_ffi.lib().pmb_cf_laplacian_planes(
+            dev.ptr(self.image), dev.ptr(self.known), self.h, self.w, self.epsilon,
+            dev.ptr(self.diag_mask), self.diag_value, dev.ptr(out), dev.stream()),
+            "cf_laplacian planes")
+        return out
+
+    def planes(self):
+        if self._planes is None:
+            self._planes = self.assemble_planes(dev.empty(self.plane_elems, torch.float64))
+        return self._planes
+
+    def ell(self):
+        """Reference CSR arrays of L (+ diagonal): (values, indices, indptr)."""
+        S = (4 * self.radius + 1) ** 2
+        values = dev.empty(self.n * S, torch.float64)
+        indices = dev.empty(self.n * S, torch.int64)
+        indptr = dev.empty(self.n + 1, torch.int64)
+        _ffi.check(_ffi.lib().pmb_cf_laplacian_ell(
+            dev.ptr(self.image), dev.ptr(self.known), self.h, self.w, self.radius,
+            self.epsilon, dev.ptr(self.diag_mask), self.diag_value, dev.ptr(values),
+            dev.ptr(indices), dev.ptr(indptr), dev.stream()), "cf_laplacian")
+        return values, indices, indptr
+
+    def csr(self):
+        """Device CSR arrays identical to the host matrix this source stands for.
+
+        Without a diagonal term this is ``cf_laplacian``'s non-canonical CSR
+        ((4r+1)^2 slots per row). With one it is the canonical CSR of
+        ``L + C`` that scipy forms in ``make_linear_system`` (explicit zeros
+        and the out-of-image slots dropped)."""
+        if self._csr is not None:
+            return self._csr
+        values, indices, indptr = self.ell()
+        if self.diag_mask is None:
+            self._csr = (indptr, indices, values)
+            return self._csr
+        lib = _ffi.lib()
+        n = self.n
+        rowptr = dev.empty(n + 1, torch.int64)
+        scratch = dev.empty(int(lib.pmb_scan_scratch_elems(n + 1)), torch.int64)
+        _ffi.check(lib.pmb_ell_csr_rowptr(dev.ptr(values), self.h, self.w, self.radius,
+                                          dev.ptr(rowptr), dev.ptr(scratch), dev.stream()),
+                   "make_linear_system rowptr")
+        nnz = int(rowptr[n].item())
+        cidx = dev.empty(max(nnz, 1), torch.int64)
+        data = dev.empty(max(nnz, 1), torch.float64)
+        _ffi.check(lib.pmb_ell_csr_fill(dev.ptr(values), self.h, self.w, self.radius,
+                                        dev.ptr(rowptr), dev.ptr(cidx), dev.ptr(data),
+                                        dev.stream()), "make_linear_system fill")
+        self._csr = (rowptr, cidx[:nnz], data[:nnz])
+        return self._csr
+
+
+class DeviceCSRMatrix(scipy.sparse.csr_matrix):
+    """``csr_matrix`` whose arrays live on the GPU until host code reads them.
+
+    ``data``, ``indices`` and ``indptr`` are deliberately absent from the
+    instance until first access; ``__getattr__`` then copies them from the
+    device. Every scipy operation therefore works unchanged. Construction by
+    scipy itself (results of arithmetic, ``copy()``...) falls through to the
+    plain ``csr_matrix`` constructor.
+    """
+
+    def __init__(self, arg1=None, shape=None, dtype=None, copy=False, maxprint=None, *,
+                 pmb_source=None, pmb_arrays=None):
+        if pmb_source is None and pmb_arrays is None:
+            super().__init__(arg1, shape=shape, dtype=dtype, copy=copy, maxprint=maxprint)
+            return
+        d = self.__dict__
+        d["_pmb_source"] = pmb_source
+        d["_pmb_arrays"] = pmb_arrays
+        self._shape = tuple(int(s) for s in shape)
+        self.maxprint = 50 if maxprint is None else maxprint
+
+    def __getattr__(self, name):
+        d = self.__dict__
+        if name in ("data", "indices", "indptr") and (
+                "_pmb_source" in d or "_pmb_arrays" in d):
+            self._pmb_materialize()
+            return d[name]
+        raise AttributeError(name)
+
+    def _pmb_materialize(self):
+        d = self.__dict__
+        if "data" in d:
+            return
+        indptr, indices, data = device_csr_arrays(self)
+        d["indptr"] = dev.to_host(indptr)
+        d["indices"] = dev.to_host(indices)
+        d["data"] = dev.to_host(data)
+
+    @property
+    def dtype(self):
+        if "data" not in self.__dict__:
+            return np.dtype(np.float64)
+        return self.data.dtype
+
+    @dtype.setter
+    def dtype(self, newtype):
+        self.data = self.data.view(newtype)
+
+    @property
+    def pmb_on_device(self):
+        """True while the host arrays were never exposed."""
+        return "data" not in self.__dict__
+
+    def __reduce__(self):
+        self._pmb_materialize()
+        return (scipy.sparse.csr_matrix, ((self.data, self.indices, self.indptr), self.shape))
+
+
+def device_source(A):
+    """The CFSource behind ``A`` if its host arrays were never exposed."""
+    if isinstance(A, DeviceCSRMatrix) and A.pmb_on_device:
+        return A.__dict__.get("_pmb_source")
+    return None
+
+
+def device_csr_arrays(A):
+    """Device (indptr, indices, data) of a DeviceCSRMatrix."""
+    d = A.__dict__
+    arrays = d.get("_pmb_arrays")
+    if arrays is None:
+        arrays = d["_pmb_source"].csr()
+        d["_pmb_arrays"] = arrays
+    return arrays
+
+
+def _image_to_device(image):
+    if dev.is_device_tensor(image):
+        t = image.to(torch.float64).contiguous()
+    else:
+        t = dev.to_device(np.asarray(image), torch.float64)
+    return t
+
+
+def _mask_to_device(mask, h, w):
+    if mask is None:
+        return None
+    if dev.is_device_tensor(mask):
+        return mask.reshape(h, w).to(torch.uint8).contiguous()
+    return dev.to_device(np.asarray(mask).reshape(h, w).astype(np.uint8), torch.uint8)
+
+
+def cf_laplacian(image, epsilon=1e-7, radius=1, is_known=None):
+    """Closed-form matting Laplacian of Levin et al., assembled on the GPU.
+
+    Same signature and result as pymatting's ``cf_laplacian``
+    (pymatting/laplacian/cf_laplacian.py:132): an ``(h*w, h*w)`` CSR matrix
+    with ``(4r+1)^2`` stored entries per row, out-of-image slots holding
+    column 0 and value 0, and values bitwise equal to the reference.
+    ``image`` is ``(h, w, 3)`` (numpy or a CUDA tensor); windows whose pixels
+    are all in ``is_known`` are skipped. ``radius`` 1 or 2.
+    """
+    h, w, d = image.shape
+    assert d == 3
+    if radius not in (1, 2):
+        raise NotImplementedError("cf_laplacian on the device supports radius 1 and 2")
+    src = CFSource(_image_to_device(image), _mask_to_device(is_known, h, w), h, w,
+                   epsilon, radius)
+    n = h * w
+    return DeviceCSRMatrix(shape=(n, n), pmb_source=src)
+
+
+def make_linear_system(L, trimap, lambda_value=100.0, return_c=False):
+    """``A = L + lambda * diag(is_known)``, ``b = lambda * is_fg``.
+
+    Same contract as pymatting/laplacian/laplacian.py:5-60. When ``L`` is a
+    device-resident Laplacian of this package, ``A`` is assembled on the GPU
+    (the diagonal folded into the centre plane) and returned as a
+    DeviceCSRMatrix whose host arrays equal scipy's canonical ``L + C``.
+    """
+    h, w = trimap.shape[:2]
+    is_fg, is_bg, is_known, is_unknown = trimap_split(trimap)
+    c = lambda_value * is_known
+    b = lambda_value * is_fg
+    src = device_source(L)
+    if src is not None and src.diag_mask is None and src.n == h * w:
+        known_t = _mask_to_device(is_known, h, w)
+        A = DeviceCSRMatrix(shape=L.shape, pmb_source=src.with_diag(known_t, lambda_value))
+    else:
+        from .sparse import add_diagonal
+        A = add_diagonal(L, c)
+    if return_c:
+        return A, b, c
+    return A, b
