@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the closed-form alpha solve on B200.
+
+Metric: Mpix/s of soft-constraint closed-form alpha solves, each to FP64
+relative residual 1e-7, on the 1920x1080 synthetic workload (one image per
+GPU): assembly of the matting Laplacian, V-cycle hierarchy setup and the
+preconditioned CG solve, from image + trimap resident in HBM to alpha
+resident in HBM. ``value`` is the mixed-precision path (FP32 inner V-cycle
+PCG inside FP64 iterative refinement); the plain FP64 path is reported
+beside it. ``e2e`` is the same metric through the public ``solve_alpha`` API
+with host numpy buffers (uploads and the alpha download inside the timed
+region). ``--impl reference`` times the CPU restatement of PyMatting's own
+path (cf_laplacian + make_linear_system + vcycle + cg) on host cores.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: launched by torch.distributed.run, one rank per GPU; every rank
+solves its own image (weak scaling, no collective on the data path).
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "Mpix/s of cf alpha solves at FP64 rel-residual 1e-7: mixed vs FP64 GPU; % HBM"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["1080p", "4096", "batch64"], default="1080p")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+WORKLOADS = {
+    # name: list of (h, w, seed offset, unknown fraction)
+    "1080p": dict(sizes=[(1080, 1920, 0.08)], sigma=3.0, band=10),
+    "4096": dict(sizes=[(4096, 4096, 0.15)], sigma=3.0, band=10),
+}
+
+
+def make_inputs(workload, rank):
+    from pymatting_b200.synthetic import make_matting_problem, batch_sizes
+    if workload == "batch64":
+        spec = [(h, w, frac, seed) for (h, w, frac, seed) in batch_sizes(64, 1000)]
+        from pymatting_b200.shard import shard_sizes
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        mine = shard_sizes([(h, w) for h, w, _, _ in spec], world)[rank]
+        spec = [spec[k] for k in mine]
+        sigma, band = 3.0, 10
+    else:
+        wl = WORKLOADS[workload]
+        spec = [(h, w, frac, 100 + rank) for (h, w, frac) in wl["sizes"]]
+        sigma, band = wl["sigma"], wl["band"]
+    imgs, tris, fracs = [], [], []
+    for h, w, frac, seed in spec:
+        img, tri, _a, real = make_matting_problem(h, w, seed, sigma=sigma, band=band,
+                                                  unknown_fraction=frac)
+        imgs.append(img)
+        tris.append(tri)
+        fracs.append(real)
+    return imgs, tris, fracs
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(kind, npx):
+    """DRAM bytes per apply launch from the committed ncu summary, scaled."""
+    path = os.path.join(HERE, "profiles", "apply_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(kind)
+    if not e:
+        return None
+    return float(e["dram_bytes"]) * npx / float(e["pixels"])
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference path on host cores (rank 0 only)."""
+    if rank != 0:
+        return None
+    import oracle
+    imgs, tris, fracs = make_inputs(args.workload if args.workload != "batch64" else "1080p", 0)
+    img, tri = imgs[0], tris[0]
+    h, w = tri.shape
+    # Bound the run to a few minutes: full image for short runs, a crop
+    # otherwise (throughput per pixel is close to size-independent).
+    steps = args.steps + args.warmup
+    if steps > 6:
+        hh, ww = h // 2, w // 2
+        y0, x0 = (h - hh) // 2, (w - ww) // 2
+        img, tri = img[y0:y0 + hh, x0:x0 + ww].copy(), tri[y0:y0 + hh, x0:x0 + ww].copy()
+    sample = "%dx%d soft system from the %s workload" % (tri.shape[1], tri.shape[0], args.workload)
+    times = []
+    for s in range(steps):
+        t0 = time.perf_counter()
+        x, iters = oracle.solve_soft(img, tri, preconditioner="vcycle", rtol=1e-7)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    npx = tri.size
+    value = npx * len(times) / sum(times) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "cf_alpha_soft_vcycle_rtol1e-7_" + args.workload,
+                   "image": "%dx%d" % (tri.shape[1], tri.shape[0]),
+                   "path": "cf_laplacian + make_linear_system + vcycle + cg (CPU restatement)"},
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "iters": iters,
+    }
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def cpu_baseline(img, tri):
+    import oracle
+    t0 = time.perf_counter()
+    x, iters = oracle.solve_soft(img, tri, preconditioner="vcycle", rtol=1e-7)
+    dt = time.perf_counter() - t0
+    return {"value": tri.size / dt / 1e6, "unit": "Mpix/s", "cores": 1, "kind": "port",
+            "sample": "one %dx%d soft-constraint vcycle CG solve to rtol 1e-7 (oracle: C "
+                      "cf_laplacian, scipy make_linear_system / vcycle / cg), %d iterations, "
+                      "%.1f s" % (tri.shape[1], tri.shape[0], iters, dt)}, x
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    import pymatting_b200  # noqa: F401
+    from pymatting_b200.batch import AlphaBatch, solve_alpha
+
+    imgs, tris, fracs = make_inputs(args.workload, rank)
+    npx = sum(t.size for t in tris)
+    imgs_d = [torch.as_tensor(i, device=dev) for i in imgs]
+    tris_d = [torch.as_tensor(t, device=dev) for t in tris]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def device_step(precision):
+        batch = AlphaBatch(imgs_d, tris_d, precision=precision)
+        x = batch.solve()
+        alphas = batch.alphas(x)
+        return batch, x, alphas
+
+    def timed(fn, steps):
+        times, info = [], None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            info = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times, info
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world > 1:
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    results = {}
+    clocks = ClockSampler(local)
+    for precision in ["fp64", "mixed"]:
+        for _ in range(args.warmup):
+            device_step(precision)
+        barrier()
+        if precision == "mixed":
+            clocks.start()
+        times, info = timed(lambda: device_step(precision), args.steps)
+        if precision == "mixed":
+            clock_rec = clocks.stop()
+        barrier()
+        total_ms = max_over_ranks(sum(times))
+        batch = info[0]
+        launches = sum(batch.system.launch_count() for _ in [0]) + 4 * len(imgs)
+        results[precision] = dict(total_ms=total_ms, batch=batch, x=info[1],
+                                  launches_per_step=launches)
+
+    # FP64 relative residual of the mixed result, measured with the FP64
+    # operator of an FP64 system on the same inputs.
+    b64 = results["fp64"]["batch"]
+    ax = b64.system.apply(results["mixed"]["x"])
+    rel_mixed = float(torch.linalg.norm(b64.b - ax) / torch.linalg.norm(b64.b))
+    ax = b64.system.apply(results["fp64"]["x"])
+    rel_fp64 = float(torch.linalg.norm(b64.b - ax) / torch.linalg.norm(b64.b))
+    alpha_diff = float((torch.clamp(results["mixed"]["x"], 0, 1) -
+                        torch.clamp(results["fp64"]["x"], 0, 1)).abs().max())
+
+    # End to end through the public API with host buffers.
+    for _ in range(max(1, args.warmup)):
+        solve_alpha(imgs, tris, precision="mixed")
+    barrier()
+    e2e_times, _ = timed(lambda: solve_alpha(imgs, tris, precision="mixed"), args.steps)
+    e2e_ms = max_over_ranks(sum(e2e_times))
+
+    # Roofline of the Laplacian apply (the operator kernel of the solve).
+    peak, peak_kind = measured_peaks()
+    apply = {}
+    for precision, es in [("mixed", 4), ("fp64", 8)]:
+        ms = results[precision]["batch"].system.time_apply(50)
+        bytes_alg = npx * 15 * es
+        apply[precision] = dict(ms=ms, bytes=bytes_alg, gbs=bytes_alg / (ms * 1e-3) / 1e9)
+    traffic = traffic_per_launch("fp32", npx)
+
+    if rank == 0:
+        k = args.steps
+        value = world * npx * k / (results["mixed"]["total_ms"] * 1e-3) / 1e6
+        value64 = world * npx * k / (results["fp64"]["total_ms"] * 1e-3) / 1e6
+        e2e_value = world * npx * k / (e2e_ms * 1e-3) / 1e6
+        st_m = results["mixed"]["batch"].stats()[0]
+        st_d = results["fp64"]["batch"].stats()[0]
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "Mpix/s",
+            "n_gpus": world,
+            "steps": k,
+            "warmup": args.warmup,
+            "ms_per_step": results["mixed"]["total_ms"] / k,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 inner / f64 refinement",
+            "data": "synthetic",
+            "config": {
+                "workload": "cf_alpha_soft_vcycle_rtol1e-7_" + args.workload,
+                "images_per_gpu": len(imgs),
+                "image": "x".join(str(s) for s in (tris[0].shape[1], tris[0].shape[0])),
+                "unknown_fraction": round(float(np.mean(fracs)), 4),
+                "lambda": 100.0, "epsilon": 1e-7, "preconditioner": "vcycle",
+                "precision": "mixed (FP32 inner rtol 1e-4, FP64 refinement)",
+                "l2": "flushed between steps (256 MB write); planes exceed L2",
+                "parallelism": "weak: one image per GPU, no collective",
+            },
+            "fp64_value": value64,
+            "mixed_over_fp64": value / value64,
+            "iters": {"mixed_inner_total": st_m.iters, "mixed_outer": st_m.outer_iters,
+                      "fp64": st_d.iters},
+            "rel_residual_fp64": {"mixed": rel_mixed, "fp64": rel_fp64},
+            "alpha_maxabs_mixed_vs_fp64": alpha_diff,
+            "roofline": {
+                "bound": "hbm",
+                "kernel": "half-stencil Laplacian apply y = (L + lambda D) x, FP32",
+                "achieved": apply["mixed"]["gbs"],
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": apply["mixed"]["gbs"] / peak,
+                "peak_source": peak_kind,
+                "traffic": traffic,
+                "bytes_per_launch": apply["mixed"]["bytes"],
+                "bytes_formula": "pixels x 15 values (13 half-stencil planes + x + y) x 4 B",
+                "fp64": {"achieved": apply["fp64"]["gbs"], "frac": apply["fp64"]["gbs"] / peak,
+                         "bytes_per_launch": apply["fp64"]["bytes"]},
+            },
+            "e2e": {"value": e2e_value, "unit": "Mpix/s",
+                    "h2d_bytes_per_step": int(npx * (24 + 8)),
+                    "d2h_bytes_per_step": int(npx * 8)},
+            "gpu_launches": int(results["mixed"]["launches_per_step"] * k),
+            "clocks": clock_rec,
+        }
+        if world == 1 and not args.no_cpu_baseline and args.workload == "1080p":
+            cb, _x = cpu_baseline(imgs[0], tris[0])
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

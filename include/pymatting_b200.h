@@ -48,10 +48,11 @@ int pmb_grid_pitch(int w);
  * (pymatting/laplacian/cf_laplacian.py:132-177): fills the CSR arrays
  * exactly as the reference does — (4r+1)^2 slots per row, out-of-image
  * slots holding column 0 and value 0 — with bitwise-identical values.
- * is_known may be NULL (no window skipped). radius 1 or 2. */
+ * is_known may be NULL (no window skipped). radius 1 or 2. With diag_mask,
+ * diag_value is added to the diagonal slot where the mask is set. */
 int pmb_cf_laplacian_ell(const double* image, const uint8_t* is_known, int h, int w,
-                         int radius, double epsilon, double* values, int64_t* indices,
-                         int64_t* indptr, void* stream);
+                         int radius, double epsilon, const uint8_t* diag_mask, double diag_value,
+                         double* values, int64_t* indices, int64_t* indptr, void* stream);
 
 /* Radius-1 Laplacian as 13 half-stencil planes, plus diag_value on the
  * diagonal where diag_mask is set: with diag_mask = is_known and
@@ -104,9 +105,130 @@ int pmb_stencil_apply(pmb_stencil* s, const double* x, double* y, void* stream);
  * for precision 1); outer_iters: refinement steps. */
 int pmb_stencil_stats(pmb_stencil* s, int image, int* iters, int* status, double* norm_r,
                       double* norm_b, int* outer_iters);
-/* Kernel launches issued by this object so far (graph replays excluded). */
+/* Kernel launches issued by this object so far (kernels replayed from its
+ * CUDA graphs included). */
 int64_t pmb_stencil_launch_count(const pmb_stencil* s);
 int pmb_stencil_destroy(pmb_stencil* s);
+/* Average milliseconds of one level-0 operator apply y = A x (inner
+ * precision), timed with CUDA events on the solver's stream over `iters`
+ * launches. Benchmark hook; no reference counterpart. */
+int pmb_stencil_time_apply(pmb_stencil* s, int iters, double* ms, void* stream);
+
+/* ---- Sparse-format helpers (device arrays, int64 indices) ---------------- */
+
+/* Scratch elements (int64) the scans below need for n entries. */
+int64_t pmb_scan_scratch_elems(int64_t n);
+/* Canonical CSR of an assembled ELL (values from pmb_cf_laplacian_ell):
+ * in-image slots with a non-zero value, ascending columns — the form scipy
+ * gives L + C in make_linear_system (pymatting/laplacian/laplacian.py:50-55).
+ * rowptr has n+1 entries; rowptr[n] = nnz. */
+int pmb_ell_csr_rowptr(const double* values, int h, int w, int radius, int64_t* rowptr,
+                       int64_t* scratch, void* stream);
+int pmb_ell_csr_fill(const double* values, int h, int w, int radius, const int64_t* rowptr,
+                     int64_t* indices, double* data, void* stream);
+/* Canonical CSR of A + diag(c) for a general CSR A with rows of at most 64
+ * entries (make_linear_system on a matrix not assembled by this library,
+ * pymatting/laplacian/laplacian.py:50-55). *overflow = 1 for longer rows. */
+int pmb_csr_add_diag_rowptr(int64_t n, const int64_t* indptr, const int64_t* indices,
+                            const double* data, const double* c, int64_t* rowptr, int* overflow,
+                            int64_t* scratch, void* stream);
+int pmb_csr_add_diag_fill(int64_t n, const int64_t* indptr, const int64_t* indices,
+                          const double* data, const double* c, const int64_t* rowptr,
+                          int64_t* out_indices, double* out_data, void* stream);
+
+/* ---- Trimap and hard-constraint system --------------------------------- */
+
+/* trimap_split (pymatting/util/util.py:510-525): is_fg = t >= fg_threshold,
+ * is_known = is_fg | (t <= bg_threshold); counts[0] = #fg, counts[1] = #bg. */
+int pmb_trimap_masks(const double* trimap, int64_t n, double fg_threshold, double bg_threshold,
+                     uint8_t* is_fg, uint8_t* is_known, unsigned long long* counts, void* stream);
+/* Compact index of every unknown pixel (exclusive scan); cidx[n] = #unknown. */
+int pmb_unknown_index(const uint8_t* is_known, int64_t n, int64_t* cidx, int64_t* scratch,
+                      void* stream);
+/* L_U = L[U, :][:, U] and b_U = -L[U, :][:, K] is_fg[K] from the ELL of the
+ * Laplacian assembled with is_known (estimate_alpha_cf.py:64-74). */
+int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, const int64_t* cidx,
+                       int64_t n_unknown, int64_t* rowptr, int64_t* scratch, void* stream);
+int pmb_hard_lu_fill(const double* ell_values, const uint8_t* is_known, const uint8_t* is_fg,
+                     int h, int w, const int64_t* cidx, const int64_t* rowptr, int64_t* indices,
+                     double* data, double* rhs, void* stream);
+/* alpha = clip(trimap on known pixels, x_U on unknown ones) to [0, 1]
+ * (estimate_alpha_cf.py:72-76). */
+int pmb_alpha_compose(const double* trimap, const uint8_t* is_known, const int64_t* cidx,
+                      const double* x_unknown, int64_t n, double* alpha, void* stream);
+/* out = value * mask (b = lambda * is_fg, laplacian.py:48). */
+int pmb_mask_scale(const uint8_t* mask, int64_t n, double value, double* out, void* stream);
+/* out = clip(x, 0, 1). */
+int pmb_clip01(const double* x, int64_t n, double* out, void* stream);
+
+/* ---- General CSR systems ------------------------------------------------ */
+
+/* One system A x = b with A in CSR (or applied by the caller) solved by
+ * cg (pymatting/solver/cg.py:4-117). preconditioner: 0 none, 1 Jacobi (1/diag
+ * in the invd row of the vector block), 2 matrix (M.dot, cg.py:58-62),
+ * 3 incomplete Cholesky (pmb_ichol), 4 applied by the caller. */
+int pmb_csr_create(int64_t n, int64_t nnz, int preconditioner, pmb_csr** out);
+int64_t pmb_csr_workspace_bytes(const pmb_csr* c);
+/* vectors: 8 n doubles, rows x r z p0 p1 Ap dr invd. indptr/indices/data
+ * may be NULL when the caller applies A. */
+int pmb_csr_bind(pmb_csr* c, void* workspace, double* vectors, const int64_t* indptr,
+                 const int64_t* indices, const double* data);
+int pmb_csr_set_matrix_preconditioner(pmb_csr* c, int64_t nnz, const int64_t* indptr,
+                                      const int64_t* indices, const double* data, void* stream);
+int pmb_csr_set_ichol(pmb_csr* c, pmb_ichol* factor, void* stream);
+int pmb_csr_solve(pmb_csr* c, const double* b, const double* x0, double* x_out, double atol,
+                  double rtol, int maxiter, int reorthogonalize, void* stream);
+/* Step interface for callbacks and caller-applied A or M: begin, then per
+ * iteration step(0) (or step(1), caller writes A p into the Ap row,
+ * step(2)), stats, and after a caller-applied M finish_precondition. */
+int pmb_csr_begin(pmb_csr* c, const double* b, const double* x0, double atol, double rtol,
+                  int maxiter, int reorthogonalize, void* stream);
+int pmb_csr_step(pmb_csr* c, int mode, void* stream);
+int pmb_csr_finish_precondition(pmb_csr* c, void* stream);
+/* Row (0 or 1) of the p double-buffer that holds the current direction. */
+int pmb_csr_p_index(pmb_csr* c);
+int pmb_csr_stats(pmb_csr* c, int* iters, int* status, double* norm_r, double* norm_b);
+int pmb_csr_destroy(pmb_csr* c);
+/* y = A x; invd = 1 / diag(A) (duplicates summed, jacobi.py:24-26);
+ * out = a * b element-wise (the Jacobi apply, jacobi.py:28-29). */
+int pmb_csr_spmv(int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
+                 const double* x, double* y, void* stream);
+int pmb_csr_inv_diag(int64_t n, const int64_t* indptr, const int64_t* indices,
+                     const double* data, double* invd, void* stream);
+int pmb_vec_mul(int64_t n, const double* a, const double* b, double* out, void* stream);
+/* 1 / diagonal of a radius-1 plane set, in user layout. */
+int pmb_planes_inv_diag(const double* planes, int h, int w, double* inv_diag, void* stream);
+/* x = A^-1 b for a small square CSR matrix (n <= 4096) by Gaussian
+ * elimination with partial pivoting — the direct branch of the V-cycle
+ * (vcycle.py:59-60). scratch n*n doubles; x holds b on entry. */
+int pmb_dense_solve(int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
+                    double* scratch, double* x, int* singular, void* stream);
+
+/* ---- Thresholded incomplete Cholesky ----------------------------------- */
+
+/* Lower-part profile of a CSC matrix: out[0] = bandwidth, out[1] = envelope
+ * (bound on the factor size). scratch: n + 2 uint64. */
+int pmb_csc_profile(int64_t n, const int64_t* Ap, const int64_t* Ar, const double* Av,
+                    uint64_t* scratch, uint64_t* out, void* stream);
+/* Factor object for ichol(A, discard_threshold, shifts, max_nnz,
+ * relative_discard_threshold, diag_keep_discarded)
+ * (pymatting/preconditioner/ichol.py:184-301). capacity >= factor nnz. */
+int pmb_ichol_create(int64_t n, int64_t bandwidth, int64_t capacity, pmb_ichol** out);
+int64_t pmb_ichol_workspace_bytes(const pmb_ichol* f);
+int pmb_ichol_bind(pmb_ichol* f, void* workspace);
+/* One attempt with a diagonal shift (ichol.py:259-276); *result = factor nnz,
+ * -1 (not positive definite) or -2 (more than max_nnz entries). */
+int pmb_ichol_factor(pmb_ichol* f, const int64_t* Ap, const int64_t* Ar, const double* Av,
+                     double discard_threshold, double shift, int64_t max_nnz,
+                     double relative_discard_threshold, int diag_keep_discarded,
+                     int64_t* result, void* stream);
+/* Dependency levels of the factor (length of the triangular-solve schedule). */
+int pmb_ichol_levels(const pmb_ichol* f);
+/* Device pointers of the CSC factor (values, row indices, column pointers). */
+int pmb_ichol_factor_arrays(pmb_ichol* f, void** Lv, void** Lr, void** Lp);
+/* x = L^-T L^-1 b (CholeskyDecomposition.__call__, ichol.py:175-181). */
+int pmb_ichol_apply(pmb_ichol* f, const double* b, double* x, void* stream);
+int pmb_ichol_destroy(pmb_ichol* f);
 
 #ifdef __cplusplus
 }

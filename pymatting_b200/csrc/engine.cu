@@ -10,6 +10,7 @@
 // size it needs and carves it up at bind time. The only things an object
 // allocates itself are a stream, two events, CUDA graphs and a small pinned
 // status buffer, all released by its destroy call.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -80,14 +81,28 @@ struct Carve {
 
 static int tiles_of(int h, int w, int th, int tw) { return ((h + th - 1) / th) * ((w + tw - 1) / tw); }
 
-static int persistent_grid(int total) {
-    // 8 resident 256-thread CTAs per SM on the 148-SM part.
-    return std::max(1, std::min(total, 148 * 8));
-}
 
 // --------------------------------------------------------------------------
 // Stencil batch solver
 // --------------------------------------------------------------------------
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
 
 struct HostList {
     std::vector<GridDesc> grids;     // descriptors of this list
@@ -96,6 +111,7 @@ struct HostList {
     size_t d_grids = 0, d_partner = 0, d_starts = 0;  // workspace offsets
     WorkList wl{};                   // device view, filled at bind
     const GridDesc* partner_dev = nullptr;
+    int per_sm = 8;                  // resident CTAs per SM of the kernels using it
 };
 
 struct Level {
@@ -107,8 +123,9 @@ struct Level {
     // device offsets (levels >= 1 only, level 0 uses the solver vectors)
     size_t b64 = 0, x64 = 0, xa64 = 0, xb64 = 0, P64 = 0;
     size_t b32 = 0, x32 = 0, xa32 = 0, xb32 = 0, P32 = 0;
-    HostList fine;    // fine tiles of level-l grids that have a level l+1
-    HostList coarse;  // coarse tiles of the level l+1 grids of the same images
+    HostList fine;    // 64x8 tiles of level-l grids that have a level l+1
+    HostList coarse;  // restriction tiles of the level l+1 grids of the same images
+    HostList flat;    // element chunks of the same level-l grids
 };
 
 struct Stencil {
@@ -119,20 +136,23 @@ struct Stencil {
     int pre = 1, post = 1;
     double omega = 0.8;
     int direct = 64;
+    int cy = 3;                      // restriction tile height (inner precision)
     std::vector<int> coarsest;      // per image: index of the level solved directly
     std::vector<Level> levels;      // level 0 .. L
-    HostList all0;                  // every image's level-0 grid
+    HostList fine0;                 // 64x8 tiles of every image's level-0 grid
+    HostList flat0;                 // element chunks of every level-0 grid
     std::vector<int64_t> user_off;  // offset of image k in user vectors
     int64_t user_total = 0;
+    int nmaps = 0;                  // grids with a TMA descriptor block
     std::vector<DirectDesc> direct64, direct32;
     std::vector<int64_t> direct_inv_off;   // per direct desc: inverse offset (doubles)
     int64_t direct_doubles = 0;
     // workspace offsets
     size_t ws_bytes = 0;
     size_t o_state = 0, o_outer = 0, o_part = 0, o_uoff = 0, o_direct64 = 0, o_direct32 = 0;
-    size_t o_inv = 0, o_invwork = 0, o_status = 0;
+    size_t o_inv = 0, o_invwork = 0, o_status = 0, o_err = 0, o_maps = 0;
     size_t o_b64 = 0, o_x64 = 0, o_r64 = 0, o_z64 = 0, o_p064 = 0, o_p164 = 0, o_ap64 = 0, o_dr64 = 0;
-    size_t o_x032 = 0, o_P032 = 0;
+    size_t o_P032 = 0;
     size_t o_r32 = 0, o_z32 = 0, o_p032 = 0, o_p132 = 0, o_ap32 = 0, o_dr32 = 0, o_xin32 = 0;
     int64_t partials_count = 0;
     // bound state
@@ -145,6 +165,7 @@ struct Stencil {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     int graph_reorth = -1;
+    int64_t graph_kernels = 0;      // kernel nodes of one graph replay
     bool bound = false, setup_done = false;
     // last solve
     int64_t launches = 0;
@@ -154,7 +175,19 @@ struct Stencil {
     InstState* state() const { return at<InstState>(o_state); }
     InstState* outer() const { return at<InstState>(o_outer); }
     double* partials() const { return at<double>(o_part); }
+    int* err() const { return at<int>(o_err); }
+    const CUtensorMap* maps() const { return at<CUtensorMap>(o_maps); }
 };
+
+static int blocks_per_sm(size_t smem) {
+    const size_t usable = 227 * 1024;
+    int b = (int)(usable / (smem + 1024));
+    return std::max(1, std::min(8, b));
+}
+
+static int persistent_grid(const HostList& L) {
+    return std::max(1, std::min(L.wl.total, 148 * L.per_sm));
+}
 
 static void build_list(HostList& L, const std::vector<GridDesc>& grids,
                        const std::vector<GridDesc>& partner, int th, int tw) {
@@ -165,6 +198,16 @@ static void build_list(HostList& L, const std::vector<GridDesc>& grids,
         L.starts[g + 1] = L.starts[g] + tiles_of(grids[g].h, grids[g].w, th, tw);
 }
 
+static void build_flat(HostList& L, const std::vector<GridDesc>& grids) {
+    L.grids = grids;
+    L.partner.clear();
+    L.starts.assign(grids.size() + 1, 0);
+    for (size_t g = 0; g < grids.size(); ++g) {
+        const int64_t n = (int64_t)grids[g].h * grids[g].pitch;
+        L.starts[g + 1] = L.starts[g] + (int)((n + kFlat - 1) / kFlat);
+    }
+}
+
 static void carve_list(Carve& c, HostList& L) {
     L.d_grids = c.take<GridDesc>((int64_t)L.grids.size());
     L.d_partner = c.take<GridDesc>((int64_t)L.partner.size());
@@ -173,6 +216,8 @@ static void carve_list(Carve& c, HostList& L) {
 
 static int plan_stencil(Stencil& S) {
     const int n = S.nimg;
+    const bool mixed = S.precision == 1;
+    S.cy = mixed ? Coarse<float>::CY : Coarse<double>::CY;
     S.coarsest.assign(n, 0);
     // Level shapes per image: h // 2^l, w // 2^l until h*w <= direct size
     // (vcycle.py:59, :83-86). With no V-cycle only level 0 exists.
@@ -197,6 +242,7 @@ static int plan_stencil(Stencil& S) {
     S.user_off.assign(n + 1, 0);
     for (int k = 0; k < n; ++k) S.user_off[k + 1] = S.user_off[k] + (int64_t)S.h[k] * S.w[k];
     S.user_total = S.user_off[n];
+    int map_base = 0;
     for (int l = 0; l < L; ++l) {
         Level& lv = S.levels[l];
         int64_t voff = 0, poff = 0;
@@ -210,6 +256,7 @@ static int plan_stencil(Stencil& S) {
             g.voff = voff;
             g.poff = poff;
             g.pstride = (int64_t)g.h * g.pitch;
+            g.map_base = map_base++;
             voff += (int64_t)g.h * g.pitch;
             poff += (int64_t)kNH * g.h * g.pitch;
             lv.grids.push_back(g);
@@ -219,8 +266,15 @@ static int plan_stencil(Stencil& S) {
         lv.vec_elems = voff;
         lv.plane_elems = poff;
     }
-    // Work lists.
-    build_list(S.all0, S.levels[0].grids, {}, kTY, kTX);
+    S.nmaps = map_base;
+    // Work lists and the residency of the kernels that walk them.
+    const int per_fine = blocks_per_sm(mixed ? smem_apply<float>() : smem_apply<double>());
+    const int per_up = blocks_per_sm(mixed ? smem_up<float>(S.pre) : smem_up<double>(S.pre));
+    const int per_down = blocks_per_sm(mixed ? smem_down<float>(S.pre) : smem_down<double>(S.pre));
+    build_list(S.fine0, S.levels[0].grids, {}, kTY, kTX);
+    S.fine0.per_sm = per_fine;
+    build_flat(S.flat0, S.levels[0].grids);
+    S.flat0.per_sm = 8;
     for (int l = 0; l + 1 < L; ++l) {
         Level& lv = S.levels[l];
         Level& nx = S.levels[l + 1];
@@ -233,7 +287,11 @@ static int plan_stencil(Stencil& S) {
             c.push_back(nx.grids[it - nx.image.begin()]);
         }
         build_list(lv.fine, f, c, kTY, kTX);
-        build_list(lv.coarse, c, f, kCY, kCX);
+        lv.fine.per_sm = per_up;
+        build_list(lv.coarse, c, f, S.cy, kCX);
+        lv.coarse.per_sm = per_down;
+        build_flat(lv.flat, f);
+        lv.flat.per_sm = 8;
     }
     // Dense coarsest solves.
     S.direct64.clear();
@@ -256,21 +314,25 @@ static int plan_stencil(Stencil& S) {
     // Workspace layout.
     Carve c;
     const int64_t v0 = S.levels[0].vec_elems;
-    const bool mixed = S.precision == 1;
     S.o_state = c.take<InstState>(n);
     S.o_outer = c.take<InstState>(n);
-    int64_t maxt = S.all0.starts.back();
+    int64_t maxt = std::max(S.fine0.starts.back(), S.flat0.starts.back());
     for (auto& lv : S.levels) {
         if (!lv.fine.starts.empty()) maxt = std::max<int64_t>(maxt, lv.fine.starts.back());
+        if (!lv.flat.starts.empty()) maxt = std::max<int64_t>(maxt, lv.flat.starts.back());
     }
     S.partials_count = maxt;
     S.o_part = c.take<double>(3 * maxt);
     S.o_uoff = c.take<int64_t>(n + 1);
     S.o_status = c.take<int>(4);
-    carve_list(c, S.all0);
+    S.o_err = c.take<int>(4);
+    S.o_maps = c.take<CUtensorMap>((int64_t)S.nmaps * kMapsPerGrid);
+    carve_list(c, S.fine0);
+    carve_list(c, S.flat0);
     for (auto& lv : S.levels) {
         carve_list(c, lv.fine);
         carve_list(c, lv.coarse);
+        carve_list(c, lv.flat);
     }
     S.o_direct64 = c.take<DirectDesc>((int64_t)S.direct64.size());
     S.o_direct32 = c.take<DirectDesc>((int64_t)S.direct64.size());
@@ -358,16 +420,107 @@ static int on_stream(Stencil& S, cudaStream_t caller, Fn fn) {
     return rc;
 }
 
+// Plane base pointer of level l (FP64 / FP32).
+static const double* planes64(const Stencil& S, int l) {
+    return l == 0 ? S.P0 : S.at<double>(S.levels[l].P64);
+}
+static const float* planes32(const Stencil& S, int l) {
+    return l == 0 ? S.at<float>(S.o_P032) : S.at<float>(S.levels[l].P32);
+}
+
+// Encode one tiled TMA descriptor of a pitched 2D vector or of the 13-plane
+// 3D operator block of grid g.
+static int encode_map(CUtensorMap* out, const void* base, const GridDesc& g, bool planes,
+                      bool fp32, int box_w, int box_h) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return fail(kErrCuda, "cuTensorMapEncodeTiled is not available");
+    const size_t es = fp32 ? 4 : 8;
+    const CUtensorMapDataType dt = fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    cuuint64_t dims[3] = {(cuuint64_t)g.w, (cuuint64_t)g.h, (cuuint64_t)kNH};
+    cuuint64_t strides[2] = {(cuuint64_t)g.pitch * es, (cuuint64_t)g.pitch * g.h * es};
+    cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)box_h, (cuuint32_t)kNH};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const char* ptr = static_cast<const char*>(base) + (planes ? g.poff : g.voff) * es;
+    CUresult r = enc(out, dt, planes ? 3 : 2, const_cast<char*>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(kErrCuda, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return 0;
+}
+
+// Fill every grid's descriptor block. Slots that a configuration never
+// reads are left zero.
+static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
+    maps.assign((size_t)S.nmaps * kMapsPerGrid, CUtensorMap{});
+    const bool mixed = S.precision == 1;
+    const int DH = 2 * S.cy + 5;
+    for (int l = 0; l < (int)S.levels.size(); ++l) {
+        Level& lv = S.levels[l];
+        const void* P = mixed ? (const void*)planes32(S, l) : (const void*)planes64(S, l);
+        const void* B; const void* X; const void* XA = nullptr; const void* XB = nullptr;
+        if (l == 0) {
+            B = mixed ? (const void*)S.at<float>(S.o_r32) : (const void*)S.at<double>(S.o_r64);
+            X = mixed ? (const void*)S.at<float>(S.o_z32) : (const void*)S.at<double>(S.o_z64);
+        } else {
+            B = mixed ? (const void*)S.at<float>(lv.b32) : (const void*)S.at<double>(lv.b64);
+            X = mixed ? (const void*)S.at<float>(lv.x32) : (const void*)S.at<double>(lv.x64);
+        }
+        if (S.precond == kPrecVcycle && (S.pre > 1 || S.post > 1)) {
+            XA = mixed ? (const void*)S.at<float>(lv.xa32) : (const void*)S.at<double>(lv.xa64);
+            XB = mixed ? (const void*)S.at<float>(lv.xb32) : (const void*)S.at<double>(lv.xb64);
+        }
+        for (const GridDesc& g : lv.grids) {
+            if (g.w <= 0 || g.h <= 0) continue;
+            CUtensorMap* m = &maps[(size_t)g.map_base * kMapsPerGrid];
+            int rc = 0;
+            rc |= encode_map(m + kMapPlF, P, g, true, mixed, kBW, kBH);
+            rc |= encode_map(m + kMapPlD, P, g, true, mixed, kBW, DH);
+            rc |= encode_map(m + kMapBF, B, g, false, mixed, kBW, kBH);
+            rc |= encode_map(m + kMapBD, B, g, false, mixed, kBW, DH);
+            rc |= encode_map(m + kMapXC, X, g, false, mixed, kCBW, kCBH);
+            rc |= encode_map(m + kMapXF, X, g, false, mixed, kBW, kBH);
+            if (XA) {
+                rc |= encode_map(m + kMapXAF, XA, g, false, mixed, kBW, kBH);
+                rc |= encode_map(m + kMapXAD, XA, g, false, mixed, kBW, DH);
+                rc |= encode_map(m + kMapXBF, XB, g, false, mixed, kBW, kBH);
+                rc |= encode_map(m + kMapXBD, XB, g, false, mixed, kBW, DH);
+            }
+            if (l == 0) {
+                const void* Z = X;
+                const void* Q0 = mixed ? (const void*)S.at<float>(S.o_p032) : (const void*)S.at<double>(S.o_p064);
+                const void* Q1 = mixed ? (const void*)S.at<float>(S.o_p132) : (const void*)S.at<double>(S.o_p164);
+                rc |= encode_map(m + kMapZF, Z, g, false, mixed, kBW, kBH);
+                rc |= encode_map(m + kMapP0F, Q0, g, false, mixed, kBW, kBH);
+                rc |= encode_map(m + kMapP1F, Q1, g, false, mixed, kBW, kBH);
+                if (mixed) {
+                    rc |= encode_map(m + kMapX64F, S.at<double>(S.o_x64), g, false, false, kBW, kBH);
+                    rc |= encode_map(m + kMapP64F, S.P0, g, true, false, kBW, kBH);
+                }
+            }
+            if (rc) return rc;
+        }
+    }
+    return 0;
+}
+
 static int bind_stencil(Stencil& S, void* ws, const double* P0) {
     S.ws = reinterpret_cast<char*>(ws);
     S.P0 = P0;
-    if (int rc = upload_list(S, S.all0)) return rc;
+    stencil_prepare();
+    if (int rc = upload_list(S, S.fine0)) return rc;
+    if (int rc = upload_list(S, S.flat0)) return rc;
     for (auto& lv : S.levels) {
         if (int rc = upload_list(S, lv.fine)) return rc;
         if (int rc = upload_list(S, lv.coarse)) return rc;
+        if (int rc = upload_list(S, lv.flat)) return rc;
     }
     PMB_CUDA(cudaMemcpyAsync(S.ws + S.o_uoff, S.user_off.data(), sizeof(int64_t) * S.user_off.size(),
                              cudaMemcpyHostToDevice, S.stream));
+    std::vector<CUtensorMap> maps;
+    if (int rc = encode_maps(S, maps)) return rc;
+    if (!maps.empty())
+        PMB_CUDA(cudaMemcpyAsync(S.ws + S.o_maps, maps.data(), sizeof(CUtensorMap) * maps.size(),
+                                 cudaMemcpyHostToDevice, S.stream));
     // Direct descriptors: the inverse pointers are absolute.
     S.direct32 = S.direct64;
     for (size_t i = 0; i < S.direct64.size(); ++i) {
@@ -382,6 +535,7 @@ static int bind_stencil(Stencil& S, void* ws, const double* P0) {
     }
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_state, 0, sizeof(InstState) * S.nimg, S.stream));
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_outer, 0, sizeof(InstState) * S.nimg, S.stream));
+    PMB_CUDA(cudaMemsetAsync(S.ws + S.o_err, 0, sizeof(int) * 4, S.stream));
     PMB_CUDA(cudaStreamSynchronize(S.stream));
     if (S.graph) {
         cudaGraphExecDestroy(S.graph);
@@ -392,12 +546,12 @@ static int bind_stencil(Stencil& S, void* ws, const double* P0) {
     return 0;
 }
 
-// Plane base pointer of level l (FP64 / FP32).
-static const double* planes64(const Stencil& S, int l) {
-    return l == 0 ? S.P0 : S.at<double>(S.levels[l].P64);
-}
-static const float* planes32(const Stencil& S, int l) {
-    return l == 0 ? S.at<float>(S.o_P032) : S.at<float>(S.levels[l].P32);
+static int check_err(Stencil& S) {
+    int e = 0;
+    PMB_CUDA(cudaMemcpyAsync(&e, S.err(), sizeof(int), cudaMemcpyDeviceToHost, S.stream));
+    PMB_CUDA(cudaStreamSynchronize(S.stream));
+    if (e) return fail(kErrState, "a TMA transfer did not complete in time");
+    return 0;
 }
 
 static int setup_stencil(Stencil& S) {
@@ -414,26 +568,11 @@ static int setup_stencil(Stencil& S) {
         ++S.launches;
     }
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_status, 0, sizeof(int), s));
-    if (!S.direct64.empty()) {
-        // Planes of each image's coarsest level: per-level launches.
-        for (int l = 0; l < L; ++l) {
-            std::vector<DirectDesc> dl;
-            int first = -1;
-            for (size_t i = 0; i < S.direct64.size(); ++i) {
-                if (S.coarsest[S.direct64[i].g.inst] == l) {
-                    if (first < 0) first = (int)i;
-                }
-            }
-            if (first < 0) continue;
-            // Descriptors of one level are contiguous only when the images
-            // are sorted; launch per descriptor to stay general.
-            for (size_t i = 0; i < S.direct64.size(); ++i) {
-                if (S.coarsest[S.direct64[i].g.inst] != l) continue;
-                launch_dense_inverse(S.at<DirectDesc>(S.o_direct64) + i, 1, planes64(S, l),
-                                     S.at<double>(S.o_invwork), S.at<int>(S.o_status), s);
-                ++S.launches;
-            }
-        }
+    for (size_t i = 0; i < S.direct64.size(); ++i) {
+        const int l = S.coarsest[S.direct64[i].g.inst];
+        launch_dense_inverse(S.at<DirectDesc>(S.o_direct64) + i, 1, planes64(S, l),
+                             S.at<double>(S.o_invwork), S.at<int>(S.o_status), s);
+        ++S.launches;
     }
     if (S.precision == 1) {
         launch_convert_f32(S.P0, S.at<float>(S.o_P032), (int64_t)kNH * S.levels[0].vec_elems, s);
@@ -489,8 +628,9 @@ template <typename T> static const DirectDesc* direct_dev(Stencil& S);
 template <> const DirectDesc* direct_dev<double>(Stencil& S) { return S.at<DirectDesc>(S.o_direct64); }
 template <> const DirectDesc* direct_dev<float>(Stencil& S) { return S.at<DirectDesc>(S.o_direct32); }
 
-// V-cycle z = M r (vcycle.py:46-100) at level 0 with r = b0. With st != null
-// the level-0 pass also reduces r . z and finishes beta.
+// V-cycle z = M r (vcycle.py:46-100) at level 0 with r = b0 (the level-0 b
+// buffer) and z = z0 (the level-0 x buffer). With st != null the level-0
+// pass also reduces r . z and finishes beta.
 template <typename T>
 static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* dr, int reorth) {
     cudaStream_t s = S.stream;
@@ -499,66 +639,67 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
     const int pre = S.pre, post = S.post;
     auto B = [&](int l) -> T* { return l == 0 ? const_cast<T*>(b0) : lvl_b<T>(S, l); };
     auto X = [&](int l) -> T* { return l == 0 ? z0 : lvl_x<T>(S, l); };
-    // Pre-smoothed iterate per level when more than one sweep is requested.
-    std::vector<const T*> xs(L, nullptr);
+    // Map slot of each level's pre-smoothed iterate (pre > 1).
+    std::vector<int> xs_slot_f(L, -1), xs_slot_d(L, -1);
     for (int l = 0; l + 1 < L; ++l) {
         HostList& f = S.levels[l].fine;
         HostList& c = S.levels[l].coarse;
         if (f.wl.total == 0) continue;
-        LaunchCfg Lf{persistent_grid(f.wl.total)};
         if (pre > 1) {
+            // Sweeps alternate A / B; the first writes A (from zero).
             T* a = lvl_xa<T>(S, l);
             T* bb = lvl_xb<T>(S, l);
-            launch_vc_smooth<T>(Lf, f.wl, lvl_P<T>(S, l), B(l), nullptr, a, om, st, s);
+            launch_vc_smooth<T>(LaunchCfg{persistent_grid(f)}, f.wl, S.maps(), -1, lvl_P<T>(S, l),
+                                B(l), a, om, st, S.err(), s);
             ++S.launches;
+            bool in_a = true;
             for (int k = 1; k < pre; ++k) {
-                launch_vc_smooth<T>(Lf, f.wl, lvl_P<T>(S, l), B(l), a, bb, om, st, s);
+                launch_vc_smooth<T>(LaunchCfg{persistent_grid(f)}, f.wl, S.maps(),
+                                    in_a ? kMapXAF : kMapXBF, lvl_P<T>(S, l), B(l), in_a ? bb : a,
+                                    om, st, S.err(), s);
                 ++S.launches;
-                std::swap(a, bb);
+                in_a = !in_a;
             }
-            xs[l] = a;
+            xs_slot_f[l] = in_a ? kMapXAF : kMapXBF;
+            xs_slot_d[l] = in_a ? kMapXAD : kMapXBD;
         }
-        LaunchCfg Lc{persistent_grid(c.wl.total)};
-        launch_vc_down<T>(pre, Lc, c.wl, c.partner_dev, lvl_P<T>(S, l), B(l), xs[l], B(l + 1), om,
-                          st, s);
+        launch_vc_down<T>(pre, LaunchCfg{persistent_grid(c)}, c.wl, c.partner_dev, S.maps(),
+                          xs_slot_d[l], B(l + 1), om, st, S.err(), s);
         ++S.launches;
     }
     // Coarsest solves: every image, whatever its depth.
-    {
-        const int nd = (int)S.direct64.size();
-        // Images whose coarsest level is 0 read r and write z directly.
-        for (int i = 0; i < nd; ++i) {
-            const int k = S.direct64[i].g.inst;
-            const int l = S.coarsest[k];
-            const bool z_out = (l == 0);
-            launch_vc_direct<T>(direct_dev<T>(S) + i, 1, B(l), X(l), st, z_out && st != nullptr, s);
-            ++S.launches;
-        }
+    for (size_t i = 0; i < S.direct64.size(); ++i) {
+        const int k = S.direct64[i].g.inst;
+        const int l = S.coarsest[k];
+        const bool z_out = (l == 0);
+        launch_vc_direct<T>(direct_dev<T>(S) + i, 1, B(l), X(l), st, z_out && st != nullptr, s);
+        ++S.launches;
     }
     for (int l = L - 2; l >= 0; --l) {
         HostList& f = S.levels[l].fine;
         if (f.wl.total == 0) continue;
-        LaunchCfg Lf{persistent_grid(f.wl.total)};
+        LaunchCfg Lf{persistent_grid(f)};
         const int extra = post > 1 ? post - 1 : 0;
-        T* out = X(l);
-        T* tmpa = extra ? lvl_xa<T>(S, l) : nullptr;
         // Sweeps alternate buffers so that the last one lands in X(l).
-        T* first_out = (extra % 2 == 0) ? out : tmpa;
+        const bool first_in_x = (extra % 2 == 0);
+        T* first_out = first_in_x ? X(l) : lvl_xa<T>(S, l);
         const bool reduce_here = (l == 0) && st && extra == 0;
-        launch_vc_up<T>(pre, post, Lf, f.wl, f.partner_dev, lvl_P<T>(S, l), B(l), xs[l], X(l + 1),
-                        first_out, om, st, reduce_here ? 1 : 0, dr, reorth, S.partials(), s);
+        launch_vc_up<T>(pre, post, Lf, f.wl, f.partner_dev, S.maps(), xs_slot_f[l], B(l), first_out,
+                        om, st, reduce_here ? 1 : 0, dr, reorth, S.partials(), S.err(), s);
         ++S.launches;
-        T* cur = first_out;
+        bool cur_x = first_in_x;
         for (int k = 0; k < extra; ++k) {
-            T* nxt = (cur == out) ? tmpa : out;
-            launch_vc_smooth<T>(Lf, f.wl, lvl_P<T>(S, l), B(l), cur, nxt, om, st, s);
+            T* nxt = cur_x ? lvl_xa<T>(S, l) : X(l);
+            launch_vc_smooth<T>(Lf, f.wl, S.maps(), cur_x ? kMapXF : kMapXAF, lvl_P<T>(S, l), B(l),
+                                nxt, om, st, S.err(), s);
             ++S.launches;
-            cur = nxt;
+            cur_x = !cur_x;
         }
         if (l == 0 && st && extra > 0) {
             // r . z for the images that own coarser levels (the others were
             // reduced by their direct solve).
-            launch_cg_rz<T>(Lf, f.wl, b0, z0, dr, reorth, st, S.partials(), s);
+            launch_cg_rz<T>(LaunchCfg{persistent_grid(S.levels[0].flat)}, S.levels[0].flat.wl, b0,
+                            z0, dr, reorth, st, S.partials(), s);
             ++S.launches;
         }
     }
@@ -569,14 +710,13 @@ template <typename T>
 static void cg_iteration(Stencil& S, int reorth) {
     cudaStream_t s = S.stream;
     CgVecs<T> v = cg_vecs<T>(S);
-    HostList& a = S.all0;
-    LaunchCfg L0{persistent_grid(a.wl.total)};
     InstState* st = S.state();
     // Without a preconditioner z is r itself (cg.py:53-55).
-    const T* zsrc = S.precond == kPrecNone ? v.r : v.z;
-    launch_cg_apply<T>(L0, a.wl, v.P, zsrc, v.p0, v.p1, v.ap, st, S.partials(), s);
-    launch_cg_update<T>(S.precond, L0, a.wl, v.P, v.x, v.r, v.z, v.p0, v.p1, v.ap, v.dr, reorth, st,
-                        S.partials(), s);
+    const int zslot = S.precond == kPrecNone ? kMapBF : kMapZF;
+    launch_cg_apply<T>(LaunchCfg{persistent_grid(S.fine0)}, S.fine0.wl, S.maps(), zslot, v.p0, v.p1,
+                       v.ap, st, S.partials(), S.err(), s);
+    launch_cg_update<T>(S.precond, LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, v.P, v.x, v.r,
+                        v.z, v.p0, v.p1, v.ap, v.dr, reorth, st, S.partials(), s);
     S.launches += 2;
     if (S.precond == kPrecVcycle) run_vcycle<T>(S, v.r, v.z, st, v.dr, reorth);
 }
@@ -612,10 +752,15 @@ static int iterate(Stencil& S, int reorth, int maxiter) {
         PMB_CUDA(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < chunk; ++i) cg_iteration<T>(S, reorth);
         PMB_CUDA(cudaStreamEndCapture(S.stream, &g));
+        size_t nodes = 0;
+        PMB_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
         PMB_CUDA(cudaGraphInstantiate(&S.graph, g, 0));
         cudaGraphDestroy(g);
         S.graph_iters = chunk;
         S.graph_reorth = reorth;
+        S.graph_kernels = (int64_t)nodes;
+        // Capture only recorded the launches; they did not run.
+        S.launches -= (int64_t)nodes;
     }
     int done_iters = 0;
     for (;;) {
@@ -623,25 +768,23 @@ static int iterate(Stencil& S, int reorth, int maxiter) {
         if (!any_running(S.h_state, S.nimg)) break;
         if (done_iters > maxiter + chunk) return fail(kErrState, "iteration control lost");
         PMB_CUDA(cudaGraphLaunch(S.graph, S.stream));
+        S.launches += S.graph_kernels;
         done_iters += chunk;
     }
-    return 0;
+    return check_err(S);
 }
 
 static int solve_fp64(Stencil& S, const double* x0, double atol, double rtol, int maxiter,
                       int reorth) {
     cudaStream_t s = S.stream;
     CgVecs<double> v = cg_vecs<double>(S);
-    HostList& a = S.all0;
-    LaunchCfg L0{persistent_grid(a.wl.total)};
-    const double* x0p = nullptr;
-    if (x0) {
+    HostList& a = S.fine0;
+    if (x0)
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), x0, v.p0,
                                     S.user_total, s);
-        x0p = v.p0;
-    }
-    launch_cg_init<double>(S.precond, L0, a.wl, v.P, S.at<double>(S.o_b64), v.x, x0p, v.r, v.z,
-                           S.state(), S.partials(), atol, rtol, maxiter, s);
+    launch_cg_init<double>(S.precond, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), v.P,
+                           S.at<double>(S.o_b64), v.x, x0 != nullptr, v.r, v.z, S.state(),
+                           S.partials(), atol, rtol, maxiter, S.err(), s);
     S.launches += 1;
     if (S.precond == kPrecVcycle) run_vcycle<double>(S, v.r, v.z, S.state(), v.dr, 0);
     return iterate<double>(S, reorth, maxiter);
@@ -651,8 +794,7 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
                        int reorth, double inner_rtol, int max_outer) {
     cudaStream_t s = S.stream;
     CgVecs<float> v = cg_vecs<float>(S);
-    HostList& a = S.all0;
-    LaunchCfg L0{persistent_grid(a.wl.total)};
+    HostList& a = S.fine0;
     double* x64 = S.at<double>(S.o_x64);
     if (x0)
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), x0, x64,
@@ -670,9 +812,9 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
     PMB_CUDA(cudaStreamSynchronize(s));
     S.inner_total.assign(S.nimg, 0);
     for (int outer = 0;; ++outer) {
-        launch_refine_residual(S.precond, L0, a.wl, S.P0, v.P, S.at<double>(S.o_b64), x64, v.r, v.x,
-                               v.z, S.outer(), S.state(), S.partials(), atol, rtol, inner_rtol,
-                               maxiter, max_outer, s);
+        launch_refine_residual(S.precond, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), v.P,
+                               S.at<double>(S.o_b64), v.r, v.x, v.z, S.outer(), S.state(),
+                               S.partials(), atol, rtol, inner_rtol, maxiter, max_outer, S.err(), s);
         S.launches += 1;
         if (int rc = read_states(S, true)) return rc;
         if (!any_running(S.h_outer, S.nimg)) break;
@@ -680,10 +822,11 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
         if (int rc = iterate<float>(S, reorth, maxiter)) return rc;
         // Inner iterations of this refinement step, summed per image.
         for (int k = 0; k < S.nimg; ++k) S.inner_total[k] += S.h_state[k].iters;
-        launch_refine_correct(L0, a.wl, x64, v.x, S.outer(), S.state(), S.nimg, s);
+        launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, x64, v.x, S.outer(),
+                              S.nimg, s);
         S.launches += 2;
     }
-    return 0;
+    return check_err(S);
 }
 
 }  // namespace pmb
@@ -902,7 +1045,7 @@ PMB_API int pmb_stencil_solve(pmb_stencil* p, const double* b, const double* x0,
         if (!S.setup_done) {
             if (int rc = setup_stencil(S)) return rc;
         }
-        HostList& a = S.all0;
+        HostList& a = S.fine0;
         cudaStream_t s = S.stream;
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), b,
                                     S.at<double>(S.o_b64), S.user_total, s);
@@ -910,12 +1053,8 @@ PMB_API int pmb_stencil_solve(pmb_stencil* p, const double* b, const double* x0,
         if (S.precision == 0) rc = solve_fp64(S, x0, atol, rtol, maxiter, reorthogonalize);
         else rc = solve_mixed(S, x0, atol, rtol, maxiter, reorthogonalize, inner_rtol, max_outer);
         if (rc) return rc;
-        if (S.precision == 0)
-            launch_unpack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff),
-                                          S.at<double>(S.o_x64), x_out, S.user_total, s);
-        else
-            launch_unpack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff),
-                                          S.at<double>(S.o_x64), x_out, S.user_total, s);
+        launch_unpack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff),
+                                      S.at<double>(S.o_x64), x_out, S.user_total, s);
         PMB_CUDA(cudaGetLastError());
         return 0;
     });
@@ -930,7 +1069,7 @@ PMB_API int pmb_stencil_precondition(pmb_stencil* p, const double* r, double* z,
         if (!S.setup_done) {
             if (int rc = setup_stencil(S)) return rc;
         }
-        HostList& a = S.all0;
+        HostList& a = S.fine0;
         cudaStream_t s = S.stream;
         CgVecs<double> v = cg_vecs<double>(S);
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), r, v.r,
@@ -938,10 +1077,9 @@ PMB_API int pmb_stencil_precondition(pmb_stencil* p, const double* r, double* z,
         if (S.precond == kPrecVcycle) {
             run_vcycle<double>(S, v.r, v.z, nullptr, nullptr, 0);
         } else if (S.precond == kPrecJacobi) {
-            // z = r * (1 / diag): the plane-0 diagonal, applied through the
-            // Jacobi path of the smoother (omega = 1, from zero).
-            launch_vc_smooth<double>(LaunchCfg{persistent_grid(a.wl.total)}, a.wl, S.P0, v.r,
-                                     nullptr, v.z, 1.0, nullptr, s);
+            // z = r / diag: the first Jacobi sweep from zero with omega = 1.
+            launch_vc_smooth<double>(LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), -1, S.P0, v.r,
+                                     v.z, 1.0, nullptr, S.err(), s);
         } else {
             PMB_CUDA(cudaMemcpyAsync(v.z, v.r, sizeof(double) * S.levels[0].vec_elems,
                                      cudaMemcpyDeviceToDevice, s));
@@ -949,7 +1087,7 @@ PMB_API int pmb_stencil_precondition(pmb_stencil* p, const double* r, double* z,
         launch_unpack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), v.z, z,
                                       S.user_total, s);
         PMB_CUDA(cudaGetLastError());
-        return 0;
+        return check_err(S);
     });
 }
 
@@ -957,18 +1095,19 @@ PMB_API int pmb_stencil_apply(pmb_stencil* p, const double* x, double* y, void* 
     if (!p || !x || !y) return fail(kErrArg, "pmb_stencil_apply: bad arguments");
     Stencil& S = p->S;
     if (!S.bound) return fail(kErrState, "pmb_stencil_apply: not bound");
+    if (S.precision != 0) return fail(kErrArg, "pmb_stencil_apply needs the fp64 solver");
     return on_stream(S, (cudaStream_t)stream, [&]() -> int {
-        HostList& a = S.all0;
+        HostList& a = S.fine0;
         cudaStream_t s = S.stream;
-        double* tx = S.precision == 0 ? S.at<double>(S.o_r64) : S.at<double>(S.o_b64);
-        double* ty = S.at<double>(S.o_x64);
+        double* tx = S.at<double>(S.o_r64);   // level-0 b buffer: map slot kMapBF
+        double* ty = S.at<double>(S.o_ap64);
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), x, tx,
                                     S.user_total, s);
-        launch_apply<double>(LaunchCfg{persistent_grid(a.wl.total)}, a.wl, S.P0, tx, ty, s);
+        launch_apply<double>(LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), ty, S.err(), s);
         launch_unpack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), ty, y,
                                       S.user_total, s);
         PMB_CUDA(cudaGetLastError());
-        return 0;
+        return check_err(S);
     });
 }
 
@@ -1607,4 +1746,44 @@ PMB_API int pmb_clip01(const double* x, int64_t n, double* out, void* stream) {
     k_clip01<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(x, n, out);
     PMB_CUDA(cudaGetLastError());
     return 0;
+}
+
+
+// Average duration (ms) of the level-0 operator apply y = A x over `iters`
+// back-to-back launches on the solver's stream, timed with CUDA events on
+// that stream. The solver's inner precision decides FP64 or FP32. Used by
+// the benchmark to relate the Laplacian apply to the HBM roofline.
+PMB_API int pmb_stencil_time_apply(pmb_stencil* p, int iters, double* ms, void* stream) {
+    if (!p || iters <= 0 || !ms) return fail(kErrArg, "pmb_stencil_time_apply: bad arguments");
+    Stencil& S = p->S;
+    if (!S.bound) return fail(kErrState, "pmb_stencil_time_apply: not bound");
+    return on_stream(S, (cudaStream_t)stream, [&]() -> int {
+        if (!S.setup_done) {
+            if (int rc = setup_stencil(S)) return rc;
+        }
+        cudaEvent_t e0, e1;
+        PMB_CUDA(cudaEventCreate(&e0));
+        PMB_CUDA(cudaEventCreate(&e1));
+        HostList& a = S.fine0;
+        const LaunchCfg L{persistent_grid(a)};
+        auto launch = [&]() {
+            if (S.precision == 0)
+                launch_apply<double>(L, a.wl, S.maps(), S.at<double>(S.o_ap64), S.err(), S.stream);
+            else
+                launch_apply<float>(L, a.wl, S.maps(), S.at<float>(S.o_ap32), S.err(), S.stream);
+        };
+        launch();
+        PMB_CUDA(cudaEventRecord(e0, S.stream));
+        for (int i = 0; i < iters; ++i) launch();
+        PMB_CUDA(cudaEventRecord(e1, S.stream));
+        PMB_CUDA(cudaEventSynchronize(e1));
+        float t = 0.f;
+        PMB_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        *ms = (double)t / iters;
+        S.launches += iters + 1;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        PMB_CUDA(cudaGetLastError());
+        return check_err(S);
+    });
 }

@@ -17,11 +17,45 @@ namespace pmb {
 
 constexpr int kRS = 2;       // stencil radius of the stored operator
 constexpr int kNH = 13;      // stored planes (centre + 12 forward offsets)
-constexpr int kTX = 32;      // fine tile width  (one thread per pixel)
-constexpr int kTY = 8;       // fine tile height
-constexpr int kCX = 16;      // coarse tile width used by the restriction
-constexpr int kCY = 8;       // coarse tile height
-constexpr int kThreads = kTX * kTY;
+constexpr int kTX = 64;      // fine tile width
+constexpr int kTY = 8;       // fine tile height (two pixels per thread)
+constexpr int kThreads = 256;
+constexpr int kFlat = 1024;  // elements per tile of the element-wise kernels
+
+// Shared-memory boxes loaded by TMA around a fine tile at (x0, y0): origin
+// (x0 - kBOX, y0 - 2), kBW x kBH elements. x0 - kBOX keeps the box start
+// 16-byte aligned for both precisions.
+constexpr int kBOX = 4;
+constexpr int kBW = kTX + 2 * kBOX;   // 72
+constexpr int kBH = kTY + 4;          // 12
+// Restriction tiles: kCX x CY coarse pixels; the fine box starts at
+// (2 X0 - 4, 2 Y0 - 3) and is kBW x (2 CY + 5).
+constexpr int kCX = 32;
+// Prolongation: coarse box at (x0/2 - 4, y0/2 - 2), kCBW x kCBH.
+constexpr int kCBW = 40;
+constexpr int kCBH = 8;
+
+template <typename T> struct Coarse { static constexpr int CY = sizeof(T) == 8 ? 3 : 4; };
+
+// TMA descriptor slots of one grid (see engine.cu for what each maps).
+enum : int {
+    kMapPlF = 0,   // planes, fine box (inner precision)
+    kMapPlD,       // planes, restriction box
+    kMapBF,        // level right-hand side b, fine box (r at level 0)
+    kMapBD,        // b, restriction box
+    kMapXC,        // level solution x as a coarse operand (z at level 0)
+    kMapXF,        // x, fine box
+    kMapXAF,       // smoothing ping-pong buffer A, fine box
+    kMapXAD,       // buffer A, restriction box
+    kMapXBF,       // smoothing ping-pong buffer B, fine box
+    kMapXBD,       // buffer B, restriction box
+    kMapZF,        // CG z, fine box (level 0)
+    kMapP0F,       // CG p parity 0 (also x0 scratch), fine box
+    kMapP1F,       // CG p parity 1, fine box
+    kMapX64F,      // FP64 refinement iterate, fine box
+    kMapP64F,      // FP64 planes, fine box (refinement residual)
+    kMapsPerGrid
+};
 
 __host__ __device__ constexpr int half_dy(int p) { return p < 3 ? 0 : (p < 8 ? 1 : 2); }
 __host__ __device__ constexpr int half_dx(int p) { return p < 3 ? p : (p < 8 ? p - 5 : p - 10); }
@@ -38,6 +72,8 @@ struct GridDesc {
     int64_t voff;           // offset of element (0, 0) in the level's vectors
     int64_t poff;           // offset of plane 0 in the level's plane buffer
     int64_t pstride;        // elements between consecutive planes (h * pitch)
+    int map_base;           // first TMA descriptor of this grid (kMapsPerGrid each)
+    int pad_;
 };
 
 // Tiles of one tile shape over the grids of one level. Grid g owns the global

@@ -2,6 +2,13 @@
 // the fused preconditioned conjugate-gradient steps, and the geometric
 // multigrid V-cycle used as its preconditioner.
 //
+// Every stencil kernel works on 64 x 8 pixel tiles. One thread of the CTA
+// issues TMA loads of the tile plus its halo: a single 3D box holds all 13
+// operator planes (72 x 12 x 13), 2D boxes hold the vector operands; the
+// hardware zero-fills everything outside the image, which supplies the
+// stencil's border terms. The kernels then read operators and operands from
+// shared memory only. Element-wise kernels stream 1024-element chunks.
+//
 // Every kernel walks a WorkList of tiles over a batch of grids (images of
 // different sizes, or the same multigrid level of several images) with a
 // grid-stride loop, so one launch serves the whole batch. Per-image scalars
@@ -15,51 +22,13 @@
 //               and border mask, jacobi_step, _vcycle_step)
 #include "pm_common.cuh"
 #include "stencil.cuh"
+#include "tma.cuh"
 
 namespace pmb {
 
 // --------------------------------------------------------------------------
 // Tile helpers
 // --------------------------------------------------------------------------
-
-// Stage v over [y0-2, y0+H+1] x [x0-2, x0+W+1] (zero outside the grid).
-template <typename T, int H, int W>
-__device__ __forceinline__ void stage_halo(T* s, const T* __restrict__ v, const GridDesc& g,
-                                           int y0, int x0) {
-    constexpr int SW = W + 4, SH = H + 4;
-    for (int q = threadIdx.x; q < SW * SH; q += blockDim.x) {
-        const int ly = q / SW, lx = q - ly * SW;
-        const int y = y0 - 2 + ly, x = x0 - 2 + lx;
-        T val = T(0);
-        if (y >= 0 && y < g.h && x >= 0 && x < g.w) val = v[g.voff + (int64_t)y * g.pitch + x];
-        s[q] = val;
-    }
-}
-
-// (A x)_i at pixel (y, x) with x staged in shared memory: s is the staged
-// tile, (ly, lx) the pixel's position in it and sw its row stride.
-template <typename T>
-__device__ __forceinline__ T apply_at(const T* __restrict__ P, const GridDesc& g, int y, int x,
-                                      const T* s, int ly, int lx, int sw) {
-    const int64_t i = (int64_t)y * g.pitch + x;
-    const T* Pg = P + g.poff;
-    T acc = __ldg(Pg + i) * s[ly * sw + lx];
-#pragma unroll
-    for (int p = 1; p < kNH; ++p) {
-        const int dy = half_dy(p), dx = half_dx(p);
-        const T* Pp = Pg + p * g.pstride;
-        acc += __ldg(Pp + i) * s[(ly + dy) * sw + lx + dx];
-        const int yy = y - dy, xx = x - dx;
-        if (yy >= 0 && xx >= 0 && xx < g.w)
-            acc += __ldg(Pp + i - (int64_t)dy * g.pitch - dx) * s[(ly - dy) * sw + lx - dx];
-    }
-    return acc;
-}
-
-template <typename T>
-__device__ __forceinline__ T diag_at(const T* __restrict__ P, const GridDesc& g, int y, int x) {
-    return __ldg(P + g.poff + (int64_t)y * g.pitch + x);
-}
 
 struct TileCoord { int g, y0, x0; };
 
@@ -73,6 +42,63 @@ __device__ __forceinline__ TileCoord tile_coord(const WorkList& wl, int t) {
     c.y0 = ty * H;
     c.x0 = (local - ty * tiles_x) * W;
     return c;
+}
+
+// Shared-memory carve-up with 128-byte alignment (TMA destinations).
+struct SmemCarve {
+    char* p;
+    __device__ explicit SmemCarve(char* base) : p(base) {}
+    template <typename T>
+    __device__ T* take(int count) {
+        T* r = reinterpret_cast<T*>(p);
+        p += ((size_t)count * sizeof(T) + 127) & ~size_t(127);
+        return r;
+    }
+};
+
+extern __shared__ __align__(128) char g_smem[];
+
+// Per-CTA TMA state: the barrier and its phase.
+struct Tma {
+    uint64_t* bar;
+    uint32_t phase;
+    int* err;
+    __device__ void init(uint64_t* b, int* e) {
+        bar = b;
+        phase = 0;
+        err = e;
+        if (threadIdx.x == 0) mbar_init(bar, 1);
+        __syncthreads();
+    }
+    // Called by every thread after thread 0 issued the loads.
+    __device__ bool wait() {
+        const bool ok = mbar_wait(bar, phase);
+        phase ^= 1u;
+        if (!ok && err) atomicExch(err, 1);
+        return ok;
+    }
+};
+
+__device__ __forceinline__ const CUtensorMap* map_of(const CUtensorMap* maps, const GridDesc& g,
+                                                     int slot) {
+    return maps + (size_t)g.map_base * kMapsPerGrid + slot;
+}
+
+// (A x) at the pixel whose box coordinates are (r, c): P is the 13-plane
+// box (planes of kBW x ph elements), X the operand box (kBW wide). The
+// backward entries A[i, i - d] are plane d at (r - dy, c - dx).
+template <typename T>
+__device__ __forceinline__ T stencil_at(const T* P, int ph, const T* X, int r, int c) {
+    const int ps = ph * kBW;
+    const int i = r * kBW + c;
+    T acc = P[i] * X[i];
+#pragma unroll
+    for (int p = 1; p < kNH; ++p) {
+        const int d = half_dy(p) * kBW + half_dx(p);
+        acc += P[p * ps + i] * X[i + d];
+        acc += P[p * ps + i - d] * X[i - d];
+    }
+    return acc;
 }
 
 // --------------------------------------------------------------------------
@@ -103,46 +129,63 @@ __device__ __forceinline__ void finish_beta_reorth(InstState* st, double rz_new,
 }
 
 // r = b - A x0 (or r = b), |b|, |r|, and for Jacobi / no preconditioner also
-// z and r.z. Finaliser sets norm_b, tol, status (cg.py:64-80).
-template <typename T, int PREC>
+// z and r.z. Finaliser sets norm_b, tol, status (cg.py:64-80). x0 arrives in
+// the p-parity-0 buffer (map slot kMapP0F).
+template <typename T, int PREC, bool X0>
 __global__ void __launch_bounds__(kThreads)
-k_cg_init(WorkList wl, const T* __restrict__ P, const T* __restrict__ b, T* x,
-          const T* __restrict__ x0, T* r, T* z, InstState* st, double* partials,
-          double atol, double rtol, int maxiter) {
-    __shared__ T s_x[(kTY + 4) * (kTX + 4)];
+k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T* __restrict__ b,
+          T* x, T* r, T* z, InstState* st, double* partials, double atol, double rtol,
+          int maxiter, int* err) {
     __shared__ double s_red[3 * 32];
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    T* sP = X0 ? sc.take<T>(kNH * kBH * kBW) : nullptr;
+    T* sX = X0 ? sc.take<T>(kBH * kBW) : nullptr;
+    Tma tma;
+    tma.init(&s_bar, err);
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
         const TileCoord c = tile_coord<kTY, kTX>(wl, t);
         const GridDesc g = wl.grids[c.g];
         InstState* s = st + g.inst;
-        if (x0) {
+        if (X0) {
             __syncthreads();
-            stage_halo<T, kTY, kTX>(s_x, x0, g, c.y0, c.x0);
-            __syncthreads();
-        }
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, xx = c.x0 + lx;
-        double v[3] = {0.0, 0.0, 0.0};
-        if (y < g.h && xx < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
-            const T bi = b[i];
-            T ri = bi;
-            if (x0) {
-                ri = bi - apply_at<T>(P, g, y, xx, s_x, ly + 2, lx + 2, kTX + 4);
-                x[i] = s_x[(ly + 2) * (kTX + 4) + lx + 2];
-            } else {
-                x[i] = T(0);
+            if (threadIdx.x == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(T));
+                tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
+                tma_load_2d(sX, map_of(maps, g, kMapP0F), c.x0 - kBOX, c.y0 - 2, tma.bar);
             }
-            r[i] = ri;
-            v[0] = (double)bi * (double)bi;
-            v[1] = (double)ri * (double)ri;
-            if (PREC == kPrecJacobi) {
-                const T inv = T(1) / diag_at<T>(P, g, y, xx);
-                const T zi = ri * inv;
-                z[i] = zi;
-                v[2] = (double)ri * (double)zi;
-            } else if (PREC == kPrecNone) {
-                v[2] = v[1];
+            if (!tma.wait()) return;
+        }
+        double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
+            const int y = c.y0 + ly, xx = c.x0 + lx;
+            if (y < g.h && xx < g.w) {
+                const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+                const T bi = b[i];
+                T ri = bi;
+                T d;
+                if (X0) {
+                    const int q = (ly + 2) * kBW + lx + kBOX;
+                    ri = bi - stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
+                    x[i] = sX[q];
+                    d = sP[q];
+                } else {
+                    x[i] = T(0);
+                    d = P[g.poff + (int64_t)y * g.pitch + xx];
+                }
+                r[i] = ri;
+                v[0] += (double)bi * (double)bi;
+                v[1] += (double)ri * (double)ri;
+                if (PREC == kPrecJacobi) {
+                    const T zi = ri * (T(1) / d);
+                    z[i] = zi;
+                    v[2] += (double)ri * (double)zi;
+                } else if (PREC == kPrecNone) {
+                    v[2] += (double)ri * (double)ri;
+                }
             }
         }
         const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
@@ -166,14 +209,20 @@ k_cg_init(WorkList wl, const T* __restrict__ P, const T* __restrict__ b, T* x,
 // p_new = z + beta p_old (p_new = z on the first pass), Ap = A p_new and
 // p_new . Ap; finaliser: alpha = rz / (p . Ap)   (cg.py:85-90, 111-113).
 // p is double-buffered by iteration parity: neighbouring tiles still read
-// p_old while this tile writes p_new.
+// p_old while this tile writes p_new. zslot selects z (r without a
+// preconditioner).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_cg_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ z, T* p0, T* p1,
-           T* Ap, InstState* st, double* partials) {
-    __shared__ T s_p[(kTY + 4) * (kTX + 4)];
+k_cg_apply(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap, InstState* st,
+           double* partials, int* err) {
     __shared__ double s_red[32];
-    constexpr int SW = kTX + 4, SH = kTY + 4;
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    T* sP = sc.take<T>(kNH * kBH * kBW);
+    T* sZ = sc.take<T>(kBH * kBW);
+    T* sQ = sc.take<T>(kBH * kBW);
+    Tma tma;
+    tma.init(&s_bar, err);
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
         const TileCoord c = tile_coord<kTY, kTX>(wl, t);
         const GridDesc g = wl.grids[c.g];
@@ -182,30 +231,35 @@ k_cg_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ z, T* p0,
         const bool first = (s->flags & kFirst) != 0;
         const T beta = (T)s->beta;
         const int par = s->iters & 1;
-        const T* pold = par ? p1 : p0;
         T* pnew = par ? p0 : p1;
         __syncthreads();
-        for (int q = threadIdx.x; q < SW * SH; q += blockDim.x) {
-            const int ly = q / SW, lx = q - ly * SW;
-            const int y = c.y0 - 2 + ly, x = c.x0 - 2 + lx;
-            T val = T(0);
-            if (y >= 0 && y < g.h && x >= 0 && x < g.w) {
-                const int64_t i = g.voff + (int64_t)y * g.pitch + x;
-                val = first ? z[i] : (T)(z[i] + beta * pold[i]);
-            }
-            s_p[q] = val;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(tma.bar, (kNH + (first ? 1 : 2)) * kBH * kBW * sizeof(T));
+            tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
+            tma_load_2d(sZ, map_of(maps, g, zslot), c.x0 - kBOX, c.y0 - 2, tma.bar);
+            if (!first)
+                tma_load_2d(sQ, map_of(maps, g, par ? kMapP1F : kMapP0F), c.x0 - kBOX, c.y0 - 2,
+                            tma.bar);
         }
-        __syncthreads();
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, x = c.x0 + lx;
+        if (!tma.wait()) return;
+        if (!first) {
+            for (int q = threadIdx.x; q < kBH * kBW; q += blockDim.x) sZ[q] = sZ[q] + beta * sQ[q];
+            __syncthreads();
+        }
         double v[1] = {0.0};
-        if (y < g.h && x < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + x;
-            const T pi = s_p[(ly + 2) * SW + lx + 2];
-            const T api = apply_at<T>(P, g, y, x, s_p, ly + 2, lx + 2, SW);
-            pnew[i] = pi;
-            Ap[i] = api;
-            v[0] = (double)pi * (double)api;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
+            const int y = c.y0 + ly, x = c.x0 + lx;
+            if (y < g.h && x < g.w) {
+                const int64_t i = g.voff + (int64_t)y * g.pitch + x;
+                const T pi = sZ[(ly + 2) * kBW + lx + kBOX];
+                const T api = stencil_at<T>(sP, kBH, sZ, ly + 2, lx + kBOX);
+                pnew[i] = pi;
+                Ap[i] = api;
+                v[0] += (double)pi * (double)api;
+            }
         }
         const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
         tile_reduce<1>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
@@ -216,47 +270,64 @@ k_cg_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ z, T* p0,
     }
 }
 
+// Element-wise chunk of a flat work list: the element range of tile t.
+struct FlatCoord { int g; int64_t e0, e1; };
+
+__device__ __forceinline__ FlatCoord flat_coord(const WorkList& wl, int t) {
+    FlatCoord f;
+    f.g = find_grid(wl, t);
+    const GridDesc& g = wl.grids[f.g];
+    const int64_t n = (int64_t)g.h * g.pitch;
+    f.e0 = (int64_t)(t - wl.tile_start[f.g]) * kFlat;
+    f.e1 = min(f.e0 + kFlat, n);
+    return f;
+}
+
 // x += alpha p; r -= alpha Ap; |r|; convergence test (cg.py:89-99). For the
 // Jacobi / identity preconditioners also z = M r and beta (cg.py:101-113).
 // With reorthogonalisation the change r - r_old is kept in `dr` (or reduced
-// directly against z for Jacobi).
+// directly against z for Jacobi). Padding columns of the pitched rows are
+// excluded from the sums.
 template <typename T, int PREC>
 __global__ void __launch_bounds__(kThreads)
 k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0, const T* p1,
             const T* __restrict__ Ap, T* dr, int reorth, InstState* st, double* partials) {
     __shared__ double s_red[3 * 32];
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
+        const FlatCoord f = flat_coord(wl, t);
+        const GridDesc g = wl.grids[f.g];
         InstState* s = st + g.inst;
         if (s->status != kRunning) continue;
-        const double alpha = s->alpha;
+        const T a = (T)s->alpha;
         const T* p = (s->iters & 1) ? p0 : p1;   // the buffer k_cg_apply wrote
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, xx = c.x0 + lx;
         double v[3] = {0.0, 0.0, 0.0};
-        if (y < g.h && xx < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
-            const T a = (T)alpha;
+#pragma unroll
+        for (int k = 0; k < kFlat / kThreads; ++k) {
+            const int64_t e = f.e0 + threadIdx.x + k * kThreads;
+            if (e >= f.e1) break;
+            const int col = (int)(e % g.pitch);
+            if (col >= g.w) continue;
+            const int64_t i = g.voff + e;
             const T rold = r[i];
             x[i] = x[i] + a * p[i];
             const T ri = rold - a * Ap[i];
             r[i] = ri;
-            v[0] = (double)ri * (double)ri;
+            v[0] += (double)ri * (double)ri;
             if (PREC == kPrecJacobi) {
-                const T inv = T(1) / diag_at<T>(P, g, y, xx);
-                const T zi = ri * inv;
+                const int row = (int)(e / g.pitch);
+                const T d = P[g.poff + (int64_t)row * g.pitch + col];
+                const T zi = ri * (T(1) / d);
                 z[i] = zi;
-                v[1] = (double)ri * (double)zi;
-                if (reorth) v[2] = (double)(ri - rold) * (double)zi;
+                v[1] += (double)ri * (double)zi;
+                if (reorth) v[2] += (double)(ri - rold) * (double)zi;
             } else if (PREC == kPrecNone) {
-                v[1] = v[0];
-                if (reorth) v[2] = (double)(ri - rold) * (double)ri;
+                v[1] += (double)ri * (double)ri;
+                if (reorth) v[2] += (double)(ri - rold) * (double)ri;
             } else if (reorth) {
                 dr[i] = ri - rold;
             }
         }
-        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        const int t0 = wl.tile_start[f.g], t1 = wl.tile_start[f.g + 1];
         tile_reduce<3>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
             const double nr = sqrt(sum[0]);
             s->norm_r = nr;
@@ -280,19 +351,21 @@ k_cg_rz(WorkList wl, const T* __restrict__ r, const T* __restrict__ z, const T* 
         int reorth, InstState* st, double* partials) {
     __shared__ double s_red[2 * 32];
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
+        const FlatCoord f = flat_coord(wl, t);
+        const GridDesc g = wl.grids[f.g];
         InstState* s = st + g.inst;
         if (s->status != kRunning) continue;
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, xx = c.x0 + lx;
         double v[2] = {0.0, 0.0};
-        if (y < g.h && xx < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
-            v[0] = (double)r[i] * (double)z[i];
-            if (reorth) v[1] = (double)dr[i] * (double)z[i];
+#pragma unroll
+        for (int k = 0; k < kFlat / kThreads; ++k) {
+            const int64_t e = f.e0 + threadIdx.x + k * kThreads;
+            if (e >= f.e1) break;
+            if ((int)(e % g.pitch) >= g.w) continue;
+            const int64_t i = g.voff + e;
+            v[0] += (double)r[i] * (double)z[i];
+            if (reorth) v[1] += (double)dr[i] * (double)z[i];
         }
-        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
+        const int t0 = wl.tile_start[f.g], t1 = wl.tile_start[f.g + 1];
         tile_reduce<2>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
             if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
             else finish_beta(s, sum[0]);
@@ -306,56 +379,70 @@ k_cg_rz(WorkList wl, const T* __restrict__ r, const T* __restrict__ z, const T* 
 
 __device__ __forceinline__ double pw(int a) { return a == 0 ? 2.0 : 1.0; }
 
-// Restriction of the pre-smoothed residual. One CTA per coarse tile:
+// Restriction of the pre-smoothed residual. One CTA per tile of kCX x CY
+// coarse pixels:
 //   x1 = omega b / d         (first Jacobi sweep from zero, vcycle.py:33-36)
 //        or x1 = 0 (no pre-smoothing) or x1 = xs (explicit sweeps);
 //   res = b - A x1 on the fine pixels under the tile (vcycle.py:77);
 //   b_coarse = R res with full-weighting [1 2 1]^2 / 16 (vcycle.py:12-26, 80).
-// Status of the image is checked through `st` when st != null.
+// The fine box starts at (2 X0 - 4, 2 Y0 - 3): rows 2 Y0 - 3 .. 2 Y0 + 2 CY + 1
+// cover x1 around the residual rows 2 Y0 - 1 .. 2 Y0 + 2 CY - 1.
 template <typename T, int PRE>
 __global__ void __launch_bounds__(kThreads)
-k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const T* __restrict__ P,
-          const T* __restrict__ b, const T* __restrict__ xs, T* bc, double omega,
-          const InstState* st) {
-    constexpr int RW = 2 * kCX + 1, RH = 2 * kCY + 1;   // residual region
-    constexpr int XW = RW + 4, XH = RH + 4;             // x1 region
-    __shared__ T s_x[XH * XW];
-    __shared__ T s_r[RH * RW];
+k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMap* maps,
+          int xs_slot, T* bc, double omega, const InstState* st, int* err) {
+    constexpr int CY = Coarse<T>::CY;
+    constexpr int DH = 2 * CY + 5;                      // box rows
+    constexpr int RH = 2 * CY + 1, RW = 2 * kCX + 1;    // residual region
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    T* sP = PRE != 0 ? sc.take<T>(kNH * DH * kBW) : nullptr;
+    T* sB = sc.take<T>(DH * kBW);
+    T* sX = PRE != 0 ? sc.take<T>(DH * kBW) : nullptr;
+    T* sR = sc.take<T>(RH * RW);
+    Tma tma;
+    tma.init(&s_bar, err);
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kCY, kCX>(wl, t);
+        const TileCoord c = tile_coord<CY, kCX>(wl, t);
         const GridDesc gc = wl.grids[c.g];
         const GridDesc gf = fine[c.g];
         if (st && st[gc.inst].status != kRunning) continue;
-        const int fy0 = 2 * c.y0 - 1, fx0 = 2 * c.x0 - 1;   // residual region origin
+        const int bx = 2 * c.x0 - 4, by = 2 * c.y0 - 3;   // box origin (fine)
         __syncthreads();
-        if (PRE != 0) {
-            for (int q = threadIdx.x; q < XW * XH; q += blockDim.x) {
-                const int ly = q / XW, lx = q - ly * XW;
-                const int y = fy0 - 2 + ly, x = fx0 - 2 + lx;
-                T val = T(0);
-                if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
-                    const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
-                    if (PRE == 1) val = (T)omega * b[i] / diag_at<T>(P, gf, y, x);
-                    else val = xs[i];
-                }
-                s_x[q] = val;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            const uint32_t nbox = 1 + (PRE != 0 ? kNH : 0) + (PRE > 1 ? 1 : 0);
+            mbar_expect_tx(tma.bar, nbox * DH * kBW * sizeof(T));
+            tma_load_2d(sB, map_of(maps, gf, kMapBD), bx, by, tma.bar);
+            if (PRE != 0) tma_load_3d(sP, map_of(maps, gf, kMapPlD), bx, by, 0, tma.bar);
+            if (PRE > 1) tma_load_2d(sX, map_of(maps, gf, xs_slot), bx, by, tma.bar);
+        }
+        if (!tma.wait()) return;
+        if (PRE == 1) {
+            // x1 = omega b / d inside the image, 0 outside.
+            for (int q = threadIdx.x; q < DH * kBW; q += blockDim.x) {
+                const int rr = q / kBW, cc = q - rr * kBW;
+                const int fy = by + rr, fx = bx + cc;
+                T v = T(0);
+                if (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) v = (T)omega * sB[q] / sP[q];
+                sX[q] = v;
             }
             __syncthreads();
         }
-        for (int q = threadIdx.x; q < RW * RH; q += blockDim.x) {
-            const int ly = q / RW, lx = q - ly * RW;
-            const int y = fy0 + ly, x = fx0 + lx;
-            T val = T(0);
-            if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
-                const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
-                val = b[i];
-                if (PRE != 0) val = val - apply_at<T>(P, gf, y, x, s_x, ly + 2, lx + 2, XW);
+        for (int q = threadIdx.x; q < RH * RW; q += blockDim.x) {
+            const int rr = q / RW, cc = q - rr * RW;
+            const int br = rr + 2, bcol = cc + 3;           // box coordinates
+            const int fy = by + br, fx = bx + bcol;
+            T v = T(0);
+            if (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) {
+                v = sB[br * kBW + bcol];
+                if (PRE != 0) v = v - stencil_at<T>(sP, DH, sX, br, bcol);
             }
-            s_r[q] = val;
+            sR[q] = v;
         }
         __syncthreads();
-        const int lx = threadIdx.x % kCX, ly = threadIdx.x / kCX;
-        if (ly < kCY) {
+        for (int q = threadIdx.x; q < kCX * CY; q += blockDim.x) {
+            const int ly = q / kCX, lx = q - ly * kCX;
             const int Y = c.y0 + ly, X = c.x0 + lx;
             if (Y < gc.h && X < gc.w) {
                 T sum = T(0);
@@ -364,7 +451,7 @@ k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const T* __restr
 #pragma unroll
                     for (int ax = -1; ax <= 1; ++ax)
                         sum += (T)(pw(ax) * pw(ay) / 16.0) *
-                               s_r[(2 * ly + 1 + ay) * RW + (2 * lx + 1 + ax)];
+                               sR[(2 * ly + 1 + ay) * RW + (2 * lx + 1 + ax)];
                 bc[gc.voff + (int64_t)Y * gc.pitch + X] = sum;
             }
         }
@@ -375,44 +462,50 @@ k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const T* __restr
 //   x2 = x1 + P xc           (vcycle.py:95; P = R^T)
 //   x3 = x2 + omega (b - A x2) / d    (vcycle.py:98, one sweep; POST = 0
 //                                       stores x2 unchanged)
-// At level 0 (rz != 0) the block also accumulates r . z with r = b, and
+// At level 0 (level0 != 0) the block also accumulates r . z with r = b, and
 // (r - r_old) . z when reorthogonalising, finishing beta.
 template <typename T, int PRE, int POST>
 __global__ void __launch_bounds__(kThreads)
-k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const T* __restrict__ P,
-        const T* __restrict__ b, const T* __restrict__ xs, const T* __restrict__ xc, T* xout,
-        double omega, InstState* st, int level0, const T* __restrict__ dr, int reorth,
-        double* partials) {
-    constexpr int SW = kTX + 4, SH = kTY + 4;
-    constexpr int CW = (kTX + 5) / 2 + 3, CH = (kTY + 5) / 2 + 3;
-    __shared__ T s_x[SH * SW];
-    __shared__ T s_c[CH * CW];
+k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap* maps,
+        int xs_slot, const T* __restrict__ b, T* xout, double omega, InstState* st, int level0,
+        const T* __restrict__ dr, int reorth, double* partials, int* err) {
     __shared__ double s_red[2 * 32];
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    T* sP = sc.take<T>(kNH * kBH * kBW);
+    T* sX = sc.take<T>(kBH * kBW);          // b, then x2 in place
+    T* sS = PRE > 1 ? sc.take<T>(kBH * kBW) : nullptr;
+    T* sC = sc.take<T>(kCBH * kCBW);
+    Tma tma;
+    tma.init(&s_bar, err);
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
         const TileCoord c = tile_coord<kTY, kTX>(wl, t);
         const GridDesc gf = wl.grids[c.g];
         const GridDesc gc = coarse[c.g];
         InstState* s = st ? st + gf.inst : nullptr;
         if (s && s->status != kRunning) continue;
-        const int cy0 = (c.y0 - 3) >> 1, cx0 = (c.x0 - 3) >> 1;
+        const int bx = c.x0 - kBOX, by = c.y0 - 2;
+        const int cx0 = (c.x0 >> 1) - 4, cy0 = (c.y0 >> 1) - 2;
         __syncthreads();
-        for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
-            const int ly = q / CW, lx = q - ly * CW;
-            const int Y = cy0 + ly, X = cx0 + lx;
-            T val = T(0);
-            if (Y >= 0 && Y < gc.h && X >= 0 && X < gc.w) val = xc[gc.voff + (int64_t)Y * gc.pitch + X];
-            s_c[q] = val;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(tma.bar, ((kNH + 1 + (PRE > 1 ? 1 : 0)) * kBH * kBW + kCBH * kCBW) *
+                                        sizeof(T));
+            tma_load_3d(sP, map_of(maps, gf, kMapPlF), bx, by, 0, tma.bar);
+            tma_load_2d(sX, map_of(maps, gf, kMapBF), bx, by, tma.bar);
+            if (PRE > 1) tma_load_2d(sS, map_of(maps, gf, xs_slot), bx, by, tma.bar);
+            tma_load_2d(sC, map_of(maps, gc, kMapXC), cx0, cy0, tma.bar);
         }
-        __syncthreads();
-        for (int q = threadIdx.x; q < SW * SH; q += blockDim.x) {
-            const int ly = q / SW, lx = q - ly * SW;
-            const int y = c.y0 - 2 + ly, x = c.x0 - 2 + lx;
+        if (!tma.wait()) return;
+        // Each element is read and rewritten by the same thread: no hazard.
+        for (int q = threadIdx.x; q < kBH * kBW; q += blockDim.x) {
+            const int rr = q / kBW, cc = q - rr * kBW;
+            const int y = by + rr, x = bx + cc;
             T val = T(0);
             if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
-                const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
                 T x1 = T(0);
-                if (PRE == 1) x1 = (T)omega * b[i] / diag_at<T>(P, gf, y, x);
-                else if (PRE > 1) x1 = xs[i];
+                if (PRE == 1) x1 = (T)omega * sX[q] / sP[q];
+                else if (PRE > 1) x1 = sS[q];
                 // Coarse pixels whose 3x3 support contains (y, x), in raster
                 // order of the coarse grid: |y - 2Y| <= 1 and |x - 2X| <= 1.
                 T sum = T(0);
@@ -422,29 +515,33 @@ k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const T* __restric
                     const int ay = y - 2 * Y;
                     for (int X = x >> 1; X <= Xhi; ++X) {
                         const int ax = x - 2 * X;
-                        sum += (T)(pw(ax) * pw(ay) / 16.0) * s_c[(Y - cy0) * CW + (X - cx0)];
+                        sum += (T)(pw(ax) * pw(ay) / 16.0) * sC[(Y - cy0) * kCBW + (X - cx0)];
                     }
                 }
                 val = x1 + sum;
             }
-            s_x[q] = val;
+            sX[q] = val;
         }
         __syncthreads();
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, x = c.x0 + lx;
         double v[2] = {0.0, 0.0};
-        if (y < gf.h && x < gf.w) {
-            const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
-            T x3 = s_x[(ly + 2) * SW + lx + 2];
-            if (POST > 0) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
+            const int y = c.y0 + ly, x = c.x0 + lx;
+            if (y < gf.h && x < gf.w) {
+                const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
+                const int q = (ly + 2) * kBW + lx + kBOX;
+                T x3 = sX[q];
                 const T bi = b[i];
-                const T ax = apply_at<T>(P, gf, y, x, s_x, ly + 2, lx + 2, SW);
-                x3 = x3 + (T)omega * (bi - ax) / diag_at<T>(P, gf, y, x);
-            }
-            xout[i] = x3;
-            if (level0) {
-                v[0] = (double)b[i] * (double)x3;
-                if (reorth) v[1] = (double)dr[i] * (double)x3;
+                if (POST > 0) {
+                    const T ax = stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
+                    x3 = x3 + (T)omega * (bi - ax) / sP[q];
+                }
+                xout[i] = x3;
+                if (level0) {
+                    v[0] += (double)bi * (double)x3;
+                    if (reorth) v[1] += (double)dr[i] * (double)x3;
+                }
             }
         }
         if (level0 && s) {
@@ -458,34 +555,47 @@ k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const T* __restric
 }
 
 // One weighted Jacobi sweep xout = xin + omega (b - A xin) / d, or the first
-// sweep from zero xout = omega b / d when xin == null (vcycle.py:32-43).
+// sweep from zero xout = omega b / d when xin_slot < 0 (vcycle.py:32-43).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_vc_smooth(WorkList wl, const T* __restrict__ P, const T* __restrict__ b,
-            const T* __restrict__ xin, T* xout, double omega, const InstState* st) {
-    __shared__ T s_x[(kTY + 4) * (kTX + 4)];
+k_vc_smooth(WorkList wl, const CUtensorMap* maps, int xin_slot, const T* __restrict__ P,
+            const T* __restrict__ b, T* xout, double omega, const InstState* st, int* err) {
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    T* sP = sc.take<T>(kNH * kBH * kBW);
+    T* sX = sc.take<T>(kBH * kBW);
+    Tma tma;
+    tma.init(&s_bar, err);
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
         const TileCoord c = tile_coord<kTY, kTX>(wl, t);
         const GridDesc g = wl.grids[c.g];
         if (st && st[g.inst].status != kRunning) continue;
-        if (xin) {
+        if (xin_slot >= 0) {
             __syncthreads();
-            stage_halo<T, kTY, kTX>(s_x, xin, g, c.y0, c.x0);
-            __syncthreads();
-        }
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, x = c.x0 + lx;
-        if (y < g.h && x < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + x;
-            const T d = diag_at<T>(P, g, y, x);
-            T out;
-            if (xin) {
-                const T ax = apply_at<T>(P, g, y, x, s_x, ly + 2, lx + 2, kTX + 4);
-                out = s_x[(ly + 2) * (kTX + 4) + lx + 2] + (T)omega * (b[i] - ax) / d;
-            } else {
-                out = (T)omega * b[i] / d;
+            if (threadIdx.x == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(T));
+                tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
+                tma_load_2d(sX, map_of(maps, g, xin_slot), c.x0 - kBOX, c.y0 - 2, tma.bar);
             }
-            xout[i] = out;
+            if (!tma.wait()) return;
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
+            const int y = c.y0 + ly, x = c.x0 + lx;
+            if (y < g.h && x < g.w) {
+                const int64_t i = g.voff + (int64_t)y * g.pitch + x;
+                T out;
+                if (xin_slot >= 0) {
+                    const int q = (ly + 2) * kBW + lx + kBOX;
+                    const T ax = stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
+                    out = sX[q] + (T)omega * (b[i] - ax) / sP[q];
+                } else {
+                    out = (T)omega * b[i] / P[g.poff + (int64_t)y * g.pitch + x];
+                }
+                xout[i] = out;
+            }
         }
     }
 }
@@ -523,6 +633,38 @@ __global__ void k_vc_direct(const DirectDesc* dd, int count, const T* __restrict
     }
 }
 
+// y = A x on pitched vectors (no reductions): used by A.dot(x). x is the
+// level-0 b buffer (map slot kMapBF).
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_apply(WorkList wl, const CUtensorMap* maps, T* y, int* err) {
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    T* sP = sc.take<T>(kNH * kBH * kBW);
+    T* sX = sc.take<T>(kBH * kBW);
+    Tma tma;
+    tma.init(&s_bar, err);
+    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
+        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
+        const GridDesc g = wl.grids[c.g];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(T));
+            tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
+            tma_load_2d(sX, map_of(maps, g, kMapBF), c.x0 - kBOX, c.y0 - 2, tma.bar);
+        }
+        if (!tma.wait()) return;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
+            const int yy = c.y0 + ly, xx = c.x0 + lx;
+            if (yy < g.h && xx < g.w)
+                y[g.voff + (int64_t)yy * g.pitch + xx] = stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
+        }
+    }
+}
+
 // --------------------------------------------------------------------------
 // Setup: Galerkin coarse operator, dense coarsest inverse, precision copies
 // --------------------------------------------------------------------------
@@ -545,8 +687,6 @@ __global__ void k_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int
                            const double* __restrict__ Pf, double* Pc, int64_t total) {
     int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= total) return;
-    // Locate the grid: coarse pixel counts are prefix-summed on the fly
-    // (ngrids is small).
     int g = 0;
     int64_t base = 0;
     for (; g < ngrids; ++g) {
@@ -589,12 +729,12 @@ __global__ void k_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int
 // partial pivoting. One CTA per image; n <= kMaxDirect.
 __global__ void k_dense_inverse(const DirectDesc* dd, int count, const double* __restrict__ Pc,
                                 double* work, int* status) {
-    if (blockIdx.x >= count) return;
+    if ((int)blockIdx.x >= count) return;
     const DirectDesc d = dd[blockIdx.x];
     const GridDesc g = d.g;
     const int n = g.h * g.w;
-    double* A = work + d.work_off;           // n x n
-    double* Inv = d.inv;                      // n x n
+    double* A = work + d.work_off;
+    double* Inv = d.inv;
     for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
         const int i = q / n, j = q - i * n;
         const int yi = i / g.w, xi = i - yi * g.w, yj = j / g.w, xj = j - yj * g.w;
@@ -636,9 +776,8 @@ __global__ void k_dense_inverse(const DirectDesc* dd, int count, const double* _
         __syncthreads();
         for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
             const int i = q / n, j = q - i * n;
-            if (i == k) continue;
+            if (i == k || j == k) continue;
             const double f = A[(int64_t)i * n + k];
-            if (j == k) continue;
             A[q] -= f * A[(int64_t)k * n + j];
             Inv[q] -= f * Inv[(int64_t)k * n + j];
         }
@@ -690,24 +829,6 @@ __global__ void k_unpack(const GridDesc* grids, int ngrids, const int64_t* user_
     }
 }
 
-// y = A x on pitched vectors (no reductions): used by A.dot(x).
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ x, T* y) {
-    __shared__ T s_x[(kTY + 4) * (kTX + 4)];
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
-        __syncthreads();
-        stage_halo<T, kTY, kTX>(s_x, x, g, c.y0, c.x0);
-        __syncthreads();
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int yy = c.y0 + ly, xx = c.x0 + lx;
-        if (yy < g.h && xx < g.w)
-            y[g.voff + (int64_t)yy * g.pitch + xx] = apply_at<T>(P, g, yy, xx, s_x, ly + 2, lx + 2, kTX + 4);
-    }
-}
-
 // --------------------------------------------------------------------------
 // Iterative refinement around the FP32 inner solve
 // --------------------------------------------------------------------------
@@ -716,12 +837,17 @@ k_apply(WorkList wl, const T* __restrict__ P, const T* __restrict__ x, T* y) {
 // (re)starts the inner FP32 solve on r32 = (float) r64 with x32 = 0.
 template <int PREC>
 __global__ void __launch_bounds__(kThreads)
-k_refine_residual(WorkList wl, const double* __restrict__ P64, const float* __restrict__ P32,
-                  const double* __restrict__ b, const double* __restrict__ x64, float* r32,
-                  float* x32, float* z32, InstState* outer, InstState* inner, double* partials,
-                  double atol, double rtol, double inner_rtol, int maxiter, int max_outer) {
-    __shared__ double s_x[(kTY + 4) * (kTX + 4)];
+k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict__ P32,
+                  const double* __restrict__ b, float* r32, float* x32, float* z32,
+                  InstState* outer, InstState* inner, double* partials, double atol, double rtol,
+                  double inner_rtol, int maxiter, int max_outer, int* err) {
     __shared__ double s_red[3 * 32];
+    __shared__ __align__(8) uint64_t s_bar;
+    SmemCarve sc(g_smem);
+    double* sP = sc.take<double>(kNH * kBH * kBW);
+    double* sX = sc.take<double>(kBH * kBW);
+    Tma tma;
+    tma.init(&s_bar, err);
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
         const TileCoord c = tile_coord<kTY, kTX>(wl, t);
         const GridDesc g = wl.grids[c.g];
@@ -729,26 +855,34 @@ k_refine_residual(WorkList wl, const double* __restrict__ P64, const float* __re
         InstState* si = inner + g.inst;
         if (so->status != kRunning) continue;
         __syncthreads();
-        stage_halo<double, kTY, kTX>(s_x, x64, g, c.y0, c.x0);
-        __syncthreads();
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, xx = c.x0 + lx;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(double));
+            tma_load_3d(sP, map_of(maps, g, kMapP64F), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
+            tma_load_2d(sX, map_of(maps, g, kMapX64F), c.x0 - kBOX, c.y0 - 2, tma.bar);
+        }
+        if (!tma.wait()) return;
         double v[3] = {0.0, 0.0, 0.0};
-        if (y < g.h && xx < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
-            const double bi = b[i];
-            const double ri = bi - apply_at<double>(P64, g, y, xx, s_x, ly + 2, lx + 2, kTX + 4);
-            const float rf = (float)ri;
-            r32[i] = rf;
-            x32[i] = 0.0f;
-            v[0] = bi * bi;
-            v[1] = ri * ri;
-            if (PREC == kPrecJacobi) {
-                const float zi = rf * (1.0f / diag_at<float>(P32, g, y, xx));
-                z32[i] = zi;
-                v[2] = (double)rf * (double)zi;
-            } else if (PREC == kPrecNone) {
-                v[2] = (double)rf * (double)rf;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
+            const int y = c.y0 + ly, xx = c.x0 + lx;
+            if (y < g.h && xx < g.w) {
+                const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+                const double bi = b[i];
+                const double ri = bi - stencil_at<double>(sP, kBH, sX, ly + 2, lx + kBOX);
+                const float rf = (float)ri;
+                r32[i] = rf;
+                x32[i] = 0.0f;
+                v[0] += bi * bi;
+                v[1] += ri * ri;
+                if (PREC == kPrecJacobi) {
+                    const float zi = rf * (1.0f / P32[g.poff + (int64_t)y * g.pitch + xx]);
+                    z32[i] = zi;
+                    v[2] += (double)rf * (double)zi;
+                } else if (PREC == kPrecNone) {
+                    v[2] += (double)rf * (double)rf;
+                }
             }
         }
         const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
@@ -780,18 +914,19 @@ k_refine_residual(WorkList wl, const double* __restrict__ P64, const float* __re
     }
 }
 
-// x64 += x32 for images whose inner solve ran; counts outer iterations.
+// x64 += x32 for images whose refinement is still running.
 __global__ void __launch_bounds__(kThreads)
-k_refine_correct(WorkList wl, double* x64, const float* __restrict__ x32, InstState* outer,
-                 const InstState* inner) {
+k_refine_correct(WorkList wl, double* x64, const float* __restrict__ x32, const InstState* outer) {
     for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
+        const FlatCoord f = flat_coord(wl, t);
+        const GridDesc g = wl.grids[f.g];
         if (outer[g.inst].status != kRunning) continue;
-        const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
-        const int y = c.y0 + ly, xx = c.x0 + lx;
-        if (y < g.h && xx < g.w) {
-            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+#pragma unroll
+        for (int k = 0; k < kFlat / kThreads; ++k) {
+            const int64_t e = f.e0 + threadIdx.x + k * kThreads;
+            if (e >= f.e1) break;
+            if ((int)(e % g.pitch) >= g.w) continue;
+            const int64_t i = g.voff + e;
             x64[i] += (double)x32[i];
         }
     }
@@ -803,25 +938,58 @@ __global__ void k_refine_count(InstState* outer, int n) {
 }
 
 // --------------------------------------------------------------------------
-// Explicit instantiation helpers used by the engine
+// Launchers
 // --------------------------------------------------------------------------
 
-template <typename T>
-void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, const T* b,
-                    T* x, const T* x0, T* r, T* z, InstState* st, double* part, double atol,
-                    double rtol, int maxiter, cudaStream_t s) {
-    switch (prec) {
-    case kPrecNone: k_cg_init<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
-    case kPrecJacobi: k_cg_init<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
-    case kPrecVcycle: k_cg_init<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
-    default: k_cg_init<T, kPrecExternal><<<L.grid, kThreads, 0, s>>>(wl, P, b, x, x0, r, z, st, part, atol, rtol, maxiter); break;
-    }
+template <typename T> size_t smem_apply() { return 128 * 4 + (kNH + 2) * kBH * kBW * sizeof(T); }
+template <typename T> size_t smem_init() { return 128 * 4 + (kNH + 1) * kBH * kBW * sizeof(T); }
+template <typename T> size_t smem_down(int pre) {
+    constexpr int CY = Coarse<T>::CY;
+    constexpr int DH = 2 * CY + 5;
+    size_t s = 128 * 6 + (size_t)DH * kBW * sizeof(T) + (size_t)(2 * CY + 1) * (2 * kCX + 1) * sizeof(T);
+    if (pre != 0) s += (size_t)(kNH + 1) * DH * kBW * sizeof(T);
+    return s;
+}
+template <typename T> size_t smem_up(int pre) {
+    return 128 * 6 + (size_t)(kNH + 1 + (pre > 1 ? 1 : 0)) * kBH * kBW * sizeof(T) +
+           (size_t)kCBH * kCBW * sizeof(T);
+}
+
+// Raise the dynamic shared-memory limit of a kernel. Done once for every
+// instantiation by stencil_prepare(), before any stream capture.
+template <typename K>
+static void allow_smem(K kernel, size_t bytes) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 template <typename T>
-void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const T* P, const T* z, T* p0, T* p1,
-                     T* Ap, InstState* st, double* part, cudaStream_t s) {
-    k_cg_apply<T><<<L.grid, kThreads, 0, s>>>(wl, P, z, p0, p1, Ap, st, part);
+void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
+                    const T* P, const T* b, T* x, bool have_x0, T* r, T* z, InstState* st,
+                    double* part, double atol, double rtol, int maxiter, int* err, cudaStream_t s) {
+#define PMB_INIT(PK, X0)                                                                        \
+    do {                                                                                        \
+        const size_t sm = X0 ? smem_init<T>() : 128;                                            \
+                                                                                    \
+        k_cg_init<T, PK, X0><<<L.grid, kThreads, sm, s>>>(wl, maps, P, b, x, r, z, st, part,   \
+                                                          atol, rtol, maxiter, err);            \
+    } while (0)
+    if (have_x0) {
+        if (prec == kPrecNone) PMB_INIT(kPrecNone, true);
+        else if (prec == kPrecJacobi) PMB_INIT(kPrecJacobi, true);
+        else PMB_INIT(kPrecVcycle, true);
+    } else {
+        if (prec == kPrecNone) PMB_INIT(kPrecNone, false);
+        else if (prec == kPrecJacobi) PMB_INIT(kPrecJacobi, false);
+        else PMB_INIT(kPrecVcycle, false);
+    }
+#undef PMB_INIT
+}
+
+template <typename T>
+void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, int zslot,
+                     T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s) {
+    const size_t sm = smem_apply<T>();
+    k_cg_apply<T><<<L.grid, kThreads, sm, s>>>(wl, maps, zslot, p0, p1, Ap, st, part, err);
 }
 
 template <typename T>
@@ -843,21 +1011,35 @@ void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z
 
 template <typename T>
 void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridDesc* fine,
-                    const T* P, const T* b, const T* xs, T* bc, double omega,
-                    const InstState* st, cudaStream_t s) {
-    if (pre == 0) k_vc_down<T, 0><<<L.grid, kThreads, 0, s>>>(wl, fine, P, b, xs, bc, omega, st);
-    else if (pre == 1) k_vc_down<T, 1><<<L.grid, kThreads, 0, s>>>(wl, fine, P, b, xs, bc, omega, st);
-    else k_vc_down<T, 2><<<L.grid, kThreads, 0, s>>>(wl, fine, P, b, xs, bc, omega, st);
+                    const CUtensorMap* maps, int xs_slot, T* bc, double omega,
+                    const InstState* st, int* err, cudaStream_t s) {
+    const int pk = pre > 1 ? 2 : pre;
+    const size_t sm = smem_down<T>(pk);
+#define PMB_DOWN(PK)                                                                         \
+    do {                                                                                     \
+                                                                                    \
+        k_vc_down<T, PK><<<L.grid, kThreads, sm, s>>>(wl, fine, maps, xs_slot, bc, omega, st, err); \
+    } while (0)
+    if (pk == 0) PMB_DOWN(0);
+    else if (pk == 1) PMB_DOWN(1);
+    else PMB_DOWN(2);
+#undef PMB_DOWN
 }
 
 template <typename T>
 void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
-                  const T* P, const T* b, const T* xs, const T* xc, T* xout, double omega,
-                  InstState* st, int level0, const T* dr, int reorth, double* part,
+                  const CUtensorMap* maps, int xs_slot, const T* b, T* xout, double omega,
+                  InstState* st, int level0, const T* dr, int reorth, double* part, int* err,
                   cudaStream_t s) {
     const int pk = pre > 1 ? 2 : pre;
     const int qk = post > 0 ? 1 : 0;
-#define PMB_UP(PK, QK) k_vc_up<T, PK, QK><<<L.grid, kThreads, 0, s>>>(wl, coarse, P, b, xs, xc, xout, omega, st, level0, dr, reorth, part)
+    const size_t sm = smem_up<T>(pk);
+#define PMB_UP(PK, QK)                                                                       \
+    do {                                                                                     \
+                                                                                    \
+        k_vc_up<T, PK, QK><<<L.grid, kThreads, sm, s>>>(wl, coarse, maps, xs_slot, b, xout,   \
+                                                        omega, st, level0, dr, reorth, part, err); \
+    } while (0)
     if (pk == 0 && qk == 0) PMB_UP(0, 0);
     else if (pk == 0) PMB_UP(0, 1);
     else if (pk == 1 && qk == 0) PMB_UP(1, 0);
@@ -868,9 +1050,11 @@ void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, con
 }
 
 template <typename T>
-void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const T* P, const T* b, const T* xin,
-                      T* xout, double omega, const InstState* st, cudaStream_t s) {
-    k_vc_smooth<T><<<L.grid, kThreads, 0, s>>>(wl, P, b, xin, xout, omega, st);
+void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
+                      int xin_slot, const T* P, const T* b, T* xout, double omega,
+                      const InstState* st, int* err, cudaStream_t s) {
+    const size_t sm = smem_init<T>();
+    k_vc_smooth<T><<<L.grid, kThreads, sm, s>>>(wl, maps, xin_slot, P, b, xout, omega, st, err);
 }
 
 template <typename T>
@@ -880,9 +1064,10 @@ void launch_vc_direct(const DirectDesc* dd, int count, const T* b, T* x, InstSta
 }
 
 template <typename T>
-void launch_apply(const LaunchCfg& L, const WorkList& wl, const T* P, const T* x, T* y,
+void launch_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, T* y, int* err,
                   cudaStream_t s) {
-    k_apply<T><<<L.grid, kThreads, 0, s>>>(wl, P, x, y);
+    const size_t sm = smem_init<T>();
+    k_apply<T><<<L.grid, kThreads, sm, s>>>(wl, maps, y, err);
 }
 
 template <typename TS, typename TD>
@@ -921,12 +1106,20 @@ void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s
     k_convert_f32<<<blocks, 256, 0, s>>>(src, dst, n);
 }
 
-void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl, const double* P64,
-                            const float* P32, const double* b, const double* x64, float* r32,
-                            float* x32, float* z32, InstState* outer, InstState* inner,
-                            double* part, double atol, double rtol, double inner_rtol,
-                            int maxiter, int max_outer, cudaStream_t s) {
-#define PMB_RR(PK) k_refine_residual<PK><<<L.grid, kThreads, 0, s>>>(wl, P64, P32, b, x64, r32, x32, z32, outer, inner, part, atol, rtol, inner_rtol, maxiter, max_outer)
+void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl,
+                            const CUtensorMap* maps, const float* P32, const double* b,
+                            float* r32, float* x32, float* z32, InstState* outer,
+                            InstState* inner, double* part, double atol, double rtol,
+                            double inner_rtol, int maxiter, int max_outer, int* err,
+                            cudaStream_t s) {
+    const size_t sm = smem_init<double>();
+#define PMB_RR(PK)                                                                              \
+    do {                                                                                        \
+                                                                                    \
+        k_refine_residual<PK><<<L.grid, kThreads, sm, s>>>(wl, maps, P32, b, r32, x32, z32,    \
+                                                           outer, inner, part, atol, rtol,      \
+                                                           inner_rtol, maxiter, max_outer, err); \
+    } while (0)
     if (prec == kPrecNone) PMB_RR(kPrecNone);
     else if (prec == kPrecJacobi) PMB_RR(kPrecJacobi);
     else PMB_RR(kPrecVcycle);
@@ -934,35 +1127,70 @@ void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl, co
 }
 
 void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, const float* x32,
-                           InstState* outer, const InstState* inner, int ninst, cudaStream_t s) {
-    k_refine_correct<<<L.grid, kThreads, 0, s>>>(wl, x64, x32, outer, inner);
+                           InstState* outer, int ninst, cudaStream_t s) {
+    k_refine_correct<<<L.grid, kThreads, 0, s>>>(wl, x64, x32, outer);
     k_refine_count<<<(ninst + 127) / 128, 128, 0, s>>>(outer, ninst);
 }
 
-#define PMB_INST(T)                                                                          \
-    template void launch_cg_init<T>(int, const LaunchCfg&, const WorkList&, const T*, const T*, \
-                                    T*, const T*, T*, T*, InstState*, double*, double, double, \
-                                    int, cudaStream_t);                                      \
-    template void launch_cg_apply<T>(const LaunchCfg&, const WorkList&, const T*, const T*, T*, \
-                                     T*, T*, InstState*, double*, cudaStream_t);             \
-    template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*, \
-                                      T*, const T*, const T*, const T*, T*, int, InstState*,  \
-                                      double*, cudaStream_t);                                \
-    template void launch_cg_rz<T>(const LaunchCfg&, const WorkList&, const T*, const T*,      \
-                                  const T*, int, InstState*, double*, cudaStream_t);         \
-    template void launch_vc_down<T>(int, const LaunchCfg&, const WorkList&, const GridDesc*,  \
-                                    const T*, const T*, const T*, T*, double,                \
-                                    const InstState*, cudaStream_t);                         \
-    template void launch_vc_up<T>(int, int, const LaunchCfg&, const WorkList&,                \
-                                  const GridDesc*, const T*, const T*, const T*, const T*, T*, \
-                                  double, InstState*, int, const T*, int, double*,           \
-                                  cudaStream_t);                                             \
-    template void launch_vc_smooth<T>(const LaunchCfg&, const WorkList&, const T*, const T*,  \
-                                      const T*, T*, double, const InstState*, cudaStream_t); \
-    template void launch_vc_direct<T>(const DirectDesc*, int, const T*, T*, InstState*, int,  \
-                                      cudaStream_t);                                         \
-    template void launch_apply<T>(const LaunchCfg&, const WorkList&, const T*, const T*, T*,  \
-                                  cudaStream_t);
+
+template <typename T>
+static void prepare_type() {
+    allow_smem(k_cg_init<T, kPrecNone, true>, smem_init<T>());
+    allow_smem(k_cg_init<T, kPrecJacobi, true>, smem_init<T>());
+    allow_smem(k_cg_init<T, kPrecVcycle, true>, smem_init<T>());
+    allow_smem(k_cg_apply<T>, smem_apply<T>());
+    allow_smem(k_vc_down<T, 0>, smem_down<T>(0));
+    allow_smem(k_vc_down<T, 1>, smem_down<T>(1));
+    allow_smem(k_vc_down<T, 2>, smem_down<T>(2));
+    allow_smem(k_vc_up<T, 0, 0>, smem_up<T>(0));
+    allow_smem(k_vc_up<T, 0, 1>, smem_up<T>(0));
+    allow_smem(k_vc_up<T, 1, 0>, smem_up<T>(1));
+    allow_smem(k_vc_up<T, 1, 1>, smem_up<T>(1));
+    allow_smem(k_vc_up<T, 2, 0>, smem_up<T>(2));
+    allow_smem(k_vc_up<T, 2, 1>, smem_up<T>(2));
+    allow_smem(k_vc_smooth<T>, smem_init<T>());
+    allow_smem(k_apply<T>, smem_init<T>());
+}
+
+void stencil_prepare() {
+    static bool done = false;
+    if (done) return;
+    prepare_type<double>();
+    prepare_type<float>();
+    allow_smem(k_refine_residual<kPrecNone>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecJacobi>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecVcycle>, smem_init<double>());
+    done = true;
+}
+
+#define PMB_INST(T)                                                                              \
+    template void launch_cg_init<T>(int, const LaunchCfg&, const WorkList&, const CUtensorMap*,   \
+                                    const T*, const T*, T*, bool, T*, T*, InstState*, double*,    \
+                                    double, double, int, int*, cudaStream_t);                     \
+    template void launch_cg_apply<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int,  \
+                                     T*, T*, T*, InstState*, double*, int*, cudaStream_t);        \
+    template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*,   \
+                                      T*, const T*, const T*, const T*, T*, int, InstState*,      \
+                                      double*, cudaStream_t);                                    \
+    template void launch_cg_rz<T>(const LaunchCfg&, const WorkList&, const T*, const T*,          \
+                                  const T*, int, InstState*, double*, cudaStream_t);             \
+    template void launch_vc_down<T>(int, const LaunchCfg&, const WorkList&, const GridDesc*,      \
+                                    const CUtensorMap*, int, T*, double, const InstState*, int*, \
+                                    cudaStream_t);                                               \
+    template void launch_vc_up<T>(int, int, const LaunchCfg&, const WorkList&, const GridDesc*,   \
+                                  const CUtensorMap*, int, const T*, T*, double, InstState*, int, \
+                                  const T*, int, double*, int*, cudaStream_t);                   \
+    template void launch_vc_smooth<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int, \
+                                      const T*, const T*, T*, double, const InstState*, int*,    \
+                                      cudaStream_t);                                             \
+    template void launch_vc_direct<T>(const DirectDesc*, int, const T*, T*, InstState*, int,      \
+                                      cudaStream_t);                                             \
+    template void launch_apply<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, T*, int*, \
+                                  cudaStream_t);                                                 \
+    template size_t smem_apply<T>();                                                              \
+    template size_t smem_init<T>();                                                               \
+    template size_t smem_down<T>(int);                                                            \
+    template size_t smem_up<T>(int);
 
 PMB_INST(double)
 PMB_INST(float)

@@ -1,6 +1,8 @@
 // Launch interface of the half-stencil kernels (stencil.cu) for the engine.
 #pragma once
 
+#include <cuda.h>
+
 #include "pm_common.cuh"
 
 namespace pmb {
@@ -18,13 +20,22 @@ struct DirectDesc {
     int64_t work_off;   // n x n scratch used while inverting (setup only)
 };
 
+// Shared memory (bytes) of the TMA-tiled kernels, for launch sizing.
+template <typename T> size_t smem_apply();
+template <typename T> size_t smem_init();
+template <typename T> size_t smem_down(int pre);
+template <typename T> size_t smem_up(int pre);
+
+// Raise the dynamic shared-memory limits once (before any graph capture).
+void stencil_prepare();
+
 template <typename T>
-void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, const T* b,
-                    T* x, const T* x0, T* r, T* z, InstState* st, double* part, double atol,
-                    double rtol, int maxiter, cudaStream_t s);
+void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
+                    const T* P, const T* b, T* x, bool have_x0, T* r, T* z, InstState* st,
+                    double* part, double atol, double rtol, int maxiter, int* err, cudaStream_t s);
 template <typename T>
-void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const T* P, const T* z, T* p0, T* p1,
-                     T* Ap, InstState* st, double* part, cudaStream_t s);
+void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, int zslot,
+                     T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s);
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
                       T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth,
@@ -34,21 +45,22 @@ void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z
                   int reorth, InstState* st, double* part, cudaStream_t s);
 template <typename T>
 void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridDesc* fine,
-                    const T* P, const T* b, const T* xs, T* bc, double omega,
-                    const InstState* st, cudaStream_t s);
+                    const CUtensorMap* maps, int xs_slot, T* bc, double omega,
+                    const InstState* st, int* err, cudaStream_t s);
 template <typename T>
 void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
-                  const T* P, const T* b, const T* xs, const T* xc, T* xout, double omega,
-                  InstState* st, int level0, const T* dr, int reorth, double* part,
+                  const CUtensorMap* maps, int xs_slot, const T* b, T* xout, double omega,
+                  InstState* st, int level0, const T* dr, int reorth, double* part, int* err,
                   cudaStream_t s);
 template <typename T>
-void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const T* P, const T* b, const T* xin,
-                      T* xout, double omega, const InstState* st, cudaStream_t s);
+void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
+                      int xin_slot, const T* P, const T* b, T* xout, double omega,
+                      const InstState* st, int* err, cudaStream_t s);
 template <typename T>
 void launch_vc_direct(const DirectDesc* dd, int count, const T* b, T* x, InstState* st,
                       int rz_level0, cudaStream_t s);
 template <typename T>
-void launch_apply(const LaunchCfg& L, const WorkList& wl, const T* P, const T* x, T* y,
+void launch_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, T* y, int* err,
                   cudaStream_t s);
 template <typename TS, typename TD>
 void launch_pack(const GridDesc* grids, int ngrids, const int64_t* uoff, const TS* src, TD* dst,
@@ -61,12 +73,13 @@ void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrid
 void launch_dense_inverse(const DirectDesc* dd, int count, const double* Pc, double* work,
                           int* status, cudaStream_t s);
 void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s);
-void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl, const double* P64,
-                            const float* P32, const double* b, const double* x64, float* r32,
-                            float* x32, float* z32, InstState* outer, InstState* inner,
-                            double* part, double atol, double rtol, double inner_rtol,
-                            int maxiter, int max_outer, cudaStream_t s);
+void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl,
+                            const CUtensorMap* maps, const float* P32, const double* b,
+                            float* r32, float* x32, float* z32, InstState* outer,
+                            InstState* inner, double* part, double atol, double rtol,
+                            double inner_rtol, int maxiter, int max_outer, int* err,
+                            cudaStream_t s);
 void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, const float* x32,
-                           InstState* outer, const InstState* inner, int ninst, cudaStream_t s);
+                           InstState* outer, int ninst, cudaStream_t s);
 
 }  // namespace pmb

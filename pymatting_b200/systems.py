@@ -119,7 +119,16 @@ class StencilSystem:
         return y
 
     def launch_count(self):
+        """Kernel launches issued by this system so far (graph replays included)."""
         return int(_ffi.lib().pmb_stencil_launch_count(self._h))
+
+    def time_apply(self, iters=20):
+        """Average milliseconds of one level-0 operator apply (CUDA events on
+        the solver's stream)."""
+        ms = ctypes.c_double()
+        _ffi.check(_ffi.lib().pmb_stencil_time_apply(self._h, int(iters), ctypes.byref(ms),
+                                                     dev.stream()), "pmb_stencil_time_apply")
+        return ms.value
 
 
 M_NONE, M_JACOBI, M_MATRIX, M_ICHOL, M_EXTERNAL = 0, 1, 2, 3, 4

@@ -1,0 +1,105 @@
+"""Host-side logic: input checks, synthetic inputs, batch sharding."""
+
+import os
+import warnings
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import oracle
+from pymatting_b200.shard import shard_sizes
+from pymatting_b200.synthetic import batch_sizes, make_matting_problem
+from pymatting_b200.util import sanity_check_image, trimap_split
+
+
+def test_trimap_split_matches_oracle():
+    rng = np.random.default_rng(0)
+    t = rng.choice([0.0, 0.05, 0.5, 0.95, 1.0], size=(17, 23))
+    for a, b in zip(trimap_split(t), oracle.trimap_split(t)):
+        np.testing.assert_array_equal(a, b)
+    fg, bg, known, unknown = trimap_split(t, flatten=False)
+    assert fg.shape == (17, 23)
+
+
+def test_trimap_split_errors_and_warnings():
+    with pytest.raises(ValueError, match="background"):
+        trimap_split(np.array([[1.0, 0.5]]))
+    with pytest.raises(ValueError, match="foreground"):
+        trimap_split(np.array([[0.0, 0.5]]))
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        trimap_split(np.array([[-0.5, 1.5]]))
+        trimap_split(np.array([[0, 1]], dtype=np.int64))
+    assert len(w) == 3
+
+
+def test_sanity_check_image_warnings():
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        sanity_check_image((np.random.default_rng(0).standard_normal((8, 8, 2)) * 255)
+                           .astype(np.int32))
+    assert len(w) == 4
+
+
+def test_synthetic_is_deterministic_and_calibrated():
+    a = make_matting_problem(120, 160, 5, sigma=2.0, band=7, unknown_fraction=0.12)
+    b = make_matting_problem(120, 160, 5, sigma=2.0, band=7, unknown_fraction=0.12)
+    for x, y in zip(a[:3], b[:3]):
+        np.testing.assert_array_equal(x, y)
+    img, tri, alpha, frac = a
+    assert img.shape == (120, 160, 3) and tri.shape == (120, 160)
+    assert 0.0 <= img.min() and img.max() <= 1.0
+    assert set(np.unique(tri)) <= {0.0, 0.5, 1.0}
+    assert (tri == 1.0).any() and (tri == 0.0).any()
+    assert abs(frac - np.mean(tri == 0.5)) < 1e-12
+
+
+def test_batch_sizes():
+    spec = batch_sizes(64, 1000)
+    assert len(spec) == 64
+    assert all(0.05 <= f <= 0.25 for _h, _w, f, _s in spec)
+    assert spec == batch_sizes(64, 1000)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_shard_sizes_partition(world):
+    sizes = [(h, w) for h, w, _f, _s in batch_sizes(64, 1000)]
+    parts = shard_sizes(sizes, world)
+    flat = sorted(k for p in parts for k in p)
+    assert flat == list(range(64))
+    loads = [sum(sizes[k][0] * sizes[k][1] for k in p) for p in parts]
+    biggest = max(h * w for h, w in sizes)
+    assert max(loads) - min(loads) <= biggest
+
+
+def _gloo_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sizes = [(h, w) for h, w, _f, _s in batch_sizes(64, 1000)]
+    mine = shard_sizes(sizes, world)[rank]
+    gathered = [None] * world
+    dist.all_gather_object(gathered, mine)
+    if rank == 0:
+        out.put(gathered)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_shard_ranks_agree_without_communication():
+    """Each rank computes its shard alone; the union over ranks is the batch."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + (os.getpid() % 2000)
+    procs = [ctx.Process(target=_gloo_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    gathered = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sorted(k for part in gathered for k in part) == list(range(64))
+    assert not set(gathered[0]) & set(gathered[1])
