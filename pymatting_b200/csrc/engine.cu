@@ -179,10 +179,11 @@ struct Stencil {
     const CUtensorMap* maps() const { return at<CUtensorMap>(o_maps); }
 };
 
+// Resident CTAs per SM of a 512-thread tile kernel using `smem` bytes.
 static int blocks_per_sm(size_t smem) {
     const size_t usable = 227 * 1024;
     int b = (int)(usable / (smem + 1024));
-    return std::max(1, std::min(8, b));
+    return std::max(1, std::min(4, b));
 }
 
 static int persistent_grid(const HostList& L) {

@@ -18,8 +18,9 @@ namespace pmb {
 constexpr int kRS = 2;       // stencil radius of the stored operator
 constexpr int kNH = 13;      // stored planes (centre + 12 forward offsets)
 constexpr int kTX = 64;      // fine tile width
-constexpr int kTY = 8;       // fine tile height (two pixels per thread)
-constexpr int kThreads = 256;
+constexpr int kTY = 8;       // fine tile height
+constexpr int kThreads = 256;      // element-wise kernels
+constexpr int kTileThreads = 512;  // tiled stencil kernels: one pixel per thread
 constexpr int kFlat = 1024;  // elements per tile of the element-wise kernels
 
 // Shared-memory boxes loaded by TMA around a fine tile at (x0, y0): origin
@@ -180,6 +181,53 @@ __device__ __forceinline__ bool tile_reduce(double (&v)[NQ], double* partials, i
     }
     __syncthreads();
     return true;
+}
+
+// Per-CTA variant for grid-stride tile loops. A CTA walking tiles t, t + G,
+// t + 2G, ... (G = gridDim.x) accumulates its sums for one image and calls
+// cta_flush once, after its last tile of that image. Partial sums live at
+// partials[(inst * 3 + q) * G + cta]; the CTA that completes the image's tile
+// count adds the partials of every CTA that owned one of its tiles, in CTA
+// order, and runs `fin` (thread 0). Deterministic for a fixed grid size.
+template <int NQ, typename Fin>
+__device__ __forceinline__ void cta_flush(double (&v)[NQ], double* partials, int inst, int t0,
+                                          int t1, unsigned int mine, InstState* st, double* smem,
+                                          Fin fin) {
+    const int G = gridDim.x;
+    block_sum<NQ>(v, smem);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) partials[((int64_t)inst * 3 + q) * G + blockIdx.x] = v[q];
+        __threadfence();
+        const unsigned int done = atomicAdd(&st->counter, mine);
+        last = (done + mine == (unsigned int)(t1 - t0));
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        const int n = t1 - t0;
+        double s[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            s[q] = 0.0;
+            const double* p = partials + ((int64_t)inst * 3 + q) * G;
+            if (n >= G) {
+                for (int c = threadIdx.x; c < G; c += blockDim.x) s[q] += __ldcg(p + c);
+            } else {
+                // Fewer tiles than CTAs: tile t0 + k belonged to CTA (t0 + k) % G.
+                for (int k = threadIdx.x; k < n; k += blockDim.x) s[q] += __ldcg(p + (t0 + k) % G);
+            }
+        }
+        block_sum<NQ>(s, smem);
+        if (threadIdx.x == 0) {
+            st->counter = 0u;
+            fin(s);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
 }
 
 }  // namespace pmb

@@ -30,20 +30,6 @@ namespace pmb {
 // Tile helpers
 // --------------------------------------------------------------------------
 
-struct TileCoord { int g, y0, x0; };
-
-template <int H, int W>
-__device__ __forceinline__ TileCoord tile_coord(const WorkList& wl, int t) {
-    TileCoord c;
-    c.g = find_grid(wl, t);
-    const int local = t - wl.tile_start[c.g];
-    const int tiles_x = (wl.grids[c.g].w + W - 1) / W;
-    const int ty = local / tiles_x;
-    c.y0 = ty * H;
-    c.x0 = (local - ty * tiles_x) * W;
-    return c;
-}
-
 // Shared-memory carve-up with 128-byte alignment (TMA destinations).
 struct SmemCarve {
     char* p;
@@ -58,8 +44,44 @@ struct SmemCarve {
 
 extern __shared__ __align__(128) char g_smem[];
 
-// Per-CTA TMA state: the barrier and its phase.
-struct Tma {
+// Description of one tile, prepared by thread 0 for the whole CTA.
+struct Meta {
+    int t, g, y0, x0;     // tile, grid index in the list, tile origin
+    int inst, t0, t1;     // image and its tile range in the list
+    int run;              // 0: image not running, the tile is skipped
+    int par, first;       // CG: iteration parity and first-pass flag
+    double beta;          // CG: current beta
+};
+
+template <int H, int W>
+__device__ __forceinline__ void make_meta(const WorkList& wl, int t, const InstState* st,
+                                          Meta& m, GridDesc& gd) {
+    m.t = t;
+    m.g = find_grid(wl, t);
+    gd = wl.grids[m.g];
+    m.t0 = wl.tile_start[m.g];
+    m.t1 = wl.tile_start[m.g + 1];
+    const int local = t - m.t0;
+    const int tiles_x = (gd.w + W - 1) / W;
+    const int ty = local / tiles_x;
+    m.y0 = ty * H;
+    m.x0 = (local - ty * tiles_x) * W;
+    m.inst = gd.inst;
+    m.run = 1;
+    m.par = 0;
+    m.first = 0;
+    m.beta = 0.0;
+    if (st) {
+        const InstState& s = st[gd.inst];
+        m.run = s.status == kRunning;
+        m.par = s.iters & 1;
+        m.first = (s.flags & kFirst) != 0;
+        m.beta = s.beta;
+    }
+}
+
+// Two mbarriers (one per pipeline buffer) and their phase bits.
+struct Pipe {
     uint64_t* bar;
     uint32_t phase;
     int* err;
@@ -67,13 +89,15 @@ struct Tma {
         bar = b;
         phase = 0;
         err = e;
-        if (threadIdx.x == 0) mbar_init(bar, 1);
+        if (threadIdx.x == 0) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+        }
         __syncthreads();
     }
-    // Called by every thread after thread 0 issued the loads.
-    __device__ bool wait() {
-        const bool ok = mbar_wait(bar, phase);
-        phase ^= 1u;
+    __device__ bool wait(int b) {
+        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1u);
+        phase ^= 1u << b;
         if (!ok && err) atomicExch(err, 1);
         return ok;
     }
@@ -100,6 +124,60 @@ __device__ __forceinline__ T stencil_at(const T* P, int ph, const T* X, int r, i
     }
     return acc;
 }
+
+// The pipelined tile loop shared by the TMA kernels. For every tile the CTA
+// owns (t = blockIdx.x, + gridDim.x, ...): thread 0 prepares the meta of the
+// next tile and issues its loads into the other buffer, then the CTA waits
+// for the current buffer, runs `body`, and (for kernels with reductions)
+// flushes its per-image partial sums after its last tile of an image.
+//   issue(meta, gd, buf)            thread 0 only
+//   body(meta, gd, buf)             all threads; returns nothing
+//   flush(meta, mine)               all threads, after an image's last tile
+template <int H, int W, typename Issue, typename Body, typename Flush>
+__device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* st, Pipe& pipe,
+                                          Meta* s_m, GridDesc* s_g, Issue issue, Body body,
+                                          Flush flush) {
+    const int G = gridDim.x;
+    int t = blockIdx.x;
+    int b = 0;
+    unsigned int mine = 0;
+    if (threadIdx.x == 0 && t < wl.total) {
+        make_meta<H, W>(wl, t, st, s_m[0], s_g[0]);
+        if (s_m[0].run) {
+            fence_proxy_async();
+            issue(s_m[0], s_g[0], 0);
+        }
+    }
+    while (t < wl.total) {
+        const int tn = t + G;
+        if (threadIdx.x == 0 && tn < wl.total) {
+            make_meta<H, W>(wl, tn, st, s_m[b ^ 1], s_g[b ^ 1]);
+            if (s_m[b ^ 1].run) {
+                fence_proxy_async();
+                issue(s_m[b ^ 1], s_g[b ^ 1], b ^ 1);
+            }
+        }
+        __syncthreads();
+        const Meta m = s_m[b];
+        if (m.run) {
+            if (!pipe.wait(b)) return;
+            body(m, s_g[b], b);
+            ++mine;
+            const bool last_of_image = (tn >= wl.total) || (s_m[b ^ 1].inst != m.inst);
+            if (last_of_image) {
+                flush(m, mine);
+                mine = 0;
+            }
+        }
+        __syncthreads();
+        b ^= 1;
+        t = tn;
+    }
+}
+
+struct NoFlush {
+    __device__ void operator()(const Meta&, unsigned int) const {}
+};
 
 // --------------------------------------------------------------------------
 // Conjugate gradient steps (cg.py:64-117)
@@ -132,36 +210,38 @@ __device__ __forceinline__ void finish_beta_reorth(InstState* st, double rz_new,
 // z and r.z. Finaliser sets norm_b, tol, status (cg.py:64-80). x0 arrives in
 // the p-parity-0 buffer (map slot kMapP0F).
 template <typename T, int PREC, bool X0>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T* __restrict__ b,
           T* x, T* r, T* z, InstState* st, double* partials, double atol, double rtol,
           int maxiter, int* err) {
     __shared__ double s_red[3 * 32];
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP = X0 ? sc.take<T>(kNH * kBH * kBW) : nullptr;
-    T* sX = X0 ? sc.take<T>(kBH * kBW) : nullptr;
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
-        InstState* s = st + g.inst;
-        if (X0) {
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                fence_proxy_async();
-                mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(T));
-                tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
-                tma_load_2d(sX, map_of(maps, g, kMapP0F), c.x0 - kBOX, c.y0 - 2, tma.bar);
-            }
-            if (!tma.wait()) return;
+    T* sP[2];
+    T* sX[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = X0 ? sc.take<T>(kNH * kBH * kBW) : nullptr;
+        sX[k] = X0 ? sc.take<T>(kBH * kBW) : nullptr;
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    double v[3] = {0.0, 0.0, 0.0};
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        if (!X0) {
+            // Nothing to stage: complete the phase with an empty arrival.
+            mbar_expect_tx(&pipe.bar[bb], 0);
+            return;
         }
-        double v[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
-            const int y = c.y0 + ly, xx = c.x0 + lx;
+        mbar_expect_tx(&pipe.bar[bb], (kNH + 1) * kBH * kBW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapPlF), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sX[bb], map_of(maps, g, kMapP0F), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        {
+            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+            const int y = m.y0 + ly, xx = m.x0 + lx;
             if (y < g.h && xx < g.w) {
                 const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
                 const T bi = b[i];
@@ -169,9 +249,9 @@ k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T
                 T d;
                 if (X0) {
                     const int q = (ly + 2) * kBW + lx + kBOX;
-                    ri = bi - stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
-                    x[i] = sX[q];
-                    d = sP[q];
+                    ri = bi - stencil_at<T>(sP[bb], kBH, sX[bb], ly + 2, lx + kBOX);
+                    x[i] = sX[bb][q];
+                    d = sP[bb][q];
                 } else {
                     x[i] = T(0);
                     d = P[g.poff + (int64_t)y * g.pitch + xx];
@@ -188,8 +268,10 @@ k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T
                 }
             }
         }
-        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
-        tile_reduce<3>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+    };
+    auto flush = [&](const Meta& m, unsigned int mine) {
+        InstState* s = st + m.inst;
+        cta_flush<3>(v, partials, m.inst, m.t0, m.t1, mine, s, s_red, [&](double* sum) {
             s->norm_b = sqrt(sum[0]);
             s->norm_r = sqrt(sum[1]);
             s->tol = fmax(atol, rtol * s->norm_b);
@@ -203,7 +285,9 @@ k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T
             else s->status = kRunning;
             if (PREC != kPrecVcycle && PREC != kPrecExternal) s->rz = sum[2];
         });
-    }
+    };
+    // Every image starts from scratch: its tiles run whatever its status.
+    tile_loop<kTY, kTX>(wl, nullptr, pipe, s_m, s_g, issue, body, flush);
 }
 
 // p_new = z + beta p_old (p_new = z on the first pass), Ap = A p_new and
@@ -212,99 +296,122 @@ k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T
 // p_old while this tile writes p_new. zslot selects z (r without a
 // preconditioner).
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_cg_apply(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap, InstState* st,
            double* partials, int* err) {
     __shared__ double s_red[32];
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP = sc.take<T>(kNH * kBH * kBW);
-    T* sZ = sc.take<T>(kBH * kBW);
-    T* sQ = sc.take<T>(kBH * kBW);
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
-        InstState* s = st + g.inst;
-        if (s->status != kRunning) continue;
-        const bool first = (s->flags & kFirst) != 0;
-        const T beta = (T)s->beta;
-        const int par = s->iters & 1;
-        T* pnew = par ? p0 : p1;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(tma.bar, (kNH + (first ? 1 : 2)) * kBH * kBW * sizeof(T));
-            tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
-            tma_load_2d(sZ, map_of(maps, g, zslot), c.x0 - kBOX, c.y0 - 2, tma.bar);
-            if (!first)
-                tma_load_2d(sQ, map_of(maps, g, par ? kMapP1F : kMapP0F), c.x0 - kBOX, c.y0 - 2,
-                            tma.bar);
-        }
-        if (!tma.wait()) return;
-        if (!first) {
-            for (int q = threadIdx.x; q < kBH * kBW; q += blockDim.x) sZ[q] = sZ[q] + beta * sQ[q];
+    T* sP[2];
+    T* sZ[2];
+    T* sQ[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kBH * kBW);
+        sZ[k] = sc.take<T>(kBH * kBW);
+        sQ[k] = sc.take<T>(kBH * kBW);
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    double v[1] = {0.0};
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        mbar_expect_tx(&pipe.bar[bb], (kNH + (m.first ? 1 : 2)) * kBH * kBW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapPlF), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sZ[bb], map_of(maps, g, zslot), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+        if (!m.first)
+            tma_load_2d(sQ[bb], map_of(maps, g, m.par ? kMapP1F : kMapP0F), m.x0 - kBOX, m.y0 - 2,
+                        &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        T* Z = sZ[bb];
+        if (!m.first) {
+            const T beta = (T)m.beta;
+            const T* Q = sQ[bb];
+            for (int q = threadIdx.x; q < kBH * kBW; q += blockDim.x) Z[q] = Z[q] + beta * Q[q];
             __syncthreads();
         }
-        double v[1] = {0.0};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
-            const int y = c.y0 + ly, x = c.x0 + lx;
+        T* pnew = m.par ? p0 : p1;
+        {
+            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+            const int y = m.y0 + ly, x = m.x0 + lx;
             if (y < g.h && x < g.w) {
                 const int64_t i = g.voff + (int64_t)y * g.pitch + x;
-                const T pi = sZ[(ly + 2) * kBW + lx + kBOX];
-                const T api = stencil_at<T>(sP, kBH, sZ, ly + 2, lx + kBOX);
+                const T pi = Z[(ly + 2) * kBW + lx + kBOX];
+                const T api = stencil_at<T>(sP[bb], kBH, Z, ly + 2, lx + kBOX);
                 pnew[i] = pi;
                 Ap[i] = api;
                 v[0] += (double)pi * (double)api;
             }
         }
-        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
-        tile_reduce<1>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+    };
+    auto flush = [&](const Meta& m, unsigned int mine) {
+        InstState* s = st + m.inst;
+        cta_flush<1>(v, partials, m.inst, m.t0, m.t1, mine, s, s_red, [&](double* sum) {
             s->pap = sum[0];
             s->alpha = s->rz / sum[0];
             s->flags &= ~kFirst;
         });
-    }
+    };
+    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
 }
 
-// Element-wise chunk of a flat work list: the element range of tile t.
-struct FlatCoord { int g; int64_t e0, e1; };
-
-__device__ __forceinline__ FlatCoord flat_coord(const WorkList& wl, int t) {
-    FlatCoord f;
-    f.g = find_grid(wl, t);
-    const GridDesc& g = wl.grids[f.g];
-    const int64_t n = (int64_t)g.h * g.pitch;
-    f.e0 = (int64_t)(t - wl.tile_start[f.g]) * kFlat;
-    f.e1 = min(f.e0 + kFlat, n);
-    return f;
+// Element-wise loop over a flat work list (1024-element chunks) with the same
+// per-CTA, per-image flush as the tiled kernels. Chunks cover the pitched
+// rows; padding columns are skipped.
+template <typename Body, typename Flush>
+__device__ __forceinline__ void flat_loop(const WorkList& wl, const InstState* st, Body body,
+                                          Flush flush) {
+    __shared__ int s_inst[2], s_run, s_t0, s_t1;
+    __shared__ GridDesc s_gd;
+    const int G = gridDim.x;
+    unsigned int mine = 0;
+    for (int t = blockIdx.x; t < wl.total; t += G) {
+        const int tn = t + G;
+        if (threadIdx.x == 0) {
+            const int g = find_grid(wl, t);
+            s_gd = wl.grids[g];
+            s_t0 = wl.tile_start[g];
+            s_t1 = wl.tile_start[g + 1];
+            s_inst[0] = s_gd.inst;
+            s_inst[1] = tn < wl.total ? wl.grids[find_grid(wl, tn)].inst : -1;
+            s_run = st ? st[s_gd.inst].status == kRunning : 1;
+        }
+        __syncthreads();
+        if (s_run) {
+            const GridDesc g = s_gd;
+            const int64_t n = (int64_t)g.h * g.pitch;
+            const int64_t e0 = (int64_t)(t - s_t0) * kFlat;
+            const int64_t e1 = min(e0 + kFlat, n);
+            body(g, e0, e1);
+            ++mine;
+            if (s_inst[1] != s_inst[0]) {
+                flush(s_inst[0], s_t0, s_t1, mine);
+                mine = 0;
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // x += alpha p; r -= alpha Ap; |r|; convergence test (cg.py:89-99). For the
 // Jacobi / identity preconditioners also z = M r and beta (cg.py:101-113).
 // With reorthogonalisation the change r - r_old is kept in `dr` (or reduced
-// directly against z for Jacobi). Padding columns of the pitched rows are
-// excluded from the sums.
+// directly against z for Jacobi).
 template <typename T, int PREC>
 __global__ void __launch_bounds__(kThreads)
 k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0, const T* p1,
             const T* __restrict__ Ap, T* dr, int reorth, InstState* st, double* partials) {
     __shared__ double s_red[3 * 32];
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const FlatCoord f = flat_coord(wl, t);
-        const GridDesc g = wl.grids[f.g];
-        InstState* s = st + g.inst;
-        if (s->status != kRunning) continue;
-        const T a = (T)s->alpha;
-        const T* p = (s->iters & 1) ? p0 : p1;   // the buffer k_cg_apply wrote
-        double v[3] = {0.0, 0.0, 0.0};
+    double v[3] = {0.0, 0.0, 0.0};
+    auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
+        const InstState& s = st[g.inst];
+        const T a = (T)s.alpha;
+        const T* p = (s.iters & 1) ? p0 : p1;   // the buffer k_cg_apply wrote
 #pragma unroll
         for (int k = 0; k < kFlat / kThreads; ++k) {
-            const int64_t e = f.e0 + threadIdx.x + k * kThreads;
-            if (e >= f.e1) break;
+            const int64_t e = e0 + threadIdx.x + k * kThreads;
+            if (e >= e1) break;
             const int col = (int)(e % g.pitch);
             if (col >= g.w) continue;
             const int64_t i = g.voff + e;
@@ -327,8 +434,10 @@ k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0,
                 dr[i] = ri - rold;
             }
         }
-        const int t0 = wl.tile_start[f.g], t1 = wl.tile_start[f.g + 1];
-        tile_reduce<3>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+    };
+    auto flush = [&](int inst, int t0, int t1, unsigned int mine) {
+        InstState* s = st + inst;
+        cta_flush<3>(v, partials, inst, t0, t1, mine, s, s_red, [&](double* sum) {
             const double nr = sqrt(sum[0]);
             s->norm_r = nr;
             s->iters += 1;
@@ -340,7 +449,8 @@ k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0,
                 else finish_beta(s, sum[1]);
             }
         });
-    }
+    };
+    flat_loop(wl, st, body, flush);
 }
 
 // r . z (and (r - r_old) . z) for preconditioners applied outside the fused
@@ -350,27 +460,26 @@ __global__ void __launch_bounds__(kThreads)
 k_cg_rz(WorkList wl, const T* __restrict__ r, const T* __restrict__ z, const T* __restrict__ dr,
         int reorth, InstState* st, double* partials) {
     __shared__ double s_red[2 * 32];
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const FlatCoord f = flat_coord(wl, t);
-        const GridDesc g = wl.grids[f.g];
-        InstState* s = st + g.inst;
-        if (s->status != kRunning) continue;
-        double v[2] = {0.0, 0.0};
+    double v[2] = {0.0, 0.0};
+    auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
 #pragma unroll
         for (int k = 0; k < kFlat / kThreads; ++k) {
-            const int64_t e = f.e0 + threadIdx.x + k * kThreads;
-            if (e >= f.e1) break;
+            const int64_t e = e0 + threadIdx.x + k * kThreads;
+            if (e >= e1) break;
             if ((int)(e % g.pitch) >= g.w) continue;
             const int64_t i = g.voff + e;
             v[0] += (double)r[i] * (double)z[i];
             if (reorth) v[1] += (double)dr[i] * (double)z[i];
         }
-        const int t0 = wl.tile_start[f.g], t1 = wl.tile_start[f.g + 1];
-        tile_reduce<2>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
+    };
+    auto flush = [&](int inst, int t0, int t1, unsigned int mine) {
+        InstState* s = st + inst;
+        cta_flush<2>(v, partials, inst, t0, t1, mine, s, s_red, [&](double* sum) {
             if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
             else finish_beta(s, sum[0]);
         });
-    }
+    };
+    flat_loop(wl, st, body, flush);
 }
 
 // --------------------------------------------------------------------------
@@ -379,8 +488,8 @@ k_cg_rz(WorkList wl, const T* __restrict__ r, const T* __restrict__ z, const T* 
 
 __device__ __forceinline__ double pw(int a) { return a == 0 ? 2.0 : 1.0; }
 
-// Restriction of the pre-smoothed residual. One CTA per tile of kCX x CY
-// coarse pixels:
+// Restriction of the pre-smoothed residual. One tile = kCX x CY coarse
+// pixels:
 //   x1 = omega b / d         (first Jacobi sweep from zero, vcycle.py:33-36)
 //        or x1 = 0 (no pre-smoothing) or x1 = xs (explicit sweeps);
 //   res = b - A x1 on the fine pixels under the tile (vcycle.py:77);
@@ -388,43 +497,49 @@ __device__ __forceinline__ double pw(int a) { return a == 0 ? 2.0 : 1.0; }
 // The fine box starts at (2 X0 - 4, 2 Y0 - 3): rows 2 Y0 - 3 .. 2 Y0 + 2 CY + 1
 // cover x1 around the residual rows 2 Y0 - 1 .. 2 Y0 + 2 CY - 1.
 template <typename T, int PRE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMap* maps,
           int xs_slot, T* bc, double omega, const InstState* st, int* err) {
     constexpr int CY = Coarse<T>::CY;
     constexpr int DH = 2 * CY + 5;                      // box rows
     constexpr int RH = 2 * CY + 1, RW = 2 * kCX + 1;    // residual region
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP = PRE != 0 ? sc.take<T>(kNH * DH * kBW) : nullptr;
-    T* sB = sc.take<T>(DH * kBW);
-    T* sX = PRE != 0 ? sc.take<T>(DH * kBW) : nullptr;
+    T* sP[2];
+    T* sB[2];
+    T* sS[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = PRE != 0 ? sc.take<T>(kNH * DH * kBW) : nullptr;
+        sB[k] = sc.take<T>(DH * kBW);
+        sS[k] = PRE > 1 ? sc.take<T>(DH * kBW) : nullptr;
+    }
+    T* sX = PRE == 1 ? sc.take<T>(DH * kBW) : nullptr;
     T* sR = sc.take<T>(RH * RW);
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<CY, kCX>(wl, t);
-        const GridDesc gc = wl.grids[c.g];
-        const GridDesc gf = fine[c.g];
-        if (st && st[gc.inst].status != kRunning) continue;
-        const int bx = 2 * c.x0 - 4, by = 2 * c.y0 - 3;   // box origin (fine)
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            const uint32_t nbox = 1 + (PRE != 0 ? kNH : 0) + (PRE > 1 ? 1 : 0);
-            mbar_expect_tx(tma.bar, nbox * DH * kBW * sizeof(T));
-            tma_load_2d(sB, map_of(maps, gf, kMapBD), bx, by, tma.bar);
-            if (PRE != 0) tma_load_3d(sP, map_of(maps, gf, kMapPlD), bx, by, 0, tma.bar);
-            if (PRE > 1) tma_load_2d(sX, map_of(maps, gf, xs_slot), bx, by, tma.bar);
-        }
-        if (!tma.wait()) return;
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    auto issue = [&](const Meta& m, const GridDesc& gc, int bb) {
+        const GridDesc gf = fine[m.g];
+        const int bx = 2 * m.x0 - 4, by = 2 * m.y0 - 3;
+        const uint32_t nbox = 1 + (PRE != 0 ? kNH : 0) + (PRE > 1 ? 1 : 0);
+        mbar_expect_tx(&pipe.bar[bb], nbox * DH * kBW * sizeof(T));
+        tma_load_2d(sB[bb], map_of(maps, gf, kMapBD), bx, by, &pipe.bar[bb]);
+        if (PRE != 0) tma_load_3d(sP[bb], map_of(maps, gf, kMapPlD), bx, by, 0, &pipe.bar[bb]);
+        if (PRE > 1) tma_load_2d(sS[bb], map_of(maps, gf, xs_slot), bx, by, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& gc, int bb) {
+        const GridDesc gf = fine[m.g];
+        const int bx = 2 * m.x0 - 4, by = 2 * m.y0 - 3;
+        const T* B = sB[bb];
+        const T* X1 = PRE > 1 ? sS[bb] : sX;
         if (PRE == 1) {
             // x1 = omega b / d inside the image, 0 outside.
             for (int q = threadIdx.x; q < DH * kBW; q += blockDim.x) {
                 const int rr = q / kBW, cc = q - rr * kBW;
                 const int fy = by + rr, fx = bx + cc;
                 T v = T(0);
-                if (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) v = (T)omega * sB[q] / sP[q];
+                if (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) v = (T)omega * B[q] / sP[bb][q];
                 sX[q] = v;
             }
             __syncthreads();
@@ -435,15 +550,15 @@ k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMa
             const int fy = by + br, fx = bx + bcol;
             T v = T(0);
             if (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) {
-                v = sB[br * kBW + bcol];
-                if (PRE != 0) v = v - stencil_at<T>(sP, DH, sX, br, bcol);
+                v = B[br * kBW + bcol];
+                if (PRE != 0) v = v - stencil_at<T>(sP[bb], DH, X1, br, bcol);
             }
             sR[q] = v;
         }
         __syncthreads();
         for (int q = threadIdx.x; q < kCX * CY; q += blockDim.x) {
             const int ly = q / kCX, lx = q - ly * kCX;
-            const int Y = c.y0 + ly, X = c.x0 + lx;
+            const int Y = m.y0 + ly, X = m.x0 + lx;
             if (Y < gc.h && X < gc.w) {
                 T sum = T(0);
 #pragma unroll
@@ -455,48 +570,57 @@ k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMa
                 bc[gc.voff + (int64_t)Y * gc.pitch + X] = sum;
             }
         }
-    }
+    };
+    tile_loop<CY, kCX>(wl, st, pipe, s_m, s_g, issue, body, NoFlush());
 }
 
 // Prolongation of the coarse correction and the first post-smoothing sweep:
 //   x2 = x1 + P xc           (vcycle.py:95; P = R^T)
 //   x3 = x2 + omega (b - A x2) / d    (vcycle.py:98, one sweep; POST = 0
 //                                       stores x2 unchanged)
-// At level 0 (level0 != 0) the block also accumulates r . z with r = b, and
+// At level 0 (level0 != 0) the CTA also accumulates r . z with r = b, and
 // (r - r_old) . z when reorthogonalising, finishing beta.
 template <typename T, int PRE, int POST>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap* maps,
         int xs_slot, const T* __restrict__ b, T* xout, double omega, InstState* st, int level0,
         const T* __restrict__ dr, int reorth, double* partials, int* err) {
     __shared__ double s_red[2 * 32];
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP = sc.take<T>(kNH * kBH * kBW);
-    T* sX = sc.take<T>(kBH * kBW);          // b, then x2 in place
-    T* sS = PRE > 1 ? sc.take<T>(kBH * kBW) : nullptr;
-    T* sC = sc.take<T>(kCBH * kCBW);
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc gf = wl.grids[c.g];
-        const GridDesc gc = coarse[c.g];
-        InstState* s = st ? st + gf.inst : nullptr;
-        if (s && s->status != kRunning) continue;
-        const int bx = c.x0 - kBOX, by = c.y0 - 2;
-        const int cx0 = (c.x0 >> 1) - 4, cy0 = (c.y0 >> 1) - 2;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(tma.bar, ((kNH + 1 + (PRE > 1 ? 1 : 0)) * kBH * kBW + kCBH * kCBW) *
-                                        sizeof(T));
-            tma_load_3d(sP, map_of(maps, gf, kMapPlF), bx, by, 0, tma.bar);
-            tma_load_2d(sX, map_of(maps, gf, kMapBF), bx, by, tma.bar);
-            if (PRE > 1) tma_load_2d(sS, map_of(maps, gf, xs_slot), bx, by, tma.bar);
-            tma_load_2d(sC, map_of(maps, gc, kMapXC), cx0, cy0, tma.bar);
-        }
-        if (!tma.wait()) return;
+    T* sP[2];
+    T* sX[2];
+    T* sS[2];
+    T* sC[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kBH * kBW);
+        sX[k] = sc.take<T>(kBH * kBW);          // b, then x2 in place
+        sS[k] = PRE > 1 ? sc.take<T>(kBH * kBW) : nullptr;
+        sC[k] = sc.take<T>(kCBH * kCBW);
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    double v[2] = {0.0, 0.0};
+    auto issue = [&](const Meta& m, const GridDesc& gf, int bb) {
+        const GridDesc gc = coarse[m.g];
+        const int bx = m.x0 - kBOX, by = m.y0 - 2;
+        const int cx0 = (m.x0 >> 1) - 4, cy0 = (m.y0 >> 1) - 2;
+        mbar_expect_tx(&pipe.bar[bb], ((kNH + 1 + (PRE > 1 ? 1 : 0)) * kBH * kBW + kCBH * kCBW) *
+                                          sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, gf, kMapPlF), bx, by, 0, &pipe.bar[bb]);
+        tma_load_2d(sX[bb], map_of(maps, gf, kMapBF), bx, by, &pipe.bar[bb]);
+        if (PRE > 1) tma_load_2d(sS[bb], map_of(maps, gf, xs_slot), bx, by, &pipe.bar[bb]);
+        tma_load_2d(sC[bb], map_of(maps, gc, kMapXC), cx0, cy0, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& gf, int bb) {
+        const GridDesc gc = coarse[m.g];
+        const int bx = m.x0 - kBOX, by = m.y0 - 2;
+        const int cx0 = (m.x0 >> 1) - 4, cy0 = (m.y0 >> 1) - 2;
+        T* X = sX[bb];
+        const T* Pl = sP[bb];
+        const T* C = sC[bb];
         // Each element is read and rewritten by the same thread: no hazard.
         for (int q = threadIdx.x; q < kBH * kBW; q += blockDim.x) {
             const int rr = q / kBW, cc = q - rr * kBW;
@@ -504,38 +628,44 @@ k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap*
             T val = T(0);
             if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
                 T x1 = T(0);
-                if (PRE == 1) x1 = (T)omega * sX[q] / sP[q];
-                else if (PRE > 1) x1 = sS[q];
+                if (PRE == 1) x1 = (T)omega * X[q] / Pl[q];
+                else if (PRE > 1) x1 = sS[bb][q];
                 // Coarse pixels whose 3x3 support contains (y, x), in raster
-                // order of the coarse grid: |y - 2Y| <= 1 and |x - 2X| <= 1.
+                // order of the coarse grid: an even coordinate has one parent
+                // (weight 2), an odd one the two neighbours (weight 1 each);
+                // parents outside the coarse grid contribute nothing.
+                const int Ya = (y - 1) >> 1, Xa = (x - 1) >> 1;   // first parent candidate
+                const bool ey = (y & 1) == 0, ex = (x & 1) == 0;
                 T sum = T(0);
-                const int Yhi = min((y + 1) >> 1, gc.h - 1);
-                const int Xhi = min((x + 1) >> 1, gc.w - 1);
-                for (int Y = y >> 1; Y <= Yhi; ++Y) {
-                    const int ay = y - 2 * Y;
-                    for (int X = x >> 1; X <= Xhi; ++X) {
-                        const int ax = x - 2 * X;
-                        sum += (T)(pw(ax) * pw(ay) / 16.0) * sC[(Y - cy0) * kCBW + (X - cx0)];
+#pragma unroll
+                for (int jy = 0; jy < 2; ++jy) {
+                    const int Y = ey ? (y >> 1) : Ya + jy;
+                    if ((ey && jy == 1) || Y >= gc.h) continue;
+                    const double wy = ey ? 2.0 : 1.0;
+#pragma unroll
+                    for (int jx = 0; jx < 2; ++jx) {
+                        const int Xc = ex ? (x >> 1) : Xa + jx;
+                        if ((ex && jx == 1) || Xc >= gc.w) continue;
+                        const double wx = ex ? 2.0 : 1.0;
+                        sum += (T)(wx * wy / 16.0) * C[(Y - cy0) * kCBW + (Xc - cx0)];
                     }
                 }
                 val = x1 + sum;
             }
-            sX[q] = val;
+            X[q] = val;
         }
         __syncthreads();
-        double v[2] = {0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
-            const int y = c.y0 + ly, x = c.x0 + lx;
+        {
+            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+            const int y = m.y0 + ly, x = m.x0 + lx;
             if (y < gf.h && x < gf.w) {
                 const int64_t i = gf.voff + (int64_t)y * gf.pitch + x;
                 const int q = (ly + 2) * kBW + lx + kBOX;
-                T x3 = sX[q];
+                T x3 = X[q];
                 const T bi = b[i];
                 if (POST > 0) {
-                    const T ax = stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
-                    x3 = x3 + (T)omega * (bi - ax) / sP[q];
+                    const T ax = stencil_at<T>(Pl, kBH, X, ly + 2, lx + kBOX);
+                    x3 = x3 + (T)omega * (bi - ax) / Pl[q];
                 }
                 xout[i] = x3;
                 if (level0) {
@@ -544,60 +674,64 @@ k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap*
                 }
             }
         }
-        if (level0 && s) {
-            const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
-            tile_reduce<2>(v, partials, wl.total, t, t0, t1, s, s_red, [&](double* sum) {
-                if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
-                else finish_beta(s, sum[0]);
-            });
-        }
-    }
+    };
+    auto flush = [&](const Meta& m, unsigned int mine) {
+        if (!level0 || !st) return;
+        InstState* s = st + m.inst;
+        cta_flush<2>(v, partials, m.inst, m.t0, m.t1, mine, s, s_red, [&](double* sum) {
+            if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
+            else finish_beta(s, sum[0]);
+        });
+    };
+    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
 }
 
 // One weighted Jacobi sweep xout = xin + omega (b - A xin) / d, or the first
 // sweep from zero xout = omega b / d when xin_slot < 0 (vcycle.py:32-43).
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_vc_smooth(WorkList wl, const CUtensorMap* maps, int xin_slot, const T* __restrict__ P,
             const T* __restrict__ b, T* xout, double omega, const InstState* st, int* err) {
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP = sc.take<T>(kNH * kBH * kBW);
-    T* sX = sc.take<T>(kBH * kBW);
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
-        if (st && st[g.inst].status != kRunning) continue;
-        if (xin_slot >= 0) {
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                fence_proxy_async();
-                mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(T));
-                tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
-                tma_load_2d(sX, map_of(maps, g, xin_slot), c.x0 - kBOX, c.y0 - 2, tma.bar);
-            }
-            if (!tma.wait()) return;
+    T* sP[2];
+    T* sX[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kBH * kBW);
+        sX[k] = sc.take<T>(kBH * kBW);
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        if (xin_slot < 0) {
+            mbar_expect_tx(&pipe.bar[bb], 0);
+            return;
         }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
-            const int y = c.y0 + ly, x = c.x0 + lx;
+        mbar_expect_tx(&pipe.bar[bb], (kNH + 1) * kBH * kBW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapPlF), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sX[bb], map_of(maps, g, xin_slot), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        {
+            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+            const int y = m.y0 + ly, x = m.x0 + lx;
             if (y < g.h && x < g.w) {
                 const int64_t i = g.voff + (int64_t)y * g.pitch + x;
                 T out;
                 if (xin_slot >= 0) {
                     const int q = (ly + 2) * kBW + lx + kBOX;
-                    const T ax = stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
-                    out = sX[q] + (T)omega * (b[i] - ax) / sP[q];
+                    const T ax = stencil_at<T>(sP[bb], kBH, sX[bb], ly + 2, lx + kBOX);
+                    out = sX[bb][q] + (T)omega * (b[i] - ax) / sP[bb][q];
                 } else {
                     out = (T)omega * b[i] / P[g.poff + (int64_t)y * g.pitch + x];
                 }
                 xout[i] = out;
             }
         }
-    }
+    };
+    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, NoFlush());
 }
 
 // Coarsest level: x = A^{-1} b with the inverse precomputed per image
@@ -633,36 +767,38 @@ __global__ void k_vc_direct(const DirectDesc* dd, int count, const T* __restrict
     }
 }
 
-// y = A x on pitched vectors (no reductions): used by A.dot(x). x is the
-// level-0 b buffer (map slot kMapBF).
+// y = A x on pitched vectors (no reductions): used by A.dot(x) and by the
+// benchmark's apply timing. x is the level-0 b buffer (map slot kMapBF).
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_apply(WorkList wl, const CUtensorMap* maps, T* y, int* err) {
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP = sc.take<T>(kNH * kBH * kBW);
-    T* sX = sc.take<T>(kBH * kBW);
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(T));
-            tma_load_3d(sP, map_of(maps, g, kMapPlF), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
-            tma_load_2d(sX, map_of(maps, g, kMapBF), c.x0 - kBOX, c.y0 - 2, tma.bar);
-        }
-        if (!tma.wait()) return;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
-            const int yy = c.y0 + ly, xx = c.x0 + lx;
-            if (yy < g.h && xx < g.w)
-                y[g.voff + (int64_t)yy * g.pitch + xx] = stencil_at<T>(sP, kBH, sX, ly + 2, lx + kBOX);
-        }
+    T* sP[2];
+    T* sX[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kBH * kBW);
+        sX[k] = sc.take<T>(kBH * kBW);
     }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        mbar_expect_tx(&pipe.bar[bb], (kNH + 1) * kBH * kBW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapPlF), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sX[bb], map_of(maps, g, kMapBF), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        {
+            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+            const int yy = m.y0 + ly, xx = m.x0 + lx;
+            if (yy < g.h && xx < g.w)
+                y[g.voff + (int64_t)yy * g.pitch + xx] =
+                    stencil_at<T>(sP[bb], kBH, sX[bb], ly + 2, lx + kBOX);
+        }
+    };
+    tile_loop<kTY, kTX>(wl, nullptr, pipe, s_m, s_g, issue, body, NoFlush());
 }
 
 // --------------------------------------------------------------------------
@@ -836,41 +972,38 @@ __global__ void k_unpack(const GridDesc* grids, int ngrids, const int64_t* user_
 // r64 = b - A64 x64 in FP64; finaliser runs the outer convergence test and
 // (re)starts the inner FP32 solve on r32 = (float) r64 with x32 = 0.
 template <int PREC>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
 k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict__ P32,
                   const double* __restrict__ b, float* r32, float* x32, float* z32,
                   InstState* outer, InstState* inner, double* partials, double atol, double rtol,
                   double inner_rtol, int maxiter, int max_outer, int* err) {
     __shared__ double s_red[3 * 32];
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    double* sP = sc.take<double>(kNH * kBH * kBW);
-    double* sX = sc.take<double>(kBH * kBW);
-    Tma tma;
-    tma.init(&s_bar, err);
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const TileCoord c = tile_coord<kTY, kTX>(wl, t);
-        const GridDesc g = wl.grids[c.g];
-        InstState* so = outer + g.inst;
-        InstState* si = inner + g.inst;
-        if (so->status != kRunning) continue;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(tma.bar, (kNH + 1) * kBH * kBW * sizeof(double));
-            tma_load_3d(sP, map_of(maps, g, kMapP64F), c.x0 - kBOX, c.y0 - 2, 0, tma.bar);
-            tma_load_2d(sX, map_of(maps, g, kMapX64F), c.x0 - kBOX, c.y0 - 2, tma.bar);
-        }
-        if (!tma.wait()) return;
-        double v[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int lx = threadIdx.x & 63, ly = (threadIdx.x >> 6) + 4 * k;
-            const int y = c.y0 + ly, xx = c.x0 + lx;
+    double* sP[2];
+    double* sX[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<double>(kNH * kBH * kBW);
+        sX[k] = sc.take<double>(kBH * kBW);
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    double v[3] = {0.0, 0.0, 0.0};
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        mbar_expect_tx(&pipe.bar[bb], (kNH + 1) * kBH * kBW * sizeof(double));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapP64F), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sX[bb], map_of(maps, g, kMapX64F), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        {
+            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+            const int y = m.y0 + ly, xx = m.x0 + lx;
             if (y < g.h && xx < g.w) {
                 const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
                 const double bi = b[i];
-                const double ri = bi - stencil_at<double>(sP, kBH, sX, ly + 2, lx + kBOX);
+                const double ri = bi - stencil_at<double>(sP[bb], kBH, sX[bb], ly + 2, lx + kBOX);
                 const float rf = (float)ri;
                 r32[i] = rf;
                 x32[i] = 0.0f;
@@ -885,8 +1018,11 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
                 }
             }
         }
-        const int t0 = wl.tile_start[c.g], t1 = wl.tile_start[c.g + 1];
-        tile_reduce<3>(v, partials, wl.total, t, t0, t1, so, s_red, [&](double* sum) {
+    };
+    auto flush = [&](const Meta& m, unsigned int mine) {
+        InstState* so = outer + m.inst;
+        InstState* si = inner + m.inst;
+        cta_flush<3>(v, partials, m.inst, m.t0, m.t1, mine, so, s_red, [&](double* sum) {
             const double nb = sqrt(sum[0]);
             const double nr = sqrt(sum[1]);
             if (so->iters == 0) {
@@ -911,25 +1047,24 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
                 si->status = kSkip;
             }
         });
-    }
+    };
+    tile_loop<kTY, kTX>(wl, outer, pipe, s_m, s_g, issue, body, flush);
 }
 
 // x64 += x32 for images whose refinement is still running.
 __global__ void __launch_bounds__(kThreads)
 k_refine_correct(WorkList wl, double* x64, const float* __restrict__ x32, const InstState* outer) {
-    for (int t = blockIdx.x; t < wl.total; t += gridDim.x) {
-        const FlatCoord f = flat_coord(wl, t);
-        const GridDesc g = wl.grids[f.g];
-        if (outer[g.inst].status != kRunning) continue;
+    auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
 #pragma unroll
         for (int k = 0; k < kFlat / kThreads; ++k) {
-            const int64_t e = f.e0 + threadIdx.x + k * kThreads;
-            if (e >= f.e1) break;
+            const int64_t e = e0 + threadIdx.x + k * kThreads;
+            if (e >= e1) break;
             if ((int)(e % g.pitch) >= g.w) continue;
             const int64_t i = g.voff + e;
             x64[i] += (double)x32[i];
         }
-    }
+    };
+    flat_loop(wl, outer, body, [](int, int, int, unsigned int) {});
 }
 
 __global__ void k_refine_count(InstState* outer, int n) {
@@ -941,18 +1076,30 @@ __global__ void k_refine_count(InstState* outer, int n) {
 // Launchers
 // --------------------------------------------------------------------------
 
-template <typename T> size_t smem_apply() { return 128 * 4 + (kNH + 2) * kBH * kBW * sizeof(T); }
-template <typename T> size_t smem_init() { return 128 * 4 + (kNH + 1) * kBH * kBW * sizeof(T); }
+// Shared-memory sizes; they follow the SmemCarve layout of each kernel (two
+// pipeline buffers, every piece rounded up to 128 bytes).
+static inline size_t rup(size_t b) { return (b + 127) & ~size_t(127); }
+template <typename T> size_t smem_apply() {
+    return 2 * (rup(kNH * kBH * kBW * sizeof(T)) + 2 * rup(kBH * kBW * sizeof(T))) + 128;
+}
+template <typename T> size_t smem_init() {
+    return 2 * (rup(kNH * kBH * kBW * sizeof(T)) + rup(kBH * kBW * sizeof(T))) + 128;
+}
 template <typename T> size_t smem_down(int pre) {
     constexpr int CY = Coarse<T>::CY;
     constexpr int DH = 2 * CY + 5;
-    size_t s = 128 * 6 + (size_t)DH * kBW * sizeof(T) + (size_t)(2 * CY + 1) * (2 * kCX + 1) * sizeof(T);
-    if (pre != 0) s += (size_t)(kNH + 1) * DH * kBW * sizeof(T);
-    return s;
+    size_t per = rup(DH * kBW * sizeof(T));
+    if (pre != 0) per += rup(kNH * DH * kBW * sizeof(T));
+    if (pre > 1) per += rup(DH * kBW * sizeof(T));
+    size_t s = 2 * per + rup((size_t)(2 * CY + 1) * (2 * kCX + 1) * sizeof(T));
+    if (pre == 1) s += rup(DH * kBW * sizeof(T));
+    return s + 128;
 }
 template <typename T> size_t smem_up(int pre) {
-    return 128 * 6 + (size_t)(kNH + 1 + (pre > 1 ? 1 : 0)) * kBH * kBW * sizeof(T) +
-           (size_t)kCBH * kCBW * sizeof(T);
+    size_t per = rup(kNH * kBH * kBW * sizeof(T)) + rup(kBH * kBW * sizeof(T)) +
+                 rup(kCBH * kCBW * sizeof(T));
+    if (pre > 1) per += rup(kBH * kBW * sizeof(T));
+    return 2 * per + 128;
 }
 
 // Raise the dynamic shared-memory limit of a kernel. Done once for every
@@ -970,7 +1117,7 @@ void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUte
     do {                                                                                        \
         const size_t sm = X0 ? smem_init<T>() : 128;                                            \
                                                                                     \
-        k_cg_init<T, PK, X0><<<L.grid, kThreads, sm, s>>>(wl, maps, P, b, x, r, z, st, part,   \
+        k_cg_init<T, PK, X0><<<L.grid, kTileThreads, sm, s>>>(wl, maps, P, b, x, r, z, st, part,   \
                                                           atol, rtol, maxiter, err);            \
     } while (0)
     if (have_x0) {
@@ -989,7 +1136,7 @@ template <typename T>
 void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, int zslot,
                      T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s) {
     const size_t sm = smem_apply<T>();
-    k_cg_apply<T><<<L.grid, kThreads, sm, s>>>(wl, maps, zslot, p0, p1, Ap, st, part, err);
+    k_cg_apply<T><<<L.grid, kTileThreads, sm, s>>>(wl, maps, zslot, p0, p1, Ap, st, part, err);
 }
 
 template <typename T>
@@ -1018,7 +1165,7 @@ void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridD
 #define PMB_DOWN(PK)                                                                         \
     do {                                                                                     \
                                                                                     \
-        k_vc_down<T, PK><<<L.grid, kThreads, sm, s>>>(wl, fine, maps, xs_slot, bc, omega, st, err); \
+        k_vc_down<T, PK><<<L.grid, kTileThreads, sm, s>>>(wl, fine, maps, xs_slot, bc, omega, st, err); \
     } while (0)
     if (pk == 0) PMB_DOWN(0);
     else if (pk == 1) PMB_DOWN(1);
@@ -1037,7 +1184,7 @@ void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, con
 #define PMB_UP(PK, QK)                                                                       \
     do {                                                                                     \
                                                                                     \
-        k_vc_up<T, PK, QK><<<L.grid, kThreads, sm, s>>>(wl, coarse, maps, xs_slot, b, xout,   \
+        k_vc_up<T, PK, QK><<<L.grid, kTileThreads, sm, s>>>(wl, coarse, maps, xs_slot, b, xout,   \
                                                         omega, st, level0, dr, reorth, part, err); \
     } while (0)
     if (pk == 0 && qk == 0) PMB_UP(0, 0);
@@ -1054,7 +1201,7 @@ void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const CUtensorMap*
                       int xin_slot, const T* P, const T* b, T* xout, double omega,
                       const InstState* st, int* err, cudaStream_t s) {
     const size_t sm = smem_init<T>();
-    k_vc_smooth<T><<<L.grid, kThreads, sm, s>>>(wl, maps, xin_slot, P, b, xout, omega, st, err);
+    k_vc_smooth<T><<<L.grid, kTileThreads, sm, s>>>(wl, maps, xin_slot, P, b, xout, omega, st, err);
 }
 
 template <typename T>
@@ -1067,7 +1214,7 @@ template <typename T>
 void launch_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, T* y, int* err,
                   cudaStream_t s) {
     const size_t sm = smem_init<T>();
-    k_apply<T><<<L.grid, kThreads, sm, s>>>(wl, maps, y, err);
+    k_apply<T><<<L.grid, kTileThreads, sm, s>>>(wl, maps, y, err);
 }
 
 template <typename TS, typename TD>
@@ -1116,7 +1263,7 @@ void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl,
 #define PMB_RR(PK)                                                                              \
     do {                                                                                        \
                                                                                     \
-        k_refine_residual<PK><<<L.grid, kThreads, sm, s>>>(wl, maps, P32, b, r32, x32, z32,    \
+        k_refine_residual<PK><<<L.grid, kTileThreads, sm, s>>>(wl, maps, P32, b, r32, x32, z32,    \
                                                            outer, inner, part, atol, rtol,      \
                                                            inner_rtol, maxiter, max_outer, err); \
     } while (0)
