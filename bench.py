@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["1080p", "4096", "batch64"], default="1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["apply", "solve"], default=None,
+                    help="profiling case: a few operator applies, or one solve per precision")
     return ap.parse_args()
 
 
@@ -212,6 +214,24 @@ def cpu_baseline(img, tri):
                       "%.1f s" % (tri.shape[1], tri.shape[0], iters, dt)}, x
 
 
+def run_profile_case(args, imgs_d, tris_d, npx):
+    """Small fixed cases for ncu captures (no timing is reported)."""
+    import torch
+    from pymatting_b200.batch import AlphaBatch
+    out = {"profile": args.profile, "workload": args.workload, "pixels": int(npx)}
+    for precision in ["fp64", "mixed"]:
+        batch = AlphaBatch(imgs_d, tris_d, precision=precision)
+        if args.profile == "apply":
+            batch.system.time_apply(2)
+        else:
+            batch.solve()
+            st = batch.stats()[0]
+            out[precision] = {"iters": st.iters, "outer": st.outer_iters,
+                              "launches": batch.system.launch_count()}
+        torch.cuda.synchronize()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -239,6 +259,9 @@ def main():
     npx = sum(t.size for t in tris)
     imgs_d = [torch.as_tensor(i, device=dev) for i in imgs]
     tris_d = [torch.as_tensor(t, device=dev) for t in tris]
+    if args.profile:
+        run_profile_case(args, imgs_d, tris_d, npx)
+        return
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
     def device_step(precision):

@@ -322,8 +322,11 @@ static int plan_stencil(Stencil& S) {
         if (!lv.fine.starts.empty()) maxt = std::max<int64_t>(maxt, lv.fine.starts.back());
         if (!lv.flat.starts.empty()) maxt = std::max<int64_t>(maxt, lv.flat.starts.back());
     }
-    S.partials_count = maxt;
-    S.o_part = c.take<double>(3 * maxt);
+    // Per-CTA partial sums: partials[(image * 3 + q) * G + cta] for the
+    // largest persistent grid G of any list (at most 148 SMs x 8 CTAs).
+    const int64_t gmax = std::min<int64_t>(maxt, 148 * 8);
+    S.partials_count = std::max<int64_t>(maxt, (int64_t)n * gmax);
+    S.o_part = c.take<double>(3 * S.partials_count);
     S.o_uoff = c.take<int64_t>(n + 1);
     S.o_status = c.take<int>(4);
     S.o_err = c.take<int>(4);
@@ -585,7 +588,9 @@ static int setup_stencil(Stencil& S) {
     int status = 0;
     PMB_CUDA(cudaMemcpyAsync(&status, S.ws + S.o_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     PMB_CUDA(cudaStreamSynchronize(s));
-    if (status) return fail(kErrState, "coarsest multigrid operator is singular");
+    // A non-finite operator (non-finite image data) is not fatal here: the
+    // solve stops that image alone with status kNonFinite.
+    if (status == 2) return fail(kErrState, "coarsest multigrid operator is singular");
     S.setup_done = true;
     return 0;
 }

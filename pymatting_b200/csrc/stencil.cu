@@ -862,7 +862,8 @@ __global__ void k_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int
 }
 
 // Dense inverse of the coarsest operator by Gauss-Jordan elimination with
-// partial pivoting. One CTA per image; n <= kMaxDirect.
+// partial pivoting. One CTA per image; n <= kMaxDirect. *status is raised to
+// 2 on an exactly zero pivot and to 1 on a non-finite one.
 __global__ void k_dense_inverse(const DirectDesc* dd, int count, const double* __restrict__ Pc,
                                 double* work, int* status) {
     if ((int)blockIdx.x >= count) return;
@@ -893,7 +894,10 @@ __global__ void k_dense_inverse(const DirectDesc* dd, int count, const double* _
             }
             s_piv = best;
             s_pval = A[(int64_t)best * n + k];
-            if (bv == 0.0 || !isfinite(bv)) atomicExch(status, 1);
+            // 2: exactly singular (fatal for the setup); 1: non-finite
+            // entries, which the solve reports per image as kNonFinite.
+            if (bv == 0.0) atomicMax(status, 2);
+            else if (!isfinite(bv)) atomicMax(status, 1);
         }
         __syncthreads();
         const int pr = s_piv;
