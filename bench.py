@@ -38,7 +38,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["1080p", "4096", "batch64"], default="1080p")
@@ -79,7 +79,11 @@ def make_inputs(workload, rank):
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples nvidia-smi clocks and throttle reasons (every 100 ms).
+
+    Started before the warm-up so that the sampler's own start-up never falls
+    inside a timed region; only samples taken inside the timed windows are
+    reported."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -88,10 +92,12 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []       # (time, line)
+        self.windows = []     # (t0, t1) of timed regions
         self.thread = None
+        self.first = threading.Event()
 
-    def start(self):
+    def start(self, wait=5.0):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
@@ -102,10 +108,15 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        self.first.wait(wait)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+            self.first.set()
+
+    def window(self, t0, t1):
+        self.windows.append((t0, t1))
 
     def stop(self):
         if self.proc is None:
@@ -117,9 +128,11 @@ class ClockSampler:
             self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
+        inside = [ln for (t, ln) in self.lines
+                  if any(a <= t <= b for (a, b) in self.windows)]
         sm, smax, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -132,7 +145,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
-            return None
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
@@ -263,6 +276,7 @@ def main():
         run_profile_case(args, imgs_d, tris_d, npx)
         return
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    clocks = ClockSampler(local)
 
     def device_step(precision):
         batch = AlphaBatch(imgs_d, tris_d, precision=precision)
@@ -272,6 +286,7 @@ def main():
 
     def timed(fn, steps):
         times, info = [], None
+        t_start = time.time()
         for _ in range(steps):
             flush.fill_(1.0)
             torch.cuda.synchronize()
@@ -282,6 +297,7 @@ def main():
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
+        clocks.window(t_start, time.time())
         return times, info
 
     def barrier():
@@ -297,16 +313,12 @@ def main():
         return v
 
     results = {}
-    clocks = ClockSampler(local)
+    clocks.start()
     for precision in ["fp64", "mixed"]:
         for _ in range(args.warmup):
             device_step(precision)
         barrier()
-        if precision == "mixed":
-            clocks.start()
         times, info = timed(lambda: device_step(precision), args.steps)
-        if precision == "mixed":
-            clock_rec = clocks.stop()
         barrier()
         total_ms = max_over_ranks(sum(times))
         batch = info[0]
@@ -330,6 +342,7 @@ def main():
     barrier()
     e2e_times, _ = timed(lambda: solve_alpha(imgs, tris, precision="mixed"), args.steps)
     e2e_ms = max_over_ranks(sum(e2e_times))
+    clock_rec = clocks.stop()
 
     # Roofline of the Laplacian apply (the operator kernel of the solve).
     peak, peak_kind = measured_peaks()

@@ -75,9 +75,12 @@ class StencilSystem:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and _ffi._lib is not None:
-            _ffi.lib().pmb_stencil_destroy(h)
-            self._h = None
+        self._h = None
+        try:
+            if h is not None and _ffi._lib is not None:
+                _ffi.lib().pmb_stencil_destroy(h)
+        except (AttributeError, TypeError):
+            pass    # interpreter shutdown: module globals already cleared
 
     def setup(self):
         _ffi.check(_ffi.lib().pmb_stencil_setup(self._h, dev.stream()), "pmb_stencil_setup")
@@ -167,9 +170,12 @@ class CsrSystem:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and _ffi._lib is not None:
-            _ffi.lib().pmb_csr_destroy(h)
-            self._h = None
+        self._h = None
+        try:
+            if h is not None and _ffi._lib is not None:
+                _ffi.lib().pmb_csr_destroy(h)
+        except (AttributeError, TypeError):
+            pass    # interpreter shutdown: module globals already cleared
 
     def row(self, k):
         return self.vectors[k]
@@ -225,9 +231,12 @@ class IcholFactor:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and _ffi._lib is not None:
-            _ffi.lib().pmb_ichol_destroy(h)
-            self._h = None
+        self._h = None
+        try:
+            if h is not None and _ffi._lib is not None:
+                _ffi.lib().pmb_ichol_destroy(h)
+        except (AttributeError, TypeError):
+            pass    # interpreter shutdown: module globals already cleared
 
     def factor(self, csc, discard_threshold, shift, max_nnz, relative_discard_threshold,
                diag_keep_discarded):
