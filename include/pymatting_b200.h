@@ -145,6 +145,18 @@ int pmb_trimap_masks(const double* trimap, int64_t n, double fg_threshold, doubl
 /* Compact index of every unknown pixel (exclusive scan); cidx[n] = #unknown. */
 int pmb_unknown_index(const uint8_t* is_known, int64_t n, int64_t* cidx, int64_t* scratch,
                       void* stream);
+/* Same result as pmb_unknown_index, but allocates nothing and takes no
+ * scratch: for callers that cannot call cudaMalloc (a host program that
+ * hands the library only buffers from its own fixed, pre-sized pool, or a
+ * binding with no device allocator). No counterpart in the reference. The
+ * scan's scratch is a 256 KB array inside the library, present on every
+ * device that loads it until the process exits; n is limited to
+ * PMB_UNKNOWN_INDEX_STATIC_MAX_N (larger n fails with status -1). The first
+ * call on a device looks up the array's device address; make that first
+ * call before any stream capture. Calls share the array, so calls whose work
+ * overlaps on the GPU race; order them on one stream. */
+#define PMB_UNKNOWN_INDEX_STATIC_MAX_N 33553407
+int pmb_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t* cidx, void* stream);
 /* L_U = L[U, :][:, U] and b_U = -L[U, :][:, K] is_fg[K] from the ELL of the
  * Laplacian assembled with is_known (estimate_alpha_cf.py:64-74). */
 int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, const int64_t* cidx,

@@ -31,6 +31,7 @@ _SIGNATURES = {
     "pmb_ell_csr_fill": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
     "pmb_trimap_masks": (c_int, [c_vp, c_i64, c_dbl, c_dbl, c_vp, c_vp, c_vp, c_vp]),
     "pmb_unknown_index": (c_int, [c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "pmb_unknown_index_static": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "pmb_hard_lu_rowptr": (c_int, [c_vp, c_int, c_int, c_vp, c_i64, c_vp, c_vp, c_vp]),
     "pmb_hard_lu_fill": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
                                  c_vp]),

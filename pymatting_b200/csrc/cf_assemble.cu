@@ -494,3 +494,61 @@ int pmb_launch_trimap_masks(const double* trimap, int64_t n, double fg_thr, doub
                                                                is_known, counts);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
+
+// --------------------------------------------------------------------------
+// Unknown-pixel index without caller scratch
+// --------------------------------------------------------------------------
+//
+// For callers that must not allocate device memory, the chunk totals of the
+// scan live in a fixed array of this file instead of a caller buffer. The
+// array is 256 KB and exists on every device that loads the library, for the
+// life of the process. The scan writes every element it reads within the same
+// call (chunk sums, then the total), so nothing in it has to start at zero.
+// All calls share the array: two calls whose work overlaps on the GPU (on
+// different streams, or from different threads) race on it.
+
+#include <mutex>
+
+namespace pmb {
+
+constexpr int64_t kStaticScanElems = 32768;
+static __device__ __align__(256) int64_t g_static_scan[kStaticScanElems];
+
+}  // namespace pmb
+
+// Largest n: the scan of n + 1 entries needs one chunk sum per 1024 entries
+// plus one slot for the total.
+int64_t pmb_static_scan_max_n() { return (pmb::kStaticScanElems - 1) * 1024 - 1; }
+
+// Device address of the array on the current device. Host code only knows a
+// host-side stand-in for g_static_scan, so the address is looked up with
+// cudaGetSymbolAddress, once per device (the first call on a device does it).
+static int static_scan_address(int64_t** out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int64_t* addr[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -2;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, pmb::g_static_scan) != cudaSuccess || !p) return -3;
+        addr[dev] = static_cast<int64_t*>(p);
+    }
+    *out = addr[dev];
+    return 0;
+}
+
+// cidx = exclusive scan of the unknown flags of is_known, cidx[n] = count,
+// with the scan's scratch in g_static_scan. Returns 0, -1 (n too large),
+// -2 (CUDA error) or -3 (the array's address could not be found).
+int pmb_launch_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t* cidx,
+                                    cudaStream_t s) {
+    if (n > pmb_static_scan_max_n()) return -1;
+    int64_t* scratch = nullptr;
+    if (int rc = static_scan_address(&scratch)) return rc;
+    const int64_t nchunks = (n + 1 + 1023) / 1024;
+    if (cudaMemsetAsync(cidx + n, 0, sizeof(int64_t), s) != cudaSuccess) return -2;
+    if (pmb_launch_flag_unknown(is_known, n, cidx, s)) return -2;
+    return pmb_scan_exclusive(cidx, n + 1, scratch, scratch + nchunks, s);
+}

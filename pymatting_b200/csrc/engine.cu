@@ -937,6 +937,26 @@ PMB_API int pmb_unknown_index(const uint8_t* is_known, int64_t n, int64_t* cidx,
     return 0;
 }
 
+int64_t pmb_static_scan_max_n();
+int pmb_launch_unknown_index_static(const uint8_t*, int64_t, int64_t*, cudaStream_t);
+
+// pmb_unknown_index for callers that cannot allocate device memory: the
+// scan's scratch is a fixed array inside the library (cf_assemble.cu).
+PMB_API int pmb_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t* cidx,
+                                     void* stream) {
+    if (!is_known || !cidx || n <= 0) return fail(kErrArg, "pmb_unknown_index_static: bad arguments");
+    if (n > pmb_static_scan_max_n())
+        return fail(kErrArg, "pmb_unknown_index_static: n = " + std::to_string(n) +
+                                 " exceeds the built-in scratch limit of " +
+                                 std::to_string(pmb_static_scan_max_n()) +
+                                 " pixels; use pmb_unknown_index with caller scratch");
+    const int rc = pmb_launch_unknown_index_static(is_known, n, cidx, (cudaStream_t)stream);
+    if (rc == -3) return fail(kErrCuda, "pmb_unknown_index_static: scratch address lookup failed");
+    if (rc) return fail(kErrCuda, std::string("pmb_unknown_index_static: ") +
+                                      cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 PMB_API int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, const int64_t* cidx,
                                int64_t n_unknown, int64_t* rowptr, int64_t* scratch, void* stream) {
     if (!is_known || !cidx || !rowptr || !scratch || h <= 0 || w <= 0)
