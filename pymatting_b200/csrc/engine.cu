@@ -165,11 +165,14 @@ struct Stencil {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     int graph_reorth = -1;
+    double graph_delta = -1.0;
+    int graph_max_outer = -1;
+    double delta = 1e-4;            // mixed: FP32 phase reduction before a residual replacement
+    int max_outer = 50;             // mixed: most residual replacements
     int64_t graph_kernels = 0;      // kernel nodes of one graph replay
     bool bound = false, setup_done = false;
     // last solve
     int64_t launches = 0;
-    std::vector<int> inner_total;   // mixed: inner iterations over all steps
 
     template <typename T> T* at(size_t off) const { return reinterpret_cast<T*>(ws + off); }
     InstState* state() const { return at<InstState>(o_state); }
@@ -721,9 +724,21 @@ static void cg_iteration(Stencil& S, int reorth) {
     const int zslot = S.precond == kPrecNone ? kMapBF : kMapZF;
     launch_cg_apply<T>(LaunchCfg{persistent_grid(S.fine0)}, S.fine0.wl, S.maps(), zslot, v.p0, v.p1,
                        v.ap, st, S.partials(), S.err(), s);
+    const bool mixed = S.precision == 1;
     launch_cg_update<T>(S.precond, LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, v.P, v.x, v.r,
-                        v.z, v.p0, v.p1, v.ap, v.dr, reorth, st, S.partials(), s);
+                        v.z, v.p0, v.p1, v.ap, v.dr, reorth, mixed ? 1 : 0, st, S.partials(), s);
     S.launches += 2;
+    if (mixed) {
+        // Residual replacement for the images whose FP32 phase just ended.
+        HostList& a = S.fine0;
+        launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl,
+                              S.at<double>(S.o_x64), S.at<float>(S.o_xin32), st, s);
+        launch_refine_residual(S.precond, 0, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(),
+                               S.at<float>(S.o_P032), S.at<double>(S.o_b64), S.at<float>(S.o_r32),
+                               S.at<float>(S.o_xin32), S.at<float>(S.o_z32), S.outer(), st,
+                               S.partials(), 0.0, 0.0, S.delta, 0, S.max_outer, S.err(), s);
+        S.launches += 2;
+    }
     if (S.precond == kPrecVcycle) run_vcycle<T>(S, v.r, v.z, st, v.dr, reorth);
 }
 
@@ -749,7 +764,8 @@ static bool any_running(const InstState* st, int n) {
 template <typename T>
 static int iterate(Stencil& S, int reorth, int maxiter) {
     const int chunk = 4;
-    if (!S.graph || S.graph_reorth != reorth || S.graph_iters != chunk) {
+    if (!S.graph || S.graph_reorth != reorth || S.graph_iters != chunk ||
+        S.graph_delta != S.delta || S.graph_max_outer != S.max_outer) {
         if (S.graph) {
             cudaGraphExecDestroy(S.graph);
             S.graph = nullptr;
@@ -764,6 +780,8 @@ static int iterate(Stencil& S, int reorth, int maxiter) {
         cudaGraphDestroy(g);
         S.graph_iters = chunk;
         S.graph_reorth = reorth;
+        S.graph_delta = S.delta;
+        S.graph_max_outer = S.max_outer;
         S.graph_kernels = (int64_t)nodes;
         // Capture only recorded the launches; they did not run.
         S.launches -= (int64_t)nodes;
@@ -807,7 +825,10 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
                                     S.user_total, s);
     else
         PMB_CUDA(cudaMemsetAsync(x64, 0, sizeof(double) * S.levels[0].vec_elems, s));
-    // Outer state: iters counts refinement steps; status running.
+    S.delta = inner_rtol;
+    S.max_outer = max_outer;
+    // Outer state: every image starts running; its first FP64 residual sets
+    // |b|, the tolerance and the first FP32 phase.
     std::vector<InstState> init(S.nimg);
     for (auto& o : init) {
         std::memset(&o, 0, sizeof(o));
@@ -815,23 +836,16 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
     }
     PMB_CUDA(cudaMemcpyAsync(S.outer(), init.data(), sizeof(InstState) * S.nimg,
                              cudaMemcpyHostToDevice, s));
-    PMB_CUDA(cudaStreamSynchronize(s));
-    S.inner_total.assign(S.nimg, 0);
-    for (int outer = 0;; ++outer) {
-        launch_refine_residual(S.precond, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), v.P,
-                               S.at<double>(S.o_b64), v.r, v.x, v.z, S.outer(), S.state(),
-                               S.partials(), atol, rtol, inner_rtol, maxiter, max_outer, S.err(), s);
-        S.launches += 1;
-        if (int rc = read_states(S, true)) return rc;
-        if (!any_running(S.h_outer, S.nimg)) break;
-        if (S.precond == kPrecVcycle) run_vcycle<float>(S, v.r, v.z, S.state(), v.dr, 0);
-        if (int rc = iterate<float>(S, reorth, maxiter)) return rc;
-        // Inner iterations of this refinement step, summed per image.
-        for (int k = 0; k < S.nimg; ++k) S.inner_total[k] += S.h_state[k].iters;
-        launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, x64, v.x, S.outer(),
-                              S.nimg, s);
-        S.launches += 2;
-    }
+    launch_refine_residual(S.precond, 1, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), v.P,
+                           S.at<double>(S.o_b64), v.r, v.x, v.z, S.outer(), S.state(),
+                           S.partials(), atol, rtol, inner_rtol, maxiter, max_outer, S.err(), s);
+    S.launches += 1;
+    if (S.precond == kPrecVcycle) run_vcycle<float>(S, v.r, v.z, S.state(), v.dr, 0);
+    if (int rc = iterate<float>(S, reorth, maxiter)) return rc;
+    // Fold the last FP32 correction into x64 (zero for converged images).
+    launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, x64, v.x, nullptr, s);
+    S.launches += 1;
+    if (int rc = read_states(S, true)) return rc;
     return check_err(S);
 }
 
@@ -1144,11 +1158,11 @@ PMB_API int pmb_stencil_stats(pmb_stencil* p, int image, int* iters, int* status
     if (!p || image < 0 || image >= p->S.nimg) return fail(kErrArg, "pmb_stencil_stats: bad image");
     Stencil& S = p->S;
     if (int rc = read_states(S, true)) return rc;
+    // Mixed precision: the FP32 state carries the final status (convergence
+    // is only declared on an FP64 residual); the norms are the FP64 ones.
     const InstState& st = S.precision == 1 ? S.h_outer[image] : S.h_state[image];
-    if (iters)
-        *iters = S.precision == 1 && (int)S.inner_total.size() == S.nimg ? S.inner_total[image]
-                                                                          : S.h_state[image].iters;
-    if (status) *status = st.status == kSkip ? kConverged : st.status;
+    if (iters) *iters = S.h_state[image].iters;
+    if (status) *status = S.h_state[image].status;
     if (norm_r) *norm_r = st.norm_r;
     if (norm_b) *norm_b = st.norm_b;
     if (outer_iters) *outer_iters = S.precision == 1 ? S.h_outer[image].iters : 0;

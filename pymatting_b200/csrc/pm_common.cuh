@@ -100,13 +100,19 @@ struct InstState {
     int iters;        // completed iterations
     int status;       // kRunning / kConverged / kMaxIter / kNonFinite
     int maxiter;
-    int flags;        // kFirst: p = z on the next apply
+    int flags;        // kFirst / kUpdate
     unsigned int counter;  // tiles finished in the current reduction
     int pad[3];
 };
 
 enum : int { kRunning = 0, kConverged = 1, kMaxIter = 2, kNonFinite = 3, kSkip = 4 };
-enum : int { kFirst = 1 };
+// flags: kFirst — p = z on the next apply; kUpdate — the FP32 recurrence
+// residual of a mixed-precision solve reached its phase tolerance and waits
+// for the FP64 residual replacement of this iteration.
+enum : int { kFirst = 1, kUpdate = 2 };
+// Which images a gated loop visits: running ones, or running ones that
+// wait for a residual replacement.
+enum : int { kGateRunning = 0, kGateUpdate = 1 };
 
 __device__ __forceinline__ int find_grid(const WorkList& wl, int tile) {
     int lo = 0, hi = wl.ngrids - 1;

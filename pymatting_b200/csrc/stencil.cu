@@ -53,7 +53,7 @@ struct Meta {
     double beta;          // CG: current beta
 };
 
-template <int H, int W>
+template <int H, int W, int GATE = kGateRunning>
 __device__ __forceinline__ void make_meta(const WorkList& wl, int t, const InstState* st,
                                           Meta& m, GridDesc& gd) {
     m.t = t;
@@ -73,7 +73,7 @@ __device__ __forceinline__ void make_meta(const WorkList& wl, int t, const InstS
     m.beta = 0.0;
     if (st) {
         const InstState& s = st[gd.inst];
-        m.run = s.status == kRunning;
+        m.run = s.status == kRunning && (GATE == kGateRunning || (s.flags & kUpdate) != 0);
         m.par = s.iters & 1;
         m.first = (s.flags & kFirst) != 0;
         m.beta = s.beta;
@@ -133,7 +133,7 @@ __device__ __forceinline__ T stencil_at(const T* P, int ph, const T* X, int r, i
 //   issue(meta, gd, buf)            thread 0 only
 //   body(meta, gd, buf)             all threads; returns nothing
 //   flush(meta, mine)               all threads, after an image's last tile
-template <int H, int W, typename Issue, typename Body, typename Flush>
+template <int H, int W, int GATE = kGateRunning, typename Issue, typename Body, typename Flush>
 __device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* st, Pipe& pipe,
                                           Meta* s_m, GridDesc* s_g, Issue issue, Body body,
                                           Flush flush) {
@@ -142,7 +142,7 @@ __device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* s
     int b = 0;
     unsigned int mine = 0;
     if (threadIdx.x == 0 && t < wl.total) {
-        make_meta<H, W>(wl, t, st, s_m[0], s_g[0]);
+        make_meta<H, W, GATE>(wl, t, st, s_m[0], s_g[0]);
         if (s_m[0].run) {
             fence_proxy_async();
             issue(s_m[0], s_g[0], 0);
@@ -151,7 +151,7 @@ __device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* s
     while (t < wl.total) {
         const int tn = t + G;
         if (threadIdx.x == 0 && tn < wl.total) {
-            make_meta<H, W>(wl, tn, st, s_m[b ^ 1], s_g[b ^ 1]);
+            make_meta<H, W, GATE>(wl, tn, st, s_m[b ^ 1], s_g[b ^ 1]);
             if (s_m[b ^ 1].run) {
                 fence_proxy_async();
                 issue(s_m[b ^ 1], s_g[b ^ 1], b ^ 1);
@@ -359,7 +359,7 @@ k_cg_apply(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap,
 // Element-wise loop over a flat work list (1024-element chunks) with the same
 // per-CTA, per-image flush as the tiled kernels. Chunks cover the pitched
 // rows; padding columns are skipped.
-template <typename Body, typename Flush>
+template <int GATE = kGateRunning, typename Body, typename Flush>
 __device__ __forceinline__ void flat_loop(const WorkList& wl, const InstState* st, Body body,
                                           Flush flush) {
     __shared__ int s_inst[2], s_run, s_t0, s_t1;
@@ -375,7 +375,12 @@ __device__ __forceinline__ void flat_loop(const WorkList& wl, const InstState* s
             s_t1 = wl.tile_start[g + 1];
             s_inst[0] = s_gd.inst;
             s_inst[1] = tn < wl.total ? wl.grids[find_grid(wl, tn)].inst : -1;
-            s_run = st ? st[s_gd.inst].status == kRunning : 1;
+            if (st) {
+                const InstState& q = st[s_gd.inst];
+                s_run = q.status == kRunning && (GATE == kGateRunning || (q.flags & kUpdate) != 0);
+            } else {
+                s_run = 1;
+            }
         }
         __syncthreads();
         if (s_run) {
@@ -401,7 +406,8 @@ __device__ __forceinline__ void flat_loop(const WorkList& wl, const InstState* s
 template <typename T, int PREC>
 __global__ void __launch_bounds__(kThreads)
 k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0, const T* p1,
-            const T* __restrict__ Ap, T* dr, int reorth, InstState* st, double* partials) {
+            const T* __restrict__ Ap, T* dr, int reorth, int reliable, InstState* st,
+            double* partials) {
     __shared__ double s_red[3 * 32];
     double v[3] = {0.0, 0.0, 0.0};
     auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
@@ -442,9 +448,15 @@ k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0,
             s->norm_r = nr;
             s->iters += 1;
             if (!isfinite(nr)) s->status = kNonFinite;
-            else if (nr < s->tol) s->status = kConverged;
-            else if (s->iters >= s->maxiter) s->status = kMaxIter;
-            if (s->status == kRunning && (PREC == kPrecJacobi || PREC == kPrecNone)) {
+            else if (nr < s->tol) {
+                // Mixed precision: the phase ends with an FP64 residual
+                // replacement (k_refine_residual, same iteration), which also
+                // finishes beta; otherwise the solve has converged.
+                if (reliable) s->flags |= kUpdate;
+                else s->status = kConverged;
+            } else if (s->iters >= s->maxiter) s->status = kMaxIter;
+            if (s->status == kRunning && !(s->flags & kUpdate) &&
+                (PREC == kPrecJacobi || PREC == kPrecNone)) {
                 if (reorth) finish_beta_reorth(s, sum[1], sum[2]);
                 else finish_beta(s, sum[1]);
             }
@@ -973,14 +985,28 @@ __global__ void k_unpack(const GridDesc* grids, int ngrids, const int64_t* user_
 // Iterative refinement around the FP32 inner solve
 // --------------------------------------------------------------------------
 
-// r64 = b - A64 x64 in FP64; finaliser runs the outer convergence test and
-// (re)starts the inner FP32 solve on r32 = (float) r64 with x32 = 0.
-template <int PREC>
+// Mixed precision: FP32 PCG with reliable updates (Sleijpen & van der Vorst,
+// 1996). The FP64 iterate x64 accumulates; the FP32 CG runs on the
+// correction x32 with its own recurrence residual r32. When |r32| has dropped
+// by `delta` since the last replacement (or below half the FP64 tolerance),
+// k_cg_update flags the image (kUpdate) and, in the same iteration,
+//   k_refine_correct   x64 += x32, x32 = 0
+//   k_refine_residual  r64 = b - A64 x64 (FP64 planes), r32 = (float) r64
+// replace the recurrence residual by the true one; CG then continues with the
+// same search direction (beta from the new r . z). Convergence is decided on
+// the FP64 residual only.
+constexpr double kReliableFloor = 0.5;   // phase tolerance floor, x the FP64 tolerance
+
+// r64 = b - A64 x64 in FP64, r32 = (float) r64. FIRST: the initial residual
+// (every image whose outer state runs): sets |b|, the FP64 tolerance and
+// starts the FP32 CG with x32 = 0. Otherwise only images flagged kUpdate:
+// the residual replacement described above.
+template <int PREC, bool FIRST>
 __global__ void __launch_bounds__(kTileThreads)
 k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict__ P32,
                   const double* __restrict__ b, float* r32, float* x32, float* z32,
                   InstState* outer, InstState* inner, double* partials, double atol, double rtol,
-                  double inner_rtol, int maxiter, int max_outer, int* err) {
+                  double delta, int maxiter, int max_outer, int* err) {
     __shared__ double s_red[3 * 32];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ Meta s_m[2];
@@ -1001,25 +1027,23 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
         tma_load_2d(sX[bb], map_of(maps, g, kMapX64F), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
     };
     auto body = [&](const Meta& m, const GridDesc& g, int bb) {
-        {
-            const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
-            const int y = m.y0 + ly, xx = m.x0 + lx;
-            if (y < g.h && xx < g.w) {
-                const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
-                const double bi = b[i];
-                const double ri = bi - stencil_at<double>(sP[bb], kBH, sX[bb], ly + 2, lx + kBOX);
-                const float rf = (float)ri;
-                r32[i] = rf;
-                x32[i] = 0.0f;
-                v[0] += bi * bi;
-                v[1] += ri * ri;
-                if (PREC == kPrecJacobi) {
-                    const float zi = rf * (1.0f / P32[g.poff + (int64_t)y * g.pitch + xx]);
-                    z32[i] = zi;
-                    v[2] += (double)rf * (double)zi;
-                } else if (PREC == kPrecNone) {
-                    v[2] += (double)rf * (double)rf;
-                }
+        const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+        const int y = m.y0 + ly, xx = m.x0 + lx;
+        if (y < g.h && xx < g.w) {
+            const int64_t i = g.voff + (int64_t)y * g.pitch + xx;
+            const double bi = b[i];
+            const double ri = bi - stencil_at<double>(sP[bb], kBH, sX[bb], ly + 2, lx + kBOX);
+            const float rf = (float)ri;
+            r32[i] = rf;
+            if (FIRST) x32[i] = 0.0f;
+            v[0] += bi * bi;
+            v[1] += ri * ri;
+            if (PREC == kPrecJacobi) {
+                const float zi = rf * (1.0f / P32[g.poff + (int64_t)y * g.pitch + xx]);
+                z32[i] = zi;
+                v[2] += (double)rf * (double)zi;
+            } else if (PREC == kPrecNone) {
+                v[2] += (double)rf * (double)rf;
             }
         }
     };
@@ -1027,37 +1051,48 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
         InstState* so = outer + m.inst;
         InstState* si = inner + m.inst;
         cta_flush<3>(v, partials, m.inst, m.t0, m.t1, mine, so, s_red, [&](double* sum) {
-            const double nb = sqrt(sum[0]);
             const double nr = sqrt(sum[1]);
-            if (so->iters == 0) {
+            if (FIRST) {
+                const double nb = sqrt(sum[0]);
                 so->norm_b = nb;
                 so->tol = fmax(atol, rtol * nb);
-            }
-            so->norm_r = nr;
-            if (!isfinite(nr)) so->status = kNonFinite;
-            else if (nr < atol || nr < rtol * so->norm_b) so->status = kConverged;
-            else if (so->iters >= max_outer) so->status = kMaxIter;
-            if (so->status == kRunning) {
-                si->norm_b = nr;
-                si->norm_r = nr;
-                si->tol = inner_rtol * nr;
+                so->iters = 0;
                 si->iters = 0;
                 si->maxiter = maxiter;
                 si->flags = kFirst;
                 si->beta = 0.0;
-                si->status = kRunning;
-                if (PREC != kPrecVcycle) si->rz = sum[2];
             } else {
-                si->status = kSkip;
+                so->iters += 1;
+                si->flags &= ~kUpdate;
+            }
+            so->norm_r = nr;
+            int status = kRunning;
+            if (!isfinite(nr)) status = kNonFinite;
+            else if (nr < atol || nr < so->tol) status = kConverged;
+            else if (so->iters >= max_outer) status = kMaxIter;
+            else if (!FIRST && si->iters >= si->maxiter) status = kMaxIter;
+            so->status = status;
+            si->status = status;
+            si->norm_r = nr;
+            if (status == kRunning) {
+                si->norm_b = nr;
+                si->tol = fmax(delta * nr, kReliableFloor * so->tol);
+                if (PREC != kPrecVcycle) {
+                    if (FIRST) si->rz = sum[2];
+                    else finish_beta(si, sum[2]);
+                }
             }
         });
     };
-    tile_loop<kTY, kTX>(wl, outer, pipe, s_m, s_g, issue, body, flush);
+    if (FIRST) tile_loop<kTY, kTX, kGateRunning>(wl, outer, pipe, s_m, s_g, issue, body, flush);
+    else tile_loop<kTY, kTX, kGateUpdate>(wl, inner, pipe, s_m, s_g, issue, body, flush);
 }
 
-// x64 += x32 for images whose refinement is still running.
+// x64 += x32, x32 = 0: for images flagged kUpdate (GATE = kGateUpdate), or
+// for every image (st == nullptr) at the end of a solve.
+template <int GATE>
 __global__ void __launch_bounds__(kThreads)
-k_refine_correct(WorkList wl, double* x64, const float* __restrict__ x32, const InstState* outer) {
+k_refine_correct(WorkList wl, double* x64, float* x32, const InstState* st) {
     auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
 #pragma unroll
         for (int k = 0; k < kFlat / kThreads; ++k) {
@@ -1066,15 +1101,12 @@ k_refine_correct(WorkList wl, double* x64, const float* __restrict__ x32, const 
             if ((int)(e % g.pitch) >= g.w) continue;
             const int64_t i = g.voff + e;
             x64[i] += (double)x32[i];
+            x32[i] = 0.0f;
         }
     };
-    flat_loop(wl, outer, body, [](int, int, int, unsigned int) {});
+    flat_loop<GATE>(wl, st, body, [](int, int, int, unsigned int) {});
 }
 
-__global__ void k_refine_count(InstState* outer, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && outer[i].status == kRunning) outer[i].iters += 1;
-}
 
 // --------------------------------------------------------------------------
 // Launchers
@@ -1145,12 +1177,12 @@ void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* 
 
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
-                      T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth,
+                      T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth, int reliable,
                       InstState* st, double* part, cudaStream_t s) {
     switch (prec) {
-    case kPrecNone: k_cg_update<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, st, part); break;
-    case kPrecJacobi: k_cg_update<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, st, part); break;
-    default: k_cg_update<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, st, part); break;
+    case kPrecNone: k_cg_update<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, st, part); break;
+    case kPrecJacobi: k_cg_update<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, st, part); break;
+    default: k_cg_update<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, st, part); break;
     }
 }
 
@@ -1257,30 +1289,33 @@ void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s
     k_convert_f32<<<blocks, 256, 0, s>>>(src, dst, n);
 }
 
-void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl,
+void launch_refine_residual(int prec, int first, const LaunchCfg& L, const WorkList& wl,
                             const CUtensorMap* maps, const float* P32, const double* b,
                             float* r32, float* x32, float* z32, InstState* outer,
                             InstState* inner, double* part, double atol, double rtol,
-                            double inner_rtol, int maxiter, int max_outer, int* err,
+                            double delta, int maxiter, int max_outer, int* err,
                             cudaStream_t s) {
     const size_t sm = smem_init<double>();
-#define PMB_RR(PK)                                                                              \
-    do {                                                                                        \
-                                                                                    \
-        k_refine_residual<PK><<<L.grid, kTileThreads, sm, s>>>(wl, maps, P32, b, r32, x32, z32,    \
-                                                           outer, inner, part, atol, rtol,      \
-                                                           inner_rtol, maxiter, max_outer, err); \
-    } while (0)
-    if (prec == kPrecNone) PMB_RR(kPrecNone);
-    else if (prec == kPrecJacobi) PMB_RR(kPrecJacobi);
-    else PMB_RR(kPrecVcycle);
+#define PMB_RR(PK, F)                                                                           \
+    k_refine_residual<PK, F><<<L.grid, kTileThreads, sm, s>>>(wl, maps, P32, b, r32, x32, z32,  \
+                                                              outer, inner, part, atol, rtol,   \
+                                                              delta, maxiter, max_outer, err)
+    if (first) {
+        if (prec == kPrecNone) PMB_RR(kPrecNone, true);
+        else if (prec == kPrecJacobi) PMB_RR(kPrecJacobi, true);
+        else PMB_RR(kPrecVcycle, true);
+    } else {
+        if (prec == kPrecNone) PMB_RR(kPrecNone, false);
+        else if (prec == kPrecJacobi) PMB_RR(kPrecJacobi, false);
+        else PMB_RR(kPrecVcycle, false);
+    }
 #undef PMB_RR
 }
 
-void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, const float* x32,
-                           InstState* outer, int ninst, cudaStream_t s) {
-    k_refine_correct<<<L.grid, kThreads, 0, s>>>(wl, x64, x32, outer);
-    k_refine_count<<<(ninst + 127) / 128, 128, 0, s>>>(outer, ninst);
+void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, float* x32,
+                           const InstState* inner, cudaStream_t s) {
+    if (inner) k_refine_correct<kGateUpdate><<<L.grid, kThreads, 0, s>>>(wl, x64, x32, inner);
+    else k_refine_correct<kGateRunning><<<L.grid, kThreads, 0, s>>>(wl, x64, x32, nullptr);
 }
 
 
@@ -1308,9 +1343,12 @@ void stencil_prepare() {
     if (done) return;
     prepare_type<double>();
     prepare_type<float>();
-    allow_smem(k_refine_residual<kPrecNone>, smem_init<double>());
-    allow_smem(k_refine_residual<kPrecJacobi>, smem_init<double>());
-    allow_smem(k_refine_residual<kPrecVcycle>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecNone, true>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecJacobi, true>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecVcycle, true>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecNone, false>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecJacobi, false>, smem_init<double>());
+    allow_smem(k_refine_residual<kPrecVcycle, false>, smem_init<double>());
     done = true;
 }
 
@@ -1321,7 +1359,7 @@ void stencil_prepare() {
     template void launch_cg_apply<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int,  \
                                      T*, T*, T*, InstState*, double*, int*, cudaStream_t);        \
     template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*,   \
-                                      T*, const T*, const T*, const T*, T*, int, InstState*,      \
+                                      T*, const T*, const T*, const T*, T*, int, int, InstState*, \
                                       double*, cudaStream_t);                                    \
     template void launch_cg_rz<T>(const LaunchCfg&, const WorkList&, const T*, const T*,          \
                                   const T*, int, InstState*, double*, cudaStream_t);             \

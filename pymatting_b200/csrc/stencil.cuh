@@ -38,7 +38,7 @@ void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* 
                      T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s);
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
-                      T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth,
+                      T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth, int reliable,
                       InstState* st, double* part, cudaStream_t s);
 template <typename T>
 void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z, const T* dr,
@@ -73,13 +73,14 @@ void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrid
 void launch_dense_inverse(const DirectDesc* dd, int count, const double* Pc, double* work,
                           int* status, cudaStream_t s);
 void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s);
-void launch_refine_residual(int prec, const LaunchCfg& L, const WorkList& wl,
+void launch_refine_residual(int prec, int first, const LaunchCfg& L, const WorkList& wl,
                             const CUtensorMap* maps, const float* P32, const double* b,
                             float* r32, float* x32, float* z32, InstState* outer,
                             InstState* inner, double* part, double atol, double rtol,
-                            double inner_rtol, int maxiter, int max_outer, int* err,
+                            double delta, int maxiter, int max_outer, int* err,
                             cudaStream_t s);
-void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, const float* x32,
-                           InstState* outer, int ninst, cudaStream_t s);
+// inner != nullptr: images flagged kUpdate; nullptr: every image.
+void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, float* x32,
+                           const InstState* inner, cudaStream_t s);
 
 }  // namespace pmb
