@@ -43,8 +43,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["1080p", "4096", "batch64"], default="1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", choices=["apply", "solve"], default=None,
-                    help="profiling case: a few operator applies, or one solve per precision")
+    ap.add_argument("--profile", choices=["apply", "solve", "solve-fp64", "solve-mixed"],
+                    default=None,
+                    help="profiling case: a few operator applies, or one solve per precision "
+                         "(or of one precision)")
     return ap.parse_args()
 
 
@@ -232,7 +234,9 @@ def run_profile_case(args, imgs_d, tris_d, npx):
     import torch
     from pymatting_b200.batch import AlphaBatch
     out = {"profile": args.profile, "workload": args.workload, "pixels": int(npx)}
-    for precision in ["fp64", "mixed"]:
+    precisions = {"solve-fp64": ["fp64"], "solve-mixed": ["mixed"]}.get(args.profile,
+                                                                      ["fp64", "mixed"])
+    for precision in precisions:
         batch = AlphaBatch(imgs_d, tris_d, precision=precision)
         if args.profile == "apply":
             batch.system.time_apply(2)

@@ -272,9 +272,14 @@ static int plan_stencil(Stencil& S) {
     }
     S.nmaps = map_base;
     // Work lists and the residency of the kernels that walk them.
-    const int per_fine = blocks_per_sm(mixed ? smem_apply<float>() : smem_apply<double>());
-    const int per_up = blocks_per_sm(mixed ? smem_up<float>(S.pre) : smem_up<double>(S.pre));
-    const int per_down = blocks_per_sm(mixed ? smem_down<float>(S.pre) : smem_down<double>(S.pre));
+    const bool vec_up = S.pre == 1 && S.post == 1, vec_down = S.pre == 1;
+    const int per_fine = blocks_per_sm(mixed ? smem_apply_v<float>() : smem_apply_v<double>());
+    const int per_up = blocks_per_sm(
+        vec_up ? (mixed ? smem_up_v<float>() : smem_up_v<double>())
+               : (mixed ? smem_up<float>(S.pre) : smem_up<double>(S.pre)));
+    const int per_down = blocks_per_sm(
+        vec_down ? (mixed ? smem_down_v<float>() : smem_down_v<double>())
+                 : (mixed ? smem_down<float>(S.pre) : smem_down<double>(S.pre)));
     build_list(S.fine0, S.levels[0].grids, {}, kTY, kTX);
     S.fine0.per_sm = per_fine;
     build_flat(S.flat0, S.levels[0].grids);
@@ -461,6 +466,7 @@ static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
     maps.assign((size_t)S.nmaps * kMapsPerGrid, CUtensorMap{});
     const bool mixed = S.precision == 1;
     const int DH = 2 * S.cy + 5;
+    const int DWV = mixed ? down_box_width<float>() : down_box_width<double>();
     for (int l = 0; l < (int)S.levels.size(); ++l) {
         Level& lv = S.levels[l];
         const void* P = mixed ? (const void*)planes32(S, l) : (const void*)planes64(S, l);
@@ -486,6 +492,9 @@ static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
             rc |= encode_map(m + kMapBD, B, g, false, mixed, kBW, DH);
             rc |= encode_map(m + kMapXC, X, g, false, mixed, kCBW, kCBH);
             rc |= encode_map(m + kMapXF, X, g, false, mixed, kBW, kBH);
+            rc |= encode_map(m + kMapPlS, P, g, true, mixed, kBW, kPH);
+            rc |= encode_map(m + kMapPlDV, P, g, true, mixed, DWV, DH);
+            rc |= encode_map(m + kMapBDV, B, g, false, mixed, DWV, DH);
             if (XA) {
                 rc |= encode_map(m + kMapXAF, XA, g, false, mixed, kBW, kBH);
                 rc |= encode_map(m + kMapXAD, XA, g, false, mixed, kBW, DH);
@@ -726,13 +735,15 @@ static void cg_iteration(Stencil& S, int reorth) {
                        v.ap, st, S.partials(), S.err(), s);
     const bool mixed = S.precision == 1;
     launch_cg_update<T>(S.precond, LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, v.P, v.x, v.r,
-                        v.z, v.p0, v.p1, v.ap, v.dr, reorth, mixed ? 1 : 0, st, S.partials(), s);
+                        v.z, v.p0, v.p1, v.ap, v.dr, reorth, mixed ? 1 : 0, S.err() + kPendingSlot, st,
+                        S.partials(), s);
     S.launches += 2;
     if (mixed) {
         // Residual replacement for the images whose FP32 phase just ended.
         HostList& a = S.fine0;
         launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl,
-                              S.at<double>(S.o_x64), S.at<float>(S.o_xin32), st, s);
+                              S.at<double>(S.o_x64), S.at<float>(S.o_xin32), st,
+                              S.err() + kPendingSlot, s);
         launch_refine_residual(S.precond, 0, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(),
                                S.at<float>(S.o_P032), S.at<double>(S.o_b64), S.at<float>(S.o_r32),
                                S.at<float>(S.o_xin32), S.at<float>(S.o_z32), S.outer(), st,
@@ -827,6 +838,7 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
         PMB_CUDA(cudaMemsetAsync(x64, 0, sizeof(double) * S.levels[0].vec_elems, s));
     S.delta = inner_rtol;
     S.max_outer = max_outer;
+    PMB_CUDA(cudaMemsetAsync(S.err() + kPendingSlot, 0, sizeof(int), s));
     // Outer state: every image starts running; its first FP64 residual sets
     // |b|, the tolerance and the first FP32 phase.
     std::vector<InstState> init(S.nimg);
@@ -843,7 +855,8 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
     if (S.precond == kPrecVcycle) run_vcycle<float>(S, v.r, v.z, S.state(), v.dr, 0);
     if (int rc = iterate<float>(S, reorth, maxiter)) return rc;
     // Fold the last FP32 correction into x64 (zero for converged images).
-    launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, x64, v.x, nullptr, s);
+    launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, x64, v.x, nullptr,
+                          S.err() + kPendingSlot, s);
     S.launches += 1;
     if (int rc = read_states(S, true)) return rc;
     return check_err(S);

@@ -21,7 +21,7 @@ constexpr int kTX = 64;      // fine tile width
 constexpr int kTY = 8;       // fine tile height
 constexpr int kThreads = 256;      // element-wise kernels
 constexpr int kTileThreads = 512;  // tiled stencil kernels: one pixel per thread
-constexpr int kFlat = 1024;  // elements per tile of the element-wise kernels
+constexpr int kFlat = 4096;  // elements per tile of the element-wise kernels
 
 // Shared-memory boxes loaded by TMA around a fine tile at (x0, y0): origin
 // (x0 - kBOX, y0 - 2), kBW x kBH elements. x0 - kBOX keeps the box start
@@ -29,6 +29,9 @@ constexpr int kFlat = 1024;  // elements per tile of the element-wise kernels
 constexpr int kBOX = 4;
 constexpr int kBW = kTX + 2 * kBOX;   // 72
 constexpr int kBH = kTY + 4;          // 12
+// Plane rows of the register-blocked apply kernels: y0 - 2 .. y0 + 7 (the
+// backward entries reach two rows up; no plane is read below the tile).
+constexpr int kPH = kTY + 2;          // 10
 // Restriction tiles: kCX x CY coarse pixels; the fine box starts at
 // (2 X0 - 4, 2 Y0 - 3) and is kBW x (2 CY + 5).
 constexpr int kCX = 32;
@@ -36,7 +39,7 @@ constexpr int kCX = 32;
 constexpr int kCBW = 40;
 constexpr int kCBH = 8;
 
-template <typename T> struct Coarse { static constexpr int CY = sizeof(T) == 8 ? 3 : 4; };
+template <typename T> struct Coarse { static constexpr int CY = 3; };
 
 // TMA descriptor slots of one grid (see engine.cu for what each maps).
 enum : int {
@@ -55,6 +58,9 @@ enum : int {
     kMapP1F,       // CG p parity 1, fine box
     kMapX64F,      // FP64 refinement iterate, fine box
     kMapP64F,      // FP64 planes, fine box (refinement residual)
+    kMapPlS,       // planes, apply box (kPH rows)
+    kMapPlDV,      // planes, register-blocked restriction box
+    kMapBDV,       // b, register-blocked restriction box
     kMapsPerGrid
 };
 
@@ -113,6 +119,9 @@ enum : int { kFirst = 1, kUpdate = 2 };
 // Which images a gated loop visits: running ones, or running ones that
 // wait for a residual replacement.
 enum : int { kGateRunning = 0, kGateUpdate = 1 };
+// Slot of the solver's error words (4 ints) that counts the images waiting
+// for a residual replacement (slot 0 is the TMA timeout flag).
+constexpr int kPendingSlot = 2;
 
 __device__ __forceinline__ int find_grid(const WorkList& wl, int tile) {
     int lo = 0, hi = wl.ngrids - 1;

@@ -44,6 +44,34 @@ struct SmemCarve {
 
 extern __shared__ __align__(128) char g_smem[];
 
+// V-element vector load / store (8 or 16 bytes, aligned).
+template <typename T, int V>
+__device__ __forceinline__ void ldv(const T* p, T* o) {
+    if constexpr (sizeof(T) == 4 && V == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        o[0] = q.x; o[1] = q.y; o[2] = q.z; o[3] = q.w;
+    } else if constexpr (sizeof(T) == 4 && V == 2) {
+        const float2 q = *reinterpret_cast<const float2*>(p);
+        o[0] = q.x; o[1] = q.y;
+    } else {
+        static_assert(sizeof(T) == 8 && V == 2, "unsupported vector");
+        const double2 q = *reinterpret_cast<const double2*>(p);
+        o[0] = q.x; o[1] = q.y;
+    }
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void stv(T* p, const T* o) {
+    if constexpr (sizeof(T) == 4 && V == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+    } else if constexpr (sizeof(T) == 4 && V == 2) {
+        *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+    } else {
+        *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+    }
+}
+
+
 // Description of one tile, prepared by thread 0 for the whole CTA.
 struct Meta {
     int t, g, y0, x0;     // tile, grid index in the list, tile origin
@@ -406,39 +434,59 @@ __device__ __forceinline__ void flat_loop(const WorkList& wl, const InstState* s
 template <typename T, int PREC>
 __global__ void __launch_bounds__(kThreads)
 k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0, const T* p1,
-            const T* __restrict__ Ap, T* dr, int reorth, int reliable, InstState* st,
+            const T* __restrict__ Ap, T* dr, int reorth, int reliable, int* pending, InstState* st,
             double* partials) {
+    constexpr int VE = 16 / sizeof(T);          // elements per 16-byte vector
     __shared__ double s_red[3 * 32];
     double v[3] = {0.0, 0.0, 0.0};
     auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
         const InstState& s = st[g.inst];
         const T a = (T)s.alpha;
         const T* p = (s.iters & 1) ? p0 : p1;   // the buffer k_cg_apply wrote
+        // Vectors never straddle rows (the pitch is a multiple of 32); padding
+        // lanes keep their values.
 #pragma unroll
-        for (int k = 0; k < kFlat / kThreads; ++k) {
-            const int64_t e = e0 + threadIdx.x + k * kThreads;
+        for (int k = 0; k < kFlat / (kThreads * VE); ++k) {
+            const int64_t e = e0 + (int64_t)(threadIdx.x + k * kThreads) * VE;
             if (e >= e1) break;
-            const int col = (int)(e % g.pitch);
-            if (col >= g.w) continue;
+            const int col0 = (int)(e % g.pitch);
+            if (col0 >= g.w) continue;
             const int64_t i = g.voff + e;
-            const T rold = r[i];
-            x[i] = x[i] + a * p[i];
-            const T ri = rold - a * Ap[i];
-            r[i] = ri;
-            v[0] += (double)ri * (double)ri;
+            T xv[VE], rv[VE], pv[VE], av[VE], zv[VE], dv[VE], drv[VE];
+            ldv<T, VE>(x + i, xv);
+            ldv<T, VE>(r + i, rv);
+            ldv<T, VE>(p + i, pv);
+            ldv<T, VE>(Ap + i, av);
             if (PREC == kPrecJacobi) {
                 const int row = (int)(e / g.pitch);
-                const T d = P[g.poff + (int64_t)row * g.pitch + col];
-                const T zi = ri * (T(1) / d);
-                z[i] = zi;
-                v[1] += (double)ri * (double)zi;
-                if (reorth) v[2] += (double)(ri - rold) * (double)zi;
-            } else if (PREC == kPrecNone) {
-                v[1] += (double)ri * (double)ri;
-                if (reorth) v[2] += (double)(ri - rold) * (double)ri;
-            } else if (reorth) {
-                dr[i] = ri - rold;
+                ldv<T, VE>(P + g.poff + (int64_t)row * g.pitch + col0, dv);
+                ldv<T, VE>(z + i, zv);
             }
+            if (PREC == kPrecVcycle && reorth) ldv<T, VE>(dr + i, drv);
+#pragma unroll
+            for (int u = 0; u < VE; ++u) {
+                if (col0 + u >= g.w) continue;
+                const T rold = rv[u];
+                xv[u] = xv[u] + a * pv[u];
+                const T ri = rold - a * av[u];
+                rv[u] = ri;
+                v[0] += (double)ri * (double)ri;
+                if (PREC == kPrecJacobi) {
+                    const T zi = ri * (T(1) / dv[u]);
+                    zv[u] = zi;
+                    v[1] += (double)ri * (double)zi;
+                    if (reorth) v[2] += (double)(ri - rold) * (double)zi;
+                } else if (PREC == kPrecNone) {
+                    v[1] += (double)ri * (double)ri;
+                    if (reorth) v[2] += (double)(ri - rold) * (double)ri;
+                } else if (reorth) {
+                    drv[u] = ri - rold;
+                }
+            }
+            stv<T, VE>(x + i, xv);
+            stv<T, VE>(r + i, rv);
+            if (PREC == kPrecJacobi) stv<T, VE>(z + i, zv);
+            if (PREC == kPrecVcycle && reorth) stv<T, VE>(dr + i, drv);
         }
     };
     auto flush = [&](int inst, int t0, int t1, unsigned int mine) {
@@ -452,8 +500,12 @@ k_cg_update(WorkList wl, const T* __restrict__ P, T* x, T* r, T* z, const T* p0,
                 // Mixed precision: the phase ends with an FP64 residual
                 // replacement (k_refine_residual, same iteration), which also
                 // finishes beta; otherwise the solve has converged.
-                if (reliable) s->flags |= kUpdate;
-                else s->status = kConverged;
+                if (reliable) {
+                    s->flags |= kUpdate;
+                    atomicAdd(pending, 1);
+                } else {
+                    s->status = kConverged;
+                }
             } else if (s->iters >= s->maxiter) s->status = kMaxIter;
             if (s->status == kRunning && !(s->flags & kUpdate) &&
                 (PREC == kPrecJacobi || PREC == kPrecNone)) {
@@ -1007,6 +1059,9 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
                   const double* __restrict__ b, float* r32, float* x32, float* z32,
                   InstState* outer, InstState* inner, double* partials, double atol, double rtol,
                   double delta, int maxiter, int max_outer, int* err) {
+    // Replacement launches with no image flagged (most iterations) end here:
+    // err[kPendingSlot] counts the images k_cg_update flagged.
+    if (!FIRST && *(volatile int*)(err + kPendingSlot) == 0) return;
     __shared__ double s_red[3 * 32];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ Meta s_m[2];
@@ -1064,6 +1119,7 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
             } else {
                 so->iters += 1;
                 si->flags &= ~kUpdate;
+                atomicSub(err + kPendingSlot, 1);
             }
             so->norm_r = nr;
             int status = kRunning;
@@ -1092,7 +1148,8 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
 // for every image (st == nullptr) at the end of a solve.
 template <int GATE>
 __global__ void __launch_bounds__(kThreads)
-k_refine_correct(WorkList wl, double* x64, float* x32, const InstState* st) {
+k_refine_correct(WorkList wl, double* x64, float* x32, const InstState* st, const int* pending) {
+    if (GATE == kGateUpdate && *(volatile const int*)pending == 0) return;
     auto body = [&](const GridDesc& g, int64_t e0, int64_t e1) {
 #pragma unroll
         for (int k = 0; k < kFlat / kThreads; ++k) {
@@ -1111,6 +1168,394 @@ k_refine_correct(WorkList wl, double* x64, float* x32, const InstState* st) {
 // --------------------------------------------------------------------------
 // Launchers
 // --------------------------------------------------------------------------
+
+
+
+// --------------------------------------------------------------------------
+// Register-blocked kernels
+// --------------------------------------------------------------------------
+//
+// Each thread computes V adjacent pixels of a row (V = 2 or 4 in FP32, 2 in
+// FP64: one 8- or 16-byte shared-memory vector). The operand window of the 25-point
+// stencil is held in registers (5 rows x 3 vectors) and every plane is read
+// with vector loads, so a pixel costs ~12 (FP32) or ~25 (FP64) shared loads
+// instead of 50. The accumulation order per pixel is that of stencil_at, so
+// the results are bit-identical to the one-pixel-per-thread kernels.
+
+// Threads of the 64x8-tile kernels: one V-pixel group each.
+template <int V> __host__ __device__ constexpr int tile_threads_v() { return kTX / V * kTY; }
+// Threads of the restriction kernel (grid-stride over its work items).
+constexpr int kDownThreads = 256;
+
+// (A x) for the V pixels at box row r, box columns c0 .. c0 + V - 1 (c0 a
+// multiple of V, c0 >= V). P: 13 planes of BW-wide rows, `ps` elements apart,
+// row 0 = two rows above the first output row of the tile; loadx(row, col, o)
+// loads V operand values at an aligned box position. Needs rows r-2 .. r+2 of
+// the operand, r-2 .. r of the planes, columns c0 - V .. c0 + 2V - 1.
+template <typename T, int V, int BW, typename LoadX>
+__device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int r, int c0,
+                                            T (&acc)[V]) {
+    T xr[5][3 * V];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) loadx(r - 2 + k, c0 - V + j * V, &xr[k][j * V]);
+    T pc[V];
+    ldv<T, V>(P + r * BW + c0, pc);
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = pc[v] * xr[2][V + v];
+#pragma unroll
+    for (int p = 1; p < kNH; ++p) {
+        const int dy = half_dy(p), dx = half_dx(p);
+        T pf[V];
+        ldv<T, V>(P + p * ps + r * BW + c0, pf);
+        // Backward entries A[i, i - d] = plane p at (r - dy, c - dx): an
+        // aligned window of one or two vectors around c0 - dx.
+        T pb[2 * V];
+        const int cb = dx > 0 ? c0 - V : c0;
+        ldv<T, V>(P + p * ps + (r - dy) * BW + cb, pb);
+        if (dx != 0) ldv<T, V>(P + p * ps + (r - dy) * BW + cb + V, pb + V);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            acc[v] += pf[v] * xr[2 + dy][V + v + dx];
+            acc[v] += pb[(dx > 0 ? V : 0) + v - dx] * xr[2 - dy][V + v - dx];
+        }
+    }
+}
+
+// y = A x (pitched vectors, no reductions). Plane box: rows y0-2 .. y0+7
+// (kMapPlS), operand box 72 x 12 (kMapBF).
+template <typename T, int V>
+__global__ void __launch_bounds__(tile_threads_v<V>())
+k_apply_v(WorkList wl, const CUtensorMap* maps, T* y, int* err) {
+    constexpr int TPR = kTX / V;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
+    SmemCarve sc(g_smem);
+    T* sP[2];
+    T* sX[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kPH * kBW);
+        sX[k] = sc.take<T>(kBH * kBW);
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        mbar_expect_tx(&pipe.bar[bb], (kNH * kPH + kBH) * kBW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapPlS), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sX[bb], map_of(maps, g, kMapBF), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        const int tx = threadIdx.x % TPR, ty = threadIdx.x / TPR;
+        const int yy = m.y0 + ty, xx = m.x0 + V * tx;
+        if (yy < g.h && xx < g.w) {
+            const T* X = sX[bb];
+            T acc[V];
+            stencil_vec<T, V, kBW>(sP[bb], kPH * kBW,
+                                [&](int rr, int cc, T* o) { ldv<T, V>(X + rr * kBW + cc, o); },
+                                ty + 2, kBOX + V * tx, acc);
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                if (xx + v >= g.w) acc[v] = T(0);
+            stv<T, V>(y + g.voff + (int64_t)yy * g.pitch + xx, acc);
+        }
+    };
+    tile_loop<kTY, kTX>(wl, nullptr, pipe, s_m, s_g, issue, body, NoFlush());
+}
+
+// p_new = z + beta p_old (z on the first pass), Ap = A p_new, p_new . Ap;
+// finaliser alpha = rz / (p . Ap) (cg.py:85-90, 111-113). p_new is formed
+// in registers from the z and p_old boxes.
+template <typename T, int V>
+__global__ void __launch_bounds__(tile_threads_v<V>())
+k_cg_apply_v(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap, InstState* st,
+             double* partials, int* err) {
+    constexpr int TPR = kTX / V;
+    __shared__ double s_red[32];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
+    SmemCarve sc(g_smem);
+    T* sP[2];
+    T* sZ[2];
+    T* sQ[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kPH * kBW);
+        sZ[k] = sc.take<T>(kBH * kBW);
+        sQ[k] = sc.take<T>(kBH * kBW);
+    }
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    double v0[1] = {0.0};
+    auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
+        mbar_expect_tx(&pipe.bar[bb], (kNH * kPH + (m.first ? 1 : 2) * kBH) * kBW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, g, kMapPlS), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sZ[bb], map_of(maps, g, zslot), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+        if (!m.first)
+            tma_load_2d(sQ[bb], map_of(maps, g, m.par ? kMapP1F : kMapP0F), m.x0 - kBOX, m.y0 - 2,
+                        &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& g, int bb) {
+        const int tx = threadIdx.x % TPR, ty = threadIdx.x / TPR;
+        const int yy = m.y0 + ty, xx = m.x0 + V * tx;
+        if (yy < g.h && xx < g.w) {
+            const T* Z = sZ[bb];
+            const T* Q = sQ[bb];
+            const bool first = m.first != 0;
+            const T beta = (T)m.beta;
+            auto loadp = [&](int rr, int cc, T* o) {
+                ldv<T, V>(Z + rr * kBW + cc, o);
+                if (!first) {
+                    T q[V];
+                    ldv<T, V>(Q + rr * kBW + cc, q);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) o[v] = o[v] + beta * q[v];
+                }
+            };
+            T acc[V], pv[V];
+            stencil_vec<T, V, kBW>(sP[bb], kPH * kBW, loadp, ty + 2, kBOX + V * tx, acc);
+            loadp(ty + 2, kBOX + V * tx, pv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (xx + v >= g.w) {
+                    acc[v] = T(0);
+                    pv[v] = T(0);
+                }
+                v0[0] += (double)pv[v] * (double)acc[v];
+            }
+            const int64_t i = g.voff + (int64_t)yy * g.pitch + xx;
+            stv<T, V>((m.par ? p0 : p1) + i, pv);
+            stv<T, V>(Ap + i, acc);
+        }
+    };
+    auto flush = [&](const Meta& m, unsigned int mine) {
+        InstState* s = st + m.inst;
+        cta_flush<1>(v0, partials, m.inst, m.t0, m.t1, mine, s, s_red, [&](double* sum) {
+            s->pap = sum[0];
+            s->alpha = s->rz / sum[0];
+            s->flags &= ~kFirst;
+        });
+    };
+    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
+}
+
+// Restriction box of the register-blocked restriction kernel: fine columns
+// from 2 X0 - DOFF, DW wide; rows 2 Y0 - 3 .. 2 Y0 + 2 CY + 1.
+template <typename T, int VV> struct DownBox {
+    static constexpr int V = VV;
+    static constexpr int CY = Coarse<T>::CY;
+    static constexpr int DH = 2 * CY + 5;
+    static constexpr int DOFF = 2 * V;
+    static constexpr int DW = kTX + DOFF + 4;      // 76 (FP32), 72 (FP64)
+    static constexpr int RH = 2 * CY + 1;          // residual rows
+    static constexpr int RW = kTX + V;             // residual columns from 2 X0 - V
+};
+
+// One pre-smoothing sweep from zero, residual and full-weighting restriction
+// (vcycle.py:33-36, 77-80; same arithmetic as k_vc_down<T, 1>):
+//   x1 = omega b / d on the box, res = b - A x1 on the fine rows
+//   2 Y0 - 1 .. 2 Y0 + 2 CY - 1, b_coarse = R res.
+template <typename T, int V>
+__global__ void __launch_bounds__(kDownThreads)
+k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMap* maps, T* bc,
+            double omega, const InstState* st, int* err) {
+    using D = DownBox<T, V>;
+    constexpr int DH = D::DH, DW = D::DW, RH = D::RH, RW = D::RW, CY = D::CY;
+    constexpr int RV = RW / V, XV = DW / V;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
+    SmemCarve sc(g_smem);
+    T* sP[2];
+    T* sB[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * DH * DW);
+        sB[k] = sc.take<T>(DH * DW);
+    }
+    T* sX = sc.take<T>(DH * DW);
+    T* sR = sc.take<T>(RH * RW);
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    auto issue = [&](const Meta& m, const GridDesc& gc, int bb) {
+        const GridDesc gf = fine[m.g];
+        const int bx = 2 * m.x0 - D::DOFF, by = 2 * m.y0 - 3;
+        mbar_expect_tx(&pipe.bar[bb], (kNH + 1) * DH * DW * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, gf, kMapPlDV), bx, by, 0, &pipe.bar[bb]);
+        tma_load_2d(sB[bb], map_of(maps, gf, kMapBDV), bx, by, &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& gc, int bb) {
+        const GridDesc gf = fine[m.g];
+        const int bx = 2 * m.x0 - D::DOFF, by = 2 * m.y0 - 3;
+        const T* B = sB[bb];
+        const T* P = sP[bb];
+        for (int q = threadIdx.x; q < DH * XV; q += kDownThreads) {
+            const int rr = q / XV, col = (q - rr * XV) * V;
+            const int fy = by + rr;
+            T bv[V], dv[V], o[V];
+            ldv<T, V>(B + rr * DW + col, bv);
+            ldv<T, V>(P + rr * DW + col, dv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int fx = bx + col + v;
+                o[v] = (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) ? (T)omega * bv[v] / dv[v]
+                                                                       : T(0);
+            }
+            stv<T, V>(sX + rr * DW + col, o);
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < RH * RV; q += kDownThreads) {
+            const int rr = q / RV, cv = q - rr * RV;
+            const int br = rr + 2, bcol = D::DOFF - V + cv * V;
+            const int fy = by + br;
+            T acc[V], bv[V], o[V];
+            stencil_vec<T, V, DW>(P, DH * DW,
+                               [&](int r2, int c2, T* out) { ldv<T, V>(sX + r2 * DW + c2, out); },
+                               br, bcol, acc);
+            ldv<T, V>(B + br * DW + bcol, bv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int fx = bx + bcol + v;
+                o[v] = (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) ? bv[v] - acc[v] : T(0);
+            }
+            stv<T, V>(sR + rr * RW + cv * V, o);
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < kCX * CY; q += kDownThreads) {
+            const int ly = q / kCX, lx = q - ly * kCX;
+            const int Y = m.y0 + ly, X = m.x0 + lx;
+            if (Y < gc.h && X < gc.w) {
+                T sum = T(0);
+#pragma unroll
+                for (int ay = -1; ay <= 1; ++ay)
+#pragma unroll
+                    for (int ax = -1; ax <= 1; ++ax)
+                        sum += (T)(pw(ax) * pw(ay) / 16.0) *
+                               sR[(2 * ly + 1 + ay) * RW + (2 * lx + ax + V)];
+                bc[gc.voff + (int64_t)Y * gc.pitch + X] = sum;
+            }
+        }
+    };
+    tile_loop<CY, kCX>(wl, st, pipe, s_m, s_g, issue, body, NoFlush());
+}
+
+// Prolongation and one post-smoothing sweep (same arithmetic as
+// k_vc_up<T, 1, 1>): x2 = x1 + P xc on the 72 x 12 box into shared memory,
+// then x3 = x2 + omega (b - A x2) / d for the tile; at level 0 also r . z
+// (and (r - r_old) . z) with beta.
+template <typename T, int V>
+__global__ void __launch_bounds__(tile_threads_v<V>())
+k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap* maps,
+          const T* __restrict__ b, T* xout, double omega, InstState* st, int level0,
+          const T* __restrict__ dr, int reorth, double* partials, int* err) {
+    constexpr int TPR = kTX / V, NT = tile_threads_v<V>(), XV = kBW / V;
+    __shared__ double s_red[2 * 32];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ Meta s_m[2];
+    __shared__ GridDesc s_g[2];
+    SmemCarve sc(g_smem);
+    T* sP[2];
+    T* sB[2];
+    T* sC[2];
+    for (int k = 0; k < 2; ++k) {
+        sP[k] = sc.take<T>(kNH * kBH * kBW);
+        sB[k] = sc.take<T>(kBH * kBW);
+        sC[k] = sc.take<T>(kCBH * kCBW);
+    }
+    T* sX = sc.take<T>(kBH * kBW);
+    Pipe pipe;
+    pipe.init(s_bar, err);
+    double acc2[2] = {0.0, 0.0};
+    auto issue = [&](const Meta& m, const GridDesc& gf, int bb) {
+        const GridDesc gc = coarse[m.g];
+        mbar_expect_tx(&pipe.bar[bb], ((kNH + 1) * kBH * kBW + kCBH * kCBW) * sizeof(T));
+        tma_load_3d(sP[bb], map_of(maps, gf, kMapPlF), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_2d(sB[bb], map_of(maps, gf, kMapBF), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
+        tma_load_2d(sC[bb], map_of(maps, gc, kMapXC), (m.x0 >> 1) - 4, (m.y0 >> 1) - 2,
+                    &pipe.bar[bb]);
+    };
+    auto body = [&](const Meta& m, const GridDesc& gf, int bb) {
+        const GridDesc gc = coarse[m.g];
+        const int bx = m.x0 - kBOX, by = m.y0 - 2;
+        const int cx0 = (m.x0 >> 1) - 4, cy0 = (m.y0 >> 1) - 2;
+        const T* P = sP[bb];
+        const T* B = sB[bb];
+        const T* C = sC[bb];
+        for (int q = threadIdx.x; q < kBH * XV; q += NT) {
+            const int rr = q / XV, col = (q - rr * XV) * V;
+            const int y = by + rr;
+            T bv[V], dv[V], o[V];
+            ldv<T, V>(B + rr * kBW + col, bv);
+            ldv<T, V>(P + rr * kBW + col, dv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int x = bx + col + v;
+                T val = T(0);
+                if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
+                    const T x1 = (T)omega * bv[v] / dv[v];
+                    // Coarse pixels whose 3x3 support holds (y, x), in raster
+                    // order: even coordinates have one parent (weight 2), odd
+                    // ones two (weight 1); parents outside the grid add nothing.
+                    const int Ya = (y - 1) >> 1, Xa = (x - 1) >> 1;
+                    const bool ey = (y & 1) == 0, ex = (x & 1) == 0;
+                    T sum = T(0);
+#pragma unroll
+                    for (int jy = 0; jy < 2; ++jy) {
+                        const int Y = ey ? (y >> 1) : Ya + jy;
+                        if ((ey && jy == 1) || Y >= gc.h) continue;
+                        const double wy = ey ? 2.0 : 1.0;
+#pragma unroll
+                        for (int jx = 0; jx < 2; ++jx) {
+                            const int Xc = ex ? (x >> 1) : Xa + jx;
+                            if ((ex && jx == 1) || Xc >= gc.w) continue;
+                            const double wx = ex ? 2.0 : 1.0;
+                            sum += (T)(wx * wy / 16.0) * C[(Y - cy0) * kCBW + (Xc - cx0)];
+                        }
+                    }
+                    val = x1 + sum;
+                }
+                o[v] = val;
+            }
+            stv<T, V>(sX + rr * kBW + col, o);
+        }
+        __syncthreads();
+        const int tx = threadIdx.x % TPR, ty = threadIdx.x / TPR;
+        const int yy = m.y0 + ty, xx = m.x0 + V * tx;
+        if (yy < gf.h && xx < gf.w) {
+            const int r = ty + 2, c0 = kBOX + V * tx;
+            T ax[V], x2[V], bv[V], dv[V], x3[V];
+            stencil_vec<T, V, kBW>(P, kBH * kBW,
+                                [&](int r2, int c2, T* out) { ldv<T, V>(sX + r2 * kBW + c2, out); },
+                                r, c0, ax);
+            ldv<T, V>(sX + r * kBW + c0, x2);
+            ldv<T, V>(B + r * kBW + c0, bv);
+            ldv<T, V>(P + r * kBW + c0, dv);
+            const int64_t i = gf.voff + (int64_t)yy * gf.pitch + xx;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (xx + v < gf.w) {
+                    x3[v] = x2[v] + (T)omega * (bv[v] - ax[v]) / dv[v];
+                    if (level0) {
+                        acc2[0] += (double)bv[v] * (double)x3[v];
+                        if (reorth) acc2[1] += (double)dr[i + v] * (double)x3[v];
+                    }
+                } else {
+                    x3[v] = T(0);
+                }
+            }
+            stv<T, V>(xout + i, x3);
+        }
+    };
+    auto flush = [&](const Meta& m, unsigned int mine) {
+        if (!level0 || !st) return;
+        InstState* s = st + m.inst;
+        cta_flush<2>(acc2, partials, m.inst, m.t0, m.t1, mine, s, s_red, [&](double* sum) {
+            if (reorth) finish_beta_reorth(s, sum[0], sum[1]);
+            else finish_beta(s, sum[0]);
+        });
+    };
+    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
+}
 
 // Shared-memory sizes; they follow the SmemCarve layout of each kernel (two
 // pipeline buffers, every piece rounded up to 128 bytes).
@@ -1137,6 +1582,29 @@ template <typename T> size_t smem_up(int pre) {
     if (pre > 1) per += rup(kBH * kBW * sizeof(T));
     return 2 * per + 128;
 }
+
+template <typename T> size_t smem_apply_v() {
+    return 2 * (rup(kNH * kPH * kBW * sizeof(T)) + 2 * rup(kBH * kBW * sizeof(T))) + 128;
+}
+// Vector widths of the register-blocked kernels, measured on B200 at
+// 1920x1080 and 4096x4096: the plain apply is fastest with 4 FP32 pixels per
+// thread (128 threads), the solver kernels (more work per tile) with 2
+// (256 threads); FP64 uses 2 (one 16-byte vector).
+template <typename T> constexpr int kVApply = sizeof(T) == 8 ? 2 : 4;
+template <typename T> constexpr int kVSolve = 2;
+
+template <typename T, int V> static size_t smem_down_vv() {
+    using D = DownBox<T, V>;
+    return 2 * (rup(kNH * D::DH * D::DW * sizeof(T)) + rup(D::DH * D::DW * sizeof(T))) +
+           rup(D::DH * D::DW * sizeof(T)) + rup(D::RH * D::RW * sizeof(T)) + 128;
+}
+template <typename T> size_t smem_up_v() {
+    return 2 * (rup(kNH * kBH * kBW * sizeof(T)) + rup(kBH * kBW * sizeof(T)) +
+                rup(kCBH * kCBW * sizeof(T))) +
+           rup(kBH * kBW * sizeof(T)) + 128;
+}
+template <typename T> size_t smem_down_v() { return smem_down_vv<T, kVSolve<T>>(); }
+template <typename T> int down_box_width() { return DownBox<T, kVSolve<T>>::DW; }
 
 // Raise the dynamic shared-memory limit of a kernel. Done once for every
 // instantiation by stencil_prepare(), before any stream capture.
@@ -1171,18 +1639,20 @@ void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUte
 template <typename T>
 void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, int zslot,
                      T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s) {
-    const size_t sm = smem_apply<T>();
-    k_cg_apply<T><<<L.grid, kTileThreads, sm, s>>>(wl, maps, zslot, p0, p1, Ap, st, part, err);
+    const size_t sm = smem_apply_v<T>();
+    constexpr int V = kVSolve<T>;
+    k_cg_apply_v<T, V><<<L.grid, tile_threads_v<V>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, st,
+                                                               part, err);
 }
 
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
                       T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth, int reliable,
-                      InstState* st, double* part, cudaStream_t s) {
+                      int* pending, InstState* st, double* part, cudaStream_t s) {
     switch (prec) {
-    case kPrecNone: k_cg_update<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, st, part); break;
-    case kPrecJacobi: k_cg_update<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, st, part); break;
-    default: k_cg_update<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, st, part); break;
+    case kPrecNone: k_cg_update<T, kPrecNone><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, pending, st, part); break;
+    case kPrecJacobi: k_cg_update<T, kPrecJacobi><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, pending, st, part); break;
+    default: k_cg_update<T, kPrecVcycle><<<L.grid, kThreads, 0, s>>>(wl, P, x, r, z, p0, p1, Ap, dr, reorth, reliable, pending, st, part); break;
     }
 }
 
@@ -1197,6 +1667,12 @@ void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridD
                     const CUtensorMap* maps, int xs_slot, T* bc, double omega,
                     const InstState* st, int* err, cudaStream_t s) {
     const int pk = pre > 1 ? 2 : pre;
+    if (pk == 1) {
+        constexpr int V = kVSolve<T>;
+        k_vc_down_v<T, V><<<L.grid, kDownThreads, smem_down_v<T>(), s>>>(wl, fine, maps, bc, omega,
+                                                                          st, err);
+        return;
+    }
     const size_t sm = smem_down<T>(pk);
 #define PMB_DOWN(PK)                                                                         \
     do {                                                                                     \
@@ -1216,6 +1692,12 @@ void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, con
                   cudaStream_t s) {
     const int pk = pre > 1 ? 2 : pre;
     const int qk = post > 0 ? 1 : 0;
+    if (pk == 1 && qk == 1) {
+        constexpr int V = kVSolve<T>;
+        k_vc_up_v<T, V><<<L.grid, tile_threads_v<V>(), smem_up_v<T>(), s>>>(
+            wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err);
+        return;
+    }
     const size_t sm = smem_up<T>(pk);
 #define PMB_UP(PK, QK)                                                                       \
     do {                                                                                     \
@@ -1249,8 +1731,9 @@ void launch_vc_direct(const DirectDesc* dd, int count, const T* b, T* x, InstSta
 template <typename T>
 void launch_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, T* y, int* err,
                   cudaStream_t s) {
-    const size_t sm = smem_init<T>();
-    k_apply<T><<<L.grid, kTileThreads, sm, s>>>(wl, maps, y, err);
+    const size_t sm = smem_apply_v<T>();
+    constexpr int V = kVApply<T>;
+    k_apply_v<T, V><<<L.grid, tile_threads_v<V>(), sm, s>>>(wl, maps, y, err);
 }
 
 template <typename TS, typename TD>
@@ -1313,9 +1796,9 @@ void launch_refine_residual(int prec, int first, const LaunchCfg& L, const WorkL
 }
 
 void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, float* x32,
-                           const InstState* inner, cudaStream_t s) {
-    if (inner) k_refine_correct<kGateUpdate><<<L.grid, kThreads, 0, s>>>(wl, x64, x32, inner);
-    else k_refine_correct<kGateRunning><<<L.grid, kThreads, 0, s>>>(wl, x64, x32, nullptr);
+                           const InstState* inner, const int* pending, cudaStream_t s) {
+    if (inner) k_refine_correct<kGateUpdate><<<L.grid, kThreads, 0, s>>>(wl, x64, x32, inner, pending);
+    else k_refine_correct<kGateRunning><<<L.grid, kThreads, 0, s>>>(wl, x64, x32, nullptr, pending);
 }
 
 
@@ -1336,6 +1819,10 @@ static void prepare_type() {
     allow_smem(k_vc_up<T, 2, 1>, smem_up<T>(2));
     allow_smem(k_vc_smooth<T>, smem_init<T>());
     allow_smem(k_apply<T>, smem_init<T>());
+    allow_smem(k_apply_v<T, kVApply<T>>, smem_apply_v<T>());
+    allow_smem(k_cg_apply_v<T, kVSolve<T>>, smem_apply_v<T>());
+    allow_smem(k_vc_down_v<T, kVSolve<T>>, smem_down_v<T>());
+    allow_smem(k_vc_up_v<T, kVSolve<T>>, smem_up_v<T>());
 }
 
 void stencil_prepare() {
@@ -1359,8 +1846,8 @@ void stencil_prepare() {
     template void launch_cg_apply<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int,  \
                                      T*, T*, T*, InstState*, double*, int*, cudaStream_t);        \
     template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*,   \
-                                      T*, const T*, const T*, const T*, T*, int, int, InstState*, \
-                                      double*, cudaStream_t);                                    \
+                                      T*, const T*, const T*, const T*, T*, int, int, int*,      \
+                                      InstState*, double*, cudaStream_t);                        \
     template void launch_cg_rz<T>(const LaunchCfg&, const WorkList&, const T*, const T*,          \
                                   const T*, int, InstState*, double*, cudaStream_t);             \
     template void launch_vc_down<T>(int, const LaunchCfg&, const WorkList&, const GridDesc*,      \
@@ -1379,7 +1866,11 @@ void stencil_prepare() {
     template size_t smem_apply<T>();                                                              \
     template size_t smem_init<T>();                                                               \
     template size_t smem_down<T>(int);                                                            \
-    template size_t smem_up<T>(int);
+    template size_t smem_up<T>(int);                                                              \
+    template size_t smem_apply_v<T>();                                                            \
+    template size_t smem_down_v<T>();                                                             \
+    template size_t smem_up_v<T>();                                                               \
+    template int down_box_width<T>();
 
 PMB_INST(double)
 PMB_INST(float)

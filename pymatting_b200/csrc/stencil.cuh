@@ -25,6 +25,12 @@ template <typename T> size_t smem_apply();
 template <typename T> size_t smem_init();
 template <typename T> size_t smem_down(int pre);
 template <typename T> size_t smem_up(int pre);
+// ... of the register-blocked kernels (default one pre- and one post-sweep).
+template <typename T> size_t smem_apply_v();
+template <typename T> size_t smem_down_v();
+template <typename T> size_t smem_up_v();
+// Width of the register-blocked restriction box (its TMA maps).
+template <typename T> int down_box_width();
 
 // Raise the dynamic shared-memory limits once (before any graph capture).
 void stencil_prepare();
@@ -39,7 +45,7 @@ void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* 
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
                       T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth, int reliable,
-                      InstState* st, double* part, cudaStream_t s);
+                      int* pending, InstState* st, double* part, cudaStream_t s);
 template <typename T>
 void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z, const T* dr,
                   int reorth, InstState* st, double* part, cudaStream_t s);
@@ -81,6 +87,6 @@ void launch_refine_residual(int prec, int first, const LaunchCfg& L, const WorkL
                             cudaStream_t s);
 // inner != nullptr: images flagged kUpdate; nullptr: every image.
 void launch_refine_correct(const LaunchCfg& L, const WorkList& wl, double* x64, float* x32,
-                           const InstState* inner, cudaStream_t s);
+                           const InstState* inner, const int* pending, cudaStream_t s);
 
 }  // namespace pmb
