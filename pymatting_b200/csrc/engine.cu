@@ -126,6 +126,7 @@ struct Level {
     HostList fine;    // 64x8 tiles of level-l grids that have a level l+1
     HostList coarse;  // restriction tiles of the level l+1 grids of the same images
     HostList flat;    // element chunks of the same level-l grids
+    HostList gal;     // every level-l grid with a level l+1 (Galerkin setup), tails included
 };
 
 struct Stencil {
@@ -145,6 +146,13 @@ struct Stencil {
     int64_t user_total = 0;
     int nmaps = 0;                  // grids with a TMA descriptor block
     std::vector<DirectDesc> direct64, direct32;
+    // Coarse-level tail: image k runs levels tail_start[k] .. coarsest[k] in
+    // k_vc_tail (-1: no tail): the deepest levels whose planes and vectors fit
+    // in kTailSmem bytes of shared memory together.
+    std::vector<int> tail_start;
+    size_t tail_smem = 0;
+    std::vector<int> tail_images;   // images with a tail, in descriptor order
+    size_t o_tail = 0;
     std::vector<int64_t> direct_inv_off;   // per direct desc: inverse offset (doubles)
     int64_t direct_doubles = 0;
     // workspace offsets
@@ -242,6 +250,29 @@ static int plan_stencil(Stencil& S) {
         }
         L = std::max(L, (int)shapes[k].size());
     }
+    // Tails: only the default cycle (one pre- and one post-sweep) has one.
+    S.tail_start.assign(n, -1);
+    S.tail_images.clear();
+    S.tail_smem = 0;
+    if (S.precond == kPrecVcycle && S.pre == 1 && S.post == 1) {
+        const size_t es = S.precision == 1 ? sizeof(float) : sizeof(double);
+        for (int k = 0; k < n; ++k) {
+            size_t bytes = 0;
+            int start = -1;
+            for (int l = S.coarsest[k]; l >= 1 && S.coarsest[k] - l + 1 <= kMaxTailLevels; --l) {
+                const size_t add = (size_t)(kNH + 3) * shapes[k][l].first *
+                                   pitch_for(std::max(shapes[k][l].second, 1)) * es;
+                if (bytes + add > kTailSmem) break;
+                bytes += add;
+                start = l;
+            }
+            if (start >= 1) {
+                S.tail_start[k] = start;
+                S.tail_images.push_back(k);
+                S.tail_smem = std::max(S.tail_smem, bytes);
+            }
+        }
+    }
     S.levels.assign(L, Level());
     S.user_off.assign(n + 1, 0);
     for (int k = 0; k < n; ++k) S.user_off[k + 1] = S.user_off[k] + (int64_t)S.h[k] * S.w[k];
@@ -287,14 +318,18 @@ static int plan_stencil(Stencil& S) {
     for (int l = 0; l + 1 < L; ++l) {
         Level& lv = S.levels[l];
         Level& nx = S.levels[l + 1];
-        std::vector<GridDesc> f, c;
+        std::vector<GridDesc> f, c, gf, gc;
         for (int gi = 0; gi < lv.ngrids; ++gi) {
             const int k = lv.image[gi];
             if (S.coarsest[k] <= l) continue;
             const auto it = std::find(nx.image.begin(), nx.image.end(), k);
+            gf.push_back(lv.grids[gi]);
+            gc.push_back(nx.grids[it - nx.image.begin()]);
+            if (S.tail_start[k] >= 0 && l >= S.tail_start[k]) continue;   // in the tail
             f.push_back(lv.grids[gi]);
             c.push_back(nx.grids[it - nx.image.begin()]);
         }
+        build_list(lv.gal, gf, gc, kTY, kTX);
         build_list(lv.fine, f, c, kTY, kTX);
         lv.fine.per_sm = per_up;
         build_list(lv.coarse, c, f, S.cy, kCX);
@@ -345,7 +380,9 @@ static int plan_stencil(Stencil& S) {
         carve_list(c, lv.fine);
         carve_list(c, lv.coarse);
         carve_list(c, lv.flat);
+        carve_list(c, lv.gal);
     }
+    S.o_tail = c.take<TailDesc<double>>((int64_t)S.tail_images.size());
     S.o_direct64 = c.take<DirectDesc>((int64_t)S.direct64.size());
     S.o_direct32 = c.take<DirectDesc>((int64_t)S.direct64.size());
     S.o_inv = c.take<double>(S.direct_doubles);
@@ -519,6 +556,8 @@ static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
     return 0;
 }
 
+static int upload_tail(Stencil& S);
+
 static int bind_stencil(Stencil& S, void* ws, const double* P0) {
     S.ws = reinterpret_cast<char*>(ws);
     S.P0 = P0;
@@ -529,6 +568,7 @@ static int bind_stencil(Stencil& S, void* ws, const double* P0) {
         if (int rc = upload_list(S, lv.fine)) return rc;
         if (int rc = upload_list(S, lv.coarse)) return rc;
         if (int rc = upload_list(S, lv.flat)) return rc;
+        if (int rc = upload_list(S, lv.gal)) return rc;
     }
     PMB_CUDA(cudaMemcpyAsync(S.ws + S.o_uoff, S.user_off.data(), sizeof(int64_t) * S.user_off.size(),
                              cudaMemcpyHostToDevice, S.stream));
@@ -549,6 +589,7 @@ static int bind_stencil(Stencil& S, void* ws, const double* P0) {
         PMB_CUDA(cudaMemcpyAsync(S.ws + S.o_direct32, S.direct32.data(),
                                  sizeof(DirectDesc) * S.direct32.size(), cudaMemcpyHostToDevice, S.stream));
     }
+    if (int rc = upload_tail(S)) return rc;
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_state, 0, sizeof(InstState) * S.nimg, S.stream));
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_outer, 0, sizeof(InstState) * S.nimg, S.stream));
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_err, 0, sizeof(int) * 4, S.stream));
@@ -575,7 +616,7 @@ static int setup_stencil(Stencil& S) {
     const int L = (int)S.levels.size();
     for (int l = 0; l + 1 < L; ++l) {
         Level& lv = S.levels[l];
-        HostList& f = lv.fine;
+        HostList& f = lv.gal;
         if (f.grids.empty()) continue;
         int64_t total = 0;
         for (auto& g : f.partner) total += (int64_t)g.h * g.w * kNH;
@@ -642,6 +683,38 @@ template <> float* lvl_xa<float>(Stencil& S, int l) { return S.at<float>(S.level
 template <> float* lvl_xb<float>(Stencil& S, int l) { return S.at<float>(S.levels[l].xb32); }
 template <> const float* lvl_P<float>(Stencil& S, int l) { return planes32(S, l); }
 
+// Tail descriptors with absolute pointers (after the direct inverses are placed).
+template <typename T>
+static int upload_tail_t(Stencil& S) {
+    std::vector<TailDesc<T>> d(S.tail_images.size());
+    for (size_t j = 0; j < S.tail_images.size(); ++j) {
+        const int k = S.tail_images[j];
+        TailDesc<T>& t = d[j];
+        std::memset(&t, 0, sizeof(t));
+        t.inst = k;
+        t.nlev = S.coarsest[k] - S.tail_start[k] + 1;
+        for (int q = 0; q < t.nlev; ++q) {
+            const int l = S.tail_start[k] + q;
+            const Level& lv = S.levels[l];
+            const auto it = std::find(lv.image.begin(), lv.image.end(), k);
+            t.lev[q].g = lv.grids[it - lv.image.begin()];
+            t.lev[q].P = lvl_P<T>(S, l);
+            t.lev[q].b = lvl_b<T>(S, l);
+            t.lev[q].x = lvl_x<T>(S, l);
+        }
+        t.inv = S.direct64[k].inv;
+    }
+    if (!d.empty())
+        PMB_CUDA(cudaMemcpyAsync(S.ws + S.o_tail, d.data(), sizeof(TailDesc<T>) * d.size(),
+                                 cudaMemcpyHostToDevice, S.stream));
+    return 0;
+}
+
+static int upload_tail(Stencil& S) {
+    if (S.tail_images.empty()) return 0;
+    return S.precision == 1 ? upload_tail_t<float>(S) : upload_tail_t<double>(S);
+}
+
 template <typename T> static const DirectDesc* direct_dev(Stencil& S);
 template <> const DirectDesc* direct_dev<double>(Stencil& S) { return S.at<DirectDesc>(S.o_direct64); }
 template <> const DirectDesc* direct_dev<float>(Stencil& S) { return S.at<DirectDesc>(S.o_direct32); }
@@ -685,9 +758,16 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
                           xs_slot_d[l], B(l + 1), om, st, S.err(), s);
         ++S.launches;
     }
-    // Coarsest solves: every image, whatever its depth.
+    // Small levels of the images that have a tail, in one clustered launch.
+    if (!S.tail_images.empty()) {
+        launch_vc_tail<T>(S.at<TailDesc<T>>(S.o_tail), (int)S.tail_images.size(), S.tail_smem, st,
+                          om, S.err(), s);
+        ++S.launches;
+    }
+    // Coarsest solves of the other images, whatever their depth.
     for (size_t i = 0; i < S.direct64.size(); ++i) {
         const int k = S.direct64[i].g.inst;
+        if (S.tail_start[k] >= 0) continue;
         const int l = S.coarsest[k];
         const bool z_out = (l == 0);
         launch_vc_direct<T>(direct_dev<T>(S) + i, 1, B(l), X(l), st, z_out && st != nullptr, s);

@@ -1557,6 +1557,205 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
     tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
 }
 
+
+// --------------------------------------------------------------------------
+// Coarse-level tail: one CTA per image, shared-memory resident
+// --------------------------------------------------------------------------
+//
+// The smallest levels of an image (a few thousand pixels in all) cost one
+// launch latency each and move almost no data. One CTA per image runs them in
+// a single launch: bulk copies bring every tail level's planes and the first
+// tail level's right-hand side into shared memory (pitched, as in global
+// memory), the CTA walks down (first Jacobi sweep, residual, restriction),
+// solves the coarsest grid with its dense inverse, walks back up
+// (prolongation, post sweep) with __syncthreads between phases, and writes the
+// first tail level's solution back. Same arithmetic as k_vc_down<T, 1> /
+// k_vc_up<T, 1, 1> (vcycle.py:74-98). Shared layout per level: 13 planes,
+// then b, x, t (t: residual, then the prolonged iterate), each h x pitch.
+
+// A[i, i + e] of a pitched plane set at offset 0 (zero outside the grid).
+template <typename T>
+__device__ __forceinline__ T tail_entry(const T* P, const GridDesc& g, int y, int x, int ey,
+                                        int ex) {
+    const int yj = y + ey, xj = x + ex;
+    if (yj < 0 || yj >= g.h || xj < 0 || xj >= g.w) return T(0);
+    int p = half_index(ey, ex);
+    if (p >= 0) return P[p * g.pstride + y * g.pitch + x];
+    p = half_index(-ey, -ex);
+    return P[p * g.pstride + yj * g.pitch + xj];
+}
+
+template <typename T>
+__device__ __forceinline__ T tail_val(const T* v, const GridDesc& g, int y, int x) {
+    if (y < 0 || y >= g.h || x < 0 || x >= g.w) return T(0);
+    return v[y * g.pitch + x];
+}
+
+// (A v) at (y, x), accumulated in the order of stencil_at.
+template <typename T>
+__device__ __forceinline__ T tail_stencil(const T* P, const T* v, const GridDesc& g, int y, int x) {
+    T acc = P[y * g.pitch + x] * v[y * g.pitch + x];
+#pragma unroll
+    for (int p = 1; p < kNH; ++p) {
+        const int dy = half_dy(p), dx = half_dx(p);
+        acc += tail_entry<T>(P, g, y, x, dy, dx) * tail_val<T>(v, g, y + dy, x + dx);
+        acc += tail_entry<T>(P, g, y, x, -dy, -dx) * tail_val<T>(v, g, y - dy, x - dx);
+    }
+    return acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads)
+k_vc_tail(const TailDesc<T>* __restrict__ descs, const InstState* st, double omega, int* err) {
+    __shared__ TailDesc<T> D;
+    __shared__ int s_off[kMaxTailLevels + 1];
+    __shared__ __align__(8) uint64_t s_bar;
+    if (threadIdx.x == 0) D = descs[blockIdx.x];
+    __syncthreads();
+    if (st && st[D.inst].status != kRunning) return;   // uniform over the CTA
+    const int nlev = D.nlev;
+    T* sm = reinterpret_cast<T*>(g_smem);
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int l = 0; l < nlev; ++l) {
+            s_off[l] = off;
+            off += (kNH + 3) * D.lev[l].g.h * D.lev[l].g.pitch;
+        }
+        s_off[nlev] = off;
+        mbar_init(&s_bar, 1);
+        // Planes of every level (one block each) and the first level's b.
+        uint32_t bytes = 0;
+        for (int l = 0; l < nlev; ++l) bytes += kNH * D.lev[l].g.pstride * sizeof(T);
+        bytes += D.lev[0].g.pstride * sizeof(T);
+        mbar_expect_tx(&s_bar, bytes);
+        for (int l = 0; l < nlev; ++l) {
+            const GridDesc g = D.lev[l].g;
+            bulk_load(sm + s_off[l], D.lev[l].P + g.poff,
+                      (uint32_t)(kNH * g.pstride * sizeof(T)), &s_bar);
+        }
+        const GridDesc g0 = D.lev[0].g;
+        bulk_load(sm + s_off[0] + kNH * g0.pstride, D.lev[0].b + g0.voff,
+                  (uint32_t)(g0.pstride * sizeof(T)), &s_bar);
+    }
+    __syncthreads();
+    if (!mbar_wait(&s_bar, 0)) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;   // every thread saw the same timeout
+    }
+    auto planes = [&](int l) { return sm + s_off[l]; };
+    auto vb = [&](int l) { return sm + s_off[l] + kNH * D.lev[l].g.pstride; };
+    auto vx = [&](int l) { return vb(l) + D.lev[l].g.pstride; };
+    auto vt = [&](int l) { return vx(l) + D.lev[l].g.pstride; };
+    const T om = (T)omega;
+    // Down.
+    for (int l = 0; l + 1 < nlev; ++l) {
+        const GridDesc g = D.lev[l].g, gc = D.lev[l + 1].g;
+        const int n = g.h * g.w;
+        const T* P = planes(l);
+        const T* b = vb(l);
+        T* x1 = vx(l);
+        T* t = vt(l);
+        for (int k = threadIdx.x; k < n; k += kTailThreads) {
+            const int y = k / g.w, x = k - y * g.w, i = y * g.pitch + x;
+            x1[i] = om * b[i] / P[i];
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += kTailThreads) {
+            const int y = k / g.w, x = k - y * g.w, i = y * g.pitch + x;
+            t[i] = b[i] - tail_stencil<T>(P, x1, g, y, x);
+        }
+        __syncthreads();
+        T* bc = vb(l + 1);
+        for (int k = threadIdx.x; k < gc.h * gc.w; k += kTailThreads) {
+            const int Y = k / gc.w, X = k - Y * gc.w;
+            T sum = T(0);
+#pragma unroll
+            for (int ay = -1; ay <= 1; ++ay)
+#pragma unroll
+                for (int ax = -1; ax <= 1; ++ax)
+                    sum += (T)(pw(ax) * pw(ay) / 16.0) * tail_val<T>(t, g, 2 * Y + ay, 2 * X + ax);
+            bc[Y * gc.pitch + X] = sum;
+        }
+        __syncthreads();
+    }
+    // Coarsest: x = inv b, one warp per row.
+    {
+        const GridDesc g = D.lev[nlev - 1].g;
+        const int n = g.h * g.w;
+        const T* b = vb(nlev - 1);
+        T* x = vx(nlev - 1);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int q = warp; q < n; q += kTailThreads / 32) {
+            const double* row = D.inv + (int64_t)q * n;
+            double acc = 0.0;
+            for (int j = lane; j < n; j += 32) {
+                const int yj = j / g.w, xj = j - yj * g.w;
+                acc += row[j] * (double)b[yj * g.pitch + xj];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                const int yq = q / g.w, xq = q - yq * g.w;
+                x[yq * g.pitch + xq] = (T)acc;
+            }
+        }
+    }
+    __syncthreads();
+    // Up.
+    for (int l = nlev - 2; l >= 0; --l) {
+        const GridDesc g = D.lev[l].g, gc = D.lev[l + 1].g;
+        const int n = g.h * g.w;
+        const T* P = planes(l);
+        const T* b = vb(l);
+        const T* xc = vx(l + 1);
+        T* x = vx(l);
+        T* t = vt(l);
+        for (int k = threadIdx.x; k < n; k += kTailThreads) {
+            const int y = k / g.w, xx = k - y * g.w;
+            const int Ya = (y - 1) >> 1, Xa = (xx - 1) >> 1;
+            const bool ey = (y & 1) == 0, ex = (xx & 1) == 0;
+            T sum = T(0);
+#pragma unroll
+            for (int jy = 0; jy < 2; ++jy) {
+                const int Y = ey ? (y >> 1) : Ya + jy;
+                if ((ey && jy == 1) || Y >= gc.h) continue;
+                const double wy = ey ? 2.0 : 1.0;
+#pragma unroll
+                for (int jx = 0; jx < 2; ++jx) {
+                    const int Xc = ex ? (xx >> 1) : Xa + jx;
+                    if ((ex && jx == 1) || Xc >= gc.w) continue;
+                    const double wx = ex ? 2.0 : 1.0;
+                    sum += (T)(wx * wy / 16.0) * xc[Y * gc.pitch + Xc];
+                }
+            }
+            const int i = y * g.pitch + xx;
+            t[i] = x[i] + sum;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += kTailThreads) {
+            const int y = k / g.w, xx = k - y * g.w, i = y * g.pitch + xx;
+            const T ax = tail_stencil<T>(P, t, g, y, xx);
+            x[i] = t[i] + om * (b[i] - ax) / P[i];
+        }
+        __syncthreads();
+    }
+    // Copy out the first level's solution.
+    {
+        const GridDesc g = D.lev[0].g;
+        const T* src = vx(0);
+        for (int k = threadIdx.x; k < g.h * g.w; k += kTailThreads) {
+            const int y = k / g.w, x = k - y * g.w;
+            D.lev[0].x[g.voff + (int64_t)y * g.pitch + x] = src[y * g.pitch + x];
+        }
+    }
+}
+
+template <typename T>
+void launch_vc_tail(const TailDesc<T>* descs, int count, size_t smem, const InstState* st,
+                    double omega, int* err, cudaStream_t s) {
+    if (count > 0) k_vc_tail<T><<<count, kTailThreads, smem, s>>>(descs, st, omega, err);
+}
+
 // Shared-memory sizes; they follow the SmemCarve layout of each kernel (two
 // pipeline buffers, every piece rounded up to 128 bytes).
 static inline size_t rup(size_t b) { return (b + 127) & ~size_t(127); }
@@ -1820,6 +2019,7 @@ static void prepare_type() {
     allow_smem(k_vc_smooth<T>, smem_init<T>());
     allow_smem(k_apply<T>, smem_init<T>());
     allow_smem(k_apply_v<T, kVApply<T>>, smem_apply_v<T>());
+    allow_smem(k_vc_tail<T>, kTailSmem);
     allow_smem(k_cg_apply_v<T, kVSolve<T>>, smem_apply_v<T>());
     allow_smem(k_vc_down_v<T, kVSolve<T>>, smem_down_v<T>());
     allow_smem(k_vc_up_v<T, kVSolve<T>>, smem_up_v<T>());
@@ -1876,6 +2076,10 @@ PMB_INST(double)
 PMB_INST(float)
 #undef PMB_INST
 
+template void launch_vc_tail<double>(const TailDesc<double>*, int, size_t, const InstState*,
+                                     double, int*, cudaStream_t);
+template void launch_vc_tail<float>(const TailDesc<float>*, int, size_t, const InstState*, double,
+                                    int*, cudaStream_t);
 template void launch_pack<double, double>(const GridDesc*, int, const int64_t*, const double*, double*, int64_t, cudaStream_t);
 template void launch_pack<double, float>(const GridDesc*, int, const int64_t*, const double*, float*, int64_t, cudaStream_t);
 template void launch_pack<float, double>(const GridDesc*, int, const int64_t*, const float*, double*, int64_t, cudaStream_t);

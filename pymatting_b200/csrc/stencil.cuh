@@ -20,6 +20,32 @@ struct DirectDesc {
     int64_t work_off;   // n x n scratch used while inverting (setup only)
 };
 
+// Coarse-level tail (one CTA per image, shared-memory resident; k_vc_tail).
+constexpr int kTailThreads = 1024;
+constexpr int kMaxTailLevels = 16;
+constexpr size_t kTailSmem = 212 * 1024;   // planes + 3 vectors of all tail levels (pitched)
+
+template <typename T>
+struct TailLevel {
+    GridDesc g;
+    const T* P;     // planes
+    T* b;           // right-hand side (read for the first tail level)
+    T* x;           // solution (written for the first tail level)
+};
+
+template <typename T>
+struct TailDesc {
+    int nlev;               // tail levels; the last is solved with `inv`
+    int inst;               // image
+    int pad_[2];
+    const double* inv;      // dense inverse of the last level
+    TailLevel<T> lev[kMaxTailLevels];
+};
+
+template <typename T>
+void launch_vc_tail(const TailDesc<T>* descs, int count, size_t smem, const InstState* st,
+                    double omega, int* err, cudaStream_t s);
+
 // Shared memory (bytes) of the TMA-tiled kernels, for launch sizing.
 template <typename T> size_t smem_apply();
 template <typename T> size_t smem_init();
