@@ -1414,6 +1414,7 @@ PMB_API int pmb_ichol_factor(pmb_ichol* p, const int64_t* Ap, const int64_t* Ar,
     Ichol& I = p->I;
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t n = I.n, W = I.W;
+    ichol_prepare();
     PMB_CUDA(cudaMemsetAsync(I.ws + I.o_F, 0, sizeof(double) * W * W, s));
     PMB_CUDA(cudaMemsetAsync(I.ws + I.o_pat, 0, (size_t)(W * W), s));
     ichol_launch_init(n, Ap, Ar, Av, shift, I.at<double>(I.o_d), I.at<double>(I.o_rsum),

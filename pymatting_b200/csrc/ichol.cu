@@ -29,6 +29,7 @@
 namespace pmb {
 
 constexpr int kIcholThreads = 1024;
+constexpr int64_t kIcholSmemRows = 27 * 1024;   // x of the shared-memory solve: 216 KB
 
 // Per-column statistics of A (lower part, CSC): diagonal (+ shift), sum of
 // |A[j:, j]| for the relative threshold, and the largest i - j.
@@ -336,6 +337,88 @@ k_ichol_solve(int64_t n, int nlevels, const int64_t* __restrict__ lptr, const in
     }
 }
 
+// The same solves with x in shared memory (n <= kIcholSmemRows) and one warp
+// per row: the lanes split the row's dot product (so the subtractions of a
+// row are summed in a different order than the reference, a difference of
+// rounding only) and each warp loads the index/value data of its first row
+// of the next level before the level barrier, so a level costs one shared-
+// memory gather, a warp reduction and a barrier.
+struct RowPrefetch {
+    int64_t i, k0, k1;
+    int64_t c;     // first entry of this lane (column / row index)
+    double v;
+};
+
+template <bool FWD>
+__device__ __forceinline__ RowPrefetch prefetch_row(int64_t q, int64_t qend, const int* order,
+                                                    const int64_t* Xp, const int64_t* Xi,
+                                                    const double* Xv, int lane) {
+    RowPrefetch r{-1, 0, 0, 0, 0.0};
+    if (q < qend) {
+        r.i = order[q];
+        r.k0 = Xp[r.i] + (FWD ? 0 : 1);
+        r.k1 = Xp[r.i + 1];
+        const int64_t k = r.k0 + lane;
+        if (k < r.k1) {
+            r.c = Xi[k];
+            r.v = Xv[k];
+        }
+    }
+    return r;
+}
+
+template <bool FWD>
+__device__ __forceinline__ void solve_sweep(int nlevels, const int64_t* __restrict__ lptr,
+                                            const int* __restrict__ order,
+                                            const int64_t* __restrict__ Xp,
+                                            const int64_t* __restrict__ Xi,
+                                            const double* __restrict__ Xv,
+                                            const int64_t* __restrict__ Lp,
+                                            const double* __restrict__ Lv, double* sx) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int l = FWD ? 0 : nlevels - 1;
+    RowPrefetch pf = prefetch_row<FWD>(lptr[l] + warp, lptr[l + 1], order, Xp, Xi, Xv, lane);
+    for (int step = 0; step < nlevels; ++step, l += FWD ? 1 : -1) {
+        const int64_t qend = lptr[l + 1];
+        int64_t q = lptr[l] + warp;
+        RowPrefetch cur = pf;
+        // Prefetch this warp's first row of the next level (its data does
+        // not depend on x).
+        if (step + 1 < nlevels) {
+            const int ln = FWD ? l + 1 : l - 1;
+            pf = prefetch_row<FWD>(lptr[ln] + warp, lptr[ln + 1], order, Xp, Xi, Xv, lane);
+        }
+        while (cur.i >= 0) {
+            double acc = (cur.k0 + lane < cur.k1) ? cur.v * sx[cur.c] : 0.0;
+            for (int64_t k = cur.k0 + 32 + lane; k < cur.k1; k += 32) acc += Xv[k] * sx[Xi[k]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) sx[cur.i] = (sx[cur.i] - acc) / Lv[Lp[cur.i]];
+            q += nw;
+            cur = prefetch_row<FWD>(q, qend, order, Xp, Xi, Xv, lane);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kIcholThreads)
+k_ichol_solve_smem(int64_t n, int nlevels, const int64_t* __restrict__ lptr,
+                   const int* __restrict__ order, const int64_t* __restrict__ Lp,
+                   const int64_t* __restrict__ Lr, const double* __restrict__ Lv,
+                   const int64_t* __restrict__ Rp, const int64_t* __restrict__ Rc,
+                   const double* __restrict__ Rv, const double* __restrict__ b, double* x,
+                   const InstState* st) {
+    extern __shared__ double s_x[];
+    if (st && st->status != kRunning) return;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s_x[i] = b[i];
+    __syncthreads();
+    if (nlevels > 0) {
+        solve_sweep<true>(nlevels, lptr, order, Rp, Rc, Rv, Lp, Lv, s_x);
+        solve_sweep<false>(nlevels, lptr, order, Lp, Lr, Lv, Lp, Lv, s_x);
+    }
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = s_x[i];
+}
+
 // The forward sweep above overwrites x in place: y lives in x. For the
 // forward pass to read y_j of earlier levels and b_i of its own row, b and
 // x may alias (the reference also works in place on a copy of b).
@@ -380,10 +463,22 @@ void ichol_launch_row_fill(int64_t n, const int64_t* Lp, const int64_t* Lr, cons
     }
 }
 
+// Raise the shared-memory limit of the shared-memory solve; called when a
+// factor is built, before any solve can be captured.
+void ichol_prepare() {
+    cudaFuncSetAttribute(k_ichol_solve_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kIcholSmemRows * sizeof(double)));
+}
+
 void ichol_launch_solve(int64_t n, int nlevels, const int64_t* lptr, const int* order,
                         const int64_t* Lp, const int64_t* Lr, const double* Lv, const int64_t* Rp,
                         const int64_t* Rc, const double* Rv, const double* b, double* x,
                         const InstState* st, cudaStream_t s) {
+    if (n <= kIcholSmemRows) {
+        k_ichol_solve_smem<<<1, kIcholThreads, n * sizeof(double), s>>>(
+            n, nlevels, lptr, order, Lp, Lr, Lv, Rp, Rc, Rv, b, x, st);
+        return;
+    }
     k_ichol_solve<<<1, kIcholThreads, 0, s>>>(n, nlevels, lptr, order, Lp, Lr, Lv, Rp, Rc, Rv, b, x, st);
 }
 

@@ -21,6 +21,7 @@ void ichol_launch_rows(int64_t n, const int64_t* Lp, const int64_t* Lr, const do
 void ichol_launch_row_fill(int64_t n, const int64_t* Lp, const int64_t* Lr, const double* Lv,
                            int64_t* rfill, int64_t* Rc, double* Rv, const int64_t* Rp,
                            cudaStream_t s);
+void ichol_prepare();
 void ichol_launch_solve(int64_t n, int nlevels, const int64_t* lptr, const int* order,
                         const int64_t* Lp, const int64_t* Lr, const double* Lv, const int64_t* Rp,
                         const int64_t* Rc, const double* Rv, const double* b, double* x,
