@@ -62,6 +62,14 @@ int pmb_cf_laplacian_planes(const double* image, const uint8_t* is_known, int h,
                             double epsilon, const uint8_t* diag_mask, double diag_value,
                             double* planes, void* stream);
 
+/* grad[k] = d(mu' L(image) x) / d image[k] (h*w*3, same layout as image)
+ * for the radius-1 Laplacian, with windows skipped where is_known (may be
+ * null) covers them, as in cf_laplacian. For the adjoint of a solve through
+ * the Laplacian; no counterpart in the reference (it has no gradients). */
+int pmb_cf_laplacian_vjp(const double* image, const uint8_t* is_known, int h, int w,
+                         double epsilon, const double* x, const double* mu, double* grad,
+                         void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

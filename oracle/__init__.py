@@ -346,3 +346,62 @@ def solve_soft(image, trimap, preconditioner="vcycle", rtol=1e-7, atol=0.0,
     cb = CounterCallback()
     x = cg(A, b, M=M, rtol=rtol, atol=atol, maxiter=maxiter, callback=cb)
     return x, cb.n
+
+
+# --------------------------------------------------------------------------
+# Gradients of the soft-constraint alpha (no reference counterpart: PyMatting
+# has no autodiff). FP64 restatement used to check the adjoint kernels.
+# --------------------------------------------------------------------------
+
+def soft_alpha_exact(image, trimap, lambda_value=100.0, epsilon=1e-7):
+    """alpha = A^-1 b for make_linear_system(cf_laplacian(image), trimap), solved
+    directly (sparse LU), as a smooth function of the image."""
+    L = cf_laplacian(image, epsilon)
+    A, b = make_linear_system(L, trimap, lambda_value)
+    return scipy.sparse.linalg.spsolve(A.tocsc(), b)
+
+
+def cf_laplacian_vjp(image, x, mu, epsilon=1e-7):
+    """d(mu' L(image) x) / d image, shape (h, w, 3), for the radius-1 matting
+    Laplacian with every window active (cf_laplacian.py:31-129 differentiated):
+    per window, mu' L_w x = sum mu_i x_i - 9 mu_bar x_bar - u' D v / 9 with
+    u = sum mu_i c_i, v = sum x_i c_i, D = ((eps I + sum c_i c_i') / 9)^-1."""
+    image = np.asarray(image, dtype=np.float64)
+    h, w, _ = image.shape
+    x = np.asarray(x, dtype=np.float64).reshape(h, w)
+    mu = np.asarray(mu, dtype=np.float64).reshape(h, w)
+    ys, xs = np.mgrid[1:h - 1, 1:w - 1]
+    ys, xs = ys.ravel(), xs.ravel()
+    offs = [(dy, dx) for dy in (-1, 0, 1) for dx in (-1, 0, 1)]
+    py = np.stack([ys + dy for dy, dx in offs], axis=1)          # (nw, 9)
+    px = np.stack([xs + dx for dy, dx in offs], axis=1)
+    I = image[py, px]                                            # (nw, 9, 3)
+    c = I - I.mean(axis=1, keepdims=True)
+    a = (epsilon * np.eye(3) + np.einsum("wki,wkj->wij", c, c)) / 9.0
+    D = np.linalg.inv(a)
+    m = mu[py, px]
+    xv = x[py, px]
+    u = np.einsum("wk,wki->wi", m, c)
+    v = np.einsum("wk,wki->wi", xv, c)
+    p = np.einsum("wij,wj->wi", D, u)
+    q = np.einsum("wij,wj->wi", D, v)
+    dm = m - m.mean(axis=1, keepdims=True)
+    dx = xv - xv.mean(axis=1, keepdims=True)
+    cq = np.einsum("wki,wi->wk", c, q)
+    cp = np.einsum("wki,wi->wk", c, p)
+    term = (dm[:, :, None] * q[:, None, :] + dx[:, :, None] * p[:, None, :]
+            - (p[:, None, :] * cq[:, :, None] + q[:, None, :] * cp[:, :, None]) / 9.0) / 9.0
+    grad = np.zeros((h, w, 3))
+    np.add.at(grad, (py.ravel(), px.ravel()), -term.reshape(-1, 3))
+    return grad
+
+
+def soft_alpha_grad(image, trimap, g, lambda_value=100.0, epsilon=1e-7):
+    """d(g . alpha) / d image with alpha = soft_alpha_exact(image, trimap):
+    adjoint solve A mu = g, then -d(mu' L x) / d image."""
+    L = cf_laplacian(image, epsilon)
+    A, b = make_linear_system(L, trimap, lambda_value)
+    lu = scipy.sparse.linalg.splu(A.tocsc())
+    x = lu.solve(b)
+    mu = lu.solve(np.asarray(g, dtype=np.float64).ravel())
+    return -cf_laplacian_vjp(image, x, mu, epsilon)

@@ -5,7 +5,8 @@ Drop-in replacements for ``cf_laplacian``, ``make_linear_system``, ``cg``
 ``vcycle`` / ``ichol`` preconditioner factories and ``estimate_alpha_cf``,
 computed by hand-written sm_100a kernels behind a C ABI
 (``include/pymatting_b200.h``). Extensions without a reference counterpart:
-``solve_alpha`` (batched, mixed-precision soft-constraint solves).
+``solve_alpha`` (batched, mixed-precision soft-constraint solves) and
+``cf_alpha`` (alpha differentiable with respect to the image).
 """
 
 from .util import trimap_split, sanity_check_image
@@ -13,11 +14,12 @@ from .laplacian import cf_laplacian, make_linear_system, DeviceCSRMatrix
 from .preconditioner import jacobi, vcycle, ichol, CholeskyDecomposition
 from .solver import cg, CounterCallback, ProgressCallback
 from .alpha import estimate_alpha_cf, estimate_alpha
+from .autograd import cf_alpha
 
 __version__ = "0.1.0"
 
 __all__ = [
     "trimap_split", "sanity_check_image", "cf_laplacian", "make_linear_system",
     "DeviceCSRMatrix", "jacobi", "vcycle", "ichol", "CholeskyDecomposition", "cg",
-    "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha",
+    "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
 ]

@@ -552,3 +552,155 @@ int pmb_launch_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t*
     if (pmb_launch_flag_unknown(is_known, n, cidx, s)) return -2;
     return pmb_scan_exclusive(cidx, n + 1, scratch, scratch + nchunks, s);
 }
+
+// --------------------------------------------------------------------------
+// Vector-Jacobian product of the Laplacian with respect to the image
+// --------------------------------------------------------------------------
+//
+// grad[k] = d(mu' L(I) x) / d I_k for the radius-1 Laplacian of
+// cf_laplacian.py (no counterpart in the reference, which has no gradients).
+// Per active window w with centred colours c_i = I_i - mean_w,
+// Delta_w = ((eps I + sum_i c_i c_i') / 9)^-1, u = sum_i mu_i c_i,
+// v = sum_i x_i c_i, p = Delta u, q = Delta v, mu_bar / x_bar the window
+// means of mu / x, the window's part of mu' L x is
+//     sum_i mu_i x_i - 9 mu_bar x_bar - u' Delta v / 9,
+// whose derivative with respect to I_k (the mean's contribution cancels
+// because sum_i c_i = 0) is
+//     -[(mu_k - mu_bar) q + (x_k - x_bar) p - (p (c_k . q) + q (c_k . p)) / 9] / 9.
+// The window coefficients are recomputed from the image (same arithmetic as
+// the assembly); each pixel gathers its windows in raster order, so the
+// result is deterministic. One 16x16 tile of pixels per CTA.
+
+namespace pmb {
+
+__global__ void __launch_bounds__(kAT * kAT)
+cf_vjp_kernel(const double* __restrict__ image, const uint8_t* __restrict__ known, int h, int w,
+              double eps, const double* __restrict__ xs, const double* __restrict__ mus,
+              double* __restrict__ grad) {
+    constexpr int IW = kAT + 4;            // pixel tile with a 2-pixel halo
+    constexpr int WW = kAT + 2;            // windows touching the tile
+    __shared__ double s_img[IW * IW * 3];
+    __shared__ double s_x[IW * IW];
+    __shared__ double s_mu[IW * IW];
+    __shared__ uint8_t s_known[IW * IW];
+    __shared__ double s_mean[WW * WW * 3];
+    __shared__ double s_p[WW * WW * 3];
+    __shared__ double s_q[WW * WW * 3];
+    __shared__ double s_bar[WW * WW * 2];
+    __shared__ uint8_t s_act[WW * WW];
+    const int x0 = blockIdx.x * kAT, y0 = blockIdx.y * kAT;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < IW * IW; q += blockDim.x) {
+        const int ly = q / IW, lx = q % IW;
+        const int y = y0 - 2 + ly, x = x0 - 2 + lx;
+        const bool in = (y >= 0 && y < h && x >= 0 && x < w);
+        const int64_t gi = (int64_t)y * w + x;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s_img[q * 3 + c] = in ? image[gi * 3 + c] : 0.0;
+        s_x[q] = in ? xs[gi] : 0.0;
+        s_mu[q] = in ? mus[gi] : 0.0;
+        s_known[q] = in ? (known ? known[gi] : 0) : 1;
+    }
+    __syncthreads();
+    const double wa = 9.0;
+    for (int q = tid; q < WW * WW; q += blockDim.x) {
+        const int ly = q / WW, lx = q % WW;
+        const int ky = y0 - 1 + ly, kx = x0 - 1 + lx;
+        bool act = (ky >= 1 && ky < h - 1 && kx >= 1 && kx < w - 1);
+        if (act) {
+            bool all_known = true;
+            for (int dy = 0; dy < 3; ++dy)
+                for (int dx = 0; dx < 3; ++dx)
+                    all_known = all_known && s_known[(ly + dy) * IW + (lx + dx)];
+            act = !all_known;
+        }
+        s_act[q] = act;
+        if (!act) continue;
+        double mean[3];
+        for (int c = 0; c < 3; ++c) {
+            double s = 0.0;
+            for (int dy = 0; dy < 3; ++dy)
+                for (int dx = 0; dx < 3; ++dx) s += s_img[((ly + dy) * IW + (lx + dx)) * 3 + c];
+            mean[c] = s / wa;
+            s_mean[q * 3 + c] = mean[c];
+        }
+        double a00 = eps, a01 = 0.0, a02 = 0.0, a11 = eps, a12 = 0.0, a22 = eps;
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0, v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        double mb = 0.0, xb = 0.0;
+        for (int dy = 0; dy < 3; ++dy) {
+            for (int dx = 0; dx < 3; ++dx) {
+                const int t = (ly + dy) * IW + (lx + dx);
+                const double* p = s_img + t * 3;
+                const double c0 = p[0] - mean[0], c1 = p[1] - mean[1], c2 = p[2] - mean[2];
+                a00 += c0 * c0;
+                a01 += c0 * c1;
+                a02 += c0 * c2;
+                a11 += c1 * c1;
+                a12 += c1 * c2;
+                a22 += c2 * c2;
+                const double m = s_mu[t], xv = s_x[t];
+                u0 += m * c0; u1 += m * c1; u2 += m * c2;
+                v0 += xv * c0; v1 += xv * c1; v2 += xv * c2;
+                mb += m;
+                xb += xv;
+            }
+        }
+        a00 /= wa; a01 /= wa; a02 /= wa;
+        a11 /= wa; a12 /= wa; a22 /= wa;
+        const double det = a00 * a12 * a12 + a01 * a01 * a22 + a02 * a02 * a11
+                           - a00 * a11 * a22 - 2 * a01 * a02 * a12;
+        const double inv_det = 1.0 / det;
+        const double m00 = (a12 * a12 - a11 * a22) * inv_det;
+        const double m01 = (a01 * a22 - a02 * a12) * inv_det;
+        const double m02 = (a02 * a11 - a01 * a12) * inv_det;
+        const double m11 = (a02 * a02 - a00 * a22) * inv_det;
+        const double m12 = (a00 * a12 - a01 * a02) * inv_det;
+        const double m22 = (a01 * a01 - a00 * a11) * inv_det;
+        s_p[q * 3 + 0] = m00 * u0 + m01 * u1 + m02 * u2;
+        s_p[q * 3 + 1] = m01 * u0 + m11 * u1 + m12 * u2;
+        s_p[q * 3 + 2] = m02 * u0 + m12 * u1 + m22 * u2;
+        s_q[q * 3 + 0] = m00 * v0 + m01 * v1 + m02 * v2;
+        s_q[q * 3 + 1] = m01 * v0 + m11 * v1 + m12 * v2;
+        s_q[q * 3 + 2] = m02 * v0 + m12 * v1 + m22 * v2;
+        s_bar[q * 2 + 0] = mb / wa;
+        s_bar[q * 2 + 1] = xb / wa;
+    }
+    __syncthreads();
+    const int tx = tid % kAT, ty = tid / kAT;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= w || y >= h) return;
+    const int t = (ty + 2) * IW + (tx + 2);
+    const double* Ik = s_img + t * 3;
+    const double mk = s_mu[t], xk = s_x[t];
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    for (int wy = 0; wy < 3; ++wy) {
+        for (int wx = 0; wx < 3; ++wx) {
+            const int q = (ty + wy) * WW + (tx + wx);
+            if (!s_act[q]) continue;
+            const double c0 = Ik[0] - s_mean[q * 3 + 0];
+            const double c1 = Ik[1] - s_mean[q * 3 + 1];
+            const double c2 = Ik[2] - s_mean[q * 3 + 2];
+            const double p0 = s_p[q * 3 + 0], p1 = s_p[q * 3 + 1], p2 = s_p[q * 3 + 2];
+            const double q0 = s_q[q * 3 + 0], q1 = s_q[q * 3 + 1], q2 = s_q[q * 3 + 2];
+            const double dm = mk - s_bar[q * 2 + 0], dx = xk - s_bar[q * 2 + 1];
+            const double cq = c0 * q0 + c1 * q1 + c2 * q2;
+            const double cp = c0 * p0 + c1 * p1 + c2 * p2;
+            g0 -= (dm * q0 + dx * p0 - (p0 * cq + q0 * cp) / wa) / wa;
+            g1 -= (dm * q1 + dx * p1 - (p1 * cq + q1 * cp) / wa) / wa;
+            g2 -= (dm * q2 + dx * p2 - (p2 * cq + q2 * cp) / wa) / wa;
+        }
+    }
+    const int64_t gi = (int64_t)y * w + x;
+    grad[gi * 3 + 0] = g0;
+    grad[gi * 3 + 1] = g1;
+    grad[gi * 3 + 2] = g2;
+}
+
+}  // namespace pmb
+
+int pmb_launch_cf_vjp(const double* image, const uint8_t* known, int h, int w, double eps,
+                      const double* x, const double* mu, double* grad, cudaStream_t s) {
+    const dim3 grid((w + pmb::kAT - 1) / pmb::kAT, (h + pmb::kAT - 1) / pmb::kAT);
+    pmb::cf_vjp_kernel<<<grid, pmb::kAT * pmb::kAT, 0, s>>>(image, known, h, w, eps, x, mu, grad);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}

@@ -983,6 +983,20 @@ PMB_API int pmb_cf_laplacian_planes(const double* image, const uint8_t* is_known
     return 0;
 }
 
+int pmb_launch_cf_vjp(const double*, const uint8_t*, int, int, double, const double*,
+                      const double*, double*, cudaStream_t);
+
+PMB_API int pmb_cf_laplacian_vjp(const double* image, const uint8_t* is_known, int h, int w,
+                                 double epsilon, const double* x, const double* mu, double* grad,
+                                 void* stream) {
+    if (!image || !x || !mu || !grad || h <= 0 || w <= 0)
+        return fail(kErrArg, "pmb_cf_laplacian_vjp: bad arguments");
+    if (pmb_launch_cf_vjp(image, is_known, h, w, epsilon, x, mu, grad, (cudaStream_t)stream))
+        return fail(kErrCuda, std::string("cf_laplacian_vjp launch: ") +
+                                  cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, const uint8_t* is_fg,
                                int h, int w, double epsilon, double* planes, double* rhs,
                                void* stream) {

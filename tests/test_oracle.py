@@ -130,3 +130,25 @@ def test_synthetic_320x240_estimate_alpha_cf():
     alpha = oracle.estimate_alpha_cf(img, tri)
     unknown = (tri > 0.1) & (tri < 0.9)
     np.testing.assert_allclose(alpha[unknown], g["alpha_unknown"], rtol=0, atol=1e-9)
+
+
+def test_oracle_laplacian_vjp_matches_finite_differences():
+    """The FP64 restatement of d(mu' L(I) x)/dI that the adjoint kernels are
+    checked against, pinned by central differences of the oracle Laplacian."""
+    rng = np.random.default_rng(3)
+    h, w = 9, 11
+    img = rng.random((h, w, 3))
+    x = rng.standard_normal(h * w)
+    mu = rng.standard_normal(h * w)
+    eps = 1e-2   # keeps the window covariances well conditioned for differences
+
+    def phi(im):
+        return mu @ (oracle.cf_laplacian(im, eps) @ x)
+
+    grad = oracle.cf_laplacian_vjp(img, x, mu, eps)
+    step = 1e-6
+    for (y, xx, c) in [(0, 0, 0), (4, 5, 1), (8, 10, 2), (3, 7, 0), (6, 2, 2)]:
+        e = np.zeros_like(img)
+        e[y, xx, c] = step
+        fd = (phi(img + e) - phi(img - e)) / (2 * step)
+        assert abs(fd - grad[y, xx, c]) <= 1e-6 * max(1.0, abs(fd)), (y, xx, c, fd, grad[y, xx, c])
