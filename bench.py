@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["1080p", "4096", "batch64"], default="1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", choices=["auto", "none"], default="auto",
+                    help="run the launch-shape autotuner before timing (none: defaults)")
     ap.add_argument("--profile", choices=["apply", "solve", "solve-fp64", "solve-mixed"],
                     default=None,
                     help="profiling case: a few operator applies, or one solve per precision "
@@ -283,7 +285,7 @@ def main():
     clocks = ClockSampler(local)
 
     def device_step(precision):
-        batch = AlphaBatch(imgs_d, tris_d, precision=precision)
+        batch = AlphaBatch(imgs_d, tris_d, precision=precision, tune="cached")
         x = batch.solve()
         alphas = batch.alphas(x)
         return batch, x, alphas
@@ -316,6 +318,10 @@ def main():
             return float(t.item())
         return v
 
+    # Launch shapes: the autotuner runs once per precision before any timing
+    # (its result is a cached launch configuration, not a cached output).
+    tunings = {p: (AlphaBatch(imgs_d, tris_d, precision=p, tune="auto").tuning
+                   if args.tune == "auto" else None) for p in ["fp64", "mixed"]}
     results = {}
     clocks.start()
     for precision in ["fp64", "mixed"]:
@@ -339,12 +345,19 @@ def main():
     rel_fp64 = float(torch.linalg.norm(b64.b - ax) / torch.linalg.norm(b64.b))
     alpha_diff = float((torch.clamp(results["mixed"]["x"], 0, 1) -
                         torch.clamp(results["fp64"]["x"], 0, 1)).abs().max())
+    # Error of both results against a tight FP64 solve (rel-res 1e-12) of the
+    # same system, outside the timed region: at rel-res 1e-7 weakly
+    # constrained unknown regions still move, in either precision.
+    x_tight = b64.solve(rtol=1e-12)
+    alpha_err = {p: float((torch.clamp(results[p]["x"], 0, 1) - torch.clamp(x_tight, 0, 1))
+                          .abs().max()) for p in ["fp64", "mixed"]}
 
     # End to end through the public API with host buffers.
     for _ in range(max(1, args.warmup)):
-        solve_alpha(imgs, tris, precision="mixed")
+        solve_alpha(imgs, tris, precision="mixed", tune="cached")
     barrier()
-    e2e_times, _ = timed(lambda: solve_alpha(imgs, tris, precision="mixed"), args.steps)
+    e2e_times, _ = timed(lambda: solve_alpha(imgs, tris, precision="mixed", tune="cached"),
+                         args.steps)
     e2e_ms = max_over_ranks(sum(e2e_times))
     clock_rec = clocks.stop()
 
@@ -386,6 +399,7 @@ def main():
                 "precision": "mixed (FP32 inner rtol 1e-4, FP64 refinement)",
                 "l2": "flushed between steps (256 MB write); planes exceed L2",
                 "parallelism": "weak: one image per GPU, no collective",
+                "launch_shapes": {p: (t or {}).get("knobs") for p, t in tunings.items()},
             },
             "fp64_value": value64,
             "mixed_over_fp64": value / value64,
@@ -393,6 +407,7 @@ def main():
                       "fp64": st_d.iters},
             "rel_residual_fp64": {"mixed": rel_mixed, "fp64": rel_fp64},
             "alpha_maxabs_mixed_vs_fp64": alpha_diff,
+            "alpha_maxabs_vs_fp64_rtol1e-12": alpha_err,
             "roofline": {
                 "bound": "hbm",
                 "kernel": "half-stencil Laplacian apply y = (L + lambda D) x, FP32",

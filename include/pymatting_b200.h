@@ -117,6 +117,15 @@ int pmb_stencil_stats(pmb_stencil* s, int image, int* iters, int* status, double
  * CUDA graphs included). */
 int64_t pmb_stencil_launch_count(const pmb_stencil* s);
 int pmb_stencil_destroy(pmb_stencil* s);
+/* Launch-shape knobs of the solver, for the autotuner (no counterpart in the
+ * reference): 0 vector width of the CG apply (2 or 4 pixels per thread, 4
+ * only for the FP32 inner solve), 1 the same for the prolongation, 2/3/4
+ * resident CTAs per SM of the level-0 tile kernels / prolongation /
+ * restriction (up to the shared-memory limit), 5 CTAs per SM of the
+ * element-wise kernels, 6 CG iterations per graph replay. Returns the value
+ * applied (after clamping) or a negative status. */
+int pmb_stencil_tune(pmb_stencil* s, int knob, int value);
+int pmb_stencil_tuning(const pmb_stencil* s, int knob);
 /* Average milliseconds of one level-0 operator apply y = A x (inner
  * precision), timed with CUDA events on the solver's stream over `iters`
  * launches. Benchmark hook; no reference counterpart. */

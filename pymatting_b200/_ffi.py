@@ -55,6 +55,8 @@ _SIGNATURES = {
     "pmb_stencil_launch_count": (c_i64, [c_vp]),
     "pmb_stencil_time_apply": (c_int, [c_vp, c_int, ctypes.POINTER(c_dbl), c_vp]),
     "pmb_stencil_destroy": (c_int, [c_vp]),
+    "pmb_stencil_tune": (c_int, [c_vp, c_int, c_int]),
+    "pmb_stencil_tuning": (c_int, [c_vp, c_int]),
     "pmb_csr_create": (c_int, [c_i64, c_i64, c_int, ctypes.POINTER(c_vp)]),
     "pmb_csr_workspace_bytes": (c_i64, [c_vp]),
     "pmb_csr_bind": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

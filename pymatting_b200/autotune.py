@@ -1,0 +1,145 @@
+"""Autotuner for the stencil solver's launch shapes (no reference counterpart).
+
+The knobs (``pmb_stencil_tune`` in the C ABI):
+
+* ``vec_apply`` / ``vec_up`` — pixels per thread of the CG apply and of the
+  prolongation kernel (2 or 4; 4 halves the threads per CTA and the shared
+  loads per pixel, FP32 only);
+* ``ctas_fine`` / ``ctas_up`` / ``ctas_down`` — resident CTAs per SM of the
+  level-0 tile kernels, the prolongation and the restriction (bounded by
+  their shared memory);
+* ``ctas_flat`` — CTAs per SM of the element-wise kernels;
+* ``chunk`` — CG iterations per CUDA-graph replay (the host reads the
+  per-image status once per replay).
+
+``autotune(batch)`` times full solves of the batch's own system with CUDA
+events and walks the knobs one at a time (coordinate descent, two passes),
+keeping a value only when it is faster by more than the noise margin. The
+result is cached in memory under a key of precision, preconditioner, device
+and problem shape, and in the JSON file named by ``PMB_TUNE_CACHE`` if set;
+``apply_tuning`` sets a cached result on another system of the same shape.
+"""
+
+import json
+import os
+
+import torch
+
+from . import _device as dev
+from . import _ffi
+
+__all__ = ["KNOBS", "tuning", "apply_tuning", "autotune", "cache_key", "cached"]
+
+KNOBS = {"vec_apply": 0, "vec_up": 1, "ctas_fine": 2, "ctas_up": 3, "ctas_down": 4,
+         "ctas_flat": 5, "chunk": 6}
+CANDIDATES = {"vec_apply": [2, 4], "vec_up": [2, 4], "ctas_fine": [1, 2, 3, 4],
+              "ctas_up": [1, 2, 3, 4], "ctas_down": [1, 2, 3, 4], "ctas_flat": [2, 4, 8, 16],
+              "chunk": [2, 4, 8]}
+_MARGIN = 0.02          # a change must win by 2 %
+_CACHE = {}
+
+
+def tuning(system):
+    """Current knob values of a StencilSystem."""
+    lib = _ffi.lib()
+    return {k: int(lib.pmb_stencil_tuning(system._h, v)) for k, v in KNOBS.items()}
+
+
+def apply_tuning(system, values):
+    """Set knob values (dict name -> int); returns the values applied."""
+    lib = _ffi.lib()
+    out = {}
+    for name, val in values.items():
+        rc = int(lib.pmb_stencil_tune(system._h, KNOBS[name], int(val)))
+        if rc < 0:
+            _ffi.check(rc, "pmb_stencil_tune")
+        out[name] = rc
+    return out
+
+
+def cache_key(batch):
+    shapes = sorted(batch.shapes)
+    if len(shapes) > 4:
+        npx = sum(h * w for h, w in shapes)
+        shape_key = ("batch", len(shapes), int(round(npx / 1e5)))
+    else:
+        shape_key = tuple(shapes)
+    return (batch.system.precision, batch.system.preconditioner,
+            torch.cuda.get_device_name(dev.device()), shape_key)
+
+
+def _file():
+    return os.environ.get("PMB_TUNE_CACHE")
+
+
+def _load_file():
+    path = _file()
+    if not path or not os.path.exists(path):
+        return
+    with open(path) as f:
+        for k, v in json.load(f).items():
+            _CACHE.setdefault(k, v)
+
+
+def _save_file():
+    path = _file()
+    if not path:
+        return
+    with open(path, "w") as f:
+        json.dump(_CACHE, f, indent=1, sort_keys=True)
+
+
+def cached(batch):
+    """The cached tuning for this batch's shape, or None."""
+    _load_file()
+    return _CACHE.get(repr(cache_key(batch)))
+
+
+def _time_solve(batch, rtol, repeats):
+    best = None
+    for _ in range(repeats):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.solve(rtol=rtol, check=False)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        best = t if best is None else min(best, t)
+    return best
+
+
+def autotune(batch, rtol=1e-7, repeats=2, passes=2, use_cache=True):
+    """Pick the fastest knob values for ``batch`` (an AlphaBatch) by timing
+    its solve; applies them and returns ``{"knobs": {...}, "ms": t}``."""
+    system = batch.system
+    key = repr(cache_key(batch))
+    if use_cache:
+        hit = cached(batch)
+        if hit is not None:
+            apply_tuning(system, hit["knobs"])
+            return hit
+    batch.solve(rtol=rtol, check=False)          # warm: graph capture, caches
+    best = tuning(system)
+    best_ms = _time_solve(batch, rtol, repeats)
+    for _ in range(passes):
+        changed = False
+        for name, cands in CANDIDATES.items():
+            for val in cands:
+                trial = dict(best)
+                applied = apply_tuning(system, {name: val})[name]
+                if applied == best[name]:
+                    continue
+                trial[name] = applied
+                batch.solve(rtol=rtol, check=False)   # recapture the graph
+                ms = _time_solve(batch, rtol, repeats)
+                if ms < best_ms * (1.0 - _MARGIN):
+                    best, best_ms, changed = trial, ms, True
+                apply_tuning(system, best)
+        if not changed:
+            break
+    apply_tuning(system, best)
+    result = {"knobs": best, "ms": best_ms}
+    _CACHE[key] = result
+    _save_file()
+    return result

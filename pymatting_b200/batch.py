@@ -40,7 +40,7 @@ class AlphaBatch:
     """A prepared batch: device inputs, assembled systems, solver."""
 
     def __init__(self, images, trimaps, lambda_value=100.0, epsilon=1e-7,
-                 preconditioner="vcycle", precision="mixed", check_trimaps=True):
+                 preconditioner="vcycle", precision="mixed", check_trimaps=True, tune=None):
         if len(images) != len(trimaps) or not images:
             raise ValueError("images and trimaps must be non-empty lists of equal length")
         self.shapes = []
@@ -73,6 +73,20 @@ class AlphaBatch:
             off += h * w
         self.system = StencilSystem(sources, _PRECISION[precision], _PREC[preconditioner])
         self.system.setup()
+        # Launch shapes: None keeps the defaults, "cached" applies a tuning
+        # found earlier for this shape (if any), "auto" tunes now if needed.
+        self.tuning = None
+        if tune is not None:
+            from . import autotune
+            if tune == "auto":
+                self.tuning = autotune.autotune(self)
+            elif tune == "cached":
+                hit = autotune.cached(self)
+                if hit is not None:
+                    autotune.apply_tuning(self.system, hit["knobs"])
+                    self.tuning = hit
+            else:
+                raise ValueError("tune must be None, 'cached' or 'auto'")
 
     def solve(self, rtol=1e-7, atol=0.0, maxiter=10000, inner_rtol=1e-4, max_outer=50,
               check=True):
@@ -98,15 +112,18 @@ class AlphaBatch:
 
 def solve_alpha(images, trimaps, lambda_value=100.0, epsilon=1e-7, preconditioner="vcycle",
                 precision="mixed", rtol=1e-7, atol=0.0, maxiter=10000, inner_rtol=1e-4,
-                return_stats=False):
+                return_stats=False, tune=None):
     """Alpha mattes of a batch of images from the soft-constraint system.
 
     ``images``: list of ``(h, w, 3)`` arrays; ``trimaps``: list of ``(h, w)``.
     Returns a list of ``(h, w)`` alphas (numpy for numpy inputs), clipped to
-    [0, 1]; with ``return_stats`` also per-image solve statistics.
+    [0, 1]; with ``return_stats`` also per-image solve statistics. ``tune``:
+    None (default launch shapes), ``"cached"`` (a tuning found earlier for
+    this shape) or ``"auto"`` (run the autotuner if nothing is cached).
     """
     host = not dev.is_device_tensor(trimaps[0])
-    batch = AlphaBatch(images, trimaps, lambda_value, epsilon, preconditioner, precision)
+    batch = AlphaBatch(images, trimaps, lambda_value, epsilon, preconditioner, precision,
+                       tune=tune)
     x = batch.solve(rtol, atol, maxiter, inner_rtol)
     alphas = batch.alphas(x)
     if host:

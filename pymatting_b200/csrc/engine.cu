@@ -134,6 +134,11 @@ struct Stencil {
     std::vector<int> h, w;
     int precision = 0;   // 0: FP64, 1: FP32 inner + FP64 refinement
     int precond = 0;     // kPrecNone / kPrecJacobi / kPrecVcycle
+    // Launch shapes (pmb_stencil_tune): vector width of the CG apply and of
+    // the prolongation, resident CTAs per SM of each list family (limit:
+    // shared memory), CG iterations per graph replay.
+    int vec_apply = 2, vec_up = 2, chunk = 4;
+    int max_fine = 1, max_up = 1, max_down = 1;
     int pre = 1, post = 1;
     double omega = 0.8;
     int direct = 64;
@@ -197,8 +202,10 @@ static int blocks_per_sm(size_t smem) {
     return std::max(1, std::min(4, b));
 }
 
+constexpr int kMaxCtasPerSm = 16;   // bound of every list's per_sm (tile kernels: 4)
+
 static int persistent_grid(const HostList& L) {
-    return std::max(1, std::min(L.wl.total, 148 * L.per_sm));
+    return std::max(1, std::min(L.wl.total, 148 * std::min(L.per_sm, kMaxCtasPerSm)));
 }
 
 static void build_list(HostList& L, const std::vector<GridDesc>& grids,
@@ -311,6 +318,9 @@ static int plan_stencil(Stencil& S) {
     const int per_down = blocks_per_sm(
         vec_down ? (mixed ? smem_down_v<float>() : smem_down_v<double>())
                  : (mixed ? smem_down<float>(S.pre) : smem_down<double>(S.pre)));
+    S.max_fine = per_fine;
+    S.max_up = per_up;
+    S.max_down = per_down;
     build_list(S.fine0, S.levels[0].grids, {}, kTY, kTX);
     S.fine0.per_sm = per_fine;
     build_flat(S.flat0, S.levels[0].grids);
@@ -366,8 +376,9 @@ static int plan_stencil(Stencil& S) {
         if (!lv.flat.starts.empty()) maxt = std::max<int64_t>(maxt, lv.flat.starts.back());
     }
     // Per-CTA partial sums: partials[(image * 3 + q) * G + cta] for the
-    // largest persistent grid G of any list (at most 148 SMs x 8 CTAs).
-    const int64_t gmax = std::min<int64_t>(maxt, 148 * 8);
+    // largest persistent grid G of any list (148 SMs x kMaxCtasPerSm, the
+    // largest CTAs-per-SM value any list can be given).
+    const int64_t gmax = std::min<int64_t>(maxt, 148 * kMaxCtasPerSm);
     S.partials_count = std::max<int64_t>(maxt, (int64_t)n * gmax);
     S.o_part = c.take<double>(3 * S.partials_count);
     S.o_uoff = c.take<int64_t>(n + 1);
@@ -782,8 +793,9 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
         const bool first_in_x = (extra % 2 == 0);
         T* first_out = first_in_x ? X(l) : lvl_xa<T>(S, l);
         const bool reduce_here = (l == 0) && st && extra == 0;
-        launch_vc_up<T>(pre, post, Lf, f.wl, f.partner_dev, S.maps(), xs_slot_f[l], B(l), first_out,
-                        om, st, reduce_here ? 1 : 0, dr, reorth, S.partials(), S.err(), s);
+        launch_vc_up<T>(S.vec_up, pre, post, Lf, f.wl, f.partner_dev, S.maps(), xs_slot_f[l], B(l),
+                        first_out, om, st, reduce_here ? 1 : 0, dr, reorth, S.partials(), S.err(),
+                        s);
         ++S.launches;
         bool cur_x = first_in_x;
         for (int k = 0; k < extra; ++k) {
@@ -811,8 +823,8 @@ static void cg_iteration(Stencil& S, int reorth) {
     InstState* st = S.state();
     // Without a preconditioner z is r itself (cg.py:53-55).
     const int zslot = S.precond == kPrecNone ? kMapBF : kMapZF;
-    launch_cg_apply<T>(LaunchCfg{persistent_grid(S.fine0)}, S.fine0.wl, S.maps(), zslot, v.p0, v.p1,
-                       v.ap, st, S.partials(), S.err(), s);
+    launch_cg_apply<T>(S.vec_apply, LaunchCfg{persistent_grid(S.fine0)}, S.fine0.wl, S.maps(), zslot,
+                       v.p0, v.p1, v.ap, st, S.partials(), S.err(), s);
     const bool mixed = S.precision == 1;
     launch_cg_update<T>(S.precond, LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, v.P, v.x, v.r,
                         v.z, v.p0, v.p1, v.ap, v.dr, reorth, mixed ? 1 : 0, S.err() + kPendingSlot, st,
@@ -854,7 +866,7 @@ static bool any_running(const InstState* st, int n) {
 // turn the remaining kernels of the chunk into no-ops.
 template <typename T>
 static int iterate(Stencil& S, int reorth, int maxiter) {
-    const int chunk = 4;
+    const int chunk = S.chunk;
     if (!S.graph || S.graph_reorth != reorth || S.graph_iters != chunk ||
         S.graph_delta != S.delta || S.graph_max_outer != S.max_outer) {
         if (S.graph) {
@@ -1277,6 +1289,60 @@ PMB_API int pmb_stencil_stats(pmb_stencil* p, int image, int* iters, int* status
 }
 
 PMB_API int64_t pmb_stencil_launch_count(const pmb_stencil* p) { return p ? p->S.launches : -1; }
+
+// Launch-shape knobs for the autotuner. Values are clamped to what the
+// kernels support; the applied value is returned. Changing a knob drops the
+// captured iteration graph (it is captured again on the next solve).
+PMB_API int pmb_stencil_tune(pmb_stencil* p, int knob, int value) {
+    if (!p) return fail(kErrArg, "pmb_stencil_tune: null solver");
+    Stencil& S = p->S;
+    const int wide = S.precision == 1 ? 4 : 2;
+    auto clampi = [](int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); };
+    int applied;
+    switch (knob) {
+    case 0: applied = S.vec_apply = (value >= 4 ? wide : 2); break;
+    case 1: applied = S.vec_up = (value >= 4 ? wide : 2); break;
+    case 2:
+        applied = clampi(value, 1, S.max_fine);
+        S.fine0.per_sm = applied;
+        break;
+    case 3:
+        applied = clampi(value, 1, S.max_up);
+        for (auto& lv : S.levels) lv.fine.per_sm = applied;
+        break;
+    case 4:
+        applied = clampi(value, 1, S.max_down);
+        for (auto& lv : S.levels) lv.coarse.per_sm = applied;
+        break;
+    case 5:
+        applied = clampi(value, 1, kMaxCtasPerSm);
+        S.flat0.per_sm = applied;
+        for (auto& lv : S.levels) lv.flat.per_sm = applied;
+        break;
+    case 6: applied = S.chunk = clampi(value, 1, 16); break;
+    default: return fail(kErrArg, "pmb_stencil_tune: unknown knob");
+    }
+    if (S.graph) {
+        cudaGraphExecDestroy(S.graph);
+        S.graph = nullptr;
+    }
+    return applied;
+}
+
+PMB_API int pmb_stencil_tuning(const pmb_stencil* p, int knob) {
+    if (!p) return fail(kErrArg, "pmb_stencil_tuning: null solver");
+    const Stencil& S = p->S;
+    switch (knob) {
+    case 0: return S.vec_apply;
+    case 1: return S.vec_up;
+    case 2: return S.fine0.per_sm;
+    case 3: return S.levels.empty() ? 0 : S.levels[0].fine.per_sm;
+    case 4: return S.levels.empty() ? 0 : S.levels[0].coarse.per_sm;
+    case 5: return S.flat0.per_sm;
+    case 6: return S.chunk;
+    default: return fail(kErrArg, "pmb_stencil_tuning: unknown knob");
+    }
+}
 
 PMB_API int pmb_stencil_destroy(pmb_stencil* p) {
     if (!p) return 0;

@@ -1791,6 +1791,9 @@ template <typename T> size_t smem_apply_v() {
 // (256 threads); FP64 uses 2 (one 16-byte vector).
 template <typename T> constexpr int kVApply = sizeof(T) == 8 ? 2 : 4;
 template <typename T> constexpr int kVSolve = 2;
+// Widest vector of the element type (the tuner may pick it for the CG apply
+// and the prolongation): 4 in FP32, 2 in FP64.
+template <typename T> constexpr int kVWide = sizeof(T) == 8 ? 2 : 4;
 
 template <typename T, int V> static size_t smem_down_vv() {
     using D = DownBox<T, V>;
@@ -1836,12 +1839,17 @@ void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUte
 }
 
 template <typename T>
-void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, int zslot,
-                     T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s) {
+void launch_cg_apply(int vec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
+                     int zslot, T* p0, T* p1, T* Ap, InstState* st, double* part, int* err,
+                     cudaStream_t s) {
     const size_t sm = smem_apply_v<T>();
-    constexpr int V = kVSolve<T>;
-    k_cg_apply_v<T, V><<<L.grid, tile_threads_v<V>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, st,
-                                                               part, err);
+    constexpr int V4 = kVWide<T>;
+    if (vec == 4 && V4 == 4)
+        k_cg_apply_v<T, V4><<<L.grid, tile_threads_v<V4>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, st,
+                                                                     part, err);
+    else
+        k_cg_apply_v<T, 2><<<L.grid, tile_threads_v<2>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, st,
+                                                                   part, err);
 }
 
 template <typename T>
@@ -1885,16 +1893,20 @@ void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridD
 }
 
 template <typename T>
-void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
+void launch_vc_up(int vec, int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
                   const CUtensorMap* maps, int xs_slot, const T* b, T* xout, double omega,
                   InstState* st, int level0, const T* dr, int reorth, double* part, int* err,
                   cudaStream_t s) {
     const int pk = pre > 1 ? 2 : pre;
     const int qk = post > 0 ? 1 : 0;
     if (pk == 1 && qk == 1) {
-        constexpr int V = kVSolve<T>;
-        k_vc_up_v<T, V><<<L.grid, tile_threads_v<V>(), smem_up_v<T>(), s>>>(
-            wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err);
+        constexpr int V4 = kVWide<T>;
+        if (vec == 4 && V4 == 4)
+            k_vc_up_v<T, V4><<<L.grid, tile_threads_v<V4>(), smem_up_v<T>(), s>>>(
+                wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err);
+        else
+            k_vc_up_v<T, 2><<<L.grid, tile_threads_v<2>(), smem_up_v<T>(), s>>>(
+                wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err);
         return;
     }
     const size_t sm = smem_up<T>(pk);
@@ -2020,7 +2032,9 @@ static void prepare_type() {
     allow_smem(k_apply<T>, smem_init<T>());
     allow_smem(k_apply_v<T, kVApply<T>>, smem_apply_v<T>());
     allow_smem(k_vc_tail<T>, kTailSmem);
-    allow_smem(k_cg_apply_v<T, kVSolve<T>>, smem_apply_v<T>());
+    allow_smem(k_cg_apply_v<T, 2>, smem_apply_v<T>());
+    allow_smem(k_cg_apply_v<T, kVWide<T>>, smem_apply_v<T>());
+    allow_smem(k_vc_up_v<T, kVWide<T>>, smem_up_v<T>());
     allow_smem(k_vc_down_v<T, kVSolve<T>>, smem_down_v<T>());
     allow_smem(k_vc_up_v<T, kVSolve<T>>, smem_up_v<T>());
 }
@@ -2043,7 +2057,7 @@ void stencil_prepare() {
     template void launch_cg_init<T>(int, const LaunchCfg&, const WorkList&, const CUtensorMap*,   \
                                     const T*, const T*, T*, bool, T*, T*, InstState*, double*,    \
                                     double, double, int, int*, cudaStream_t);                     \
-    template void launch_cg_apply<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int,  \
+    template void launch_cg_apply<T>(int, const LaunchCfg&, const WorkList&, const CUtensorMap*, int,  \
                                      T*, T*, T*, InstState*, double*, int*, cudaStream_t);        \
     template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*,   \
                                       T*, const T*, const T*, const T*, T*, int, int, int*,      \
@@ -2053,7 +2067,7 @@ void stencil_prepare() {
     template void launch_vc_down<T>(int, const LaunchCfg&, const WorkList&, const GridDesc*,      \
                                     const CUtensorMap*, int, T*, double, const InstState*, int*, \
                                     cudaStream_t);                                               \
-    template void launch_vc_up<T>(int, int, const LaunchCfg&, const WorkList&, const GridDesc*,   \
+    template void launch_vc_up<T>(int, int, int, const LaunchCfg&, const WorkList&, const GridDesc*,   \
                                   const CUtensorMap*, int, const T*, T*, double, InstState*, int, \
                                   const T*, int, double*, int*, cudaStream_t);                   \
     template void launch_vc_smooth<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int, \

@@ -66,8 +66,9 @@ void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUte
                     const T* P, const T* b, T* x, bool have_x0, T* r, T* z, InstState* st,
                     double* part, double atol, double rtol, int maxiter, int* err, cudaStream_t s);
 template <typename T>
-void launch_cg_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, int zslot,
-                     T* p0, T* p1, T* Ap, InstState* st, double* part, int* err, cudaStream_t s);
+void launch_cg_apply(int vec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
+                     int zslot, T* p0, T* p1, T* Ap, InstState* st, double* part, int* err,
+                     cudaStream_t s);
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
                       T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth, int reliable,
@@ -80,10 +81,10 @@ void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridD
                     const CUtensorMap* maps, int xs_slot, T* bc, double omega,
                     const InstState* st, int* err, cudaStream_t s);
 template <typename T>
-void launch_vc_up(int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
-                  const CUtensorMap* maps, int xs_slot, const T* b, T* xout, double omega,
-                  InstState* st, int level0, const T* dr, int reorth, double* part, int* err,
-                  cudaStream_t s);
+void launch_vc_up(int vec, int pre, int post, const LaunchCfg& L, const WorkList& wl,
+                  const GridDesc* coarse, const CUtensorMap* maps, int xs_slot, const T* b, T* xout,
+                  double omega, InstState* st, int level0, const T* dr, int reorth, double* part,
+                  int* err, cudaStream_t s);
 template <typename T>
 void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
                       int xin_slot, const T* P, const T* b, T* xout, double omega,
