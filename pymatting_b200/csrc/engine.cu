@@ -126,7 +126,7 @@ struct Level {
     HostList fine;    // 64x8 tiles of level-l grids that have a level l+1
     HostList coarse;  // restriction tiles of the level l+1 grids of the same images
     HostList flat;    // element chunks of the same level-l grids
-    HostList gal;     // every level-l grid with a level l+1 (Galerkin setup), tails included
+    HostList gal;     // 8x16 tiles of every level-(l+1) grid (Galerkin setup), tails included
 };
 
 struct Stencil {
@@ -339,7 +339,7 @@ static int plan_stencil(Stencil& S) {
             f.push_back(lv.grids[gi]);
             c.push_back(nx.grids[it - nx.image.begin()]);
         }
-        build_list(lv.gal, gf, gc, kTY, kTX);
+        build_list(lv.gal, gc, gf, kGalerkinTileY, kGalerkinTileX);   // coarse tiles
         build_list(lv.fine, f, c, kTY, kTX);
         lv.fine.per_sm = per_up;
         build_list(lv.coarse, c, f, S.cy, kCX);
@@ -543,6 +543,7 @@ static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
             rc |= encode_map(m + kMapPlS, P, g, true, mixed, kBW, kPH);
             rc |= encode_map(m + kMapPlDV, P, g, true, mixed, DWV, DH);
             rc |= encode_map(m + kMapBDV, B, g, false, mixed, DWV, DH);
+            rc |= encode_map(m + kMapPlG, planes64(S, l), g, true, false, kGCols, kGRows);
             if (XA) {
                 rc |= encode_map(m + kMapXAF, XA, g, false, mixed, kBW, kBH);
                 rc |= encode_map(m + kMapXAD, XA, g, false, mixed, kBW, DH);
@@ -629,10 +630,8 @@ static int setup_stencil(Stencil& S) {
         Level& lv = S.levels[l];
         HostList& f = lv.gal;
         if (f.grids.empty()) continue;
-        int64_t total = 0;
-        for (auto& g : f.partner) total += (int64_t)g.h * g.w * kNH;
-        launch_galerkin(f.wl.grids, f.partner_dev, (int)f.grids.size(), planes64(S, l),
-                        S.at<double>(S.levels[l + 1].P64), total, s);
+        launch_galerkin_t(f.wl, f.partner_dev, S.maps(), S.at<double>(S.levels[l + 1].P64),
+                          S.err(), s);
         ++S.launches;
     }
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_status, 0, sizeof(int), s));

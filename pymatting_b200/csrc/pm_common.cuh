@@ -61,6 +61,7 @@ enum : int {
     kMapPlS,       // planes, apply box (kPH rows)
     kMapPlDV,      // planes, register-blocked restriction box
     kMapBDV,       // b, register-blocked restriction box
+    kMapPlG,       // FP64 planes, Galerkin box (42 x 21 x 13)
     kMapsPerGrid
 };
 

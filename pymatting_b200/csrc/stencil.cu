@@ -925,6 +925,86 @@ __global__ void k_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int
     Pc[gc.poff + p * gc.pstride + (int64_t)Y * gc.pitch + X] = acc;
 }
 
+// Tiled coarse operator: one CTA per 8x16 tile of coarse pixels, one thread
+// per coarse pixel computing its 13 forward entries. One TMA box brings the
+// fine planes under the tile (rows 2 Y0 - 1 .. 2 Y0 + 19, columns
+// 2 X0 - 6 .. 2 X0 + 35) into shared memory, zero-filled outside the fine
+// grid; the zeros stand in for the bounds tests of k_galerkin (entries of A
+// that leave the grid are zero in the planes, so the terms they would skip
+// add +0). Same terms in the same order as k_galerkin: bit-identical planes.
+constexpr int kGTY = kGalerkinTileY, kGTX = kGalerkinTileX;   // coarse tile
+constexpr int kGThreads = kGTY * kGTX;
+
+template <int P>
+__device__ __forceinline__ double galerkin_entry(const double* s_pl, int ly, int lx) {
+    constexpr int DY = half_dy(P), DX = half_dx(P);
+    double acc = 0.0;
+#pragma unroll
+    for (int ay = -1; ay <= 1; ++ay) {
+#pragma unroll
+        for (int ax = -1; ax <= 1; ++ax) {
+            const double wa = pw(ax) * pw(ay) / 16.0;
+            const int r = 2 * ly + 1 + ay, c = 2 * lx + 6 + ax;   // a = (2Y + ay, 2X + ax)
+#pragma unroll
+            for (int by = -1; by <= 1; ++by) {
+#pragma unroll
+                for (int bx = -1; bx <= 1; ++bx) {
+                    const int ey = 2 * DY + by - ay, ex = 2 * DX + bx - ax;
+                    if (ey < -2 || ey > 2 || ex < -2 || ex > 2) continue;
+                    const double wb = pw(bx) * pw(by) / 16.0;
+                    const int pf = half_index(ey, ex);
+                    const double v = pf >= 0
+                        ? s_pl[(pf * kGRows + r) * kGCols + c]
+                        : s_pl[(half_index(-ey, -ex) * kGRows + r + ey) * kGCols + c + ex];
+                    acc += wa * v * wb;
+                }
+            }
+        }
+    }
+    return acc;
+}
+
+template <int P>
+__device__ __forceinline__ void galerkin_all(const double* s_pl, int ly, int lx, int Y, int X,
+                                             const GridDesc& gc, double* Pc) {
+    if constexpr (P < kNH) {
+        constexpr int DY = half_dy(P), DX = half_dx(P);
+        const int Y2 = Y + DY, X2 = X + DX;
+        double acc = 0.0;
+        if (Y2 >= 0 && Y2 < gc.h && X2 >= 0 && X2 < gc.w) acc = galerkin_entry<P>(s_pl, ly, lx);
+        Pc[gc.poff + P * gc.pstride + (int64_t)Y * gc.pitch + X] = acc;
+        galerkin_all<P + 1>(s_pl, ly, lx, Y, X, gc, Pc);
+    }
+}
+
+__global__ void __launch_bounds__(kGThreads)
+k_galerkin_t(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMap* maps,
+             double* Pc, int* err) {
+    extern __shared__ __align__(128) double s_pl[];      // [kNH][kGRows][kGCols]
+    __shared__ __align__(8) uint64_t s_bar;
+    const int t = blockIdx.x;
+    const int g = find_grid(wl, t);
+    const GridDesc gc = wl.grids[g];
+    const int local = t - wl.tile_start[g];
+    const int tiles_x = (gc.w + kGTX - 1) / kGTX;
+    const int Y0 = (local / tiles_x) * kGTY, X0 = (local % tiles_x) * kGTX;
+    if (threadIdx.x == 0) {
+        const GridDesc gf = fine[g];
+        mbar_init(&s_bar, 1);
+        mbar_expect_tx(&s_bar, kNH * kGRows * kGCols * sizeof(double));
+        tma_load_3d(s_pl, map_of(maps, gf, kMapPlG), 2 * X0 - 6, 2 * Y0 - 1, 0, &s_bar);
+    }
+    __syncthreads();
+    if (!mbar_wait(&s_bar, 0)) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
+    const int ly = threadIdx.x / kGTX, lx = threadIdx.x % kGTX;
+    const int Y = Y0 + ly, X = X0 + lx;
+    if (Y >= gc.h || X >= gc.w) return;
+    galerkin_all<0>(s_pl, ly, lx, Y, X, gc, Pc);
+}
+
 // Dense inverse of the coarsest operator by Gauss-Jordan elimination with
 // partial pivoting. One CTA per image; n <= kMaxDirect. *status is raised to
 // 2 on an exactly zero pivot and to 1 on a non-finite one.
@@ -1965,6 +2045,13 @@ void launch_unpack(const GridDesc* grids, int ngrids, const int64_t* uoff, const
     k_unpack<TS, TD><<<blocks, 256, 0, s>>>(grids, ngrids, uoff, src, dst, total);
 }
 
+void launch_galerkin_t(const WorkList& wl, const GridDesc* fine, const CUtensorMap* maps,
+                       double* Pc, int* err, cudaStream_t s) {
+    if (wl.total > 0)
+        k_galerkin_t<<<wl.total, kGThreads, kNH * kGRows * kGCols * sizeof(double), s>>>(
+            wl, fine, maps, Pc, err);
+}
+
 void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrids, const double* Pf,
                      double* Pc, int64_t total, cudaStream_t s) {
     if (total <= 0) return;
@@ -2044,6 +2131,7 @@ void stencil_prepare() {
     if (done) return;
     prepare_type<double>();
     prepare_type<float>();
+    allow_smem(k_galerkin_t, kNH * kGRows * kGCols * sizeof(double));
     allow_smem(k_refine_residual<kPrecNone, true>, smem_init<double>());
     allow_smem(k_refine_residual<kPrecJacobi, true>, smem_init<double>());
     allow_smem(k_refine_residual<kPrecVcycle, true>, smem_init<double>());

@@ -101,6 +101,14 @@ void launch_pack(const GridDesc* grids, int ngrids, const int64_t* uoff, const T
 template <typename TS, typename TD>
 void launch_unpack(const GridDesc* grids, int ngrids, const int64_t* uoff, const TS* src, TD* dst,
                    int64_t total, cudaStream_t s);
+// Coarse operators over a list of coarse-grid tiles (8 x 16 coarse pixels);
+// `fine` holds each coarse grid's fine grid, whose FP64 planes are read
+// through map slot kMapPlG (box kGCols x kGRows x 13).
+constexpr int kGalerkinTileY = 8, kGalerkinTileX = 16;
+constexpr int kGRows = 2 * kGalerkinTileY + 5;      // 21 fine rows
+constexpr int kGCols = 2 * kGalerkinTileX + 10;     // 42 fine columns (even start)
+void launch_galerkin_t(const WorkList& wl, const GridDesc* fine, const CUtensorMap* maps,
+                       double* Pc, int* err, cudaStream_t s);
 void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrids, const double* Pf,
                      double* Pc, int64_t total, cudaStream_t s);
 void launch_dense_inverse(const DirectDesc* dd, int count, const double* Pc, double* work,
