@@ -44,6 +44,15 @@ struct SmemCarve {
 
 extern __shared__ __align__(128) char g_smem[];
 
+// The two pipeline copies of one shared buffer, addressed by stage index
+// without a local-memory pointer array: copy b = p0 + b * d.
+template <typename T>
+struct Buf2 {
+    T* p0;
+    ptrdiff_t d;
+    __device__ __forceinline__ T* operator[](int b) const { return p0 + b * d; }
+};
+
 // V-element vector load / store (8 or 16 bytes, aligned).
 template <typename T, int V>
 __device__ __forceinline__ void ldv(const T* p, T* o) {
@@ -247,12 +256,14 @@ k_cg_init(WorkList wl, const CUtensorMap* maps, const T* __restrict__ P, const T
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sX[2];
+    T* sP_[2];
+    T* sX_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = X0 ? sc.take<T>(kNH * kBH * kBW) : nullptr;
-        sX[k] = X0 ? sc.take<T>(kBH * kBW) : nullptr;
+        sP_[k] = X0 ? sc.take<T>(kNH * kBH * kBW) : nullptr;
+        sX_[k] = X0 ? sc.take<T>(kBH * kBW) : nullptr;
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sX{sX_[0], sX_[1] - sX_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     double v[3] = {0.0, 0.0, 0.0};
@@ -332,14 +343,17 @@ k_cg_apply(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap,
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sZ[2];
-    T* sQ[2];
+    T* sP_[2];
+    T* sZ_[2];
+    T* sQ_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kBH * kBW);
-        sZ[k] = sc.take<T>(kBH * kBW);
-        sQ[k] = sc.take<T>(kBH * kBW);
+        sP_[k] = sc.take<T>(kNH * kBH * kBW);
+        sZ_[k] = sc.take<T>(kBH * kBW);
+        sQ_[k] = sc.take<T>(kBH * kBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sZ{sZ_[0], sZ_[1] - sZ_[0]};
+    const Buf2<T> sQ{sQ_[0], sQ_[1] - sQ_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     double v[1] = {0.0};
@@ -571,14 +585,17 @@ k_vc_down(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMa
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sB[2];
-    T* sS[2];
+    T* sP_[2];
+    T* sB_[2];
+    T* sS_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = PRE != 0 ? sc.take<T>(kNH * DH * kBW) : nullptr;
-        sB[k] = sc.take<T>(DH * kBW);
-        sS[k] = PRE > 1 ? sc.take<T>(DH * kBW) : nullptr;
+        sP_[k] = PRE != 0 ? sc.take<T>(kNH * DH * kBW) : nullptr;
+        sB_[k] = sc.take<T>(DH * kBW);
+        sS_[k] = PRE > 1 ? sc.take<T>(DH * kBW) : nullptr;
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sB{sB_[0], sB_[1] - sB_[0]};
+    const Buf2<T> sS{sS_[0], sS_[1] - sS_[0]};
     T* sX = PRE == 1 ? sc.take<T>(DH * kBW) : nullptr;
     T* sR = sc.take<T>(RH * RW);
     Pipe pipe;
@@ -654,16 +671,20 @@ k_vc_up(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap*
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sX[2];
-    T* sS[2];
-    T* sC[2];
+    T* sP_[2];
+    T* sX_[2];
+    T* sS_[2];
+    T* sC_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kBH * kBW);
-        sX[k] = sc.take<T>(kBH * kBW);          // b, then x2 in place
-        sS[k] = PRE > 1 ? sc.take<T>(kBH * kBW) : nullptr;
-        sC[k] = sc.take<T>(kCBH * kCBW);
+        sP_[k] = sc.take<T>(kNH * kBH * kBW);
+        sX_[k] = sc.take<T>(kBH * kBW);          // b, then x2 in place
+        sS_[k] = PRE > 1 ? sc.take<T>(kBH * kBW) : nullptr;
+        sC_[k] = sc.take<T>(kCBH * kCBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sX{sX_[0], sX_[1] - sX_[0]};
+    const Buf2<T> sS{sS_[0], sS_[1] - sS_[0]};
+    const Buf2<T> sC{sC_[0], sC_[1] - sC_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     double v[2] = {0.0, 0.0};
@@ -760,12 +781,14 @@ k_vc_smooth(WorkList wl, const CUtensorMap* maps, int xin_slot, const T* __restr
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sX[2];
+    T* sP_[2];
+    T* sX_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kBH * kBW);
-        sX[k] = sc.take<T>(kBH * kBW);
+        sP_[k] = sc.take<T>(kNH * kBH * kBW);
+        sX_[k] = sc.take<T>(kBH * kBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sX{sX_[0], sX_[1] - sX_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
@@ -840,12 +863,14 @@ k_apply(WorkList wl, const CUtensorMap* maps, T* y, int* err) {
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sX[2];
+    T* sP_[2];
+    T* sX_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kBH * kBW);
-        sX[k] = sc.take<T>(kBH * kBW);
+        sP_[k] = sc.take<T>(kNH * kBH * kBW);
+        sX_[k] = sc.take<T>(kBH * kBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sX{sX_[0], sX_[1] - sX_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
@@ -1147,12 +1172,14 @@ k_refine_residual(WorkList wl, const CUtensorMap* maps, const float* __restrict_
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    double* sP[2];
-    double* sX[2];
+    double* sP_[2];
+    double* sX_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<double>(kNH * kBH * kBW);
-        sX[k] = sc.take<double>(kBH * kBW);
+        sP_[k] = sc.take<double>(kNH * kBH * kBW);
+        sX_[k] = sc.take<double>(kBH * kBW);
     }
+    const Buf2<double> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<double> sX{sX_[0], sX_[1] - sX_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     double v[3] = {0.0, 0.0, 0.0};
@@ -1313,12 +1340,14 @@ k_apply_v(WorkList wl, const CUtensorMap* maps, T* y, int* err) {
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sX[2];
+    T* sP_[2];
+    T* sX_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kPH * kBW);
-        sX[k] = sc.take<T>(kBH * kBW);
+        sP_[k] = sc.take<T>(kNH * kPH * kBW);
+        sX_[k] = sc.take<T>(kBH * kBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sX{sX_[0], sX_[1] - sX_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     auto issue = [&](const Meta& m, const GridDesc& g, int bb) {
@@ -1357,14 +1386,17 @@ k_cg_apply_v(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* A
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sZ[2];
-    T* sQ[2];
+    T* sP_[2];
+    T* sZ_[2];
+    T* sQ_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kPH * kBW);
-        sZ[k] = sc.take<T>(kBH * kBW);
-        sQ[k] = sc.take<T>(kBH * kBW);
+        sP_[k] = sc.take<T>(kNH * kPH * kBW);
+        sZ_[k] = sc.take<T>(kBH * kBW);
+        sQ_[k] = sc.take<T>(kBH * kBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sZ{sZ_[0], sZ_[1] - sZ_[0]};
+    const Buf2<T> sQ{sQ_[0], sQ_[1] - sQ_[0]};
     Pipe pipe;
     pipe.init(s_bar, err);
     double v0[1] = {0.0};
@@ -1447,12 +1479,14 @@ k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensor
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sB[2];
+    T* sP_[2];
+    T* sB_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * DH * DW);
-        sB[k] = sc.take<T>(DH * DW);
+        sP_[k] = sc.take<T>(kNH * DH * DW);
+        sB_[k] = sc.take<T>(DH * DW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sB{sB_[0], sB_[1] - sB_[0]};
     T* sX = sc.take<T>(DH * DW);
     T* sR = sc.take<T>(RH * RW);
     Pipe pipe;
@@ -1534,14 +1568,17 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP[2];
-    T* sB[2];
-    T* sC[2];
+    T* sP_[2];
+    T* sB_[2];
+    T* sC_[2];
     for (int k = 0; k < 2; ++k) {
-        sP[k] = sc.take<T>(kNH * kBH * kBW);
-        sB[k] = sc.take<T>(kBH * kBW);
-        sC[k] = sc.take<T>(kCBH * kCBW);
+        sP_[k] = sc.take<T>(kNH * kBH * kBW);
+        sB_[k] = sc.take<T>(kBH * kBW);
+        sC_[k] = sc.take<T>(kCBH * kCBW);
     }
+    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    const Buf2<T> sB{sB_[0], sB_[1] - sB_[0]};
+    const Buf2<T> sC{sC_[0], sC_[1] - sC_[0]};
     T* sX = sc.take<T>(kBH * kBW);
     Pipe pipe;
     pipe.init(s_bar, err);
