@@ -1708,9 +1708,21 @@ __device__ __forceinline__ T tail_val(const T* v, const GridDesc& g, int y, int 
     return v[y * g.pitch + x];
 }
 
-// (A v) at (y, x), accumulated in the order of stencil_at.
+// (A v) at (y, x), accumulated in the order of stencil_at. Pixels at least
+// two away from every border take the unchecked path.
 template <typename T>
 __device__ __forceinline__ T tail_stencil(const T* P, const T* v, const GridDesc& g, int y, int x) {
+    const int i = y * g.pitch + x;
+    if (y >= 2 && y < g.h - 2 && x >= 2 && x < g.w - 2) {
+        T acc = P[i] * v[i];
+#pragma unroll
+        for (int p = 1; p < kNH; ++p) {
+            const int d = half_dy(p) * g.pitch + half_dx(p);
+            acc += P[p * g.pstride + i] * v[i + d];
+            acc += P[p * g.pstride + i - d] * v[i - d];
+        }
+        return acc;
+    }
     T acc = P[y * g.pitch + x] * v[y * g.pitch + x];
 #pragma unroll
     for (int p = 1; p < kNH; ++p) {
