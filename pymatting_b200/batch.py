@@ -48,7 +48,7 @@ class AlphaBatch:
         for img, tri in zip(images, trimaps):
             h, w = tri.shape[:2]
             self.shapes.append((h, w))
-            tri_t = dev.to_device(tri if dev.is_device_tensor(tri)
+            tri_t = dev.to_device(tri if isinstance(tri, torch.Tensor)
                                   else np.asarray(tri, dtype=np.float64), torch.float64).reshape(-1)
             fg, known, cnt = _device_masks(tri_t)
             counts.append(cnt)
@@ -115,18 +115,23 @@ def solve_alpha(images, trimaps, lambda_value=100.0, epsilon=1e-7, preconditione
                 return_stats=False, tune=None):
     """Alpha mattes of a batch of images from the soft-constraint system.
 
-    ``images``: list of ``(h, w, 3)`` arrays; ``trimaps``: list of ``(h, w)``.
-    Returns a list of ``(h, w)`` alphas (numpy for numpy inputs), clipped to
+    ``images``: list of ``(h, w, 3)`` arrays or tensors; ``trimaps``: list of
+    ``(h, w)``. Returns a list of ``(h, w)`` alphas (numpy for numpy inputs,
+    CPU tensors for CPU tensors, device tensors for device tensors), clipped to
     [0, 1]; with ``return_stats`` also per-image solve statistics. ``tune``:
     None (default launch shapes), ``"cached"`` (a tuning found earlier for
     this shape) or ``"auto"`` (run the autotuner if nothing is cached).
     """
+    host_tensor = isinstance(trimaps[0], torch.Tensor) and not trimaps[0].is_cuda
     host = not dev.is_device_tensor(trimaps[0])
     batch = AlphaBatch(images, trimaps, lambda_value, epsilon, preconditioner, precision,
                        tune=tune)
     x = batch.solve(rtol, atol, maxiter, inner_rtol)
     alphas = batch.alphas(x)
-    if host:
+    if host_tensor:
+        # CPU tensors in, CPU tensors out (pinned inputs copy at full speed).
+        alphas = [a.cpu() for a in alphas]
+    elif host:
         alphas = [dev.to_host(a) for a in alphas]
     if return_stats:
         return alphas, batch.stats()

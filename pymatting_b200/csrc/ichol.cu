@@ -12,8 +12,10 @@
 // reference's left-looking linked lists, one CTA runs it right-looking over
 // a dense band "front": when column k is final, its kept entries update the
 // pending columns k+1 .. k+B directly (B = bandwidth of A; fill never leaves
-// the envelope). Each column then costs a handful of block-wide steps, all
-// of them parallel across the column's entries and entry pairs. Diagonal
+// the envelope). Per column, warp 0 does the serial part with warp ballots
+// (candidate rows, pivot, thresholding, compaction), then the whole CTA does
+// the pair updates while the last warp recycles the column's front slot:
+// two block barriers per column. Diagonal
 // updates happen in the same column order as the reference; the off-
 // diagonal accumulations differ only in summation order.
 //
@@ -29,6 +31,7 @@
 namespace pmb {
 
 constexpr int kIcholThreads = 1024;
+constexpr int kIcholChunks = 8;      // front columns of up to 256 rows load in one burst
 constexpr int64_t kIcholSmemRows = 27 * 1024;   // x of the shared-memory solve: 216 KB
 
 // Per-column statistics of A (lower part, CSC): diagonal (+ shift), sum of
@@ -72,33 +75,6 @@ __device__ __forceinline__ void load_column(int64_t j, int64_t W, const int64_t*
     }
 }
 
-__device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += t;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        int y = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, y, o);
-            if (lane >= o) y += t;
-        }
-        s_warp[lane] = y;
-    }
-    __syncthreads();
-    const int base = warp > 0 ? s_warp[warp - 1] : 0;
-    if (total) *total = s_warp[(blockDim.x >> 5) - 1];
-    const int r = base + x - v;
-    __syncthreads();
-    return r;
-}
-
 // The factorisation. One CTA. Front F / pat: W x W (W = B + 1), slot of
 // column j = j % W, entry (i, j) at offset i - j. cand / kept: scratch of
 // at least W entries each.
@@ -109,10 +85,10 @@ k_ichol_factor(int64_t n, int64_t W, const int64_t* __restrict__ Ap,
                double* keptv, int64_t* kepti, int64_t* Lp, int64_t* Lr, double* Lv,
                int64_t cap, double discard, int64_t max_nnz, double rel_discard, int diag_keep,
                int64_t* result) {
-    __shared__ int s_warp[32];
     __shared__ int64_t s_nnz;
-    __shared__ int s_cn, s_m, s_fail;
-    __shared__ double s_dj;
+    __shared__ int s_m, s_fail;
+    __shared__ double s_keptv[kIcholChunks * 32];     // kept entries of the column
+    __shared__ int64_t s_kepti[kIcholChunks * 32];
 
     // Initial front: columns 0 .. W-1.
     for (int64_t j = 0; j < W && j < n; ++j) load_column(j, W, Ap, Ar, Av, F, pat);
@@ -123,85 +99,101 @@ k_ichol_factor(int64_t n, int64_t W, const int64_t* __restrict__ Ap,
     }
     __syncthreads();
 
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int64_t j = 0; j < n; ++j) {
         const int64_t slot = (j % W) * W;
-        // Candidate rows of column j, ascending (the reference sorts them,
-        // ichol.py:87-89).
-        int cn_total = 0;
-        int written = 0;
-        for (int64_t base = 1; base < W; base += blockDim.x) {
-            const int64_t o = base + threadIdx.x;
-            const int flag = (o < W && j + o < n && pat[slot + o]) ? 1 : 0;
-            int chunk_total;
-            const int pos = block_exclusive_scan(flag, s_warp, &chunk_total);
-            if (flag) cand[written + pos] = (int)o;
-            written += chunk_total;
-            cn_total += chunk_total;
-        }
-        if (threadIdx.x == 0) {
-            s_cn = cn_total;
+        // Warp 0: the serial part of column j, warp-synchronous. Offsets
+        // o = 1 + lane + 32 k: chunk k, lane order = ascending rows, the
+        // order in which the reference sorts its candidates (ichol.py:87-89).
+        // The pattern flags and front values of the first kIcholChunks
+        // chunks, the pivot and the threshold are loaded in one burst.
+        if (warp == 0) {
+            bool flag[kIcholChunks];
+            double aval[kIcholChunks];
+#pragma unroll
+            for (int k = 0; k < kIcholChunks; ++k) {
+                const int64_t o = 1 + lane + 32 * k;
+                flag[k] = o < W && j + o < n && pat[slot + o];
+                aval[k] = flag[k] ? F[slot + o] : 0.0;
+            }
             const double dj = d[j];
-            if (!(dj > 0.0)) {
-                s_fail = -1;               // ichol.py:80-81
-            } else if (s_nnz + 1 + cn_total > max_nnz || s_nnz + 1 + cn_total > cap) {
-                s_fail = -2;               // ichol.py:82-83
-            } else {
+            const double rel = rel_discard * rsum[j];
+            int cn = 0;
+#pragma unroll
+            for (int k = 0; k < kIcholChunks; ++k) cn += __popc(__ballot_sync(0xffffffffu, flag[k]));
+            for (int64_t base = 1 + 32 * kIcholChunks; base < W; base += 32) {   // wide bands
+                const int64_t o = base + lane;
+                cn += __popc(__ballot_sync(0xffffffffu, o < W && j + o < n && pat[slot + o]));
+            }
+            int fail = 0;
+            const int64_t nnz = s_nnz;
+            if (!(dj > 0.0)) fail = -1;                                   // ichol.py:80-81
+            else if (nnz + 1 + cn > max_nnz || nnz + 1 + cn > cap) fail = -2;   // ichol.py:82-83
+            int kept = 0;
+            int64_t nnz0 = nnz + 1;
+            if (!fail) {
                 const double sj = sqrt(dj);
-                d[j] = sj;
-                s_dj = sj;
-                Lv[s_nnz] = sj;
-                Lr[s_nnz] = j;
-                s_nnz += 1;
+                if (lane == 0) {
+                    d[j] = sj;
+                    Lv[nnz] = sj;
+                    Lr[nnz] = j;
+                }
+                auto take = [&](bool fl, double a, int64_t o) {
+                    bool keep = false;
+                    double L = 0.0;
+                    const int64_t i = j + o;
+                    if (fl) {
+                        L = a / sj;
+                        if (diag_keep) d[i] -= L * L;
+                        keep = fabs(L) > discard && fabs(a) > rel;
+                        if (keep && !diag_keep) d[i] -= L * L;
+                    }
+                    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
+                        const int pos = kept + __popc(mask & ((1u << lane) - 1u));
+                        Lv[nnz0 + pos] = L;
+                        Lr[nnz0 + pos] = i;
+                        keptv[pos] = L;
+                        kepti[pos] = i;
+                        if (pos < kIcholChunks * 32) {
+                            s_keptv[pos] = L;
+                            s_kepti[pos] = i;
+                        }
+                    }
+                    kept += __popc(mask);
+                };
+#pragma unroll
+                for (int k = 0; k < kIcholChunks; ++k) take(flag[k], aval[k], 1 + lane + 32 * k);
+                for (int64_t base = 1 + 32 * kIcholChunks; base < W; base += 32) {
+                    const int64_t o = base + lane;
+                    const bool fl = o < W && j + o < n && pat[slot + o];
+                    take(fl, fl ? F[slot + o] : 0.0, o);
+                }
+            }
+            if (lane == 0) {
+                s_fail = fail;
+                if (!fail) {
+                    s_m = kept;
+                    s_nnz = nnz0 + kept;
+                    Lp[j + 1] = nnz0 + kept;
+                }
             }
         }
         __syncthreads();
         if (s_fail) break;
-        const int cn = s_cn;
-        const double dj = s_dj;
-        const int64_t nnz0 = s_nnz;
-        const double rel = rel_discard * rsum[j];
-        // Scale, threshold, diagonal updates; compact the kept entries.
-        int kept_total = 0;
-        for (int base = 0; base < cn; base += blockDim.x) {
-            const int q = base + threadIdx.x;
-            int keep = 0;
-            double L = 0.0;
-            int64_t i = 0;
-            if (q < cn) {
-                const int o = cand[q];
-                i = j + o;
-                const double a = F[slot + o];
-                L = a / dj;
-                if (diag_keep) d[i] -= L * L;
-                keep = (fabs(L) > discard && fabs(a) > rel) ? 1 : 0;
-                if (keep && !diag_keep) d[i] -= L * L;
-            }
-            int chunk_total;
-            const int pos = block_exclusive_scan(keep, s_warp, &chunk_total);
-            if (keep) {
-                const int64_t at = nnz0 + kept_total + pos;
-                Lv[at] = L;
-                Lr[at] = i;
-                keptv[kept_total + pos] = L;
-                kepti[kept_total + pos] = i;
-            }
-            kept_total += chunk_total;
-        }
-        if (threadIdx.x == 0) {
-            s_m = kept_total;
-            s_nnz = nnz0 + kept_total;
-            Lp[j + 1] = nnz0 + kept_total;
-        }
-        __syncthreads();
         const int m = s_m;
         // Levels of the rows this column feeds.
         const int lj = level[j] + 1;
         for (int q = threadIdx.x; q < m; q += blockDim.x) {
-            const int64_t i = kepti[q];
+            const int64_t i = m <= kIcholChunks * 32 ? s_kepti[q] : kepti[q];
             if (level[i] < lj) level[i] = lj;
         }
         // Right-looking update of the pending columns: for kept rows
-        // ia > ib, F[ib][ia - ib] -= L_ia L_ib.
+        // ia > ib, F[ib][ia - ib] -= L_ia L_ib, one pair per thread. Rows ib
+        // lie in (j, j + W), so no update touches slot j.
+        const bool shared_list = m <= kIcholChunks * 32;
+        const double* kv = shared_list ? s_keptv : keptv;
+        const int64_t* ki = shared_list ? s_kepti : kepti;
         const int64_t pairs = (int64_t)m * (m - 1) / 2;
         for (int64_t p = threadIdx.x; p < pairs; p += blockDim.x) {
             // Invert p = a (a - 1) / 2 + b with 0 <= b < a.
@@ -209,19 +201,31 @@ k_ichol_factor(int64_t n, int64_t W, const int64_t* __restrict__ Ap,
             while (a * (a - 1) / 2 > p) --a;
             while ((a + 1) * a / 2 <= p) ++a;
             const int64_t b = p - a * (a - 1) / 2;
-            const int64_t ia = kepti[a], ib = kepti[b];
+            const int64_t ia = ki[a], ib = ki[b];
             const int64_t off = ((ib % W) * W) + (ia - ib);
-            F[off] -= keptv[a] * keptv[b];
+            F[off] -= kv[a] * kv[b];
             pat[off] = 1;
         }
-        __syncthreads();
-        // Recycle the slot for column j + W.
-        for (int64_t o = threadIdx.x; o < W; o += blockDim.x) {
-            F[slot + o] = 0.0;
-            pat[slot + o] = 0;
+        // Meanwhile the last warp recycles slot j for column j + W (clear,
+        // then load; ordered within the warp).
+        if (warp == (int)(blockDim.x >> 5) - 1) {
+            for (int64_t o = lane; o < W; o += 32) {
+                F[slot + o] = 0.0;
+                pat[slot + o] = 0;
+            }
+            __syncwarp();
+            if (j + W < n) {
+                const int64_t jn = j + W;
+                for (int64_t k = Ap[jn] + lane; k < Ap[jn + 1]; k += 32) {
+                    const int64_t i = Ar[k];
+                    const double v = Av[k];
+                    if (i > jn && v != 0.0) {
+                        F[slot + (i - jn)] += v;
+                        pat[slot + (i - jn)] = 1;
+                    }
+                }
+            }
         }
-        __syncthreads();
-        if (j + W < n) load_column(j + W, W, Ap, Ar, Av, F, pat);
         __syncthreads();
     }
     if (threadIdx.x == 0) *result = s_fail ? (int64_t)s_fail : s_nnz;

@@ -198,6 +198,8 @@ def device_csr_arrays(A):
 def _image_to_device(image):
     if dev.is_device_tensor(image):
         t = image.to(torch.float64).contiguous()
+    elif isinstance(image, torch.Tensor):
+        t = dev.to_device(image, torch.float64)     # pinned host tensors copy directly
     else:
         t = dev.to_device(np.asarray(image), torch.float64)
     return t

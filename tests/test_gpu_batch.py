@@ -66,3 +66,16 @@ def test_batch_jacobi_and_none(problems):
             alphas, stats = solve_alpha(imgs, tris, preconditioner=pre, precision=precision,
                                         return_stats=True)
             assert all(s.status == 1 for s in stats)
+
+
+def test_solve_alpha_host_tensor_io(problems):
+    """Pinned CPU tensors in, CPU tensors out; same alphas as numpy inputs."""
+    import torch
+    from pymatting_b200.batch import solve_alpha
+    imgs = [torch.from_numpy(p[0]).pin_memory() for p in problems[:2]]
+    tris = [torch.from_numpy(p[1]).pin_memory() for p in problems[:2]]
+    out = solve_alpha(imgs, tris, precision="fp64")
+    ref = solve_alpha([p[0] for p in problems[:2]], [p[1] for p in problems[:2]], precision="fp64")
+    for a, r in zip(out, ref):
+        assert isinstance(a, torch.Tensor) and not a.is_cuda
+        assert np.array_equal(a.numpy(), r)
