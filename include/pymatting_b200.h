@@ -70,6 +70,25 @@ int pmb_cf_laplacian_vjp(const double* image, const uint8_t* is_known, int h, in
                          double epsilon, const double* x, const double* mu, double* grad,
                          void* stream);
 
+/* ---- Large-kernel matting Laplacian (matrix-free) ---------------------- */
+
+/* Replaces lkm_laplacian(image, epsilon, radius)
+ * (pymatting/laplacian/lkm_laplacian.py:6-76). windows: (h-2r)(w-2r)*10
+ * doubles (per window V, V mean, 1/|w| + mean' V mean), computed by
+ * pmb_lkm_setup; scratch: pmb_lkm_scratch_elems doubles (-1: image not
+ * larger than 2 radius). */
+int64_t pmb_lkm_scratch_elems(int h, int w, int radius);
+int pmb_lkm_setup(const double* image, int h, int w, int radius, double epsilon, double* windows,
+                  double* scratch, void* stream);
+/* out = L p (+ diag_add * p when diag_add is not null): L_matvec. */
+int pmb_lkm_apply(const double* image, int h, int w, int radius, const double* windows,
+                  const double* diag_add, const double* p, double* out, double* scratch,
+                  void* stream);
+/* diag = diag(L) (+ diag_add), inv_diag = 1 / diag if not null: diag_L. */
+int pmb_lkm_diagonal(const double* image, int h, int w, int radius, const double* windows,
+                     const double* diag_add, double* diag, double* inv_diag, double* scratch,
+                     void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

@@ -405,3 +405,54 @@ def soft_alpha_grad(image, trimap, g, lambda_value=100.0, epsilon=1e-7):
     x = lu.solve(b)
     mu = lu.solve(np.asarray(g, dtype=np.float64).ravel())
     return -cf_laplacian_vjp(image, x, mu, epsilon)
+
+
+# --------------------------------------------------------------------------
+# Large-kernel matting Laplacian (pymatting/laplacian/lkm_laplacian.py:6-76)
+# --------------------------------------------------------------------------
+
+def _box(a, r, mode):
+    """Box sums over (2r+1)^2 windows along the first two axes: 'valid'
+    (h-2r, w-2r) or 'full' (h+2r, w+2r, zeros outside), by cumulative sums
+    (pymatting/util/boxfilter.py:6-82 restated)."""
+    if mode == "full":
+        pad = [(2 * r, 2 * r), (2 * r, 2 * r)] + [(0, 0)] * (a.ndim - 2)
+        a = np.pad(a, pad)
+    k = 2 * r + 1
+    c = np.cumsum(a, axis=0)
+    c = np.concatenate([np.zeros_like(c[:1]), c], axis=0)
+    a = c[k:] - c[:-k]
+    c = np.cumsum(a, axis=1)
+    c = np.concatenate([np.zeros_like(c[:, :1]), c], axis=1)
+    return c[:, k:] - c[:, :-k]
+
+
+def lkm_laplacian(image, epsilon=1e-7, radius=10):
+    """(L_matvec, diag_L) of the large-kernel Laplacian."""
+    image = np.asarray(image, dtype=np.float64)
+    r = radius
+    area = (2 * r + 1) ** 2
+    h, w, _ = image.shape
+    means = _box(image, r, "valid") / area
+    covs = _box(image[:, :, :, None] * image[:, :, None, :], r, "valid") / area
+    covs -= means[:, :, :, None] * means[:, :, None, :]
+    V = np.linalg.inv(covs + epsilon / area * np.eye(3)) / area
+    Vm = np.einsum("...ij,...j->...i", V, means)
+    mVm = 1.0 / area + np.einsum("...i,...i->...", means, Vm)
+    c = _box(np.ones((h - 2 * r, w - 2 * r)), r, "full")
+
+    def L_matvec(p):
+        p = np.asarray(p, dtype=np.float64).reshape(h, w)
+        ps = _box(p, r, "valid")
+        pI = _box(p[:, :, None] * image, r, "valid")
+        out = c * p
+        t3 = ps[:, :, None] * Vm - np.einsum("...ij,...j->...i", V, pI)
+        out += np.einsum("...i,...i->...", image, _box(t3, r, "full"))
+        t1 = ps * mVm - np.einsum("...i,...i->...", pI, Vm)
+        out -= _box(t1, r, "full")
+        return out.ravel()
+
+    diag = _box(1.0 - mVm, r, "full")
+    t = 2 * _box(Vm, r, "full") - np.einsum("...ij,...j->...i", _box(V, r, "full"), image)
+    diag += np.einsum("...i,...i->...", image, t)
+    return L_matvec, diag.ravel()

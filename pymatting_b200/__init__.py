@@ -1,8 +1,9 @@
 """pymatting_b200 — PyMatting's closed-form alpha path on NVIDIA B200.
 
-Drop-in replacements for ``cf_laplacian``, ``make_linear_system``, ``cg``
+Drop-in replacements for ``cf_laplacian``, ``lkm_laplacian``, ``make_linear_system``, ``cg``
 (with ``CounterCallback`` / ``ProgressCallback``), the ``jacobi`` /
-``vcycle`` / ``ichol`` preconditioner factories and ``estimate_alpha_cf``,
+``vcycle`` / ``ichol`` preconditioner factories, ``estimate_alpha_cf`` and
+``estimate_alpha_lkm``,
 computed by hand-written sm_100a kernels behind a C ABI
 (``include/pymatting_b200.h``). Extensions without a reference counterpart:
 ``solve_alpha`` (batched, mixed-precision soft-constraint solves) and
@@ -15,6 +16,7 @@ from .preconditioner import jacobi, vcycle, ichol, CholeskyDecomposition
 from .solver import cg, CounterCallback, ProgressCallback
 from .alpha import estimate_alpha_cf, estimate_alpha
 from .autograd import cf_alpha
+from .lkm import lkm_laplacian, estimate_alpha_lkm
 
 __version__ = "0.1.0"
 
@@ -22,4 +24,5 @@ __all__ = [
     "trimap_split", "sanity_check_image", "cf_laplacian", "make_linear_system",
     "DeviceCSRMatrix", "jacobi", "vcycle", "ichol", "CholeskyDecomposition", "cg",
     "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
+    "lkm_laplacian", "estimate_alpha_lkm",
 ]

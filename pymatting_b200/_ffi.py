@@ -25,6 +25,10 @@ _SIGNATURES = {
                                      c_vp, c_vp, c_vp, c_vp]),
     "pmb_cf_laplacian_planes": (c_int, [c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_dbl, c_vp,
                                         c_vp]),
+    "pmb_lkm_scratch_elems": (c_i64, [c_int, c_int, c_int]),
+    "pmb_lkm_setup": (c_int, [c_vp, c_int, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
+    "pmb_lkm_apply": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_lkm_diagonal": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_cf_laplacian_vjp": (c_int, [c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp, c_vp]),
     "pmb_cf_hard_system": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
     "pmb_scan_scratch_elems": (c_i64, [c_i64]),

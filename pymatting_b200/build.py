@@ -23,6 +23,7 @@ SOURCES = {
     "cf_assemble.cu": ["-fmad=false"],
     "stencil.cu": [],
     "csr.cu": [],
+    "lkm.cu": [],
     "ichol.cu": ["-fmad=false"],
     "engine.cu": [],
 }

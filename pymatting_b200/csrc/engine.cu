@@ -994,6 +994,51 @@ PMB_API int pmb_cf_laplacian_planes(const double* image, const uint8_t* is_known
     return 0;
 }
 
+int64_t pmb_launch_lkm_scratch(int, int, int);
+int pmb_launch_lkm_setup(const double*, int, int, int, double, double*, double*, cudaStream_t);
+int pmb_launch_lkm_apply(const double*, int, int, int, const double*, const double*, const double*,
+                         double*, double*, cudaStream_t);
+int pmb_launch_lkm_diag(const double*, int, int, int, const double*, const double*, double*,
+                        double*, double*, cudaStream_t);
+
+PMB_API int64_t pmb_lkm_scratch_elems(int h, int w, int radius) {
+    if (h <= 2 * radius || w <= 2 * radius || radius < 0) return -1;
+    return pmb_launch_lkm_scratch(h, w, radius);
+}
+
+PMB_API int pmb_lkm_setup(const double* image, int h, int w, int radius, double epsilon,
+                          double* windows, double* scratch, void* stream) {
+    if (!image || !windows || !scratch || radius < 0 || h <= 2 * radius || w <= 2 * radius)
+        return fail(kErrArg, "pmb_lkm_setup: bad arguments (the image must exceed 2 radius)");
+    if (pmb_launch_lkm_setup(image, h, w, radius, epsilon, windows, scratch, (cudaStream_t)stream))
+        return fail(kErrCuda, std::string("lkm setup: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+PMB_API int pmb_lkm_apply(const double* image, int h, int w, int radius, const double* windows,
+                          const double* diag_add, const double* p, double* out, double* scratch,
+                          void* stream) {
+    if (!image || !windows || !p || !out || !scratch || radius < 0 || h <= 2 * radius ||
+        w <= 2 * radius)
+        return fail(kErrArg, "pmb_lkm_apply: bad arguments");
+    if (pmb_launch_lkm_apply(image, h, w, radius, windows, diag_add, p, out, scratch,
+                             (cudaStream_t)stream))
+        return fail(kErrCuda, std::string("lkm apply: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+PMB_API int pmb_lkm_diagonal(const double* image, int h, int w, int radius, const double* windows,
+                             const double* diag_add, double* diag, double* inv_diag,
+                             double* scratch, void* stream) {
+    if (!image || !windows || !diag || !scratch || radius < 0 || h <= 2 * radius ||
+        w <= 2 * radius)
+        return fail(kErrArg, "pmb_lkm_diagonal: bad arguments");
+    if (pmb_launch_lkm_diag(image, h, w, radius, windows, diag_add, diag, inv_diag, scratch,
+                            (cudaStream_t)stream))
+        return fail(kErrCuda, std::string("lkm diagonal: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 int pmb_launch_cf_vjp(const double*, const uint8_t*, int, int, double, const double*,
                       const double*, double*, cudaStream_t);
 

@@ -54,6 +54,16 @@ class JacobiPreconditioner:
                                                    dev.ptr(data), dev.ptr(self.inv_diag),
                                                    dev.stream()), "jacobi")
 
+    @classmethod
+    def from_inverse_diagonal(cls, inv_diag):
+        """Jacobi preconditioner of an operator given only as a function
+        (e.g. lkm_laplacian): ``inv_diag`` is 1 / diag(A) on the device."""
+        obj = cls.__new__(cls)
+        obj.A = None
+        obj.source = None
+        obj.inv_diag = inv_diag
+        return obj
+
     def apply_device(self, r):
         z = dev.empty(r.numel(), torch.float64)
         _ffi.check(_ffi.lib().pmb_vec_mul(r.numel(), dev.ptr(r), dev.ptr(self.inv_diag),

@@ -216,6 +216,37 @@ def gen_lemur(pm, root):
         os.chdir(cwd)
 
 
+def gen_lkm(pm, root, rng):
+    """lkm_laplacian on small random images (L p and diag_L), and the
+    reference test's lemur comparison of the LKM and CF solves
+    (tests/test_lkm.py), plus estimate_alpha_lkm on that image."""
+    out = {}
+    for name, (h, w, r) in {"a": (29, 37, 2), "b": (41, 53, 4), "c": (47, 45, 10)}.items():
+        img = rng.random((h, w, 3))
+        p = rng.standard_normal(h * w)
+        L, diag = pm.lkm_laplacian(img, epsilon=1e-7, radius=r)
+        out[f"{name}_image"], out[f"{name}_p"] = img, p
+        out[f"{name}_Lp"], out[f"{name}_diag"] = L(p), diag
+        out[f"{name}_radius"] = np.array([r])
+    cwd = os.getcwd()
+    os.chdir(root)
+    try:
+        image = pm.load_image("data/lemur/lemur.png", "rgb", 0.125, "bilinear")
+        trimap = pm.load_image("data/lemur/lemur_trimap.png", "gray", 0.125, "nearest")
+    finally:
+        os.chdir(cwd)
+    L_lkm, diag_lkm = pm.lkm_laplacian(image, epsilon=1e-7, radius=2)
+    A_cf, b, c = pm.make_linear_system(pm.cf_laplacian(image, epsilon=1e-7, radius=2), trimap,
+                                       return_c=True)
+    inv = 1.0 / (diag_lkm + c)
+    cb_l, cb_c = pm.CounterCallback(), pm.CounterCallback()
+    out["lemur_x_lkm"] = pm.cg(lambda x: L_lkm(x) + c * x, b, M=lambda r: inv * r, callback=cb_l)
+    out["lemur_x_cf"] = pm.cg(A_cf, b, M=pm.jacobi(A_cf), callback=cb_c)
+    out["lemur_it_lkm"], out["lemur_it_cf"] = np.array([cb_l.n]), np.array([cb_c.n])
+    out["lemur_alpha_lkm"] = pm.estimate_alpha_lkm(image, trimap)
+    np.savez_compressed(os.path.join(HERE, "lkm_small.npz"), **out)
+
+
 def gen_c1(pm):
     """estimate_alpha_cf on the 320x240 synthetic workload (default ichol)."""
     from pymatting_b200.synthetic import make_matting_problem
@@ -235,7 +266,8 @@ def main():
     only = sys.argv[2:]
     for name, fn in [("cf", lambda: gen_cf(pm, rng)), ("cg", lambda: gen_cg(pm)),
                      ("ichol", lambda: gen_ichol(pm, rng)), ("soft", lambda: gen_soft(pm)),
-                     ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm))]:
+                     ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm)),
+                     ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77)))]:
         if not only or name in only:
             fn()
     for f in sorted(os.listdir(HERE)):

@@ -152,3 +152,12 @@ def test_oracle_laplacian_vjp_matches_finite_differences():
         e[y, xx, c] = step
         fd = (phi(img + e) - phi(img - e)) / (2 * step)
         assert abs(fd - grad[y, xx, c]) <= 1e-6 * max(1.0, abs(fd)), (y, xx, c, fd, grad[y, xx, c])
+
+
+def test_oracle_lkm_matches_reference():
+    d = golden("lkm_small.npz")
+    for name in "abc":
+        L, diag = oracle.lkm_laplacian(d[f"{name}_image"], 1e-7, int(d[f"{name}_radius"][0]))
+        ref_lp, ref_diag = d[f"{name}_Lp"], d[f"{name}_diag"]
+        assert np.abs(L(d[f"{name}_p"]) - ref_lp).max() <= 1e-8 * np.abs(ref_lp).max()
+        assert np.abs(diag - ref_diag).max() <= 1e-8 * np.abs(ref_diag).max()
