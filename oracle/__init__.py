@@ -15,6 +15,8 @@ Pieces and the reference code each restates (paths inside PyMatting 1.1.15):
 * ``make_P`` / ``vcycle`` pymatting/preconditioner/vcycle.py:6-153
 * ``ichol``              pymatting/preconditioner/ichol.py:6-301 (C)
 * ``estimate_alpha_cf``  pymatting/alpha/estimate_alpha_cf.py:8-78
+* ``lkm_laplacian``      pymatting/laplacian/lkm_laplacian.py:6-76
+* ``estimate_foreground_ml`` pymatting/foreground/estimate_foreground_ml.py:5-253 (C)
 
 Parity of this restatement with the reference itself is pinned by
 ``tests/test_oracle.py`` against the fixtures in ``tests/golden/`` that
@@ -456,3 +458,73 @@ def lkm_laplacian(image, epsilon=1e-7, radius=10):
     t = 2 * _box(Vm, r, "full") - np.einsum("...ij,...j->...i", _box(V, r, "full"), image)
     diag += np.einsum("...i,...i->...", image, t)
     return L_matvec, diag.ravel()
+
+
+# --------------------------------------------------------------------------
+# Foreground / background estimation
+# --------------------------------------------------------------------------
+
+def _fg_inputs(image, alpha):
+    image = np.ascontiguousarray(image, dtype=np.float32)
+    alpha = np.ascontiguousarray(alpha, dtype=np.float32)
+    h, w = alpha.shape
+    assert image.ndim == 3 and image.shape[:2] == (h, w) and 1 <= image.shape[2] <= 8
+    return image, alpha, h, w
+
+
+def fg_mean_colors(image, alpha):
+    """estimate_foreground_ml.py:79-95: the 2 depth seed colours (F then B)."""
+    lib = _load()
+    image, alpha, h, w = _fg_inputs(image, alpha)
+    depth = image.shape[2]
+    seed = np.zeros(2 * depth, dtype=np.float32)
+    lib.oracle_fg_mean_colors(_p(image, ctypes.c_float), _p(alpha, ctypes.c_float),
+                              ctypes.c_int64(h), ctypes.c_int64(w), ctypes.c_int(depth),
+                              _p(seed, ctypes.c_float))
+    return seed
+
+
+def fg_levels(h, w):
+    """estimate_foreground_ml.py:101-105: the (h, w) of every level."""
+    lib = _load()
+    hs = np.zeros(64, dtype=np.int64)
+    ws = np.zeros(64, dtype=np.int64)
+    lib.oracle_fg_levels.restype = ctypes.c_int
+    n = lib.oracle_fg_levels(ctypes.c_int64(h), ctypes.c_int64(w), _p(hs, ctypes.c_int64),
+                             _p(ws, ctypes.c_int64), 64)
+    if n < 0:
+        raise ZeroDivisionError("division by zero")
+    return list(zip(hs[:n].tolist(), ws[:n].tolist()))
+
+
+def estimate_foreground_ml(image, alpha, regularization=1e-5, n_small_iterations=10,
+                           n_big_iterations=2, small_size=32, return_background=False,
+                           gradient_weight=1.0, seed=None):
+    """estimate_foreground_ml.py:186-253 over _estimate_fb_ml (:61-183).
+
+    ``seed`` replaces the 2 depth mean colours the reference starts from."""
+    lib = _load()
+    image, alpha, h, w = _fg_inputs(image, alpha)
+    depth = image.shape[2]
+    F = np.zeros((h, w, depth), dtype=np.float32)
+    B = np.zeros((h, w, depth), dtype=np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    sp = None
+    if seed is not None:
+        seed = np.ascontiguousarray(seed, dtype=np.float32).reshape(2 * depth)
+        sp = _p(seed, ctypes.c_float)
+    lib.oracle_fg_ml.restype = ctypes.c_int
+    lib.oracle_fg_ml.argtypes = [fp, fp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_float, fp, fp, fp]
+    rc = lib.oracle_fg_ml(_p(image, ctypes.c_float), _p(alpha, ctypes.c_float), h, w, depth,
+                          float(regularization), int(n_small_iterations),
+                          int(n_big_iterations), int(small_size), float(gradient_weight),
+                          sp, _p(F, ctypes.c_float), _p(B, ctypes.c_float))
+    if rc == -1:
+        raise ZeroDivisionError("division by zero")
+    if rc != 0:
+        raise ValueError("oracle_fg_ml failed (%d)" % rc)
+    if return_background:
+        return F, B
+    return F

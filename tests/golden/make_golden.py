@@ -259,6 +259,64 @@ def gen_c1(pm):
                         alpha_unknown=alpha[unknown], frac=np.array([frac]))
 
 
+def _fg_case(rng, h, w, depth=3, kind="random"):
+    img = rng.random((h, w, depth)).astype(np.float32)
+    if kind == "random":
+        alpha = np.clip(rng.random((h, w)) * 1.4 - 0.2, 0.0, 1.0)
+    elif kind == "mostly_bg":
+        # alpha 0 almost everywhere: F there keeps the seed colour, which pins
+        # the seed computation
+        alpha = np.zeros((h, w))
+        alpha[h // 3: h // 3 + 2, w // 2: w // 2 + 3] = 1.0
+    else:  # "mostly_fg"
+        alpha = np.ones((h, w))
+        alpha[: 2, : 3] = 0.0
+        alpha[h // 2, w // 2] = 0.5
+    return img, alpha.astype(np.float32)
+
+
+def gen_foreground(pm, root, rng):
+    """estimate_foreground_ml on small float32 inputs with several parameter
+    sets and depths, and the reference test's lemur case
+    (tests/test_foreground.py: scale 0.1, box resize, mse <= 0.022)."""
+    from pymatting.foreground.estimate_foreground_ml import estimate_foreground_ml
+    cases = [
+        ((1, 2), {}, 3, "random"), ((2, 1), {}, 3, "random"), ((1, 7), {}, 3, "random"),
+        ((7, 9), {}, 3, "random"), ((33, 17), {}, 3, "random"), ((40, 65), {}, 3, "random"),
+        ((64, 64), {}, 3, "random"), ((100, 37), {}, 3, "random"),
+        ((45, 70), dict(regularization=1e-3, gradient_weight=0.5, n_small_iterations=3,
+                        n_big_iterations=4, small_size=16), 3, "random"),
+        ((29, 31), dict(n_big_iterations=0), 3, "random"),
+        ((50, 20), dict(n_small_iterations=0, n_big_iterations=1), 3, "random"),
+        ((24, 36), {}, 1, "random"), ((37, 23), {}, 4, "random"),
+        ((16, 16), {}, 3, "mostly_bg"), ((21, 18), {}, 3, "mostly_fg"),
+    ]
+    out = {"n_cases": np.array([len(cases)])}
+    for i, ((h, w), kw, depth, kind) in enumerate(cases):
+        img, alpha = _fg_case(rng, h, w, depth, kind)
+        F, B = estimate_foreground_ml(img, alpha, return_background=True, **kw)
+        out[f"c{i}_image"], out[f"c{i}_alpha"] = img, alpha
+        out[f"c{i}_F"], out[f"c{i}_B"] = F, B
+        out[f"c{i}_params"] = np.array([kw.get("regularization", 1e-5),
+                                        kw.get("n_small_iterations", 10),
+                                        kw.get("n_big_iterations", 2),
+                                        kw.get("small_size", 32),
+                                        kw.get("gradient_weight", 1.0)])
+    cwd = os.getcwd()
+    os.chdir(root)
+    try:
+        image = pm.load_image("data/lemur/lemur.png", "RGB", 0.1, "box")
+        trimap = pm.load_image("data/lemur/lemur_trimap.png", "GRAY", 0.1, "nearest")
+        alpha = pm.load_image("data/lemur/lemur_alpha.png", "GRAY", 0.1, "box")
+        expected = pm.load_image("data/lemur/lemur_foreground.png", "RGB", 0.1, "box")
+    finally:
+        os.chdir(cwd)
+    F, B = estimate_foreground_ml(image, alpha, return_background=True)
+    out["lemur_image"], out["lemur_alpha"], out["lemur_trimap"] = image, alpha, trimap
+    out["lemur_expected"], out["lemur_F"], out["lemur_B"] = expected, F, B
+    np.savez_compressed(os.path.join(HERE, "foreground_small.npz"), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     pm = import_reference(root)
@@ -267,7 +325,8 @@ def main():
     for name, fn in [("cf", lambda: gen_cf(pm, rng)), ("cg", lambda: gen_cg(pm)),
                      ("ichol", lambda: gen_ichol(pm, rng)), ("soft", lambda: gen_soft(pm)),
                      ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm)),
-                     ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77)))]:
+                     ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77))),
+                     ("foreground", lambda: gen_foreground(pm, root, np.random.default_rng(91)))]:
         if not only or name in only:
             fn()
     for f in sorted(os.listdir(HERE)):

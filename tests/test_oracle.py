@@ -161,3 +161,44 @@ def test_oracle_lkm_matches_reference():
         ref_lp, ref_diag = d[f"{name}_Lp"], d[f"{name}_diag"]
         assert np.abs(L(d[f"{name}_p"]) - ref_lp).max() <= 1e-8 * np.abs(ref_lp).max()
         assert np.abs(diag - ref_diag).max() <= 1e-8 * np.abs(ref_diag).max()
+
+
+def _fg_kwargs(p):
+    return dict(regularization=float(p[0]), n_small_iterations=int(p[1]),
+                n_big_iterations=int(p[2]), small_size=int(p[3]), gradient_weight=float(p[4]))
+
+
+def test_oracle_foreground_matches_reference():
+    """estimate_foreground_ml (numba, sequential Gauss-Seidel) against the C
+    restatement: bit-exact F and B on every fixture case, including depths 1
+    and 4, zero-iteration levels and the cases whose output keeps the seed
+    colours (which pins the running float32 mean)."""
+    g = golden("foreground_small.npz")
+    for i in range(int(g["n_cases"][0])):
+        kw = _fg_kwargs(g[f"c{i}_params"])
+        F, B = oracle.estimate_foreground_ml(g[f"c{i}_image"], g[f"c{i}_alpha"],
+                                             return_background=True, **kw)
+        assert np.array_equal(F, g[f"c{i}_F"]), i
+        assert np.array_equal(B, g[f"c{i}_B"]), i
+    F, B = oracle.estimate_foreground_ml(g["lemur_image"], g["lemur_alpha"],
+                                         return_background=True)
+    assert np.array_equal(F, g["lemur_F"]) and np.array_equal(B, g["lemur_B"])
+
+
+def test_oracle_foreground_reference_test_threshold():
+    """tests/test_foreground.py of the reference: alpha-weighted mean error
+    against the expected lemur foreground over unknown pixels <= 0.022."""
+    g = golden("foreground_small.npz")
+    alpha = g["lemur_alpha"]
+    F = oracle.estimate_foreground_ml(g["lemur_image"], alpha)
+    unknown = (g["lemur_trimap"] > 0.1) & (g["lemur_trimap"] < 0.9)
+    diff = (alpha[:, :, None] * np.abs(F - g["lemur_expected"]))[unknown]
+    assert np.mean(diff) <= 0.022
+
+
+def test_oracle_foreground_levels_and_errors():
+    assert oracle.fg_levels(1, 2) == [(1, 1), (1, 2)]
+    lv = oracle.fg_levels(1080, 1920)
+    assert len(lv) == 12 and lv[0] == (1, 1) and lv[-1] == (1080, 1920)
+    with pytest.raises(ZeroDivisionError):
+        oracle.estimate_foreground_ml(np.zeros((1, 1, 3)), np.zeros((1, 1)))
