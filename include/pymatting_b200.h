@@ -4,6 +4,7 @@
  * Plain C types only: device pointers, sizes and a cudaStream_t passed as
  * void*. Every function returns 0 on success or a negative status
  *   -1  invalid argument         -2  CUDA error         -3  invalid state
+ *   -4  division by zero (where the reference raises ZeroDivisionError)
  * and pmb_last_error() describes the last failure of the calling thread.
  * The caller owns every device buffer. Objects (pmb_stencil, pmb_csr,
  * pmb_ichol) report the workspace they need; the caller allocates it and
@@ -88,6 +89,32 @@ int pmb_lkm_apply(const double* image, int h, int w, int radius, const double* w
 int pmb_lkm_diagonal(const double* image, int h, int w, int radius, const double* windows,
                      const double* diag_add, double* diag, double* inv_diag, double* scratch,
                      void* stream);
+
+/* ---- Foreground / background estimation -------------------------------- */
+
+/* Replace estimate_foreground_ml(image, alpha, regularization,
+ * n_small_iterations, n_big_iterations, small_size, return_background,
+ * gradient_weight) (pymatting/foreground/estimate_foreground_ml.py:186-253,
+ * kernel _estimate_fb_ml :61-183). image: (h, w, depth) float32, alpha:
+ * (h, w) float32, F and B: (h, w, depth) float32 (B may be null), all on the
+ * device; depth 1..8. seed: the 2*depth starting colours (F then B) on the
+ * device, or null for the mean foreground / background colours of the input
+ * (summed in float64; the reference sums in float32, so seeds agree to
+ * rounding). With equal seeds F and B are bit-identical to the reference.
+ * Asynchronous on `stream`; pmb_fg_status reports a failed sweep.
+ * Returns -4 ("division by zero") for a 1x1 image, where the reference
+ * raises ZeroDivisionError. */
+int64_t pmb_fg_workspace_bytes(int h, int w, int depth);
+int pmb_fg_ml(const float* image, const float* alpha, int h, int w, int depth,
+              float regularization, int n_small_iterations, int n_big_iterations,
+              int small_size, float gradient_weight, const float* seed, float* F, float* B,
+              void* workspace, int64_t workspace_bytes, void* stream);
+/* Synchronises `stream`; 0 if the last pmb_fg_ml on `workspace` completed. */
+int pmb_fg_status(void* workspace, void* stream);
+/* Level sizes of estimate_foreground_ml.py:101-105 as (h, w) pairs in hw
+ * (host memory); returns the number of levels. */
+int pmb_fg_levels(int h, int w, int n_small_iterations, int n_big_iterations, int small_size,
+                  int* hw, int max_levels);
 
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of

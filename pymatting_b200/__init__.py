@@ -17,6 +17,7 @@ from .solver import cg, CounterCallback, ProgressCallback
 from .alpha import estimate_alpha_cf, estimate_alpha
 from .autograd import cf_alpha
 from .lkm import lkm_laplacian, estimate_alpha_lkm
+from .foreground import estimate_foreground_ml
 
 __version__ = "0.1.0"
 
@@ -24,5 +25,5 @@ __all__ = [
     "trimap_split", "sanity_check_image", "cf_laplacian", "make_linear_system",
     "DeviceCSRMatrix", "jacobi", "vcycle", "ichol", "CholeskyDecomposition", "cg",
     "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
-    "lkm_laplacian", "estimate_alpha_lkm",
+    "lkm_laplacian", "estimate_alpha_lkm", "estimate_foreground_ml",
 ]

@@ -14,6 +14,7 @@ _lib = None
 c_int = ctypes.c_int
 c_i64 = ctypes.c_int64
 c_dbl = ctypes.c_double
+c_flt = ctypes.c_float
 c_vp = ctypes.c_void_p
 
 # name: (restype, argtypes)
@@ -30,6 +31,11 @@ _SIGNATURES = {
     "pmb_lkm_apply": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_lkm_diagonal": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_cf_laplacian_vjp": (c_int, [c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_fg_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_fg_ml": (c_int, [c_vp, c_vp, c_int, c_int, c_int, c_flt, c_int, c_int, c_int, c_flt,
+                          c_vp, c_vp, c_vp, c_vp, c_i64, c_vp]),
+    "pmb_fg_status": (c_int, [c_vp, c_vp]),
+    "pmb_fg_levels": (c_int, [c_int, c_int, c_int, c_int, c_int, c_vp, c_int]),
     "pmb_cf_hard_system": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
     "pmb_scan_scratch_elems": (c_i64, [c_i64]),
     "pmb_ell_csr_rowptr": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp]),

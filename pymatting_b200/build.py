@@ -24,6 +24,7 @@ SOURCES = {
     "stencil.cu": [],
     "csr.cu": [],
     "lkm.cu": [],
+    "foreground.cu": [],
     "ichol.cu": ["-fmad=false"],
     "engine.cu": [],
 }

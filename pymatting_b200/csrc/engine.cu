@@ -63,7 +63,7 @@ static int fail(int code, const std::string& msg) {
             return fail(-2, std::string(#call) + ": " + cudaGetErrorString(e_));           \
     } while (0)
 
-enum : int { kErrArg = -1, kErrCuda = -2, kErrState = -3 };
+enum : int { kErrArg = -1, kErrCuda = -2, kErrState = -3, kErrZeroDiv = -4 };
 
 static inline int pitch_for(int w) { return ((w + 31) / 32) * 32; }
 
@@ -1050,6 +1050,50 @@ PMB_API int pmb_cf_laplacian_vjp(const double* image, const uint8_t* is_known, i
     if (pmb_launch_cf_vjp(image, is_known, h, w, epsilon, x, mu, grad, (cudaStream_t)stream))
         return fail(kErrCuda, std::string("cf_laplacian_vjp launch: ") +
                                   cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+int64_t pmb_launch_fg_workspace(int, int, int);
+int pmb_launch_fg_levels(int, int, int, int, int, int*, int);
+int pmb_launch_fg(const float*, const float*, int, int, int, float, int, int, int, float,
+                  const float*, float*, float*, void*, int64_t, cudaStream_t);
+int pmb_launch_fg_status(void*, cudaStream_t, int*);
+
+PMB_API int64_t pmb_fg_workspace_bytes(int h, int w, int depth) {
+    return pmb_launch_fg_workspace(h, w, depth);
+}
+
+PMB_API int pmb_fg_levels(int h, int w, int n_small, int n_big, int small_size, int* hw,
+                          int max_levels) {
+    if (h <= 0 || w <= 0 || !hw || max_levels <= 0) return fail(kErrArg, "pmb_fg_levels: bad arguments");
+    const int n = pmb_launch_fg_levels(h, w, n_small, n_big, small_size, hw, max_levels);
+    if (n == -1) return fail(kErrZeroDiv, "division by zero");
+    if (n < 0) return fail(kErrArg, "pmb_fg_levels: too many levels");
+    return n;
+}
+
+PMB_API int pmb_fg_ml(const float* image, const float* alpha, int h, int w, int depth,
+                      float regularization, int n_small_iterations, int n_big_iterations,
+                      int small_size, float gradient_weight, const float* seed, float* F,
+                      float* B, void* workspace, int64_t workspace_bytes, void* stream) {
+    const int rc = pmb_launch_fg(image, alpha, h, w, depth, regularization, n_small_iterations,
+                                 n_big_iterations, small_size, gradient_weight, seed, F, B,
+                                 workspace, workspace_bytes, (cudaStream_t)stream);
+    if (rc == 0) return 0;
+    if (rc == -1) return fail(kErrZeroDiv, "division by zero");
+    if (rc == -2) return fail(kErrArg, "pmb_fg_ml: bad arguments");
+    if (rc == -3) return fail(kErrArg, "pmb_fg_ml: workspace smaller than pmb_fg_workspace_bytes");
+    return fail(kErrCuda, std::string("pmb_fg_ml launch: ") + cudaGetErrorString((cudaError_t)rc));
+}
+
+PMB_API int pmb_fg_status(void* workspace, void* stream) {
+    if (!workspace) return fail(kErrArg, "pmb_fg_status: bad arguments");
+    int v = 0;
+    const int rc = pmb_launch_fg_status(workspace, (cudaStream_t)stream, &v);
+    if (rc) return fail(kErrCuda, std::string("pmb_fg_status: ") + cudaGetErrorString((cudaError_t)rc));
+    if (v == 1) return fail(kErrState, "foreground sweep: a wait for a neighbouring strip timed out");
+    if (v == 2) return fail(kErrState, "foreground sweep: a coefficient copy did not complete");
+    if (v) return fail(kErrState, "foreground sweep failed (" + std::to_string(v) + ")");
     return 0;
 }
 

@@ -1,0 +1,659 @@
+// Multi-level foreground / background estimation (PyMatting's
+// estimate_foreground_ml, pymatting/foreground/estimate_foreground_ml.py:61-183)
+// on sm_100a.
+//
+// The reference sweeps every level with an in-place Gauss-Seidel pass in
+// raster order: pixel (y, x) of iteration i reads the NEW values of (y, x-1)
+// and (y-1, x) and the OLD values of (y, x+1) and (y+1, x). This file
+// reproduces that order exactly, so the results are bit-identical for the same
+// seed colours:
+//
+// * Rows are cut into strips of 32; a warp sweeps one strip for one colour
+//   channel with lane j on row 32k+j, lane j handling column s-j at step s.
+//   The new value of the row above comes from lane j-1's previous step by a
+//   shuffle, the old value of the row below from lane j+1's current load.
+//   Lane 0 reads the strip above, lane 31 the strip below, through global
+//   memory.
+// * Every (iteration, strip) pair is a unit. Units are claimed from a ticket
+//   counter in order, so a unit only ever waits on units that running CTAs
+//   already hold. Iteration i+1 of strip k runs behind iteration i of strip
+//   k+1, so all iterations of a level are in flight at once.
+// * F and B live in a diagonal layout [channel][strip][step][lane], so each
+//   warp's per-step loads and stores are one contiguous 512-byte row. Every
+//   value is stored as {float value, uint32 epoch} in one 64-bit word. The
+//   epoch is 0 for the level's starting values and i+1 for iteration i's
+//   output. A reader polls until the epoch it needs appears. A 64-bit
+//   relaxed store is single-copy atomic, so no fences or progress counters are
+//   needed. Every wait is bounded (2 s on %globaltimer); a timeout sets an
+//   error word and the kernel drains without waiting further.
+// * The per-pixel terms that depend only on alpha (the four neighbour weights
+//   and the inverse of the 2x2 system) are computed once per level by a
+//   parallel prep kernel. They are stored per (strip, 32-step chunk) as one
+//   contiguous record that the sweep brings into shared memory with bulk
+//   async copies, two chunks in flight.
+//
+// Arithmetic follows numba's typing of the reference (a00, da and the
+// right-hand side in float32; a1, a01, a11, the determinant and the inverse
+// in float64) with explicitly rounded intrinsics, so nothing is contracted
+// into fused multiply-adds.
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "tma.cuh"
+
+namespace pmb {
+namespace fg {
+
+constexpr int kLanes = 32;
+constexpr int kChunk = 32;  // diagonal steps per staged coefficient chunk
+constexpr int kMaxDepth = 8;
+constexpr int kMaxLevels = 40;
+constexpr int kRing = 8;  // steps of F/B loads in flight per lane
+constexpr unsigned long long kTimeoutNs = 2000000000ull;
+constexpr int kMeanBlocks = 592;
+constexpr int kMeanThreads = 256;
+enum : int { kErrTimeout = 1, kErrStage = 2 };
+
+// Coefficient record of one (strip, chunk): 32 steps x 32 lanes of
+//   float4 da             (weights of the left, right, upper, lower neighbour)
+//   double b00, b01, b11  (inverse of the 2x2 system)
+//   float2 pI[depth]      (a0 * I_c, float32(a1 * I_c))
+constexpr int kOffDa = 0;
+constexpr int kOffB00 = kChunk * kLanes * 16;
+constexpr int kOffB01 = kOffB00 + kChunk * kLanes * 8;
+constexpr int kOffB11 = kOffB01 + kChunk * kLanes * 8;
+constexpr int kOffPI = kOffB11 + kChunk * kLanes * 8;
+constexpr int kPIBytes = kChunk * kLanes * 8;
+__host__ __device__ constexpr int rec_bytes(int depth) { return kOffPI + depth * kPIBytes; }
+
+struct Level {
+    int h, w;    // level size
+    int S, Q;    // strips, 32-step chunks per strip
+    int Sp;      // steps per strip row in the diagonal layout (32 Q >= w + 31)
+    int n_iter;  // Gauss-Seidel sweeps on this level
+};
+
+__device__ __forceinline__ uint64_t pack(float v, uint32_t epoch) {
+    return ((uint64_t)epoch << 32) | (uint64_t)__float_as_uint(v);
+}
+__device__ __forceinline__ float value_of(uint64_t u) { return __uint_as_float((uint32_t)u); }
+__device__ __forceinline__ uint32_t epoch_of(uint64_t u) { return (uint32_t)(u >> 32); }
+
+__device__ __forceinline__ ulonglong2 ld_fb(const ulonglong2* p) {
+    ulonglong2 v;
+    asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];"
+                 : "=l"(v.x), "=l"(v.y)
+                 : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st_fb(ulonglong2* p, uint64_t a, uint64_t b) {
+    asm volatile("st.relaxed.gpu.global.v2.b64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b)
+                 : "memory");
+}
+__device__ __forceinline__ int ld_err(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Poll until both words of *p carry `want`. Bounded: gives up (returning
+// false) when the error word is set or after kTimeoutNs, which it reports.
+__device__ __noinline__ bool wait_epoch(const ulonglong2* p, ulonglong2& v, uint32_t want, int* err) {
+    unsigned long long t0 = 0;
+    for (uint32_t n = 0;; ++n) {
+        if ((n & 63) == 0) {
+            if (ld_err(err)) return false;
+            if (n == 0) {
+                t0 = now_ns();
+            } else if (now_ns() - t0 > kTimeoutNs) {
+                atomicCAS(err, 0, kErrTimeout);
+                return false;
+            }
+        }
+        v = ld_fb(p);
+        if (epoch_of(v.x) == want && epoch_of(v.y) == want) return true;
+    }
+}
+
+// Named barrier 1 over the CTA's `nthreads` threads.
+__device__ __forceinline__ void bar_sync1(int nthreads) {
+    asm volatile("barrier.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Seed colours: mean image colour over alpha > 0.9 (foreground) and
+// alpha < 0.1 (background), estimate_foreground_ml.py:79-95. Sums are taken
+// in float64 in a fixed order (deterministic); the reference accumulates a
+// running float32 sum, so the seeds agree to float32 rounding, not bitwise.
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kMeanThreads) k_fg_mean_partial(const float* __restrict__ image,
+                                                                  const float* __restrict__ alpha,
+                                                                  long long n, int depth,
+                                                                  double* __restrict__ part) {
+    double accF[kMaxDepth], accB[kMaxDepth], nF = 0.0, nB = 0.0;
+#pragma unroll
+    for (int c = 0; c < kMaxDepth; ++c) accF[c] = accB[c] = 0.0;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const float a = alpha[p];
+        if (a > 0.9f) {
+#pragma unroll
+            for (int c = 0; c < kMaxDepth; ++c)
+                if (c < depth) accF[c] += (double)image[p * depth + c];
+            nF += 1.0;
+        } else if (a < 0.1f) {
+#pragma unroll
+            for (int c = 0; c < kMaxDepth; ++c)
+                if (c < depth) accB[c] += (double)image[p * depth + c];
+            nB += 1.0;
+        }
+    }
+    double acc[2 * kMaxDepth + 2];
+#pragma unroll
+    for (int c = 0; c < kMaxDepth; ++c) {
+        acc[c] = accF[c];
+        acc[kMaxDepth + c] = accB[c];
+    }
+    acc[2 * kMaxDepth] = nF;
+    acc[2 * kMaxDepth + 1] = nB;
+    __shared__ double red[kMeanThreads];
+    constexpr int nv = 2 * kMaxDepth + 2;
+#pragma unroll
+    for (int i = 0; i < nv; ++i) {
+        red[threadIdx.x] = acc[i];
+        __syncthreads();
+        for (int st = kMeanThreads / 2; st > 0; st >>= 1) {
+            if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(long long)blockIdx.x * nv + i] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kMeanThreads) k_fg_mean_final(const double* __restrict__ part,
+                                                                int nblocks, int depth,
+                                                                float* __restrict__ seed) {
+    __shared__ double red[kMeanThreads];
+    __shared__ double tot[2 * kMaxDepth + 2];
+    constexpr int nv = 2 * kMaxDepth + 2;
+    for (int i = 0; i < nv; ++i) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += kMeanThreads) a += part[(long long)b * nv + i];
+        red[threadIdx.x] = a;
+        __syncthreads();
+        for (int st = kMeanThreads / 2; st > 0; st >>= 1) {
+            if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) tot[i] = red[0];
+        __syncthreads();
+    }
+    if (threadIdx.x < depth) {
+        const int c = threadIdx.x;
+        seed[c] = (float)(tot[c] / (tot[2 * kMaxDepth] + 1e-5));
+        seed[depth + c] = (float)(tot[kMaxDepth + c] / (tot[2 * kMaxDepth + 1] + 1e-5));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Prep: coefficients of one level and its starting F/B (epoch 0), both in
+// the diagonal layout. The level's image and alpha are the nearest-neighbour
+// resize of the input (estimate_foreground_ml.py:5-55, x_src = x w_src / w),
+// the starting F/B the nearest-neighbour resize of the previous level's
+// result (or the seed colours for the 1x1 level).
+// ---------------------------------------------------------------------------
+
+struct PrepArgs {
+    const float* image;  // (h0, w0, depth)
+    const float* alpha;  // (h0, w0)
+    int h0, w0, depth;
+    float reg, gw;
+    Level L, P;                 // this level and the previous one (P.h == 0: seed)
+    const ulonglong2* fb_prev;  // previous level, diagonal layout
+    const float* seed;          // F[depth], B[depth]
+    unsigned char* rec;
+    ulonglong2* fb;
+};
+
+__device__ __forceinline__ int src_index(int v, int n_dst, int n_src) {
+    const long long s = (long long)v * n_src / n_dst;
+    return (int)(s < 0 ? 0 : (s > n_src - 1 ? n_src - 1 : s));
+}
+
+__global__ void __launch_bounds__(256) k_fg_prep(PrepArgs A) {
+    const Level L = A.L;
+    const long long total = (long long)L.S * L.Sp * kLanes;
+    const long long plane = total;
+    const int rb = rec_bytes(A.depth);
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx & 31);
+        const long long t = idx >> 5;
+        const int s = (int)(t % L.Sp);
+        const int k = (int)(t / L.Sp);
+        const int y = kLanes * k + j, x = s - j;
+        const bool valid = y < L.h && x >= 0 && x < L.w;
+        unsigned char* R = A.rec + ((long long)k * L.Q + (s >> 5)) * rb;
+        const int e = ((s & 31) << 5) | j;  // entry within the record
+        float4 da = make_float4(0.f, 0.f, 0.f, 0.f);
+        double b00 = 0.0, b01 = 0.0, b11 = 0.0;
+        if (valid) {
+            const int yc = src_index(y, L.h, A.h0), xc = src_index(x, L.w, A.w0);
+            const int ym = src_index(max(y - 1, 0), L.h, A.h0);
+            const int yp = src_index(min(y + 1, L.h - 1), L.h, A.h0);
+            const int xm = src_index(max(x - 1, 0), L.w, A.w0);
+            const int xp = src_index(min(x + 1, L.w - 1), L.w, A.w0);
+            const long long pc = (long long)yc * A.w0 + xc;
+            const float a0 = A.alpha[pc];
+            const float an[4] = {A.alpha[(long long)yc * A.w0 + xm], A.alpha[(long long)yc * A.w0 + xp],
+                                 A.alpha[(long long)ym * A.w0 + xc], A.alpha[(long long)yp * A.w0 + xc]};
+            const double a1 = __dsub_rn(1.0, (double)a0);
+            float a00 = __fmul_rn(a0, a0);
+            const double a01 = __dmul_rn((double)a0, a1);
+            double a11 = __dmul_rn(a1, a1);
+            float d[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float g = fabsf(__fsub_rn(a0, an[q]));
+                d[q] = __fadd_rn(A.reg, __fmul_rn(A.gw, g));
+                a00 = __fadd_rn(a00, d[q]);
+                a11 = __dadd_rn(a11, (double)d[q]);
+            }
+            const double det = __dsub_rn(__dmul_rn((double)a00, a11), __dmul_rn(a01, a01));
+            const double inv = __ddiv_rn(1.0, det);
+            b00 = __dmul_rn(inv, a11);
+            b01 = __dmul_rn(inv, -a01);
+            b11 = __dmul_rn(inv, (double)a00);
+            da = make_float4(d[0], d[1], d[2], d[3]);
+            for (int c = 0; c < A.depth; ++c) {
+                const float I = A.image[pc * A.depth + c];
+                *(float2*)(R + kOffPI + c * kPIBytes + e * 8) =
+                    make_float2(__fmul_rn(a0, I), __double2float_rn(__dmul_rn(a1, (double)I)));
+            }
+        } else {
+            for (int c = 0; c < A.depth; ++c)
+                *(float2*)(R + kOffPI + c * kPIBytes + e * 8) = make_float2(0.f, 0.f);
+        }
+        *(float4*)(R + kOffDa + e * 16) = da;
+        *(double*)(R + kOffB00 + e * 8) = b00;
+        *(double*)(R + kOffB01 + e * 8) = b01;
+        *(double*)(R + kOffB11 + e * 8) = b11;
+
+        // starting values (epoch 0)
+        long long src = -1;
+        if (valid && A.P.h > 0) {
+            const int yq = src_index(y, L.h, A.P.h), xq = src_index(x, L.w, A.P.w);
+            src = ((long long)(yq >> 5) * A.P.Sp + (xq + (yq & 31))) * kLanes + (yq & 31);
+        }
+        const long long pplane = (long long)A.P.S * A.P.Sp * kLanes;
+        for (int c = 0; c < A.depth; ++c) {
+            float Fv = 0.f, Bv = 0.f;
+            if (valid) {
+                if (src >= 0) {
+                    const ulonglong2 v = A.fb_prev[c * pplane + src];
+                    Fv = value_of(v.x);
+                    Bv = value_of(v.y);
+                } else {
+                    Fv = A.seed[c];
+                    Bv = A.seed[A.depth + c];
+                }
+            }
+            A.fb[c * plane + idx] = make_ulonglong2(pack(Fv, 0u), pack(Bv, 0u));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sweep: all iterations of one level. One CTA = depth warps (one per colour
+// channel) working on one unit (iteration it, strip k) at a time.
+// ---------------------------------------------------------------------------
+
+struct SweepArgs {
+    Level L;
+    int depth;
+    const unsigned char* rec;
+    ulonglong2* fb;
+    float* outF;  // last level only: the final iteration also writes (h, w, depth)
+    float* outB;
+    int* ticket;
+    int* err;
+};
+
+__global__ void __launch_bounds__(kLanes * kMaxDepth, 1) k_fg_sweep(SweepArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_unit;
+    const Level L = A.L;
+    const int nthr = kLanes * A.depth;
+    const int tid = threadIdx.x, c = tid >> 5, j = tid & 31;
+    const int rb = rec_bytes(A.depth);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+    }
+    __syncthreads();
+    uint32_t phase0 = 0, phase1 = 0;
+    const int units = L.n_iter * L.S;
+    const long long plane = (long long)L.S * L.Sp * kLanes;
+    ulonglong2* fbc = A.fb + c * plane;
+    const long long strip = (long long)L.Sp * kLanes;
+
+    for (;;) {
+        if (tid == 0) {
+            const int u = atomicAdd(A.ticket, 1);
+            s_unit = ld_err(A.err) ? units : u;
+        }
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= units) break;
+        const int it = u / L.S, k = u - it * L.S;
+        const unsigned char* rec_k = A.rec + (long long)k * L.Q * rb;
+        if (tid == 0) {
+            fence_proxy_async();
+            for (int b = 0; b < 2 && b < L.Q; ++b) {
+                mbar_expect_tx(&bars[b], rb);
+                bulk_load(smem + b * rb, rec_k + (long long)b * rb, rb, &bars[b]);
+            }
+        }
+
+        const int y0 = kLanes * k, y = y0 + j;
+        const bool rowv = y < L.h;
+        const uint32_t e_old = it, e_new = it + 1;
+        const bool has_up = j == 0 && k > 0;
+        const bool has_dn = j == 31 && y0 + kLanes < L.h;
+        const bool last_out = A.outF != nullptr && it == L.n_iter - 1;
+        ulonglong2* row_self = fbc + k * strip + j;
+        const ulonglong2* row_up = fbc + (k - 1) * strip + 31;  // used only if has_up
+        const ulonglong2* row_dn = fbc + (k + 1) * strip;       // used only if has_dn
+
+        ulonglong2 ringR[kRing], ringA[kRing];
+        auto issue = [&](int s, ulonglong2& R, ulonglong2& Ax) {
+            const int cr = s + 1 - j;
+            if (rowv && cr >= 0 && cr < L.w) R = ld_fb(row_self + (long long)(s + 1) * kLanes);
+            const int cc = s - j;
+            if (cc >= 0 && cc < L.w) {
+                if (has_up) Ax = ld_fb(row_up + (long long)(s + 31) * kLanes);
+                else if (has_dn) Ax = ld_fb(row_dn + (long long)(s - 31) * kLanes);
+            }
+        };
+#pragma unroll
+        for (int r = 0; r < kRing; ++r) {
+            ringR[r] = make_ulonglong2(0, 0);
+            ringA[r] = make_ulonglong2(0, 0);
+            issue(r, ringR[r], ringA[r]);
+        }
+
+        float myF = 0.f, myB = 0.f;  // this lane's value from the previous step
+        float pF = 0.f, pB = 0.f;    // old value of this lane's current column
+        for (int q = 0; q < L.Q; ++q) {
+            uint64_t* bar = &bars[q & 1];
+            const uint32_t ph = (q & 1) ? phase1 : phase0;
+            if (!mbar_wait(bar, ph)) atomicCAS(A.err, 0, kErrStage);
+            if (q & 1) phase1 ^= 1u; else phase0 ^= 1u;
+            const unsigned char* cb = smem + (q & 1) * rb;
+            for (int sb = 0; sb < kChunk; sb += kRing) {
+#pragma unroll
+                for (int r = 0; r < kRing; ++r) {
+                    const int s = kChunk * q + sb + r;
+                    const int cur = s - j;
+                    ulonglong2 Rv = ringR[r];
+                    ulonglong2 Av = ringA[r];
+                    const bool hasR = rowv && cur + 1 >= 0 && cur + 1 < L.w;
+                    const bool inCol = cur >= 0 && cur < L.w;
+                    if (hasR && (epoch_of(Rv.x) != e_old || epoch_of(Rv.y) != e_old))
+                        wait_epoch(row_self + (long long)(s + 1) * kLanes, Rv, e_old, A.err);
+                    if (inCol && has_up && (epoch_of(Av.x) != e_new || epoch_of(Av.y) != e_new))
+                        wait_epoch(row_up + (long long)(s + 31) * kLanes, Av, e_new, A.err);
+                    if (inCol && has_dn && (epoch_of(Av.x) != e_old || epoch_of(Av.y) != e_old))
+                        wait_epoch(row_dn + (long long)(s - 31) * kLanes, Av, e_old, A.err);
+                    issue(s + kRing, ringR[r], ringA[r]);
+                    const float rF = value_of(Rv.x), rB = value_of(Rv.y);
+                    const float uF = __shfl_up_sync(0xffffffffu, myF, 1);
+                    const float uB = __shfl_up_sync(0xffffffffu, myB, 1);
+                    const float dF = __shfl_down_sync(0xffffffffu, rF, 1);
+                    const float dB = __shfl_down_sync(0xffffffffu, rB, 1);
+                    if (rowv && inCol) {
+                        const float Fl = cur == 0 ? pF : myF, Bl = cur == 0 ? pB : myB;
+                        const bool rin = cur + 1 < L.w;
+                        const float Fr = rin ? rF : pF, Br = rin ? rB : pB;
+                        float Fu, Bu, Fd, Bd;
+                        if (y == 0) { Fu = pF; Bu = pB; }
+                        else if (j == 0) { Fu = value_of(Av.x); Bu = value_of(Av.y); }
+                        else { Fu = uF; Bu = uB; }
+                        if (y == L.h - 1) { Fd = pF; Bd = pB; }
+                        else if (j == 31) { Fd = value_of(Av.x); Bd = value_of(Av.y); }
+                        else { Fd = dF; Bd = dB; }
+                        const int e = ((sb + r) << 5) | j;
+                        const float4 da = *(const float4*)(cb + kOffDa + e * 16);
+                        const double b00 = *(const double*)(cb + kOffB00 + e * 8);
+                        const double b01 = *(const double*)(cb + kOffB01 + e * 8);
+                        const double b11 = *(const double*)(cb + kOffB11 + e * 8);
+                        const float2 pI = *(const float2*)(cb + kOffPI + c * kPIBytes + e * 8);
+                        float f0 = pI.x, f1 = pI.y;
+                        f0 = __fadd_rn(f0, __fmul_rn(da.x, Fl));
+                        f1 = __fadd_rn(f1, __fmul_rn(da.x, Bl));
+                        f0 = __fadd_rn(f0, __fmul_rn(da.y, Fr));
+                        f1 = __fadd_rn(f1, __fmul_rn(da.y, Br));
+                        f0 = __fadd_rn(f0, __fmul_rn(da.z, Fu));
+                        f1 = __fadd_rn(f1, __fmul_rn(da.z, Bu));
+                        f0 = __fadd_rn(f0, __fmul_rn(da.w, Fd));
+                        f1 = __fadd_rn(f1, __fmul_rn(da.w, Bd));
+                        double Fc = __dadd_rn(__dmul_rn(b00, (double)f0), __dmul_rn(b01, (double)f1));
+                        double Bc = __dadd_rn(__dmul_rn(b01, (double)f0), __dmul_rn(b11, (double)f1));
+                        // max(0.0, min(1.0, v)) with Python's argument order
+                        Fc = Fc < 1.0 ? Fc : 1.0;
+                        Fc = Fc > 0.0 ? Fc : 0.0;
+                        Bc = Bc < 1.0 ? Bc : 1.0;
+                        Bc = Bc > 0.0 ? Bc : 0.0;
+                        const float nF = __double2float_rn(Fc), nB = __double2float_rn(Bc);
+                        st_fb(row_self + (long long)s * kLanes, pack(nF, e_new), pack(nB, e_new));
+                        if (last_out) {
+                            const long long o = ((long long)y * L.w + cur) * A.depth + c;
+                            A.outF[o] = nF;
+                            if (A.outB) A.outB[o] = nB;
+                        }
+                        myF = nF;
+                        myB = nB;
+                    }
+                    pF = rF;
+                    pB = rB;
+                }
+            }
+            // all warps are done with this buffer: refill it with chunk q + 2
+            bar_sync1(nthr);
+            if (tid == 0 && q + 2 < L.Q) {
+                fence_proxy_async();
+                mbar_expect_tx(bar, rb);
+                bulk_load(smem + (q & 1) * rb, rec_k + (long long)(q + 2) * rb, rb, bar);
+            }
+        }
+    }
+}
+
+// Final values when the last level runs no sweep (n_iter == 0): gather the
+// level's starting values out of the diagonal layout.
+__global__ void __launch_bounds__(256) k_fg_output(Level L, int depth, const ulonglong2* __restrict__ fb,
+                                                   float* __restrict__ outF, float* __restrict__ outB) {
+    const long long n = (long long)L.h * L.w;
+    const long long plane = (long long)L.S * L.Sp * kLanes;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(p / L.w), x = (int)(p % L.w);
+        const long long d = ((long long)(y >> 5) * L.Sp + (x + (y & 31))) * kLanes + (y & 31);
+        for (int c = 0; c < depth; ++c) {
+            const ulonglong2 v = fb[c * plane + d];
+            outF[p * depth + c] = value_of(v.x);
+            if (outB) outB[p * depth + c] = value_of(v.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+// Level sizes of estimate_foreground_ml.py:101-105 (glibc pow and log2, ties
+// of round() to even). Returns the level count, or -1 for a 1x1 image (the
+// reference divides by zero there).
+static int plan_levels(int h0, int w0, int n_small, int n_big, int small_size, Level* out) {
+    const int m = std::max(h0, w0);
+    const int n = (int)std::ceil(std::log2((double)m));
+    if (n == 0) return -1;
+    if (n + 1 > kMaxLevels) return -2;
+    for (int i = 0; i <= n; ++i) {
+        const double e = (double)i / (double)n;
+        Level& L = out[i];
+        L.w = (int)std::nearbyint(std::pow((double)w0, e));
+        L.h = (int)std::nearbyint(std::pow((double)h0, e));
+        L.S = (L.h + kLanes - 1) / kLanes;
+        L.Q = (L.w + kLanes - 1 + kChunk - 1) / kChunk;
+        L.Sp = L.Q * kChunk;
+        L.n_iter = (L.w <= small_size && L.h <= small_size) ? n_small : n_big;
+    }
+    return n + 1;
+}
+
+static long long align256(long long v) { return (v + 255) & ~255LL; }
+
+struct Layout {
+    long long hdr, part, seed, fb0, fb1, rec, total;
+};
+
+static Layout layout(int h0, int w0, int depth) {
+    const int S = (h0 + kLanes - 1) / kLanes;
+    const int Q = (w0 + kLanes - 1 + kChunk - 1) / kChunk;
+    const long long fb = (long long)depth * S * Q * kChunk * kLanes * 16;
+    Layout l;
+    l.hdr = 0;
+    l.part = 1024;
+    l.seed = l.part + align256((long long)kMeanBlocks * (2 * kMaxDepth + 2) * 8);
+    l.fb0 = l.seed + 256;
+    l.fb1 = l.fb0 + align256(fb);
+    l.rec = l.fb1 + align256(fb);
+    l.total = l.rec + align256((long long)S * Q * rec_bytes(depth));
+    return l;
+}
+
+}  // namespace fg
+}  // namespace pmb
+
+using namespace pmb::fg;
+
+int64_t pmb_launch_fg_workspace(int h, int w, int depth) {
+    if (h <= 0 || w <= 0 || depth < 1 || depth > kMaxDepth) return -1;
+    return layout(h, w, depth).total;
+}
+
+int pmb_launch_fg_levels(int h, int w, int n_small, int n_big, int small_size, int* hw, int max_levels) {
+    Level lv[kMaxLevels];
+    const int n = plan_levels(h, w, n_small, n_big, small_size, lv);
+    if (n < 0) return n;
+    for (int i = 0; i < n && i < max_levels; ++i) {
+        hw[2 * i] = lv[i].h;
+        hw[2 * i + 1] = lv[i].w;
+    }
+    return n;
+}
+
+// Returns 0, -1 (1x1 image), -2 (bad arguments), -3 (workspace too small) or
+// a positive CUDA error code.
+int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int depth, float reg,
+                  int n_small, int n_big, int small_size, float gw, const float* seed_in,
+                  float* outF, float* outB, void* workspace, int64_t ws_bytes, cudaStream_t st) {
+    if (!image || !alpha || !outF || !workspace || h0 <= 0 || w0 <= 0 || depth < 1 ||
+        depth > kMaxDepth || n_small < 0 || n_big < 0)
+        return -2;
+    Level lv[kMaxLevels];
+    const int nl = plan_levels(h0, w0, n_small, n_big, small_size, lv);
+    if (nl == -1) return -1;
+    if (nl < 0) return -2;
+    const Layout l = layout(h0, w0, depth);
+    if (ws_bytes < l.total) return -3;
+    unsigned char* ws = (unsigned char*)workspace;
+    int* hdr = (int*)(ws + l.hdr);  // [0] error word, [1 + level] ticket counters
+    double* part = (double*)(ws + l.part);
+    float* seed = (float*)(ws + l.seed);
+    ulonglong2* fbs[2] = {(ulonglong2*)(ws + l.fb0), (ulonglong2*)(ws + l.fb1)};
+    unsigned char* rec = ws + l.rec;
+
+    int dev = 0, num_sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (num_sms <= 0) num_sms = 148;
+    cudaError_t e = cudaFuncSetAttribute(k_fg_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         2 * rec_bytes(kMaxDepth));
+    if (e != cudaSuccess) return (int)e;
+    e = cudaMemsetAsync(hdr, 0, 1024, st);
+    if (e != cudaSuccess) return (int)e;
+    if (!seed_in) {
+        const long long n = (long long)h0 * w0;
+        k_fg_mean_partial<<<kMeanBlocks, kMeanThreads, 0, st>>>(image, alpha, n, depth, part);
+        k_fg_mean_final<<<1, kMeanThreads, 0, st>>>(part, kMeanBlocks, depth, seed);
+        seed_in = seed;
+    }
+    Level none{};
+    for (int i = 0; i < nl; ++i) {
+        const Level& L = lv[i];
+        PrepArgs P;
+        P.image = image;
+        P.alpha = alpha;
+        P.h0 = h0;
+        P.w0 = w0;
+        P.depth = depth;
+        P.reg = reg;
+        P.gw = gw;
+        P.L = L;
+        P.P = i > 0 ? lv[i - 1] : none;
+        P.fb_prev = fbs[(i + 1) & 1];
+        P.seed = seed_in;
+        P.rec = rec;
+        P.fb = fbs[i & 1];
+        const long long entries = (long long)L.S * L.Sp * kLanes;
+        const int blocks = (int)std::min<long long>((entries + 255) / 256, (long long)num_sms * 16);
+        k_fg_prep<<<blocks, 256, 0, st>>>(P);
+        const bool last = i == nl - 1;
+        if (L.n_iter > 0) {
+            SweepArgs S;
+            S.L = L;
+            S.depth = depth;
+            S.rec = rec;
+            S.fb = fbs[i & 1];
+            S.outF = last ? outF : nullptr;
+            S.outB = last ? outB : nullptr;
+            S.ticket = hdr + 1 + i;
+            S.err = hdr;
+            const int units = L.n_iter * L.S;
+            const int grid = std::min(units, num_sms);
+            k_fg_sweep<<<grid, kLanes * depth, 2 * rec_bytes(depth), st>>>(S);
+        } else if (last) {
+            const long long n = (long long)L.h * L.w;
+            const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)num_sms * 16);
+            k_fg_output<<<blocks, 256, 0, st>>>(L, depth, fbs[i & 1], outF, outB);
+        }
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+// Error word of the last run in `workspace` (synchronises the stream).
+int pmb_launch_fg_status(void* workspace, cudaStream_t st, int* status) {
+    int v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, workspace, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return (int)e;
+    *status = v;
+    return 0;
+}

@@ -1,0 +1,89 @@
+"""Foreground and background estimation on the device.
+
+Drop-in for ``estimate_foreground_ml(image, alpha, regularization=1e-5,
+n_small_iterations=10, n_big_iterations=2, small_size=32,
+return_background=False, gradient_weight=1.0)``
+(pymatting/foreground/estimate_foreground_ml.py:186-253). The library runs
+the reference's multi-level Gauss-Seidel sweeps in their exact raster order
+(``pmb_fg_ml``), so with the same starting colours F and B are bit-identical
+to the reference.
+
+The starting colours are the mean foreground (alpha > 0.9) and background
+(alpha < 0.1) colours of the input. The library sums them in float64, while
+the reference keeps a running float32 sum. The seeds can therefore differ in
+their last bits, which moves a few output values by float32 rounding (about
+4e-7 on a 440x680 photograph). ``seed_colors`` (2 * depth values, F then B)
+replaces the computed seeds.
+
+numpy inputs give float32 numpy outputs, like the reference; CUDA tensors
+stay on the device.
+"""
+
+import numpy as np
+import torch
+
+from . import _device as dev
+from . import _ffi
+
+__all__ = ["estimate_foreground_ml", "foreground_levels"]
+
+
+def foreground_levels(h, w, n_small_iterations=10, n_big_iterations=2, small_size=32):
+    """(h, w) of every level, coarsest first (estimate_foreground_ml.py:101-105)."""
+    lib = _ffi.lib()
+    hw = np.zeros(128, dtype=np.int32)
+    n = lib.pmb_fg_levels(int(h), int(w), int(n_small_iterations), int(n_big_iterations),
+                          int(small_size), hw.ctypes.data, 64)
+    if n == -4:
+        raise ZeroDivisionError("division by zero")
+    _ffi.check(0 if n > 0 else n, "pmb_fg_levels")
+    return [(int(hw[2 * i]), int(hw[2 * i + 1])) for i in range(n)]
+
+
+def _to_f32(a):
+    return dev.to_device(a if dev.is_device_tensor(a) else np.asarray(a), torch.float32)
+
+
+def estimate_foreground_ml(image, alpha, regularization=1e-5, n_small_iterations=10,
+                           n_big_iterations=2, small_size=32, return_background=False,
+                           gradient_weight=1.0, seed_colors=None):
+    """Estimate the foreground (and background) colours of a matte.
+
+    image: (h, w, depth) and alpha: (h, w), cast to float32 as the reference
+    does. Returns F, or (F, B) with ``return_background``, each (h, w, depth)
+    float32. Raises ZeroDivisionError for a 1x1 image, like the reference.
+    """
+    on_device = dev.is_device_tensor(image)
+    img = _to_f32(image)
+    al = _to_f32(alpha)
+    if img.dim() != 3 or al.dim() != 2 or tuple(img.shape[:2]) != tuple(al.shape):
+        raise ValueError("image must be (h, w, depth) and alpha (h, w) of the same size")
+    h, w, depth = (int(v) for v in img.shape)
+    if not 1 <= depth <= 8:
+        raise ValueError("images with 1 to 8 channels are supported, got %d" % depth)
+    seed = None
+    if seed_colors is not None:
+        seed = _to_f32(seed_colors).reshape(-1)
+        if seed.numel() != 2 * depth:
+            raise ValueError("seed_colors needs %d values" % (2 * depth))
+    lib = _ffi.lib()
+    nbytes = int(lib.pmb_fg_workspace_bytes(h, w, depth))
+    if nbytes <= 0:
+        raise ValueError("bad image shape %r" % ((h, w, depth),))
+    ws = dev.workspace(nbytes)
+    F = dev.empty((h, w, depth), torch.float32)
+    B = dev.empty((h, w, depth), torch.float32) if return_background else None
+    rc = lib.pmb_fg_ml(dev.ptr(img), dev.ptr(al), h, w, depth, float(regularization),
+                       int(n_small_iterations), int(n_big_iterations), int(small_size),
+                       float(gradient_weight), dev.ptr(seed), dev.ptr(F), dev.ptr(B),
+                       dev.ptr(ws), nbytes, dev.stream())
+    if rc == -4:
+        raise ZeroDivisionError("division by zero")
+    _ffi.check(rc, "pmb_fg_ml")
+    _ffi.check(lib.pmb_fg_status(dev.ptr(ws), dev.stream()), "pmb_fg_ml")
+    if not on_device:
+        F = dev.to_host(F)
+        B = dev.to_host(B) if B is not None else None
+    if return_background:
+        return F, B
+    return F
