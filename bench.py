@@ -12,6 +12,12 @@ with host numpy buffers (uploads and the alpha download inside the timed
 region). ``--impl reference`` times the CPU restatement of PyMatting's own
 path (cf_laplacian + make_linear_system + vcycle + cg) on host cores.
 
+``--workload foreground`` instead times estimate_foreground_ml (the step
+after alpha in PyMatting's cutout) on a 1920x1080 image and matte: the
+multi-level Gauss-Seidel sweeps in the reference's exact order, bit-identical
+to it for equal seed colours; its reference arm is the oracle's C
+restatement on one host core.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: launched by torch.distributed.run, one rank per GPU; every rank
 solves its own image (weak scaling, no collective on the data path).
@@ -41,7 +47,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["1080p", "4096", "batch64"], default="1080p")
+    ap.add_argument("--workload", choices=["1080p", "4096", "batch64", "foreground"],
+                    default="1080p",
+                    help="foreground: estimate_foreground_ml on a 1920x1080 image + matte")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", choices=["auto", "none"], default="auto",
                     help="run the launch-shape autotuner before timing (none: defaults)")
@@ -220,6 +228,163 @@ def run_reference(args, rank, world):
     return line
 
 
+FG_METRIC = "Mpix/s of estimate_foreground_ml (reference sweep order, bit-exact for equal seeds)"
+
+
+def foreground_inputs(rank):
+    from pymatting_b200.synthetic import make_matting_problem
+    img, _tri, alpha, _ = make_matting_problem(1080, 1920, 1 + rank, sigma=2.0, band=7,
+                                               unknown_fraction=0.12, dtype=np.float32)
+    return img, alpha
+
+
+def run_foreground_reference(args, rank):
+    """The oracle's C restatement of estimate_foreground_ml on one host core."""
+    if rank != 0:
+        return
+    import oracle
+    img, alpha = foreground_inputs(0)
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.estimate_foreground_ml(img, alpha, return_background=True)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    npx = alpha.size
+    value = npx * len(times) / sum(times) / 1e6
+    line = {"metric": FG_METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "estimate_foreground_ml_1920x1080",
+                       "path": "oracle C restatement of _estimate_fb_ml, 1 core"},
+            "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                             "sample": "full 1920x1080 image per step"},
+            "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_foreground(args, rank, world, local):
+    """estimate_foreground_ml on one 1920x1080 image per GPU (weak scaling)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import pymatting_b200 as pm
+    from pymatting_b200 import _ffi
+    lib = _ffi.lib()
+    img, alpha = foreground_inputs(rank)
+    h, w, depth = img.shape
+    npx = h * w
+    ti = torch.as_tensor(img, device=dev)
+    ta = torch.as_tensor(alpha, device=dev)
+    nb = int(lib.pmb_fg_workspace_bytes(h, w, depth))
+    ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+    F = torch.empty((h, w, depth), dtype=torch.float32, device=dev)
+    B = torch.empty_like(F)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+    levels = pm.foreground.foreground_levels(h, w)
+
+    def step():
+        rc = lib.pmb_fg_ml(ti.data_ptr(), ta.data_ptr(), h, w, depth, 1e-5, 10, 2, 32, 1.0,
+                           None, F.data_ptr(), B.data_ptr(), ws.data_ptr(), nb, st)
+        assert rc == 0, _ffi.last_error()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world > 1:
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        step()
+    _ffi.check(lib.pmb_fg_status(ws.data_ptr(), st), "pmb_fg_ml")
+    barrier()
+    t0 = time.time()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks.window(t0, time.time())
+    _ffi.check(lib.pmb_fg_status(ws.data_ptr(), st), "pmb_fg_ml")
+    barrier()
+    ms = max_over_ranks(sum(times) / len(times))
+    # end to end through the public API with host numpy buffers
+    e2e_times = []
+    for s in range(args.warmup + max(3, args.steps // 4)):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        Fh, Bh = pm.estimate_foreground_ml(img, alpha, return_background=True)
+        dt = time.perf_counter() - t1
+        if s >= args.warmup:
+            e2e_times.append(dt)
+    e2e_ms = max_over_ranks(1e3 * sum(e2e_times) / len(e2e_times))
+    clock_rec = clocks.stop()
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        alg_bytes = npx * (depth * 4 + 4 + 2 * depth * 4)
+        gbs = alg_bytes / (ms * 1e-3) / 1e9
+        line = {
+            "metric": FG_METRIC, "value": world * npx / (ms * 1e-3) / 1e6, "unit": "Mpix/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": "estimate_foreground_ml_1920x1080", "image": "1920x1080x3",
+                       "levels": len(levels), "regularization": 1e-5,
+                       "iterations": "10 on levels <= 32x32, 2 above",
+                       "l2": "flushed between steps (256 MB write)",
+                       "parallelism": "weak: one image per GPU, no collective"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / peak, "peak_source": peak_kind, "traffic": None,
+                         "bytes_per_launch": alg_bytes,
+                         "note": "latency-bound: each level is a wavefront of about "
+                                 "h + w diagonal steps; bytes are image + alpha in, F + B out"},
+            "e2e": {"value": world * npx / (e2e_ms * 1e-3) / 1e6, "unit": "Mpix/s",
+                    "h2d_bytes_per_step": int(npx * (depth + 1) * 4),
+                    "d2h_bytes_per_step": int(npx * 2 * depth * 4)},
+            "gpu_launches": int((2 + 2 * len(levels)) * args.steps),
+            "clocks": clock_rec,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            t1 = time.perf_counter()
+            oracle.estimate_foreground_ml(img, alpha, return_background=True)
+            dt = time.perf_counter() - t1
+            line["cpu_baseline"] = {"value": npx / dt / 1e6, "unit": "Mpix/s", "cores": 1,
+                                    "kind": "port",
+                                    "sample": "one full 1920x1080 estimate_foreground_ml "
+                                              "(oracle C restatement), %.0f ms" % (1e3 * dt)}
+            line["max_abs_vs_oracle"] = float(np.abs(Fh - oracle.estimate_foreground_ml(
+                img, alpha)).max())
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        barrier()
+        dist.destroy_process_group()
+
+
 def cpu_baseline(img, tri):
     import oracle
     t0 = time.perf_counter()
@@ -257,6 +422,12 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.workload == "foreground":
+        if args.impl == "reference":
+            run_foreground_reference(args, rank)
+        else:
+            run_foreground(args, rank, world, local)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

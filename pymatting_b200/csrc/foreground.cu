@@ -30,7 +30,9 @@
 //   and the inverse of the 2x2 system) are computed once per level by a
 //   parallel prep kernel. They are stored per (strip, 32-step chunk) as one
 //   contiguous record that the sweep brings into shared memory with bulk
-//   async copies, two chunks in flight.
+//   async copies, two chunks in flight. The F/B rows a step reads are copied
+//   into a per-warp shared-memory ring kDist steps ahead (cp.async groups),
+//   so each step waits only for its own rows.
 //
 // Arithmetic follows numba's typing of the reference (a00, da and the
 // right-hand side in float32; a1, a01, a11, the determinant and the inverse
@@ -53,23 +55,32 @@ constexpr int kLanes = 32;
 constexpr int kChunk = 32;  // diagonal steps per staged coefficient chunk
 constexpr int kMaxDepth = 8;
 constexpr int kMaxLevels = 40;
-constexpr int kRing = 8;  // steps of F/B loads in flight per lane
+constexpr int kGroupMax = 4;   // colour channels (warps) per sweep CTA
+constexpr int kRingSlots = 8;  // shared-memory slots of F/B rows per warp
+constexpr int kDist = 7;       // steps between a row's copy and its use
 constexpr unsigned long long kTimeoutNs = 2000000000ull;
-constexpr int kMeanBlocks = 592;
+constexpr int kMeanBlocks = 1184;
 constexpr int kMeanThreads = 256;
+constexpr int kMaxSide = 65535;
 enum : int { kErrTimeout = 1, kErrStage = 2 };
 
 // Coefficient record of one (strip, chunk): 32 steps x 32 lanes of
 //   float4 da             (weights of the left, right, upper, lower neighbour)
-//   double b00, b01, b11  (inverse of the 2x2 system)
+//   double2 {b00, b01}, double b11  (inverse of the 2x2 system)
 //   float2 pI[depth]      (a0 * I_c, float32(a1 * I_c))
 constexpr int kOffDa = 0;
-constexpr int kOffB00 = kChunk * kLanes * 16;
-constexpr int kOffB01 = kOffB00 + kChunk * kLanes * 8;
-constexpr int kOffB11 = kOffB01 + kChunk * kLanes * 8;
+constexpr int kOffB0 = kChunk * kLanes * 16;
+constexpr int kOffB11 = kOffB0 + kChunk * kLanes * 16;
 constexpr int kOffPI = kOffB11 + kChunk * kLanes * 8;
 constexpr int kPIBytes = kChunk * kLanes * 8;
+constexpr int kBaseBytes = kOffPI;  // da and the 2x2 inverse, shared by all channels
 __host__ __device__ constexpr int rec_bytes(int depth) { return kOffPI + depth * kPIBytes; }
+// Shared memory of one staged chunk for a CTA of `cpg` channels.
+__host__ __device__ constexpr int stage_bytes(int cpg) { return kBaseBytes + cpg * kPIBytes; }
+// Per-warp ring: kRingSlots x (32 right-hand values + 32 neighbour-strip
+// values, of which lanes 0 and 31 use theirs).
+constexpr int kRingRow = 2 * kLanes;
+constexpr int kWarpRingBytes = kRingSlots * kRingRow * 16;
 
 struct Level {
     int h, w;    // level size
@@ -106,23 +117,41 @@ __device__ __forceinline__ unsigned long long now_ns() {
     return t;
 }
 
-// Poll until both words of *p carry `want`. Bounded: gives up (returning
-// false) when the error word is set or after kTimeoutNs, which it reports.
-__device__ __noinline__ bool wait_epoch(const ulonglong2* p, ulonglong2& v, uint32_t want, int* err) {
+// Poll until both words of *p carry `want` and return them. Bounded: gives
+// up (returning the last read) when the error word is set or after
+// kTimeoutNs, which it reports.
+__device__ __noinline__ ulonglong2 poll_epoch(const ulonglong2* p, uint32_t want, int* err) {
     unsigned long long t0 = 0;
+    ulonglong2 v = make_ulonglong2(0, 0);
     for (uint32_t n = 0;; ++n) {
         if ((n & 63) == 0) {
-            if (ld_err(err)) return false;
+            if (ld_err(err)) return v;
             if (n == 0) {
                 t0 = now_ns();
             } else if (now_ns() - t0 > kTimeoutNs) {
                 atomicCAS(err, 0, kErrTimeout);
-                return false;
+                return v;
             }
         }
         v = ld_fb(p);
-        if (epoch_of(v.x) == want && epoch_of(v.y) == want) return true;
+        if (epoch_of(v.x) == want && epoch_of(v.y) == want) return v;
     }
+}
+
+__device__ __forceinline__ bool has_epoch(ulonglong2 v, uint32_t want) {
+    return epoch_of(v.x) == want && epoch_of(v.y) == want;
+}
+
+// 16-byte global -> shared copy cached in L2 only, tracked by commit groups.
+// With n = 0 nothing is read and the 16 bytes are zero-filled.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t n) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // Named barrier 1 over the CTA's `nthreads` threads.
@@ -137,69 +166,62 @@ __device__ __forceinline__ void bar_sync1(int nthreads) {
 // running float32 sum, so the seeds agree to float32 rounding, not bitwise.
 // ---------------------------------------------------------------------------
 
+constexpr int kMeanValues = 2 * kMaxDepth + 2;  // F sums, B sums, F count, B count
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void __launch_bounds__(kMeanThreads) k_fg_mean_partial(const float* __restrict__ image,
                                                                   const float* __restrict__ alpha,
                                                                   long long n, int depth,
                                                                   double* __restrict__ part) {
-    double accF[kMaxDepth], accB[kMaxDepth], nF = 0.0, nB = 0.0;
+    double acc[kMeanValues];
 #pragma unroll
-    for (int c = 0; c < kMaxDepth; ++c) accF[c] = accB[c] = 0.0;
+    for (int v = 0; v < kMeanValues; ++v) acc[v] = 0.0;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x) {
         const float a = alpha[p];
         if (a > 0.9f) {
 #pragma unroll
             for (int c = 0; c < kMaxDepth; ++c)
-                if (c < depth) accF[c] += (double)image[p * depth + c];
-            nF += 1.0;
+                if (c < depth) acc[c] += (double)image[p * depth + c];
+            acc[2 * kMaxDepth] += 1.0;
         } else if (a < 0.1f) {
 #pragma unroll
             for (int c = 0; c < kMaxDepth; ++c)
-                if (c < depth) accB[c] += (double)image[p * depth + c];
-            nB += 1.0;
+                if (c < depth) acc[kMaxDepth + c] += (double)image[p * depth + c];
+            acc[2 * kMaxDepth + 1] += 1.0;
         }
     }
-    double acc[2 * kMaxDepth + 2];
+    __shared__ double red[kMeanThreads / 32][kMeanValues];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-    for (int c = 0; c < kMaxDepth; ++c) {
-        acc[c] = accF[c];
-        acc[kMaxDepth + c] = accB[c];
+    for (int v = 0; v < kMeanValues; ++v) {
+        const double t = warp_sum(acc[v]);
+        if (lane == 0) red[warp][v] = t;
     }
-    acc[2 * kMaxDepth] = nF;
-    acc[2 * kMaxDepth + 1] = nB;
-    __shared__ double red[kMeanThreads];
-    constexpr int nv = 2 * kMaxDepth + 2;
-#pragma unroll
-    for (int i = 0; i < nv; ++i) {
-        red[threadIdx.x] = acc[i];
-        __syncthreads();
-        for (int st = kMeanThreads / 2; st > 0; st >>= 1) {
-            if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) part[(long long)blockIdx.x * nv + i] = red[0];
-        __syncthreads();
+    __syncthreads();
+    if (threadIdx.x < kMeanValues) {
+        double t = 0.0;
+        for (int wv = 0; wv < kMeanThreads / 32; ++wv) t += red[wv][threadIdx.x];
+        part[(long long)blockIdx.x * kMeanValues + threadIdx.x] = t;
     }
 }
 
-__global__ void __launch_bounds__(kMeanThreads) k_fg_mean_final(const double* __restrict__ part,
-                                                                int nblocks, int depth,
-                                                                float* __restrict__ seed) {
-    __shared__ double red[kMeanThreads];
-    __shared__ double tot[2 * kMaxDepth + 2];
-    constexpr int nv = 2 * kMaxDepth + 2;
-    for (int i = 0; i < nv; ++i) {
-        double a = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += kMeanThreads) a += part[(long long)b * nv + i];
-        red[threadIdx.x] = a;
-        __syncthreads();
-        for (int st = kMeanThreads / 2; st > 0; st >>= 1) {
-            if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) tot[i] = red[0];
-        __syncthreads();
-    }
+// One warp per summed value, fixed order: deterministic.
+__global__ void __launch_bounds__(32 * kMeanValues) k_fg_mean_final(const double* __restrict__ part,
+                                                                    int nblocks, int depth,
+                                                                    float* __restrict__ seed) {
+    __shared__ double tot[kMeanValues];
+    const int v = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double a = 0.0;
+    for (int b = lane; b < nblocks; b += 32) a += part[(long long)b * kMeanValues + v];
+    a = warp_sum(a);
+    if (lane == 0) tot[v] = a;
+    __syncthreads();
     if (threadIdx.x < depth) {
         const int c = threadIdx.x;
         seed[c] = (float)(tot[c] / (tot[2 * kMaxDepth] + 1e-5));
@@ -227,22 +249,25 @@ struct PrepArgs {
     ulonglong2* fb;
 };
 
+// x_src = x * n_src / n_dst (sides <= 65535, so the product fits 32 bits).
 __device__ __forceinline__ int src_index(int v, int n_dst, int n_src) {
-    const long long s = (long long)v * n_src / n_dst;
-    return (int)(s < 0 ? 0 : (s > n_src - 1 ? n_src - 1 : s));
+    if (n_dst == n_src) return v;
+    const unsigned s = (unsigned)v * (unsigned)n_src / (unsigned)n_dst;
+    return (int)min(s, (unsigned)(n_src - 1));
 }
 
+// grid: (ceil(Sp * 32 / 256), S); one thread per diagonal entry (k, s, j).
 __global__ void __launch_bounds__(256) k_fg_prep(PrepArgs A) {
     const Level L = A.L;
-    const long long total = (long long)L.S * L.Sp * kLanes;
-    const long long plane = total;
+    const long long plane = (long long)L.S * L.Sp * kLanes;
     const int rb = rec_bytes(A.depth);
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(idx & 31);
-        const long long t = idx >> 5;
-        const int s = (int)(t % L.Sp);
-        const int k = (int)(t / L.Sp);
+    {
+        const int e_strip = blockIdx.x * blockDim.x + threadIdx.x;
+        if (e_strip >= L.Sp * kLanes) return;
+        const int j = e_strip & 31;
+        const int s = e_strip >> 5;
+        const int k = blockIdx.y;
+        const long long idx = (long long)k * L.Sp * kLanes + e_strip;
         const int y = kLanes * k + j, x = s - j;
         const bool valid = y < L.h && x >= 0 && x < L.w;
         unsigned char* R = A.rec + ((long long)k * L.Q + (s >> 5)) * rb;
@@ -287,8 +312,7 @@ __global__ void __launch_bounds__(256) k_fg_prep(PrepArgs A) {
                 *(float2*)(R + kOffPI + c * kPIBytes + e * 8) = make_float2(0.f, 0.f);
         }
         *(float4*)(R + kOffDa + e * 16) = da;
-        *(double*)(R + kOffB00 + e * 8) = b00;
-        *(double*)(R + kOffB01 + e * 8) = b01;
+        *(double2*)(R + kOffB0 + e * 16) = make_double2(b00, b01);
         *(double*)(R + kOffB11 + e * 8) = b11;
 
         // starting values (epoch 0)
@@ -316,13 +340,14 @@ __global__ void __launch_bounds__(256) k_fg_prep(PrepArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// Sweep: all iterations of one level. One CTA = depth warps (one per colour
-// channel) working on one unit (iteration it, strip k) at a time.
+// Sweep: all iterations of one level. A CTA holds one warp per colour channel
+// of a channel group (at most kGroupMax channels) and works on one unit
+// (iteration it, strip k, channel group g) at a time.
 // ---------------------------------------------------------------------------
 
 struct SweepArgs {
     Level L;
-    int depth;
+    int depth, groups, cpg;  // channels, channel groups, channels per group
     const unsigned char* rec;
     ulonglong2* fb;
     float* outF;  // last level only: the final iteration also writes (h, w, depth)
@@ -331,23 +356,23 @@ struct SweepArgs {
     int* err;
 };
 
-__global__ void __launch_bounds__(kLanes * kMaxDepth, 1) k_fg_sweep(SweepArgs A) {
+__global__ void __launch_bounds__(kLanes * kGroupMax, 1) k_fg_sweep(SweepArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_unit;
     const Level L = A.L;
-    const int nthr = kLanes * A.depth;
-    const int tid = threadIdx.x, c = tid >> 5, j = tid & 31;
+    const int tid = threadIdx.x, w = tid >> 5, j = tid & 31;
     const int rb = rec_bytes(A.depth);
+    const int sbytes = stage_bytes(A.cpg);
+    ulonglong2* ring = (ulonglong2*)(smem + 2 * sbytes + w * kWarpRingBytes);
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
     }
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
-    const int units = L.n_iter * L.S;
+    const int units = L.n_iter * L.S * A.groups;
     const long long plane = (long long)L.S * L.Sp * kLanes;
-    ulonglong2* fbc = A.fb + c * plane;
     const long long strip = (long long)L.Sp * kLanes;
 
     for (;;) {
@@ -359,16 +384,31 @@ __global__ void __launch_bounds__(kLanes * kMaxDepth, 1) k_fg_sweep(SweepArgs A)
         const int u = s_unit;
         __syncthreads();
         if (u >= units) break;
-        const int it = u / L.S, k = u - it * L.S;
+        const int g = u % A.groups, ik = u / A.groups;
+        const int it = ik / L.S, k = ik - it * L.S;
+        const int c0 = g * A.cpg, ng = min(A.cpg, A.depth - c0);
         const unsigned char* rec_k = A.rec + (long long)k * L.Q * rb;
+        const uint32_t stage_tx = kBaseBytes + ng * kPIBytes;
+        auto stage = [&](int buf, int q) {
+            const unsigned char* r = rec_k + (long long)q * rb;
+            mbar_expect_tx(&bars[buf], stage_tx);
+            bulk_load(smem + buf * sbytes, r, kBaseBytes, &bars[buf]);
+            bulk_load(smem + buf * sbytes + kBaseBytes, r + kOffPI + c0 * kPIBytes, ng * kPIBytes,
+                      &bars[buf]);
+        };
         if (tid == 0) {
             fence_proxy_async();
-            for (int b = 0; b < 2 && b < L.Q; ++b) {
-                mbar_expect_tx(&bars[b], rb);
-                bulk_load(smem + b * rb, rec_k + (long long)b * rb, rb, &bars[b]);
-            }
+            for (int b = 0; b < 2 && b < L.Q; ++b) stage(b, b);
         }
-
+        if (w >= ng) {
+            // no channel for this warp in this group: keep the phase parities
+            // in step with the warps that wait on every chunk
+            phase0 ^= (uint32_t)(((L.Q + 1) >> 1) & 1);
+            phase1 ^= (uint32_t)((L.Q >> 1) & 1);
+            continue;
+        }
+        const int c = c0 + w;
+        ulonglong2* fbc = A.fb + c * plane;
         const int y0 = kLanes * k, y = y0 + j;
         const bool rowv = y < L.h;
         const uint32_t e_old = it, e_new = it + 1;
@@ -378,108 +418,120 @@ __global__ void __launch_bounds__(kLanes * kMaxDepth, 1) k_fg_sweep(SweepArgs A)
         ulonglong2* row_self = fbc + k * strip + j;
         const ulonglong2* row_up = fbc + (k - 1) * strip + 31;  // used only if has_up
         const ulonglong2* row_dn = fbc + (k + 1) * strip;       // used only if has_dn
+        const bool has_aux = has_up || has_dn;
+        const uint32_t want_aux = has_up ? e_new : e_old;
+        // Step s reads [k][s+1][j] (right-hand value), [k-1][s+31][31] (lane 0)
+        // and [k+1][s-31][0] (lane 31): three arithmetic sequences in s.
+        const ulonglong2* gR = row_self + kLanes;
+        const ulonglong2* gA = has_up ? row_up + 31 * kLanes : (has_dn ? row_dn - 31 * kLanes : row_self);
+        const uint32_t ring_lane = smem_addr(ring) + j * 16;
 
-        ulonglong2 ringR[kRing], ringA[kRing];
-        auto issue = [&](int s, ulonglong2& R, ulonglong2& Ax) {
-            const int cr = s + 1 - j;
-            if (rowv && cr >= 0 && cr < L.w) R = ld_fb(row_self + (long long)(s + 1) * kLanes);
-            const int cc = s - j;
-            if (cc >= 0 && cc < L.w) {
-                if (has_up) Ax = ld_fb(row_up + (long long)(s + 31) * kLanes);
-                else if (has_dn) Ax = ld_fb(row_dn + (long long)(s - 31) * kLanes);
-            }
+        // Copy the rows step s needs into ring slot s % kRingSlots (zero-filled
+        // where the lane has nothing to read). One commit group per step.
+        auto issue = [&](int s) {
+            const uint32_t slot = ring_lane + (uint32_t)((s & (kRingSlots - 1)) * kRingRow * 16);
+            const bool cR = rowv && (unsigned)(s + 1 - j) < (unsigned)L.w;
+            const bool cA = has_aux && (unsigned)(s - j) < (unsigned)L.w;
+            cp_async16(slot, cR ? gR + (long long)s * kLanes : row_self, cR ? 16u : 0u);
+            cp_async16(slot + kLanes * 16, cA ? gA + (long long)s * kLanes : row_self, cA ? 16u : 0u);
+            cp_async_commit();
         };
-#pragma unroll
-        for (int r = 0; r < kRing; ++r) {
-            ringR[r] = make_ulonglong2(0, 0);
-            ringA[r] = make_ulonglong2(0, 0);
-            issue(r, ringR[r], ringA[r]);
-        }
+        for (int r = 0; r < kDist; ++r) issue(r);
 
         float myF = 0.f, myB = 0.f;  // this lane's value from the previous step
         float pF = 0.f, pB = 0.f;    // old value of this lane's current column
+        // Lane j first meets its column 0 as the right-hand value of step j-1;
+        // for lane 0 that step would be -1, so its column 0 is read here.
+        if (j == 0 && rowv) {
+            ulonglong2 v = ld_fb(row_self);
+            if (!has_epoch(v, e_old)) v = poll_epoch(row_self, e_old, A.err);
+            pF = value_of(v.x);
+            pB = value_of(v.y);
+        }
+        const int nthr = kLanes * ng;
         for (int q = 0; q < L.Q; ++q) {
             uint64_t* bar = &bars[q & 1];
             const uint32_t ph = (q & 1) ? phase1 : phase0;
             if (!mbar_wait(bar, ph)) atomicCAS(A.err, 0, kErrStage);
             if (q & 1) phase1 ^= 1u; else phase0 ^= 1u;
-            const unsigned char* cb = smem + (q & 1) * rb;
-            for (int sb = 0; sb < kChunk; sb += kRing) {
-#pragma unroll
-                for (int r = 0; r < kRing; ++r) {
-                    const int s = kChunk * q + sb + r;
-                    const int cur = s - j;
-                    ulonglong2 Rv = ringR[r];
-                    ulonglong2 Av = ringA[r];
-                    const bool hasR = rowv && cur + 1 >= 0 && cur + 1 < L.w;
-                    const bool inCol = cur >= 0 && cur < L.w;
-                    if (hasR && (epoch_of(Rv.x) != e_old || epoch_of(Rv.y) != e_old))
-                        wait_epoch(row_self + (long long)(s + 1) * kLanes, Rv, e_old, A.err);
-                    if (inCol && has_up && (epoch_of(Av.x) != e_new || epoch_of(Av.y) != e_new))
-                        wait_epoch(row_up + (long long)(s + 31) * kLanes, Av, e_new, A.err);
-                    if (inCol && has_dn && (epoch_of(Av.x) != e_old || epoch_of(Av.y) != e_old))
-                        wait_epoch(row_dn + (long long)(s - 31) * kLanes, Av, e_old, A.err);
-                    issue(s + kRing, ringR[r], ringA[r]);
-                    const float rF = value_of(Rv.x), rB = value_of(Rv.y);
-                    const float uF = __shfl_up_sync(0xffffffffu, myF, 1);
-                    const float uB = __shfl_up_sync(0xffffffffu, myB, 1);
-                    const float dF = __shfl_down_sync(0xffffffffu, rF, 1);
-                    const float dB = __shfl_down_sync(0xffffffffu, rB, 1);
-                    if (rowv && inCol) {
-                        const float Fl = cur == 0 ? pF : myF, Bl = cur == 0 ? pB : myB;
-                        const bool rin = cur + 1 < L.w;
-                        const float Fr = rin ? rF : pF, Br = rin ? rB : pB;
-                        float Fu, Bu, Fd, Bd;
-                        if (y == 0) { Fu = pF; Bu = pB; }
-                        else if (j == 0) { Fu = value_of(Av.x); Bu = value_of(Av.y); }
-                        else { Fu = uF; Bu = uB; }
-                        if (y == L.h - 1) { Fd = pF; Bd = pB; }
-                        else if (j == 31) { Fd = value_of(Av.x); Bd = value_of(Av.y); }
-                        else { Fd = dF; Bd = dB; }
-                        const int e = ((sb + r) << 5) | j;
-                        const float4 da = *(const float4*)(cb + kOffDa + e * 16);
-                        const double b00 = *(const double*)(cb + kOffB00 + e * 8);
-                        const double b01 = *(const double*)(cb + kOffB01 + e * 8);
-                        const double b11 = *(const double*)(cb + kOffB11 + e * 8);
-                        const float2 pI = *(const float2*)(cb + kOffPI + c * kPIBytes + e * 8);
-                        float f0 = pI.x, f1 = pI.y;
-                        f0 = __fadd_rn(f0, __fmul_rn(da.x, Fl));
-                        f1 = __fadd_rn(f1, __fmul_rn(da.x, Bl));
-                        f0 = __fadd_rn(f0, __fmul_rn(da.y, Fr));
-                        f1 = __fadd_rn(f1, __fmul_rn(da.y, Br));
-                        f0 = __fadd_rn(f0, __fmul_rn(da.z, Fu));
-                        f1 = __fadd_rn(f1, __fmul_rn(da.z, Bu));
-                        f0 = __fadd_rn(f0, __fmul_rn(da.w, Fd));
-                        f1 = __fadd_rn(f1, __fmul_rn(da.w, Bd));
-                        double Fc = __dadd_rn(__dmul_rn(b00, (double)f0), __dmul_rn(b01, (double)f1));
-                        double Bc = __dadd_rn(__dmul_rn(b01, (double)f0), __dmul_rn(b11, (double)f1));
-                        // max(0.0, min(1.0, v)) with Python's argument order
-                        Fc = Fc < 1.0 ? Fc : 1.0;
-                        Fc = Fc > 0.0 ? Fc : 0.0;
-                        Bc = Bc < 1.0 ? Bc : 1.0;
-                        Bc = Bc > 0.0 ? Bc : 0.0;
-                        const float nF = __double2float_rn(Fc), nB = __double2float_rn(Bc);
-                        st_fb(row_self + (long long)s * kLanes, pack(nF, e_new), pack(nB, e_new));
-                        if (last_out) {
-                            const long long o = ((long long)y * L.w + cur) * A.depth + c;
-                            A.outF[o] = nF;
-                            if (A.outB) A.outB[o] = nB;
-                        }
-                        myF = nF;
-                        myB = nB;
-                    }
-                    pF = rF;
-                    pB = rB;
+            const unsigned char* cb = smem + (q & 1) * sbytes;
+#pragma unroll 4
+            for (int t = 0; t < kChunk; ++t) {
+                const int s = kChunk * q + t;
+                const int cur = s - j;
+                cp_async_wait<kDist - 1>();
+                const ulonglong2* slot = ring + (s & (kRingSlots - 1)) * kRingRow;
+                ulonglong2 Rv = slot[j];
+                ulonglong2 Av = slot[kLanes + j];
+                // the slot refilled now was read at step s - 1
+                issue(s + kDist);
+                const bool inCol = (unsigned)cur < (unsigned)L.w;
+                const bool needR = rowv && (unsigned)(cur + 1) < (unsigned)L.w;
+                const bool needA = has_aux && inCol;
+                const bool okR = !needR || has_epoch(Rv, e_old);
+                const bool okA = !needA || has_epoch(Av, want_aux);
+                if (!__all_sync(0xffffffffu, okR && okA)) {
+                    if (!okR) Rv = poll_epoch(gR + (long long)s * kLanes, e_old, A.err);
+                    if (!okA) Av = poll_epoch(gA + (long long)s * kLanes, want_aux, A.err);
                 }
+                const float rF = value_of(Rv.x), rB = value_of(Rv.y);
+                const float aF = value_of(Av.x), aB = value_of(Av.y);
+                const float uF = __shfl_up_sync(0xffffffffu, myF, 1);
+                const float uB = __shfl_up_sync(0xffffffffu, myB, 1);
+                const float dF = __shfl_down_sync(0xffffffffu, rF, 1);
+                const float dB = __shfl_down_sync(0xffffffffu, rB, 1);
+                const bool first = cur == 0, rin = cur + 1 < L.w;
+                const bool top = y == 0, bottom = y == L.h - 1;
+                const float Fl = first ? pF : myF, Bl = first ? pB : myB;
+                const float Fr = rin ? rF : pF, Br = rin ? rB : pB;
+                const float Fu = top ? pF : (j == 0 ? aF : uF);
+                const float Bu = top ? pB : (j == 0 ? aB : uB);
+                const float Fd = bottom ? pF : (j == 31 ? aF : dF);
+                const float Bd = bottom ? pB : (j == 31 ? aB : dB);
+                const int e = (t << 5) | j;
+                const float4 da = *(const float4*)(cb + kOffDa + e * 16);
+                const double2 b0 = *(const double2*)(cb + kOffB0 + e * 16);
+                const double b11 = *(const double*)(cb + kOffB11 + e * 8);
+                const float2 pI = *(const float2*)(cb + kOffPI + w * kPIBytes + e * 8);
+                float f0 = pI.x, f1 = pI.y;
+                f0 = __fadd_rn(f0, __fmul_rn(da.x, Fl));
+                f1 = __fadd_rn(f1, __fmul_rn(da.x, Bl));
+                f0 = __fadd_rn(f0, __fmul_rn(da.y, Fr));
+                f1 = __fadd_rn(f1, __fmul_rn(da.y, Br));
+                f0 = __fadd_rn(f0, __fmul_rn(da.z, Fu));
+                f1 = __fadd_rn(f1, __fmul_rn(da.z, Bu));
+                f0 = __fadd_rn(f0, __fmul_rn(da.w, Fd));
+                f1 = __fadd_rn(f1, __fmul_rn(da.w, Bd));
+                double Fc = __dadd_rn(__dmul_rn(b0.x, (double)f0), __dmul_rn(b0.y, (double)f1));
+                double Bc = __dadd_rn(__dmul_rn(b0.y, (double)f0), __dmul_rn(b11, (double)f1));
+                // max(0.0, min(1.0, v)) with Python's argument order
+                Fc = Fc < 1.0 ? Fc : 1.0;
+                Fc = Fc > 0.0 ? Fc : 0.0;
+                Bc = Bc < 1.0 ? Bc : 1.0;
+                Bc = Bc > 0.0 ? Bc : 0.0;
+                const float nF = __double2float_rn(Fc), nB = __double2float_rn(Bc);
+                if (rowv && inCol) {
+                    st_fb(row_self + (long long)s * kLanes, pack(nF, e_new), pack(nB, e_new));
+                    if (last_out) {
+                        const long long o = ((long long)y * L.w + cur) * A.depth + c;
+                        A.outF[o] = nF;
+                        if (A.outB) A.outB[o] = nB;
+                    }
+                }
+                // (garbage in lanes outside the image; nothing reads it there)
+                myF = nF;
+                myB = nB;
+                pF = rF;
+                pB = rB;
             }
-            // all warps are done with this buffer: refill it with chunk q + 2
+            // every active warp is done with this buffer: refill it with chunk q + 2
             bar_sync1(nthr);
             if (tid == 0 && q + 2 < L.Q) {
                 fence_proxy_async();
-                mbar_expect_tx(bar, rb);
-                bulk_load(smem + (q & 1) * rb, rec_k + (long long)(q + 2) * rb, rb, bar);
+                stage(q & 1, q + 2);
             }
         }
+        cp_async_wait<0>();
     }
 }
 
@@ -539,7 +591,7 @@ static Layout layout(int h0, int w0, int depth) {
     Layout l;
     l.hdr = 0;
     l.part = 1024;
-    l.seed = l.part + align256((long long)kMeanBlocks * (2 * kMaxDepth + 2) * 8);
+    l.seed = l.part + align256((long long)kMeanBlocks * kMeanValues * 8);
     l.fb0 = l.seed + 256;
     l.fb1 = l.fb0 + align256(fb);
     l.rec = l.fb1 + align256(fb);
@@ -573,8 +625,8 @@ int pmb_launch_fg_levels(int h, int w, int n_small, int n_big, int small_size, i
 int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int depth, float reg,
                   int n_small, int n_big, int small_size, float gw, const float* seed_in,
                   float* outF, float* outB, void* workspace, int64_t ws_bytes, cudaStream_t st) {
-    if (!image || !alpha || !outF || !workspace || h0 <= 0 || w0 <= 0 || depth < 1 ||
-        depth > kMaxDepth || n_small < 0 || n_big < 0)
+    if (!image || !alpha || !outF || !workspace || h0 <= 0 || w0 <= 0 || h0 > kMaxSide ||
+        w0 > kMaxSide || depth < 1 || depth > kMaxDepth || n_small < 0 || n_big < 0)
         return -2;
     Level lv[kMaxLevels];
     const int nl = plan_levels(h0, w0, n_small, n_big, small_size, lv);
@@ -593,15 +645,18 @@ int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int de
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (num_sms <= 0) num_sms = 148;
+    const int groups = (depth + kGroupMax - 1) / kGroupMax;
+    const int cpg = (depth + groups - 1) / groups;
+    const int sweep_smem = 2 * stage_bytes(cpg) + cpg * kWarpRingBytes;
     cudaError_t e = cudaFuncSetAttribute(k_fg_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         2 * rec_bytes(kMaxDepth));
+                                         2 * stage_bytes(kGroupMax) + kGroupMax * kWarpRingBytes);
     if (e != cudaSuccess) return (int)e;
     e = cudaMemsetAsync(hdr, 0, 1024, st);
     if (e != cudaSuccess) return (int)e;
     if (!seed_in) {
         const long long n = (long long)h0 * w0;
         k_fg_mean_partial<<<kMeanBlocks, kMeanThreads, 0, st>>>(image, alpha, n, depth, part);
-        k_fg_mean_final<<<1, kMeanThreads, 0, st>>>(part, kMeanBlocks, depth, seed);
+        k_fg_mean_final<<<1, 32 * kMeanValues, 0, st>>>(part, kMeanBlocks, depth, seed);
         seed_in = seed;
     }
     Level none{};
@@ -621,23 +676,24 @@ int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int de
         P.seed = seed_in;
         P.rec = rec;
         P.fb = fbs[i & 1];
-        const long long entries = (long long)L.S * L.Sp * kLanes;
-        const int blocks = (int)std::min<long long>((entries + 255) / 256, (long long)num_sms * 16);
-        k_fg_prep<<<blocks, 256, 0, st>>>(P);
+        const dim3 pgrid((L.Sp * kLanes + 255) / 256, L.S);
+        k_fg_prep<<<pgrid, 256, 0, st>>>(P);
         const bool last = i == nl - 1;
         if (L.n_iter > 0) {
             SweepArgs S;
             S.L = L;
             S.depth = depth;
+            S.groups = groups;
+            S.cpg = cpg;
             S.rec = rec;
             S.fb = fbs[i & 1];
             S.outF = last ? outF : nullptr;
             S.outB = last ? outB : nullptr;
             S.ticket = hdr + 1 + i;
             S.err = hdr;
-            const int units = L.n_iter * L.S;
+            const int units = L.n_iter * L.S * groups;
             const int grid = std::min(units, num_sms);
-            k_fg_sweep<<<grid, kLanes * depth, 2 * rec_bytes(depth), st>>>(S);
+            k_fg_sweep<<<grid, kLanes * cpg, sweep_smem, st>>>(S);
         } else if (last) {
             const long long n = (long long)L.h * L.w;
             const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)num_sms * 16);
