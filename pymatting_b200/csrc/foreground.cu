@@ -77,9 +77,10 @@ constexpr int kBaseBytes = kOffPI;  // da and the 2x2 inverse, shared by all cha
 __host__ __device__ constexpr int rec_bytes(int depth) { return kOffPI + depth * kPIBytes; }
 // Shared memory of one staged chunk for a CTA of `cpg` channels.
 __host__ __device__ constexpr int stage_bytes(int cpg) { return kBaseBytes + cpg * kPIBytes; }
-// Ring row per channel: 32 right-hand values + 32 neighbour-strip values (of
-// which lanes 0 and 31 use theirs).
+// Per-warp ring: kRingSlots x (32 right-hand values + 32 neighbour-strip
+// values, of which lanes 0 and 31 use theirs).
 constexpr int kRingRow = 2 * kLanes;
+constexpr int kWarpRingBytes = kRingSlots * kRingRow * 16;
 
 struct Level {
     int h, w;    // level size
@@ -339,16 +340,14 @@ __global__ void __launch_bounds__(256) k_fg_prep(PrepArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// Sweep: all iterations of one level. A CTA is one warp; it works on one
-// unit (iteration it, strip k, channel group g) at a time and carries the
-// group's NC colour channels as independent chains, so the per-step work
-// they share (addressing, conditions, the alpha-only coefficients) is done
-// once and their dependent arithmetic interleaves.
+// Sweep: all iterations of one level. A CTA holds one warp per colour channel
+// of a channel group (at most kGroupMax channels) and works on one unit
+// (iteration it, strip k, channel group g) at a time.
 // ---------------------------------------------------------------------------
 
 struct SweepArgs {
     Level L;
-    int depth, groups;  // channels, channel groups (of at most NC channels)
+    int depth, groups, cpg;  // channels, channel groups, channels per group
     const unsigned char* rec;
     ulonglong2* fb;
     float* outF;  // last level only: the final iteration also writes (h, w, depth)
@@ -357,36 +356,37 @@ struct SweepArgs {
     int* err;
 };
 
-template <int NC>
-__global__ void __launch_bounds__(kLanes, 1) k_fg_sweep(SweepArgs A) {
+__global__ void __launch_bounds__(kLanes * kGroupMax, 1) k_fg_sweep(SweepArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_unit;
     const Level L = A.L;
-    const int j = threadIdx.x;
+    const int tid = threadIdx.x, w = tid >> 5, j = tid & 31;
     const int rb = rec_bytes(A.depth);
-    constexpr int sbytes = stage_bytes(NC);
-    ulonglong2* ring = (ulonglong2*)(smem + 2 * sbytes);  // [slot][NC][2 * 32]
-    if (j == 0) {
+    const int sbytes = stage_bytes(A.cpg);
+    ulonglong2* ring = (ulonglong2*)(smem + 2 * sbytes + w * kWarpRingBytes);
+    if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
     }
-    __syncwarp();
+    __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
     const int units = L.n_iter * L.S * A.groups;
     const long long plane = (long long)L.S * L.Sp * kLanes;
     const long long strip = (long long)L.Sp * kLanes;
 
     for (;;) {
-        int u = 0;
-        if (j == 0) {
-            u = atomicAdd(A.ticket, 1);
-            if (ld_err(A.err)) u = units;
+        if (tid == 0) {
+            const int u = atomicAdd(A.ticket, 1);
+            s_unit = ld_err(A.err) ? units : u;
         }
-        u = __shfl_sync(0xffffffffu, u, 0);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
         if (u >= units) break;
         const int g = u % A.groups, ik = u / A.groups;
         const int it = ik / L.S, k = ik - it * L.S;
-        const int c0 = g * NC, ng = min(NC, A.depth - c0);
+        const int c0 = g * A.cpg, ng = min(A.cpg, A.depth - c0);
         const unsigned char* rec_k = A.rec + (long long)k * L.Q * rb;
         const uint32_t stage_tx = kBaseBytes + ng * kPIBytes;
         auto stage = [&](int buf, int q) {
@@ -396,178 +396,146 @@ __global__ void __launch_bounds__(kLanes, 1) k_fg_sweep(SweepArgs A) {
             bulk_load(smem + buf * sbytes + kBaseBytes, r + kOffPI + c0 * kPIBytes, ng * kPIBytes,
                       &bars[buf]);
         };
-        if (j == 0) {
+        if (tid == 0) {
             fence_proxy_async();
             for (int b = 0; b < 2 && b < L.Q; ++b) stage(b, b);
         }
-
+        if (w >= ng) {
+            // no channel for this warp in this group: keep the phase parities
+            // in step with the warps that wait on every chunk
+            phase0 ^= (uint32_t)(((L.Q + 1) >> 1) & 1);
+            phase1 ^= (uint32_t)((L.Q >> 1) & 1);
+            continue;
+        }
+        const int c = c0 + w;
+        ulonglong2* fbc = A.fb + c * plane;
         const int y0 = kLanes * k, y = y0 + j;
         const bool rowv = y < L.h;
         const uint32_t e_old = it, e_new = it + 1;
         const bool has_up = j == 0 && k > 0;
         const bool has_dn = j == 31 && y0 + kLanes < L.h;
+        const bool last_out = A.outF != nullptr && it == L.n_iter - 1;
+        ulonglong2* row_self = fbc + k * strip + j;
+        const ulonglong2* row_up = fbc + (k - 1) * strip + 31;  // used only if has_up
+        const ulonglong2* row_dn = fbc + (k + 1) * strip;       // used only if has_dn
         const bool has_aux = has_up || has_dn;
         const uint32_t want_aux = has_up ? e_new : e_old;
-        const bool last_out = A.outF != nullptr && it == L.n_iter - 1;
-        // channel c of this group: row_self + c * plane
-        ulonglong2* row_self = A.fb + c0 * plane + k * strip + j;
         // Step s reads [k][s+1][j] (right-hand value), [k-1][s+31][31] (lane 0)
-        // and [k+1][s-31][0] (lane 31): arithmetic sequences in s.
+        // and [k+1][s-31][0] (lane 31): three arithmetic sequences in s.
         const ulonglong2* gR = row_self + kLanes;
-        const ulonglong2* gA = has_up ? row_self - j - strip + 31 * kLanes + 31
-                                      : (has_dn ? row_self - j + strip - 31 * kLanes : row_self);
+        const ulonglong2* gA = has_up ? row_up + 31 * kLanes : (has_dn ? row_dn - 31 * kLanes : row_self);
         const uint32_t ring_lane = smem_addr(ring) + j * 16;
 
         // Copy the rows step s needs into ring slot s % kRingSlots (zero-filled
         // where the lane has nothing to read). One commit group per step.
         auto issue = [&](int s) {
-            const uint32_t slot = ring_lane + (uint32_t)((s & (kRingSlots - 1)) * NC * kRingRow * 16);
+            const uint32_t slot = ring_lane + (uint32_t)((s & (kRingSlots - 1)) * kRingRow * 16);
             const bool cR = rowv && (unsigned)(s + 1 - j) < (unsigned)L.w;
             const bool cA = has_aux && (unsigned)(s - j) < (unsigned)L.w;
-            const ulonglong2* pR = cR ? gR + (long long)s * kLanes : row_self;
-            const ulonglong2* pA = cA ? gA + (long long)s * kLanes : row_self;
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                if (c < ng) {
-                    cp_async16(slot + c * kRingRow * 16, pR + c * plane, cR ? 16u : 0u);
-                    cp_async16(slot + (c * kRingRow + kLanes) * 16, pA + c * plane, cA ? 16u : 0u);
-                }
-            }
+            cp_async16(slot, cR ? gR + (long long)s * kLanes : row_self, cR ? 16u : 0u);
+            cp_async16(slot + kLanes * 16, cA ? gA + (long long)s * kLanes : row_self, cA ? 16u : 0u);
             cp_async_commit();
         };
         for (int r = 0; r < kDist; ++r) issue(r);
 
-        float myF[NC], myB[NC], pF[NC], pB[NC];  // previous step's value, old value of the column
-#pragma unroll
-        for (int c = 0; c < NC; ++c) myF[c] = myB[c] = pF[c] = pB[c] = 0.f;
+        float myF = 0.f, myB = 0.f;  // this lane's value from the previous step
+        float pF = 0.f, pB = 0.f;    // old value of this lane's current column
         // Lane j first meets its column 0 as the right-hand value of step j-1;
         // for lane 0 that step would be -1, so its column 0 is read here.
         if (j == 0 && rowv) {
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                if (c < ng) {
-                    ulonglong2 v = ld_fb(row_self + c * plane);
-                    if (!has_epoch(v, e_old)) v = poll_epoch(row_self + c * plane, e_old, A.err);
-                    pF[c] = value_of(v.x);
-                    pB[c] = value_of(v.y);
-                }
-            }
+            ulonglong2 v = ld_fb(row_self);
+            if (!has_epoch(v, e_old)) v = poll_epoch(row_self, e_old, A.err);
+            pF = value_of(v.x);
+            pB = value_of(v.y);
         }
-        long long o = ((long long)y * L.w - j) * A.depth + c0;  // output index of (y, s - j) at s = 0
+        const int nthr = kLanes * ng;
         for (int q = 0; q < L.Q; ++q) {
             uint64_t* bar = &bars[q & 1];
             const uint32_t ph = (q & 1) ? phase1 : phase0;
             if (!mbar_wait(bar, ph)) atomicCAS(A.err, 0, kErrStage);
             if (q & 1) phase1 ^= 1u; else phase0 ^= 1u;
             const unsigned char* cb = smem + (q & 1) * sbytes;
-#pragma unroll 2
-            for (int t = 0; t < kChunk; ++t) {
+            // the last step with work is w + 30 (lane 31 at column w - 1)
+            const int t_end = min(kChunk, L.w + kLanes - 1 - kChunk * q);
+#pragma unroll 4
+            for (int t = 0; t < t_end; ++t) {
                 const int s = kChunk * q + t;
                 const int cur = s - j;
                 cp_async_wait<kDist - 1>();
-                const ulonglong2* slot = ring + (s & (kRingSlots - 1)) * NC * kRingRow;
-                ulonglong2 Rv[NC], Av[NC];
-#pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    Rv[c] = slot[c * kRingRow + j];
-                    Av[c] = slot[c * kRingRow + kLanes + j];
-                }
+                const ulonglong2* slot = ring + (s & (kRingSlots - 1)) * kRingRow;
+                ulonglong2 Rv = slot[j];
+                ulonglong2 Av = slot[kLanes + j];
                 // the slot refilled now was read at step s - 1
                 issue(s + kDist);
                 const bool inCol = (unsigned)cur < (unsigned)L.w;
                 const bool needR = rowv && (unsigned)(cur + 1) < (unsigned)L.w;
                 const bool needA = has_aux && inCol;
-                bool ok = true;
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    if (c < ng)
-                        ok = ok && (!needR || has_epoch(Rv[c], e_old)) &&
-                             (!needA || has_epoch(Av[c], want_aux));
-                if (!__all_sync(0xffffffffu, ok)) {
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        if (c >= ng) continue;
-                        if (needR && !has_epoch(Rv[c], e_old))
-                            Rv[c] = poll_epoch(gR + (long long)s * kLanes + c * plane, e_old, A.err);
-                        if (needA && !has_epoch(Av[c], want_aux))
-                            Av[c] = poll_epoch(gA + (long long)s * kLanes + c * plane, want_aux, A.err);
-                    }
+                const bool okR = !needR || has_epoch(Rv, e_old);
+                const bool okA = !needA || has_epoch(Av, want_aux);
+                if (!__all_sync(0xffffffffu, okR && okA)) {
+                    if (!okR) Rv = poll_epoch(gR + (long long)s * kLanes, e_old, A.err);
+                    if (!okA) Av = poll_epoch(gA + (long long)s * kLanes, want_aux, A.err);
                 }
+                const float rF = value_of(Rv.x), rB = value_of(Rv.y);
+                const float aF = value_of(Av.x), aB = value_of(Av.y);
+                const float uF = __shfl_up_sync(0xffffffffu, myF, 1);
+                const float uB = __shfl_up_sync(0xffffffffu, myB, 1);
+                const float dF = __shfl_down_sync(0xffffffffu, rF, 1);
+                const float dB = __shfl_down_sync(0xffffffffu, rB, 1);
                 const bool first = cur == 0, rin = cur + 1 < L.w;
                 const bool top = y == 0, bottom = y == L.h - 1;
-                const bool act = rowv && inCol;
+                const float Fl = first ? pF : myF, Bl = first ? pB : myB;
+                const float Fr = rin ? rF : pF, Br = rin ? rB : pB;
+                const float Fu = top ? pF : (j == 0 ? aF : uF);
+                const float Bu = top ? pB : (j == 0 ? aB : uB);
+                const float Fd = bottom ? pF : (j == 31 ? aF : dF);
+                const float Bd = bottom ? pB : (j == 31 ? aB : dB);
                 const int e = (t << 5) | j;
                 const float4 da = *(const float4*)(cb + kOffDa + e * 16);
                 const double2 b0 = *(const double2*)(cb + kOffB0 + e * 16);
                 const double b11 = *(const double*)(cb + kOffB11 + e * 8);
-#pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    const float rF = value_of(Rv[c].x), rB = value_of(Rv[c].y);
-                    const float aF = value_of(Av[c].x), aB = value_of(Av[c].y);
-                    const float uF = __shfl_up_sync(0xffffffffu, myF[c], 1);
-                    const float uB = __shfl_up_sync(0xffffffffu, myB[c], 1);
-                    const float dF = __shfl_down_sync(0xffffffffu, rF, 1);
-                    const float dB = __shfl_down_sync(0xffffffffu, rB, 1);
-                    const float Fl = first ? pF[c] : myF[c], Bl = first ? pB[c] : myB[c];
-                    const float Fr = rin ? rF : pF[c], Br = rin ? rB : pB[c];
-                    const float Fu = top ? pF[c] : (j == 0 ? aF : uF);
-                    const float Bu = top ? pB[c] : (j == 0 ? aB : uB);
-                    const float Fd = bottom ? pF[c] : (j == 31 ? aF : dF);
-                    const float Bd = bottom ? pB[c] : (j == 31 ? aB : dB);
-                    const float2 pI = *(const float2*)(cb + kOffPI + c * kPIBytes + e * 8);
-                    float f0 = pI.x, f1 = pI.y;
-                    f0 = __fadd_rn(f0, __fmul_rn(da.x, Fl));
-                    f1 = __fadd_rn(f1, __fmul_rn(da.x, Bl));
-                    f0 = __fadd_rn(f0, __fmul_rn(da.y, Fr));
-                    f1 = __fadd_rn(f1, __fmul_rn(da.y, Br));
-                    f0 = __fadd_rn(f0, __fmul_rn(da.z, Fu));
-                    f1 = __fadd_rn(f1, __fmul_rn(da.z, Bu));
-                    f0 = __fadd_rn(f0, __fmul_rn(da.w, Fd));
-                    f1 = __fadd_rn(f1, __fmul_rn(da.w, Bd));
-                    double Fc = __dadd_rn(__dmul_rn(b0.x, (double)f0), __dmul_rn(b0.y, (double)f1));
-                    double Bc = __dadd_rn(__dmul_rn(b0.y, (double)f0), __dmul_rn(b11, (double)f1));
-                    // max(0.0, min(1.0, v)) with Python's argument order
-                    Fc = Fc < 1.0 ? Fc : 1.0;
-                    Fc = Fc > 0.0 ? Fc : 0.0;
-                    Bc = Bc < 1.0 ? Bc : 1.0;
-                    Bc = Bc > 0.0 ? Bc : 0.0;
-                    const float nF = __double2float_rn(Fc), nB = __double2float_rn(Bc);
-                    if (act && c < ng) {
-                        st_fb(row_self + c * plane + (long long)s * kLanes, pack(nF, e_new),
-                              pack(nB, e_new));
-                        if (last_out) {
-                            A.outF[o + s * A.depth + c] = nF;
-                            if (A.outB) A.outB[o + s * A.depth + c] = nB;
-                        }
+                const float2 pI = *(const float2*)(cb + kOffPI + w * kPIBytes + e * 8);
+                float f0 = pI.x, f1 = pI.y;
+                f0 = __fadd_rn(f0, __fmul_rn(da.x, Fl));
+                f1 = __fadd_rn(f1, __fmul_rn(da.x, Bl));
+                f0 = __fadd_rn(f0, __fmul_rn(da.y, Fr));
+                f1 = __fadd_rn(f1, __fmul_rn(da.y, Br));
+                f0 = __fadd_rn(f0, __fmul_rn(da.z, Fu));
+                f1 = __fadd_rn(f1, __fmul_rn(da.z, Bu));
+                f0 = __fadd_rn(f0, __fmul_rn(da.w, Fd));
+                f1 = __fadd_rn(f1, __fmul_rn(da.w, Bd));
+                double Fc = __dadd_rn(__dmul_rn(b0.x, (double)f0), __dmul_rn(b0.y, (double)f1));
+                double Bc = __dadd_rn(__dmul_rn(b0.y, (double)f0), __dmul_rn(b11, (double)f1));
+                // max(0.0, min(1.0, v)) with Python's argument order
+                Fc = Fc < 1.0 ? Fc : 1.0;
+                Fc = Fc > 0.0 ? Fc : 0.0;
+                Bc = Bc < 1.0 ? Bc : 1.0;
+                Bc = Bc > 0.0 ? Bc : 0.0;
+                const float nF = __double2float_rn(Fc), nB = __double2float_rn(Bc);
+                if (rowv && inCol) {
+                    st_fb(row_self + (long long)s * kLanes, pack(nF, e_new), pack(nB, e_new));
+                    if (last_out) {
+                        const long long o = ((long long)y * L.w + cur) * A.depth + c;
+                        A.outF[o] = nF;
+                        if (A.outB) A.outB[o] = nB;
                     }
-                    // (garbage in lanes outside the image; nothing reads it there)
-                    myF[c] = nF;
-                    myB[c] = nB;
-                    pF[c] = rF;
-                    pB[c] = rB;
                 }
+                // (garbage in lanes outside the image; nothing reads it there)
+                myF = nF;
+                myB = nB;
+                pF = rF;
+                pB = rB;
             }
-            __syncwarp();
-            if (j == 0 && q + 2 < L.Q) {
+            // every active warp is done with this buffer: refill it with chunk q + 2
+            bar_sync1(nthr);
+            if (tid == 0 && q + 2 < L.Q) {
                 fence_proxy_async();
                 stage(q & 1, q + 2);
             }
         }
         cp_async_wait<0>();
-        __syncwarp();
     }
 }
-
-using SweepKernel = void (*)(SweepArgs);
-static SweepKernel sweep_kernel(int nc) {
-    switch (nc) {
-        case 1: return k_fg_sweep<1>;
-        case 2: return k_fg_sweep<2>;
-        case 3: return k_fg_sweep<3>;
-        default: return k_fg_sweep<4>;
-    }
-}
-static int sweep_smem(int nc) { return 2 * stage_bytes(nc) + kRingSlots * nc * kRingRow * 16; }
 
 // Final values when the last level runs no sweep (n_iter == 0): gather the
 // level's starting values out of the diagonal layout.
@@ -681,9 +649,9 @@ int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int de
     if (num_sms <= 0) num_sms = 148;
     const int groups = (depth + kGroupMax - 1) / kGroupMax;
     const int cpg = (depth + groups - 1) / groups;
-    const SweepKernel sweep = sweep_kernel(cpg);
-    cudaError_t e = cudaFuncSetAttribute(sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         sweep_smem(cpg));
+    const int sweep_smem = 2 * stage_bytes(cpg) + cpg * kWarpRingBytes;
+    cudaError_t e = cudaFuncSetAttribute(k_fg_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         2 * stage_bytes(kGroupMax) + kGroupMax * kWarpRingBytes);
     if (e != cudaSuccess) return (int)e;
     e = cudaMemsetAsync(hdr, 0, 1024, st);
     if (e != cudaSuccess) return (int)e;
@@ -718,6 +686,7 @@ int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int de
             S.L = L;
             S.depth = depth;
             S.groups = groups;
+            S.cpg = cpg;
             S.rec = rec;
             S.fb = fbs[i & 1];
             S.outF = last ? outF : nullptr;
@@ -726,7 +695,7 @@ int pmb_launch_fg(const float* image, const float* alpha, int h0, int w0, int de
             S.err = hdr;
             const int units = L.n_iter * L.S * groups;
             const int grid = std::min(units, num_sms);
-            sweep<<<grid, kLanes, sweep_smem(cpg), st>>>(S);
+            k_fg_sweep<<<grid, kLanes * cpg, sweep_smem, st>>>(S);
         } else if (last) {
             const long long n = (long long)L.h * L.w;
             const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)num_sms * 16);
