@@ -51,8 +51,10 @@ def parse():
                     default="1080p",
                     help="foreground: estimate_foreground_ml on a 1920x1080 image + matte")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tune", choices=["auto", "none"], default="auto",
-                    help="run the launch-shape autotuner before timing (none: defaults)")
+    ap.add_argument("--tune", choices=["auto", "none"], default="none",
+                    help="auto: run the launch-shape autotuner before timing; none (default): "
+                         "the built-in launch shapes, which matched or beat the tuner's "
+                         "picks at 1080p with L2 flushed between steps")
     ap.add_argument("--profile", choices=["apply", "solve", "solve-fp64", "solve-mixed"],
                     default=None,
                     help="profiling case: a few operator applies, or one solve per precision "
