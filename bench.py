@@ -334,6 +334,29 @@ def run_foreground(args, rank, world, local):
     _ffi.check(lib.pmb_fg_status(ws.data_ptr(), st), "pmb_fg_ml")
     barrier()
     ms = max_over_ranks(sum(times) / len(times))
+    # the reference's GPU backend (estimate_foreground_ml_cupy, Jacobi), same timing rules
+    nbj = int(lib.pmb_fg_jacobi_workspace_bytes(h, w))
+    wsj = torch.empty(nbj, dtype=torch.uint8, device=dev)
+
+    def step_jacobi():
+        rc = lib.pmb_fg_ml_jacobi(ti.data_ptr(), ta.data_ptr(), h, w, 1e-5, 10, 2, 32,
+                                  F.data_ptr(), B.data_ptr(), wsj.data_ptr(), nbj, st)
+        assert rc == 0, _ffi.last_error()
+
+    for _ in range(args.warmup):
+        step_jacobi()
+    tj = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step_jacobi()
+        e1.record()
+        torch.cuda.synchronize()
+        tj.append(e0.elapsed_time(e1))
+    ms_j = max_over_ranks(sum(tj) / len(tj))
     # end to end through the public API with host numpy buffers
     e2e_times = []
     for s in range(args.warmup + max(3, args.steps // 4)):
@@ -368,6 +391,9 @@ def run_foreground(args, rank, world, local):
                     "h2d_bytes_per_step": int(npx * (depth + 1) * 4),
                     "d2h_bytes_per_step": int(npx * 2 * depth * 4)},
             "gpu_launches": int((2 + 2 * len(levels)) * args.steps),
+            "cupy_variant": {"value": world * npx / (ms_j * 1e-3) / 1e6, "unit": "Mpix/s",
+                             "ms_per_step": ms_j,
+                             "path": "estimate_foreground_ml_cupy drop-in (Jacobi, float32)"},
             "clocks": clock_rec,
         }
         if world == 1 and not args.no_cpu_baseline:

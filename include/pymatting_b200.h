@@ -116,6 +116,20 @@ int pmb_fg_status(void* workspace, void* stream);
 int pmb_fg_levels(int h, int w, int n_small_iterations, int n_big_iterations, int small_size,
                   int* hw, int max_levels);
 
+/* Replace estimate_foreground_ml_cupy(input_image, input_alpha,
+ * regularization, n_small_iterations, n_big_iterations, small_size)
+ * (pymatting/foreground/estimate_foreground_ml_cupy.py:110-230, kernels
+ * :5-107): the reference's GPU backend, Jacobi iterations in float32 with
+ * its buffer handling (seeded with pixel (0, 0), result = the buffer named F
+ * after the swaps). image (h, w, 3), alpha (h, w), F and B (h, w, 3)
+ * float32 on the device (B may be null). Fused multiply-adds are allowed as
+ * in the reference's NVRTC build, so results agree to float32 rounding.
+ * Returns -4 for a 1x1 image (the reference divides by zero). */
+int64_t pmb_fg_jacobi_workspace_bytes(int h, int w);
+int pmb_fg_ml_jacobi(const float* image, const float* alpha, int h, int w, float regularization,
+                     int n_small_iterations, int n_big_iterations, int small_size, float* F,
+                     float* B, void* workspace, int64_t workspace_bytes, void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

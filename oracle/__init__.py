@@ -17,6 +17,7 @@ Pieces and the reference code each restates (paths inside PyMatting 1.1.15):
 * ``estimate_alpha_cf``  pymatting/alpha/estimate_alpha_cf.py:8-78
 * ``lkm_laplacian``      pymatting/laplacian/lkm_laplacian.py:6-76
 * ``estimate_foreground_ml`` pymatting/foreground/estimate_foreground_ml.py:5-253 (C)
+* ``estimate_foreground_ml_cupy`` pymatting/foreground/estimate_foreground_ml_cupy.py:5-230
 
 Parity of this restatement with the reference itself is pinned by
 ``tests/test_oracle.py`` against the fixtures in ``tests/golden/`` that
@@ -525,6 +526,98 @@ def estimate_foreground_ml(image, alpha, regularization=1e-5, n_small_iterations
         raise ZeroDivisionError("division by zero")
     if rc != 0:
         raise ValueError("oracle_fg_ml failed (%d)" % rc)
+    if return_background:
+        return F, B
+    return F
+
+
+def estimate_foreground_ml_cupy(input_image, input_alpha, regularization=1e-5,
+                                n_small_iterations=10, n_big_iterations=2, small_size=32,
+                                return_background=False):
+    """pymatting/foreground/estimate_foreground_ml_cupy.py:110-230 and its
+    kernels :5-107 (Jacobi iterations), in float32 numpy.
+
+    Restates the reference's flat buffers exactly. F and B start as the
+    colour of pixel (0, 0). Each level resizes the buffer named ``F`` (read
+    with the previous level's shape) into ``F_prev`` and iterates with
+    swaps. The result is ``F``, which is the second newest iterate when the
+    last level runs iterations. The reference compiles its kernel with
+    NVRTC (fused multiply-adds allowed), so results agree to float32
+    rounding, not bitwise."""
+    image = np.ascontiguousarray(input_image, dtype=np.float32)
+    alpha0 = np.ascontiguousarray(input_alpha, dtype=np.float32)
+    h0, w0, depth = image.shape
+    assert depth == 3
+    f32 = np.float32
+    reg = f32(regularization)
+    n = h0 * w0 * depth
+
+    def resize(dst, src, ws, hs, wd, hd, d):
+        ys = np.minimum(np.arange(hd) * hs // hd, hs - 1)
+        xs = np.minimum(np.arange(wd) * ws // wd, ws - 1)
+        s3 = src[:hs * ws * d].reshape(hs, ws, d)
+        dst[:hd * wd * d] = s3[ys][:, xs].reshape(-1)
+
+    F_prev = np.zeros(n, np.float32)
+    B_prev = np.zeros(n, np.float32)
+    F = np.zeros(n, np.float32)
+    B = np.zeros(n, np.float32)
+    image_level = np.zeros(n, np.float32)
+    alpha_level = np.zeros(h0 * w0, np.float32)
+    flat_image = image.reshape(-1)
+    flat_alpha = alpha0.reshape(-1)
+    n_levels = (max(w0, h0) - 1).bit_length()
+    w_prev = h_prev = 1
+    resize(F, flat_image, w0, h0, w_prev, h_prev, depth)
+    resize(B, flat_image, w0, h0, w_prev, h_prev, depth)
+    for i_level in range(n_levels + 1):
+        w = round(w0 ** (i_level / n_levels))
+        h = round(h0 ** (i_level / n_levels))
+        resize(image_level, flat_image, w0, h0, w, h, depth)
+        resize(alpha_level, flat_alpha, w0, h0, w, h, 1)
+        resize(F_prev, F, w_prev, h_prev, w, h, depth)
+        resize(B_prev, B, w_prev, h_prev, w, h, depth)
+        n_iter = n_big_iterations
+        if min(w, h) <= small_size:
+            n_iter = n_small_iterations
+        m = h * w
+        img = image_level[:m * 3].reshape(h, w, 3)
+        a0 = alpha_level[:m].reshape(h, w)
+        a1 = f32(1.0) - a0
+        xm = np.maximum(np.arange(w) - 1, 0)
+        xp = np.minimum(np.arange(w) + 1, w - 1)
+        ym = np.maximum(np.arange(h) - 1, 0)
+        yp = np.minimum(np.arange(h) + 1, h - 1)
+        for _ in range(n_iter):
+            Fp = F_prev[:m * 3].reshape(h, w, 3)
+            Bp = B_prev[:m * 3].reshape(h, w, 3)
+            b0 = a0[:, :, None] * img
+            b1 = a1[:, :, None] * img
+            a_sum = np.zeros_like(a0)
+            for an, Fn, Bn in ((a0[:, xm], Fp[:, xm], Bp[:, xm]),
+                               (a0[:, xp], Fp[:, xp], Bp[:, xp]),
+                               (a0[ym, :], Fp[ym, :], Bp[ym, :]),
+                               (a0[yp, :], Fp[yp, :], Bp[yp, :])):
+                da = reg + np.abs(a0 - an)
+                a_sum = a_sum + da
+                b0 = b0 + da[:, :, None] * Fn
+                b1 = b1 + da[:, :, None] * Bn
+            a00 = a0 * a0 + a_sum
+            a11 = a1 * a1 + a_sum
+            a01 = a0 * a1
+            inv_det = (f32(1.0) / (a00 * a11 - a01 * a01))[:, :, None]
+            # fmaxf(0, fminf(1, v)): NaN-ignoring, like the CUDA functions
+            Fo = np.fmax(f32(0.0), np.fmin(f32(1.0), inv_det * (a11[:, :, None] * b0 -
+                                                               a01[:, :, None] * b1)))
+            Bo = np.fmax(f32(0.0), np.fmin(f32(1.0), inv_det * (a00[:, :, None] * b1 -
+                                                               a01[:, :, None] * b0)))
+            F[:m * 3] = Fo.reshape(-1)
+            B[:m * 3] = Bo.reshape(-1)
+            F_prev, F = F, F_prev
+            B_prev, B = B, B_prev
+        w_prev, h_prev = w, h
+    F = F.reshape(h0, w0, depth).copy()
+    B = B.reshape(h0, w0, depth).copy()
     if return_background:
         return F, B
     return F

@@ -17,7 +17,7 @@ from .solver import cg, CounterCallback, ProgressCallback
 from .alpha import estimate_alpha_cf, estimate_alpha
 from .autograd import cf_alpha
 from .lkm import lkm_laplacian, estimate_alpha_lkm
-from .foreground import estimate_foreground_ml
+from .foreground import estimate_foreground_ml, estimate_foreground_ml_cupy
 
 __version__ = "0.1.0"
 
@@ -26,4 +26,5 @@ __all__ = [
     "DeviceCSRMatrix", "jacobi", "vcycle", "ichol", "CholeskyDecomposition", "cg",
     "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
     "lkm_laplacian", "estimate_alpha_lkm", "estimate_foreground_ml",
+    "estimate_foreground_ml_cupy",
 ]

@@ -36,6 +36,9 @@ _SIGNATURES = {
                           c_vp, c_vp, c_vp, c_vp, c_i64, c_vp]),
     "pmb_fg_status": (c_int, [c_vp, c_vp]),
     "pmb_fg_levels": (c_int, [c_int, c_int, c_int, c_int, c_int, c_vp, c_int]),
+    "pmb_fg_jacobi_workspace_bytes": (c_i64, [c_int, c_int]),
+    "pmb_fg_ml_jacobi": (c_int, [c_vp, c_vp, c_int, c_int, c_flt, c_int, c_int, c_int, c_vp, c_vp,
+                                 c_vp, c_i64, c_vp]),
     "pmb_cf_hard_system": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
     "pmb_scan_scratch_elems": (c_i64, [c_i64]),
     "pmb_ell_csr_rowptr": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp]),

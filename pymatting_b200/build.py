@@ -25,6 +25,7 @@ SOURCES = {
     "csr.cu": [],
     "lkm.cu": [],
     "foreground.cu": [],
+    "foreground_jacobi.cu": [],
     "ichol.cu": ["-fmad=false"],
     "engine.cu": [],
 }

@@ -1097,6 +1097,26 @@ PMB_API int pmb_fg_status(void* workspace, void* stream) {
     return 0;
 }
 
+int64_t pmb_launch_fgj_workspace(int, int);
+int pmb_launch_fgj(const float*, const float*, int, int, float, int, int, int, float*, float*,
+                   void*, int64_t, cudaStream_t);
+
+PMB_API int64_t pmb_fg_jacobi_workspace_bytes(int h, int w) { return pmb_launch_fgj_workspace(h, w); }
+
+PMB_API int pmb_fg_ml_jacobi(const float* image, const float* alpha, int h, int w,
+                             float regularization, int n_small_iterations, int n_big_iterations,
+                             int small_size, float* F, float* B, void* workspace,
+                             int64_t workspace_bytes, void* stream) {
+    const int rc = pmb_launch_fgj(image, alpha, h, w, regularization, n_small_iterations,
+                                  n_big_iterations, small_size, F, B, workspace, workspace_bytes,
+                                  (cudaStream_t)stream);
+    if (rc == 0) return 0;
+    if (rc == -1) return fail(kErrZeroDiv, "division by zero");
+    if (rc == -2) return fail(kErrArg, "pmb_fg_ml_jacobi: bad arguments");
+    if (rc == -3) return fail(kErrArg, "pmb_fg_ml_jacobi: workspace smaller than pmb_fg_jacobi_workspace_bytes");
+    return fail(kErrCuda, std::string("pmb_fg_ml_jacobi launch: ") + cudaGetErrorString((cudaError_t)rc));
+}
+
 PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, const uint8_t* is_fg,
                                int h, int w, double epsilon, double* planes, double* rhs,
                                void* stream) {

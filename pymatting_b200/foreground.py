@@ -25,7 +25,7 @@ import torch
 from . import _device as dev
 from . import _ffi
 
-__all__ = ["estimate_foreground_ml", "foreground_levels"]
+__all__ = ["estimate_foreground_ml", "estimate_foreground_ml_cupy", "foreground_levels"]
 
 
 def foreground_levels(h, w, n_small_iterations=10, n_big_iterations=2, small_size=32):
@@ -82,6 +82,45 @@ def estimate_foreground_ml(image, alpha, regularization=1e-5, n_small_iterations
     _ffi.check(rc, "pmb_fg_ml")
     _ffi.check(lib.pmb_fg_status(dev.ptr(ws), dev.stream()), "pmb_fg_ml")
     if not on_device:
+        F = dev.to_host(F)
+        B = dev.to_host(B) if B is not None else None
+    if return_background:
+        return F, B
+    return F
+
+
+def estimate_foreground_ml_cupy(input_image, input_alpha, regularization=1e-5,
+                                n_small_iterations=10, n_big_iterations=2, small_size=32,
+                                block_size=(32, 32), return_background=False, to_numpy=True):
+    """Drop-in for the reference's GPU backend ``estimate_foreground_ml_cupy``
+    (pymatting/foreground/estimate_foreground_ml_cupy.py:110-230): Jacobi
+    iterations in float32, seeded with the colour of pixel (0, 0), with the
+    reference's buffer handling. Much faster than ``estimate_foreground_ml``
+    (every pixel of an iteration is independent) and a different algorithm.
+    Its results agree with the reference to float32 rounding, not bitwise:
+    the reference's kernel is compiled with fused multiply-adds allowed.
+
+    ``block_size`` is accepted for compatibility and ignored (launch shapes
+    are chosen here). ``to_numpy=False`` returns CUDA tensors.
+    """
+    img = _to_f32(input_image)
+    al = _to_f32(input_alpha)
+    h0, w0, depth = (int(v) for v in img.shape)
+    assert depth == 3
+    if tuple(al.shape) != (h0, w0):
+        raise ValueError("alpha must be (h, w) like the image")
+    lib = _ffi.lib()
+    nbytes = int(lib.pmb_fg_jacobi_workspace_bytes(h0, w0))
+    ws = dev.workspace(nbytes)
+    F = dev.empty((h0, w0, depth), torch.float32)
+    B = dev.empty((h0, w0, depth), torch.float32) if return_background else None
+    rc = lib.pmb_fg_ml_jacobi(dev.ptr(img), dev.ptr(al), h0, w0, float(regularization),
+                              int(n_small_iterations), int(n_big_iterations), int(small_size),
+                              dev.ptr(F), dev.ptr(B), dev.ptr(ws), nbytes, dev.stream())
+    if rc == -4:
+        raise ZeroDivisionError("division by zero")
+    _ffi.check(rc, "pmb_fg_ml_jacobi")
+    if to_numpy:
         F = dev.to_host(F)
         B = dev.to_host(B) if B is not None else None
     if return_background:

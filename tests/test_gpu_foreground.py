@@ -123,3 +123,66 @@ def test_errors(gpu):
         pm.estimate_foreground_ml(np.zeros((1, 1, 3)), np.zeros((1, 1)))
     with pytest.raises(ValueError):
         pm.estimate_foreground_ml(np.zeros((4, 4, 3)), np.zeros((4, 5)))
+
+
+# --- the reference's GPU backend (estimate_foreground_ml_cupy, Jacobi) ---
+# Its kernel is built by NVRTC with fused multiply-adds allowed, as is ours;
+# the oracle restates it in numpy without them. Tolerance: JACOBI_TOL.
+
+JACOBI_TOL = 1e-4
+
+
+@pytest.mark.parametrize("h,w", [(1, 2), (2, 1), (7, 9), (33, 31), (97, 130), (257, 300)])
+def test_jacobi_matches_oracle(gpu, h, w):
+    import pymatting_b200 as pm
+    rng = np.random.default_rng(h * 7 + w)
+    img, alpha = _case(rng, h, w)
+    F, B = pm.estimate_foreground_ml_cupy(img, alpha, return_background=True)
+    Fr, Br = oracle.estimate_foreground_ml_cupy(img, alpha, return_background=True)
+    assert F.dtype == np.float32 and F.shape == (h, w, 3)
+    assert np.abs(F - Fr).max() <= JACOBI_TOL and np.abs(B - Br).max() <= JACOBI_TOL
+    assert np.abs(F - Fr).mean() <= 1e-6
+
+
+@pytest.mark.parametrize("kw", [dict(n_big_iterations=0), dict(n_small_iterations=0),
+                                dict(n_big_iterations=1), dict(n_big_iterations=3, small_size=8),
+                                dict(regularization=0.05), dict(small_size=1000)])
+def test_jacobi_parameters(gpu, kw):
+    import pymatting_b200 as pm
+    rng = np.random.default_rng(11)
+    img, alpha = _case(rng, 120, 95)
+    F, B = pm.estimate_foreground_ml_cupy(img, alpha, return_background=True, **kw)
+    Fr, Br = oracle.estimate_foreground_ml_cupy(img, alpha, return_background=True, **kw)
+    assert np.abs(F - Fr).max() <= JACOBI_TOL and np.abs(B - Br).max() <= JACOBI_TOL
+
+
+def test_jacobi_reference_lemur_test_and_full_hd(gpu):
+    """tests/test_foreground.py of the reference runs the cupy backend
+    through the same mse <= 0.022 check; and a 1080x1920 case."""
+    import pymatting_b200 as pm
+    from pymatting_b200.synthetic import make_matting_problem
+    g = golden("foreground_small.npz")
+    alpha = g["lemur_alpha"]
+    F = pm.estimate_foreground_ml_cupy(g["lemur_image"], alpha)
+    unknown = (g["lemur_trimap"] > 0.1) & (g["lemur_trimap"] < 0.9)
+    assert np.mean((alpha[:, :, None] * np.abs(F - g["lemur_expected"]))[unknown]) <= 0.022
+    img, _, alpha, _ = make_matting_problem(1080, 1920, 2, sigma=2.0, band=7,
+                                            unknown_fraction=0.12, dtype=np.float32)
+    F = pm.estimate_foreground_ml_cupy(img, alpha)
+    Fr = oracle.estimate_foreground_ml_cupy(img, alpha)
+    assert np.abs(F - Fr).max() <= JACOBI_TOL
+
+
+def test_jacobi_device_output_and_errors(gpu):
+    import torch
+    import pymatting_b200 as pm
+    rng = np.random.default_rng(5)
+    img, alpha = _case(rng, 40, 50)
+    F = pm.estimate_foreground_ml_cupy(torch.as_tensor(img, device=gpu),
+                                       torch.as_tensor(alpha, device=gpu), to_numpy=False)
+    assert F.is_cuda and F.dtype == torch.float32
+    assert np.abs(F.cpu().numpy() - oracle.estimate_foreground_ml_cupy(img, alpha)).max() <= JACOBI_TOL
+    with pytest.raises(ZeroDivisionError):
+        pm.estimate_foreground_ml_cupy(np.zeros((1, 1, 3)), np.zeros((1, 1)))
+    with pytest.raises(AssertionError):
+        pm.estimate_foreground_ml_cupy(np.zeros((4, 4, 4)), np.zeros((4, 4)))
