@@ -18,6 +18,7 @@ from .alpha import estimate_alpha_cf, estimate_alpha
 from .autograd import cf_alpha
 from .lkm import lkm_laplacian, estimate_alpha_lkm
 from .foreground import estimate_foreground_ml, estimate_foreground_ml_cupy
+from .cutout import cutout, load_image, save_image, stack_images, blend
 
 __version__ = "0.1.0"
 
@@ -26,5 +27,5 @@ __all__ = [
     "DeviceCSRMatrix", "jacobi", "vcycle", "ichol", "CholeskyDecomposition", "cg",
     "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
     "lkm_laplacian", "estimate_alpha_lkm", "estimate_foreground_ml",
-    "estimate_foreground_ml_cupy",
+    "estimate_foreground_ml_cupy", "cutout", "load_image", "save_image", "stack_images", "blend",
 ]

@@ -317,6 +317,26 @@ def gen_foreground(pm, root, rng):
     np.savez_compressed(os.path.join(HERE, "foreground_small.npz"), **out)
 
 
+def gen_cutout(pm, root):
+    """The reference's cutout test (tests/test_simple_api.py): its input
+    files as uint8 arrays, the files it compares against, and the cutout the
+    reference itself writes for them (read back with its load_image)."""
+    import tempfile
+    from PIL import Image
+    out = {}
+    d = os.path.join(root, "data", "test")
+    for name in ["test", "test_trimap", "test_alpha", "test_foreground"]:
+        out[name + "_u8"] = np.array(Image.open(os.path.join(d, name + ".png")))
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "cutout.png")
+        pm.cutout(os.path.join(d, "test.png"), os.path.join(d, "test_trimap.png"), path)
+        out["reference_cutout"] = pm.load_image(path)
+        out["reference_cutout_u8"] = np.array(Image.open(path))
+    out["true_alpha"] = pm.load_image(os.path.join(d, "test_alpha.png"), "GRAY")
+    out["true_foreground"] = pm.load_image(os.path.join(d, "test_foreground.png"), "RGB")
+    np.savez_compressed(os.path.join(HERE, "cutout_test.npz"), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     pm = import_reference(root)
@@ -326,7 +346,8 @@ def main():
                      ("ichol", lambda: gen_ichol(pm, rng)), ("soft", lambda: gen_soft(pm)),
                      ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm)),
                      ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77))),
-                     ("foreground", lambda: gen_foreground(pm, root, np.random.default_rng(91)))]:
+                     ("foreground", lambda: gen_foreground(pm, root, np.random.default_rng(91))),
+                     ("cutout", lambda: gen_cutout(pm, root))]:
         if not only or name in only:
             fn()
     for f in sorted(os.listdir(HERE)):

@@ -5,6 +5,8 @@ import warnings
 
 import numpy as np
 import pytest
+
+from tests.conftest import golden
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
@@ -103,3 +105,44 @@ def test_shard_ranks_agree_without_communication():
         assert p.exitcode == 0
     assert sorted(k for part in gathered for k in part) == list(range(64))
     assert not set(gathered[0]) & set(gathered[1])
+
+
+def _write_png(path, arr):
+    from PIL import Image
+    Image.fromarray(arr).save(path)
+
+
+def test_image_file_helpers(tmp_path):
+    """load_image / save_image / stack_images / blend (pymatting/util/util.py)
+    on the reference test's own files (tests/golden/cutout_test.npz)."""
+    import pymatting_b200 as pm
+    g = golden("cutout_test.npz")
+    p = str(tmp_path / "test.png")
+    _write_png(p, g["test_u8"])
+    img = pm.load_image(p)
+    assert img.dtype == np.float64 and np.array_equal(img, g["test_u8"] / 255.0)
+    rgb = pm.load_image(p, "RGB")
+    assert rgb.shape == (32, 32, 3) and np.array_equal(rgb, g["test_u8"][:, :, :3] / 255.0)
+    pa = str(tmp_path / "alpha.png")
+    _write_png(pa, g["test_alpha_u8"])
+    assert np.array_equal(pm.load_image(pa, "GRAY"), g["true_alpha"])
+    half = pm.load_image(p, "RGB", 0.5, "box")
+    assert half.shape == (16, 16, 3)
+    out = str(tmp_path / "sub" / "out.png")
+    pm.save_image(out, rgb)
+    assert np.array_equal(pm.load_image(out), np.clip(rgb * 255, 0, 255).astype(np.uint8) / 255.0)
+    st = pm.stack_images(rgb, g["true_alpha"])
+    assert st.shape == (32, 32, 4) and np.array_equal(st[:, :, 3], g["true_alpha"])
+    b = pm.blend(rgb, 1.0 - rgb, g["true_alpha"])
+    a = g["true_alpha"][:, :, None]
+    assert np.array_equal(b, a * rgb + (1 - a) * (1.0 - rgb))
+
+
+def test_cutout_size_mismatch(tmp_path):
+    import pymatting_b200 as pm
+    g = golden("cutout_test.npz")
+    p, t = str(tmp_path / "i.png"), str(tmp_path / "t.png")
+    _write_png(p, g["test_u8"])
+    _write_png(t, g["test_trimap_u8"][:16])
+    with pytest.raises(ValueError):
+        pm.cutout(p, t, str(tmp_path / "o.png"))
