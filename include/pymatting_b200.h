@@ -130,6 +130,19 @@ int pmb_fg_ml_jacobi(const float* image, const float* alpha, int h, int w, float
                      int n_small_iterations, int n_big_iterations, int small_size, float* F,
                      float* B, void* workspace, int64_t workspace_bytes, void* stream);
 
+/* Replace uniform_laplacian(image, radius) (mode 0,
+ * pymatting/laplacian/uniform_laplacian.py) and rw_laplacian(image, sigma,
+ * radius, regularization) (mode 1, pymatting/laplacian/rw_laplacian.py;
+ * like the reference, the weights are exp(-900 |z_i - z_j|^2) whatever
+ * sigma is), each through weights_to_laplacian (util/util.py:840-875).
+ * image: (h, w, 3) float64 (mode 1 only). px: w + 1 and py: h + 1 int64
+ * prefix sums of the clamped window width per column and height per row;
+ * the result is canonical CSR with rowptr (h w + 1), cols and vals
+ * (py[h] * px[w] entries), all on the device. */
+int pmb_window_laplacian(int mode, const double* image, int h, int w, int radius,
+                         double regularization, const int64_t* px, const int64_t* py,
+                         int64_t* rowptr, int64_t* cols, double* vals, void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

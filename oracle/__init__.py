@@ -621,3 +621,59 @@ def estimate_foreground_ml_cupy(input_image, input_alpha, regularization=1e-5,
     if return_background:
         return F, B
     return F
+
+
+# --------------------------------------------------------------------------
+# uniform_laplacian / rw_laplacian (through weights_to_laplacian)
+# --------------------------------------------------------------------------
+
+def window_laplacian(image, radius=1, regularization=0.0, kind="uniform"):
+    """pymatting/laplacian/uniform_laplacian.py and rw_laplacian.py with
+    util/util.py weights_to_laplacian (:840-875), row by row in the
+    reference's operation order: W's duplicate (clamped) entries summed,
+    rowsum(W) over ascending columns, W' = W / rowsum, rowsum(W') over
+    descending columns (the order scipy's sparse product leaves each row
+    in), L = diag(regularization + rowsum(W')) - W'. Returns a CSR matrix
+    with sorted columns."""
+    image = np.asarray(image, dtype=np.float64)
+    h, w = image.shape[:2]
+    r = int(radius)
+    flat = image.reshape(-1, image.shape[2]) if image.ndim == 3 else None
+    indptr = [0]
+    indices, data = [], []
+    for y in range(h):
+        for x in range(w):
+            i = x + y * w
+            cnt = {}
+            for dy in range(-r, r + 1):
+                for dx in range(-r, r + 1):
+                    j = min(max(x + dx, 0), w - 1) + min(max(y + dy, 0), h - 1) * w
+                    cnt[j] = cnt.get(j, 0) + 1
+            cols = sorted(cnt)
+            vals = []
+            for j in cols:
+                if kind == "uniform":
+                    wv = 1.0
+                else:
+                    nrm = float(np.linalg.norm(flat[i] - flat[j]))
+                    wv = float(np.exp(-900 * nrm ** 2))
+                v = wv
+                for _ in range(cnt[j] - 1):
+                    v = v + wv
+                vals.append(v)
+            s1 = 0.0
+            for v in vals:
+                s1 = s1 + v
+            f = 1.0 / s1
+            wp = [f * v for v in vals]
+            s2 = 0.0
+            for v in reversed(wp):
+                s2 = s2 + v
+            d = regularization + s2
+            for j, v in zip(cols, wp):
+                indices.append(j)
+                data.append(d - v if j == i else -v)
+            indptr.append(len(indices))
+    n = h * w
+    return scipy.sparse.csr_matrix((np.array(data), np.array(indices), np.array(indptr)),
+                                   shape=(n, n))

@@ -39,6 +39,8 @@ _SIGNATURES = {
     "pmb_fg_jacobi_workspace_bytes": (c_i64, [c_int, c_int]),
     "pmb_fg_ml_jacobi": (c_int, [c_vp, c_vp, c_int, c_int, c_flt, c_int, c_int, c_int, c_vp, c_vp,
                                  c_vp, c_i64, c_vp]),
+    "pmb_window_laplacian": (c_int, [c_int, c_vp, c_int, c_int, c_int, c_dbl, c_vp, c_vp, c_vp,
+                                     c_vp, c_vp, c_vp]),
     "pmb_cf_hard_system": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
     "pmb_scan_scratch_elems": (c_i64, [c_i64]),
     "pmb_ell_csr_rowptr": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp]),

@@ -26,6 +26,7 @@ SOURCES = {
     "lkm.cu": [],
     "foreground.cu": [],
     "foreground_jacobi.cu": [],
+    "laplacians.cu": [],
     "ichol.cu": ["-fmad=false"],
     "engine.cu": [],
 }

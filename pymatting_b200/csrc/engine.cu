@@ -1117,6 +1117,20 @@ PMB_API int pmb_fg_ml_jacobi(const float* image, const float* alpha, int h, int 
     return fail(kErrCuda, std::string("pmb_fg_ml_jacobi launch: ") + cudaGetErrorString((cudaError_t)rc));
 }
 
+int pmb_launch_window_laplacian(int, const double*, int, int, int, double, const int64_t*,
+                                const int64_t*, int64_t*, int64_t*, double*, cudaStream_t);
+
+PMB_API int pmb_window_laplacian(int mode, const double* image, int h, int w, int radius,
+                                 double regularization, const int64_t* px, const int64_t* py,
+                                 int64_t* rowptr, int64_t* cols, double* vals, void* stream) {
+    const int rc = pmb_launch_window_laplacian(mode, image, h, w, radius, regularization, px, py,
+                                               rowptr, cols, vals, (cudaStream_t)stream);
+    if (rc == -2) return fail(kErrArg, "pmb_window_laplacian: bad arguments");
+    if (rc) return fail(kErrCuda, std::string("pmb_window_laplacian launch: ") +
+                                      cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, const uint8_t* is_fg,
                                int h, int w, double epsilon, double* planes, double* rhs,
                                void* stream) {

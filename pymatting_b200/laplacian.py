@@ -22,8 +22,8 @@ from . import _device as dev
 from . import _ffi
 from .util import trimap_split
 
-__all__ = ["cf_laplacian", "make_linear_system", "DeviceCSRMatrix", "CFSource",
-           "device_source", "device_csr_arrays"]
+__all__ = ["cf_laplacian", "uniform_laplacian", "rw_laplacian", "make_linear_system",
+           "DeviceCSRMatrix", "CFSource", "device_source", "device_csr_arrays"]
 
 
 class CFSource:
@@ -255,3 +255,43 @@ def make_linear_system(L, trimap, lambda_value=100.0, return_c=False):
     if return_c:
         return A, b, c
     return A, b
+
+
+def _window_extents(n, r):
+    """Prefix sums of the clamped window extent min(v + r, n - 1) - max(v - r, 0) + 1."""
+    v = np.arange(n)
+    ext = np.minimum(v + r, n - 1) - np.maximum(v - r, 0) + 1
+    return np.concatenate([[0], np.cumsum(ext)]).astype(np.int64)
+
+
+def _window_laplacian(mode, image, radius, regularization):
+    h, w = image.shape[:2]
+    r = int(radius)
+    px = _window_extents(w, r)
+    py = _window_extents(h, r)
+    nnz = int(py[-1] * px[-1])
+    n = h * w
+    img = _image_to_device(image) if mode == 1 else None
+    rowptr = dev.empty(n + 1, torch.int64)
+    cols = dev.empty(max(nnz, 1), torch.int64)
+    vals = dev.empty(max(nnz, 1), torch.float64)
+    _ffi.check(_ffi.lib().pmb_window_laplacian(
+        mode, dev.ptr(img), h, w, r, float(regularization), dev.ptr(dev.to_device(px)),
+        dev.ptr(dev.to_device(py)), dev.ptr(rowptr), dev.ptr(cols), dev.ptr(vals), dev.stream()),
+        "pmb_window_laplacian")
+    return DeviceCSRMatrix(shape=(n, n), pmb_arrays=(rowptr, cols[:nnz], vals[:nnz]))
+
+
+def uniform_laplacian(image, radius=1):
+    """Uniform-weight Laplacian over (2 radius + 1)^2 windows, normalised:
+    pymatting/laplacian/uniform_laplacian.py (weights_to_laplacian of a box
+    convolution matrix). Canonical CSR on the device."""
+    return _window_laplacian(0, image, radius, 0.0)
+
+
+def rw_laplacian(image, sigma=0.033, radius=1, regularization=1e-8):
+    """Random-walk Laplacian: pymatting/laplacian/rw_laplacian.py. Weights
+    exp(-900 |z_i - z_j|^2) over (2 radius + 1)^2 windows with clamped
+    neighbours, row-normalised, plus ``regularization`` on the diagonal. As
+    in the reference, ``sigma`` does not enter the weights."""
+    return _window_laplacian(1, image, radius, regularization)

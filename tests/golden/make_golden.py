@@ -337,6 +337,45 @@ def gen_cutout(pm, root):
     np.savez_compressed(os.path.join(HERE, "cutout_test.npz"), **out)
 
 
+def gen_laplacians(pm, root, rng):
+    """uniform_laplacian and rw_laplacian on small random images (CSR arrays
+    of the reference's matrices), and the reference test's lemur errors
+    (tests/test_laplacians.py: spsolve of make_linear_system, error of the
+    clipped alpha against the good alpha on unknown pixels)."""
+    import scipy.sparse.linalg
+    out = {}
+    cases = [(1, 1, 1), (1, 5, 1), (4, 1, 1), (2, 2, 1), (7, 9, 1), (16, 13, 1), (12, 17, 2),
+             (5, 6, 3)]
+    out["n_cases"] = np.array([len(cases)])
+    for k, (h, w, r) in enumerate(cases):
+        img = rng.random((h, w, 3))
+        out[f"c{k}_image"], out[f"c{k}_radius"] = img, np.array([r])
+        for name, L in (("uniform", pm.uniform_laplacian(img, radius=r)),
+                        ("rw", pm.rw_laplacian(img, radius=r))):
+            L = scipy.sparse.csr_matrix(L)
+            L.sum_duplicates()
+            L.sort_indices()
+            out[f"c{k}_{name}_indptr"] = L.indptr.astype(np.int64)
+            out[f"c{k}_{name}_indices"] = L.indices.astype(np.int64)
+            out[f"c{k}_{name}_data"] = L.data
+    cwd = os.getcwd()
+    os.chdir(root)
+    try:
+        image = pm.load_image("data/lemur/lemur.png", "rgb", 0.1, "bilinear")
+        trimap = pm.load_image("data/lemur/lemur_trimap.png", "gray", 0.1, "nearest")
+        good = pm.load_image("data/lemur/lemur_alpha_fba.png", "gray", 0.1, "bilinear")
+    finally:
+        os.chdir(cwd)
+    is_unknown = pm.trimap_split(trimap, flatten=False)[3]
+    for name, fn in (("uniform", pm.uniform_laplacian), ("rw", pm.rw_laplacian)):
+        A, b = pm.make_linear_system(fn(image), trimap)
+        x = scipy.sparse.linalg.spsolve(A, b)
+        alpha = np.clip(x, 0, 1).reshape(trimap.shape)
+        out[f"lemur_{name}_error"] = np.array([np.linalg.norm(np.abs(alpha - good)[is_unknown])])
+    out["lemur_image"], out["lemur_trimap"], out["lemur_good"] = image, trimap, good
+    np.savez_compressed(os.path.join(HERE, "laplacians_small.npz"), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     pm = import_reference(root)
@@ -347,7 +386,8 @@ def main():
                      ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm)),
                      ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77))),
                      ("foreground", lambda: gen_foreground(pm, root, np.random.default_rng(91))),
-                     ("cutout", lambda: gen_cutout(pm, root))]:
+                     ("cutout", lambda: gen_cutout(pm, root)),
+                     ("laplacians", lambda: gen_laplacians(pm, root, np.random.default_rng(5)))]:
         if not only or name in only:
             fn()
     for f in sorted(os.listdir(HERE)):

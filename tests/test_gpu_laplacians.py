@@ -1,0 +1,65 @@
+"""uniform_laplacian and rw_laplacian assembled on the device, against the
+reference's matrices (tests/golden/laplacians_small.npz) and the reference
+test's lemur errors (tests/test_laplacians.py: error of the clipped solve
+against the good alpha on unknown pixels, 1 % regression allowed).
+
+Tolerances: uniform values identical; rw within 1e-15 absolute (entries are
+at most 1 in size; the reference's exp and norm come from numba/libm)."""
+
+import numpy as np
+import pytest
+import scipy.sparse
+
+import oracle
+from tests.conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_csr(g, k, name):
+    n = g[f"c{k}_image"].shape[0] * g[f"c{k}_image"].shape[1]
+    return scipy.sparse.csr_matrix((g[f"c{k}_{name}_data"], g[f"c{k}_{name}_indices"],
+                                    g[f"c{k}_{name}_indptr"]), shape=(n, n))
+
+
+def _maxdiff(A, B):
+    D = abs(scipy.sparse.csr_matrix(A) - B)
+    return D.max() if D.nnz else 0.0
+
+
+def test_window_laplacians_match_reference(gpu):
+    import pymatting_b200 as pm
+    g = golden("laplacians_small.npz")
+    for k in range(int(g["n_cases"][0])):
+        img, r = g[f"c{k}_image"], int(g[f"c{k}_radius"][0])
+        U = pm.uniform_laplacian(img, radius=r)
+        assert isinstance(U, scipy.sparse.csr_matrix) and U.shape == _ref_csr(g, k, "uniform").shape
+        assert _maxdiff(U, _ref_csr(g, k, "uniform")) == 0.0, k
+        assert _maxdiff(pm.rw_laplacian(img, radius=r), _ref_csr(g, k, "rw")) <= 1e-15, k
+
+
+def test_window_laplacians_match_oracle_bitwise_structure(gpu):
+    import pymatting_b200 as pm
+    rng = np.random.default_rng(9)
+    img = rng.random((37, 53, 3))
+    for name, fn, reg in (("uniform", pm.uniform_laplacian, 0.0), ("rw", pm.rw_laplacian, 1e-8)):
+        L = fn(img)
+        Lr = oracle.window_laplacian(img, 1, reg, name)
+        assert np.array_equal(L.indptr, Lr.indptr) and np.array_equal(L.indices, Lr.indices)
+        tol = 0.0 if name == "uniform" else 1e-15
+        assert np.abs(L.data - Lr.data).max() <= tol
+
+
+def test_reference_laplacian_errors_on_lemur(gpu):
+    import pymatting_b200 as pm
+    g = golden("laplacians_small.npz")
+    image, trimap, good = g["lemur_image"], g["lemur_trimap"], g["lemur_good"]
+    is_unknown = pm.trimap_split(trimap, flatten=False)[3]
+    for name, fn in (("uniform", pm.uniform_laplacian), ("rw", pm.rw_laplacian)):
+        A, b = pm.make_linear_system(fn(image), trimap)
+        x = pm.cg(A, b, M=pm.jacobi(A), rtol=1e-12, maxiter=100000)
+        alpha = np.clip(x, 0, 1).reshape(trimap.shape)
+        error = np.linalg.norm(np.abs(alpha - good)[is_unknown])
+        expected = float(g[f"lemur_{name}_error"][0])
+        assert (error - expected) / expected <= 0.01, (name, error, expected)
+        assert abs(error - expected) <= 1e-6 * expected, (name, error, expected)

@@ -215,3 +215,23 @@ def test_oracle_foreground_cupy_variant_reference_threshold():
     assert np.mean((alpha[:, :, None] * np.abs(F - g["lemur_expected"]))[unknown]) <= 0.022
     with pytest.raises(ZeroDivisionError):
         oracle.estimate_foreground_ml_cupy(np.zeros((1, 1, 3)), np.zeros((1, 1)))
+
+
+def _ref_csr(g, k, name):
+    n = g[f"c{k}_image"].shape[0] * g[f"c{k}_image"].shape[1]
+    return scipy.sparse.csr_matrix((g[f"c{k}_{name}_data"], g[f"c{k}_{name}_indices"],
+                                    g[f"c{k}_{name}_indptr"]), shape=(n, n))
+
+
+def test_oracle_window_laplacians_match_reference():
+    """uniform_laplacian: identical values. rw_laplacian: within 1e-15 (the
+    reference's exp and norm run through numba/libm; a few weights near the
+    underflow range round differently). Entries the reference's sparse
+    arithmetic drops as exact zeros are kept here as zeros."""
+    g = golden("laplacians_small.npz")
+    for k in range(int(g["n_cases"][0])):
+        img, r = g[f"c{k}_image"], int(g[f"c{k}_radius"][0])
+        for name, reg, tol in (("uniform", 0.0, 0.0), ("rw", 1e-8, 1e-15)):
+            L = oracle.window_laplacian(img, r, reg, name)
+            D = abs(L - _ref_csr(g, k, name))
+            assert (D.max() if D.nnz else 0.0) <= tol, (k, name)
