@@ -275,10 +275,13 @@ def _window_laplacian(mode, image, radius, regularization):
     rowptr = dev.empty(n + 1, torch.int64)
     cols = dev.empty(max(nnz, 1), torch.int64)
     vals = dev.empty(max(nnz, 1), torch.float64)
+    # held in names until the launch is queued: a freed temporary's block
+    # could be handed to the next upload before the kernel reads it
+    px_t = dev.to_device(px)
+    py_t = dev.to_device(py)
     _ffi.check(_ffi.lib().pmb_window_laplacian(
-        mode, dev.ptr(img), h, w, r, float(regularization), dev.ptr(dev.to_device(px)),
-        dev.ptr(dev.to_device(py)), dev.ptr(rowptr), dev.ptr(cols), dev.ptr(vals), dev.stream()),
-        "pmb_window_laplacian")
+        mode, dev.ptr(img), h, w, r, float(regularization), dev.ptr(px_t), dev.ptr(py_t),
+        dev.ptr(rowptr), dev.ptr(cols), dev.ptr(vals), dev.stream()), "pmb_window_laplacian")
     return DeviceCSRMatrix(shape=(n, n), pmb_arrays=(rowptr, cols[:nnz], vals[:nnz]))
 
 
