@@ -146,3 +146,24 @@ def test_cutout_size_mismatch(tmp_path):
     _write_png(t, g["test_trimap_u8"][:16])
     with pytest.raises(ValueError):
         pm.cutout(p, t, str(tmp_path / "o.png"))
+
+
+def test_foreground_level_plan_matches_oracle():
+    """The host-side level sizes of estimate_foreground_ml (library, no GPU
+    needed) equal the oracle's restatement of the reference's
+    round(w0 ** (i / n)) schedule, including powers of two, strips and a
+    1x1 image (ZeroDivisionError, as in the reference)."""
+    import oracle
+    from pymatting_b200.foreground import foreground_levels
+    rng = np.random.default_rng(17)
+    shapes = [(1, 2), (2, 1), (2, 2), (3, 1), (1, 1000), (31, 33), (32, 32), (64, 64), (1080, 1920),
+              (2160, 3840), (4096, 4096), (4097, 3), (10000, 3), (65535, 2)]
+    shapes += [tuple(int(v) for v in rng.integers(1, 5000, size=2)) for _ in range(200)]
+    for h, w in shapes:
+        if max(h, w) == 1:
+            continue
+        assert foreground_levels(h, w) == oracle.fg_levels(h, w), (h, w)
+    with pytest.raises(ZeroDivisionError):
+        foreground_levels(1, 1)
+    with pytest.raises(ZeroDivisionError):
+        oracle.fg_levels(1, 1)
