@@ -143,6 +143,20 @@ int pmb_window_laplacian(int mode, const double* image, int h, int w, int radius
                          double regularization, const int64_t* px, const int64_t* py,
                          int64_t* rowptr, int64_t* cols, double* vals, void* stream);
 
+/* Replace lbdm_laplacian(image, epsilon, radius)
+ * (pymatting/laplacian/lbdm_laplacian.py) for radius 1 or 2 and images
+ * larger than 2 radius in both directions: per interior window
+ * T = (I - F)(I - F)^T with F = (K + eps I)^-1 K, K = X X^T over the
+ * window's [colours, 1], summed into canonical CSR. scratch:
+ * pmb_lbdm_scratch_elems doubles (-1: unsupported). px / py (w + 1, h + 1
+ * int64): prefix sums of the number of columns / rows of pixels that share a
+ * window with a pixel of that column / row; cols and vals hold py[h] * px[w]
+ * entries. */
+int64_t pmb_lbdm_scratch_elems(int h, int w, int radius);
+int pmb_lbdm_laplacian(const double* image, int h, int w, int radius, double epsilon,
+                       double* scratch, const int64_t* px, const int64_t* py, int64_t* rowptr,
+                       int64_t* cols, double* vals, void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

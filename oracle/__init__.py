@@ -677,3 +677,32 @@ def window_laplacian(image, radius=1, regularization=0.0, kind="uniform"):
     n = h * w
     return scipy.sparse.csr_matrix((np.array(data), np.array(indices), np.array(indptr)),
                                    shape=(n, n))
+
+
+def lbdm_laplacian(image, epsilon=1e-7, radius=1):
+    """pymatting/laplacian/lbdm_laplacian.py restated with numpy: per
+    interior window X = [colours, 1], K = X X^T, F = solve(K + eps I, K),
+    T = (I - F)(I - F)^T, summed over windows into a CSR matrix by scipy (the
+    same COO -> CSR conversion as the reference)."""
+    image = np.asarray(image, dtype=np.float64)
+    h, w = image.shape[:2]
+    r = int(radius)
+    n = h * w
+    s = 2 * r + 1
+    area = s * s
+    idx = np.arange(n).reshape(h, w)
+    rows, cols, vals = [np.zeros(1, np.int64)], [np.zeros(1, np.int64)], [np.zeros(1)]
+    for y in range(r, h - r):
+        for x in range(r, w - r):
+            win = image[y - r:y + r + 1, x - r:x + r + 1].reshape(area, 3)
+            X = np.concatenate([win, np.ones((area, 1))], axis=1)
+            K = X @ X.T
+            F = np.linalg.solve(K + epsilon * np.eye(area), K)
+            T2 = np.eye(area) - F
+            T = T2 @ T2.T
+            wi = idx[y - r:y + r + 1, x - r:x + r + 1].ravel()
+            rows.append(np.repeat(wi, area))
+            cols.append(np.tile(wi, area))
+            vals.append(T.ravel())
+    return scipy.sparse.csr_matrix((np.concatenate(vals), (np.concatenate(rows),
+                                                           np.concatenate(cols))), shape=(n, n))

@@ -41,6 +41,9 @@ _SIGNATURES = {
                                  c_vp, c_i64, c_vp]),
     "pmb_window_laplacian": (c_int, [c_int, c_vp, c_int, c_int, c_int, c_dbl, c_vp, c_vp, c_vp,
                                      c_vp, c_vp, c_vp]),
+    "pmb_lbdm_scratch_elems": (c_i64, [c_int, c_int, c_int]),
+    "pmb_lbdm_laplacian": (c_int, [c_vp, c_int, c_int, c_int, c_dbl, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                   c_vp, c_vp]),
     "pmb_cf_hard_system": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
     "pmb_scan_scratch_elems": (c_i64, [c_i64]),
     "pmb_ell_csr_rowptr": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp]),

@@ -1131,6 +1131,26 @@ PMB_API int pmb_window_laplacian(int mode, const double* image, int h, int w, in
     return 0;
 }
 
+int pmb_launch_lbdm_laplacian(const double*, int, int, int, double, double*, const int64_t*,
+                              const int64_t*, int64_t*, int64_t*, double*, cudaStream_t);
+
+PMB_API int64_t pmb_lbdm_scratch_elems(int h, int w, int radius) {
+    if ((radius != 1 && radius != 2) || h <= 2 * radius || w <= 2 * radius) return -1;
+    const int64_t s = 2 * radius + 1;
+    return (int64_t)(h - 2 * radius) * (w - 2 * radius) * s * s * s * s;
+}
+
+PMB_API int pmb_lbdm_laplacian(const double* image, int h, int w, int radius, double epsilon,
+                               double* scratch, const int64_t* px, const int64_t* py,
+                               int64_t* rowptr, int64_t* cols, double* vals, void* stream) {
+    const int rc = pmb_launch_lbdm_laplacian(image, h, w, radius, epsilon, scratch, px, py, rowptr,
+                                             cols, vals, (cudaStream_t)stream);
+    if (rc == -2) return fail(kErrArg, "pmb_lbdm_laplacian: bad arguments (radius 1 or 2, image larger than 2 radius)");
+    if (rc) return fail(kErrCuda, std::string("pmb_lbdm_laplacian launch: ") +
+                                      cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, const uint8_t* is_fg,
                                int h, int w, double epsilon, double* planes, double* rhs,
                                void* stream) {

@@ -124,3 +124,146 @@ int pmb_launch_window_laplacian(int mode, const double* image, int h, int w, int
     else return -2;
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
+
+// ---------------------------------------------------------------------------
+// Learning-based digital matting Laplacian (lbdm_laplacian,
+// pymatting/laplacian/lbdm_laplacian.py). Each interior window c of
+// (2r+1)^2 pixels gives T_c = (I - F)(I - F)^T with
+// F = (K + eps I)^-1 K, K = X X^T, X = [colours, 1] of the window's pixels.
+// L_pq sums T_c[a(p), b(q)] over the windows holding both pixels. Pass 1
+// stores T_c per window (one thread per window: Gaussian elimination with
+// partial pivoting in local memory); pass 2 gathers every row in ascending
+// column order, windows in raster order (deterministic).
+// ---------------------------------------------------------------------------
+
+namespace pmb {
+namespace lbdm {
+
+template <int R>
+__global__ void __launch_bounds__(128) k_lbdm_windows(const double* __restrict__ image, int h,
+                                                      int w, double eps, double* __restrict__ T) {
+    constexpr int S = 2 * R + 1, N = S * S;
+    const int ww = w - 2 * R;
+    const long long nwin = (long long)(h - 2 * R) * ww;
+    const long long wi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (wi >= nwin) return;
+    const int cy = (int)(wi / ww) + R, cx = (int)(wi % ww) + R;
+    double X[N][4];
+    for (int k = 0; k < N; ++k) {
+        const int y2 = cy - R + k / S, x2 = cx - R + k % S;
+        const double* z = image + ((long long)y2 * w + x2) * 3;
+        X[k][0] = z[0];
+        X[k][1] = z[1];
+        X[k][2] = z[2];
+        X[k][3] = 1.0;
+    }
+    double A[N][N], B[N][N];
+    for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N; ++b) {
+            double s = 0.0;
+            for (int c = 0; c < 4; ++c) s = __dadd_rn(s, __dmul_rn(X[a][c], X[b][c]));
+            B[a][b] = s;
+            A[a][b] = (a == b) ? __dadd_rn(s, eps) : s;
+        }
+    // A F = B by elimination with partial pivoting (first maximum wins)
+    for (int k = 0; k < N; ++k) {
+        int p = k;
+        double best = fabs(A[k][k]);
+        for (int i = k + 1; i < N; ++i)
+            if (fabs(A[i][k]) > best) {
+                best = fabs(A[i][k]);
+                p = i;
+            }
+        if (p != k) {
+            for (int j = 0; j < N; ++j) {
+                double t = A[k][j]; A[k][j] = A[p][j]; A[p][j] = t;
+                t = B[k][j]; B[k][j] = B[p][j]; B[p][j] = t;
+            }
+        }
+        const double inv = __ddiv_rn(1.0, A[k][k]);
+        for (int i = k + 1; i < N; ++i) {
+            const double l = __dmul_rn(A[i][k], inv);
+            for (int j = k + 1; j < N; ++j) A[i][j] = __dsub_rn(A[i][j], __dmul_rn(l, A[k][j]));
+            for (int j = 0; j < N; ++j) B[i][j] = __dsub_rn(B[i][j], __dmul_rn(l, B[k][j]));
+        }
+    }
+    for (int i = N - 1; i >= 0; --i)
+        for (int j = 0; j < N; ++j) {
+            double s = B[i][j];
+            for (int k = i + 1; k < N; ++k) s = __dsub_rn(s, __dmul_rn(A[i][k], B[k][j]));
+            B[i][j] = __ddiv_rn(s, A[i][i]);  // B now holds F
+        }
+    // T = (I - F)(I - F)^T, reusing A for I - F
+    for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N; ++b) A[a][b] = (a == b) ? __dsub_rn(1.0, B[a][b]) : -B[a][b];
+    double* out = T + wi * (N * N);
+    for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N; ++b) {
+            double s = 0.0;
+            for (int k = 0; k < N; ++k) s = __dadd_rn(s, __dmul_rn(A[a][k], A[b][k]));
+            out[a * N + b] = s;
+        }
+}
+
+// Window centres holding pixel coordinate v: [max(R, v - R), min(n - 1 - R, v + R)].
+template <int R>
+__global__ void __launch_bounds__(256) k_lbdm_rows(int h, int w, const double* __restrict__ T,
+                                                   const int64_t* __restrict__ px,
+                                                   const int64_t* __restrict__ py,
+                                                   int64_t* __restrict__ rowptr,
+                                                   int64_t* __restrict__ cols,
+                                                   double* __restrict__ vals) {
+    constexpr int S = 2 * R + 1, N = S * S;
+    const long long n = (long long)h * w;
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int y = (int)(p / w), x = (int)(p % w);
+    const int cy0 = max(R, y - R), cy1 = min(h - 1 - R, y + R);
+    const int cx0 = max(R, x - R), cx1 = min(w - 1 - R, x + R);
+    const int ny = cy1 - cy0 + 2 * R + 1;
+    const long long base = py[y] * px[w] + (long long)ny * px[x];
+    rowptr[p] = base;
+    if (p == n - 1) rowptr[n] = py[h] * px[w];
+    const int ww = w - 2 * R;
+    long long o = base;
+    for (int qy = cy0 - R; qy <= cy1 + R; ++qy)
+        for (int qx = cx0 - R; qx <= cx1 + R; ++qx, ++o) {
+            double s = 0.0;
+            const int dy0 = max(cy0, qy - R), dy1 = min(cy1, qy + R);
+            const int dx0 = max(cx0, qx - R), dx1 = min(cx1, qx + R);
+            for (int cy = dy0; cy <= dy1; ++cy)
+                for (int cx = dx0; cx <= dx1; ++cx) {
+                    const long long wi = (long long)(cy - R) * ww + (cx - R);
+                    const int a = (y - cy + R) * S + (x - cx + R);
+                    const int b = (qy - cy + R) * S + (qx - cx + R);
+                    s = __dadd_rn(s, T[wi * (N * N) + a * N + b]);
+                }
+            cols[o] = (long long)qy * w + qx;
+            vals[o] = s;
+        }
+}
+
+}  // namespace lbdm
+}  // namespace pmb
+
+// radius 1 or 2; h, w > 2 radius. T: (h - 2r)(w - 2r) (2r+1)^4 doubles of
+// scratch. px / py: prefix sums of the per-column / per-row count of pixels
+// sharing a window with the pixel (w + 1, h + 1 int64).
+int pmb_launch_lbdm_laplacian(const double* image, int h, int w, int r, double eps, double* T,
+                              const int64_t* px, const int64_t* py, int64_t* rowptr,
+                              int64_t* cols, double* vals, cudaStream_t st) {
+    if (!image || !T || !px || !py || !rowptr || !cols || !vals || (r != 1 && r != 2) ||
+        h <= 2 * r || w <= 2 * r)
+        return -2;
+    const long long nwin = (long long)(h - 2 * r) * (w - 2 * r);
+    const long long n = (long long)h * w;
+    const int wb = (int)((nwin + 127) / 128), rb = (int)((n + 255) / 256);
+    if (r == 1) {
+        pmb::lbdm::k_lbdm_windows<1><<<wb, 128, 0, st>>>(image, h, w, eps, T);
+        pmb::lbdm::k_lbdm_rows<1><<<rb, 256, 0, st>>>(h, w, T, px, py, rowptr, cols, vals);
+    } else {
+        pmb::lbdm::k_lbdm_windows<2><<<wb, 128, 0, st>>>(image, h, w, eps, T);
+        pmb::lbdm::k_lbdm_rows<2><<<rb, 256, 0, st>>>(h, w, T, px, py, rowptr, cols, vals);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

@@ -22,7 +22,8 @@ from . import _device as dev
 from . import _ffi
 from .util import trimap_split
 
-__all__ = ["cf_laplacian", "uniform_laplacian", "rw_laplacian", "make_linear_system",
+__all__ = ["cf_laplacian", "uniform_laplacian", "rw_laplacian", "lbdm_laplacian",
+           "make_linear_system",
            "DeviceCSRMatrix", "CFSource", "device_source", "device_csr_arrays"]
 
 
@@ -298,3 +299,42 @@ def rw_laplacian(image, sigma=0.033, radius=1, regularization=1e-8):
     neighbours, row-normalised, plus ``regularization`` on the diagonal. As
     in the reference, ``sigma`` does not enter the weights."""
     return _window_laplacian(1, image, radius, regularization)
+
+
+def _lbdm_extents(n, r):
+    """Prefix sums of the number of coordinates sharing a window with v:
+    window centres [max(r, v - r), min(n - 1 - r, v + r)] widened by r."""
+    v = np.arange(n)
+    ext = np.minimum(n - 1 - r, v + r) - np.maximum(r, v - r) + 2 * r + 1
+    return np.concatenate([[0], np.cumsum(ext)]).astype(np.int64)
+
+
+def lbdm_laplacian(image, epsilon=1e-7, radius=1):
+    """Learning-based digital matting Laplacian:
+    pymatting/laplacian/lbdm_laplacian.py. Canonical CSR on the device;
+    radius 1 or 2. An image with no interior window gives the reference's
+    matrix of a single stored zero at (0, 0)."""
+    h, w = image.shape[:2]
+    r = int(radius)
+    if r not in (1, 2):
+        raise NotImplementedError("lbdm_laplacian on the device supports radius 1 and 2")
+    n = h * w
+    if h <= 2 * r or w <= 2 * r:
+        rowptr = torch.ones(n + 1, dtype=torch.int64, device=dev.device())
+        rowptr[0] = 0
+        return DeviceCSRMatrix(shape=(n, n), pmb_arrays=(rowptr, dev.zeros(1, torch.int64),
+                                                         dev.zeros(1, torch.float64)))
+    lib = _ffi.lib()
+    img = _image_to_device(image)
+    scratch = dev.empty(int(lib.pmb_lbdm_scratch_elems(h, w, r)), torch.float64)
+    px_t = dev.to_device(_lbdm_extents(w, r))
+    py_t = dev.to_device(_lbdm_extents(h, r))
+    nnz = int(_lbdm_extents(h, r)[-1] * _lbdm_extents(w, r)[-1])
+    rowptr = dev.empty(n + 1, torch.int64)
+    cols = dev.empty(nnz, torch.int64)
+    vals = dev.empty(nnz, torch.float64)
+    _ffi.check(lib.pmb_lbdm_laplacian(dev.ptr(img), h, w, r, float(epsilon), dev.ptr(scratch),
+                                      dev.ptr(px_t), dev.ptr(py_t), dev.ptr(rowptr),
+                                      dev.ptr(cols), dev.ptr(vals), dev.stream()),
+               "pmb_lbdm_laplacian")
+    return DeviceCSRMatrix(shape=(n, n), pmb_arrays=(rowptr, cols, vals))

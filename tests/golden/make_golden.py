@@ -338,8 +338,9 @@ def gen_cutout(pm, root):
 
 
 def gen_laplacians(pm, root, rng):
-    """uniform_laplacian and rw_laplacian on small random images (CSR arrays
-    of the reference's matrices), and the reference test's lemur errors
+    """uniform_laplacian, rw_laplacian and lbdm_laplacian on small random
+    images (CSR arrays of the reference's matrices), and the reference
+    test's lemur errors
     (tests/test_laplacians.py: spsolve of make_linear_system, error of the
     clipped alpha against the good alpha on unknown pixels)."""
     import scipy.sparse.linalg
@@ -372,6 +373,21 @@ def gen_laplacians(pm, root, rng):
         x = scipy.sparse.linalg.spsolve(A, b)
         alpha = np.clip(x, 0, 1).reshape(trimap.shape)
         out[f"lemur_{name}_error"] = np.array([np.linalg.norm(np.abs(alpha - good)[is_unknown])])
+    A, b = pm.make_linear_system(pm.lbdm_laplacian(image), trimap)
+    x = scipy.sparse.linalg.spsolve(A, b)
+    alpha = np.clip(x, 0, 1).reshape(trimap.shape)
+    out["lemur_lbdm_error"] = np.array([np.linalg.norm(np.abs(alpha - good)[is_unknown])])
+    lb = [(3, 3, 1), (2, 6, 1), (5, 7, 1), (12, 9, 1), (7, 8, 2), (9, 11, 2)]
+    out["lbdm_n"] = np.array([len(lb)])
+    for k, (h, w, r) in enumerate(lb):
+        img = rng.random((h, w, 3))
+        L = scipy.sparse.csr_matrix(pm.lbdm_laplacian(img, radius=r))
+        L.sum_duplicates()
+        L.sort_indices()
+        out[f"lbdm{k}_image"], out[f"lbdm{k}_radius"] = img, np.array([r])
+        out[f"lbdm{k}_indptr"] = L.indptr.astype(np.int64)
+        out[f"lbdm{k}_indices"] = L.indices.astype(np.int64)
+        out[f"lbdm{k}_data"] = L.data
     out["lemur_image"], out["lemur_trimap"], out["lemur_good"] = image, trimap, good
     np.savez_compressed(os.path.join(HERE, "laplacians_small.npz"), **out)
 

@@ -67,3 +67,38 @@ def test_reference_laplacian_errors_on_lemur(gpu):
         expected = float(g[f"lemur_{name}_error"][0])
         assert (error - expected) / expected <= 0.01, (name, error, expected)
         assert abs(error - expected) <= 1e-6 * expected, (name, error, expected)
+
+
+LBDM_TOL = 1e-8   # of max |L|: the per-window solve is ill-conditioned (rank-4 K)
+
+
+def test_lbdm_matches_reference(gpu):
+    import pymatting_b200 as pm
+    g = golden("laplacians_small.npz")
+    for k in range(int(g["lbdm_n"][0])):
+        img, r = g[f"lbdm{k}_image"], int(g[f"lbdm{k}_radius"][0])
+        n = img.shape[0] * img.shape[1]
+        R = scipy.sparse.csr_matrix((g[f"lbdm{k}_data"], g[f"lbdm{k}_indices"],
+                                     g[f"lbdm{k}_indptr"]), shape=(n, n))
+        L = pm.lbdm_laplacian(img, radius=r)
+        assert np.array_equal(L.indptr, R.indptr) and np.array_equal(L.indices, R.indices), k
+        assert np.abs(L.data - R.data).max() <= LBDM_TOL * max(np.abs(R.data).max(), 1.0), k
+
+
+def test_lbdm_larger_against_oracle_and_lemur_error(gpu):
+    import scipy.sparse.linalg
+    import pymatting_b200 as pm
+    rng = np.random.default_rng(4)
+    img = rng.random((48, 61, 3))
+    L = pm.lbdm_laplacian(img)
+    R = oracle.lbdm_laplacian(img)
+    assert _maxdiff(L, R) <= LBDM_TOL * abs(R).max()
+    g = golden("laplacians_small.npz")
+    image, trimap, good = g["lemur_image"], g["lemur_trimap"], g["lemur_good"]
+    is_unknown = pm.trimap_split(trimap, flatten=False)[3]
+    A, b = pm.make_linear_system(pm.lbdm_laplacian(image), trimap)
+    x = scipy.sparse.linalg.spsolve(scipy.sparse.csr_matrix(A), b)
+    error = np.linalg.norm(np.abs(np.clip(x, 0, 1).reshape(trimap.shape) - good)[is_unknown])
+    expected = float(g["lemur_lbdm_error"][0])
+    assert (error - expected) / expected <= 0.01
+    assert abs(error - expected) <= 1e-5 * expected, (error, expected)

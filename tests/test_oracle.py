@@ -235,3 +235,17 @@ def test_oracle_window_laplacians_match_reference():
             L = oracle.window_laplacian(img, r, reg, name)
             D = abs(L - _ref_csr(g, k, name))
             assert (D.max() if D.nnz else 0.0) <= tol, (k, name)
+
+
+def test_oracle_lbdm_matches_reference():
+    """lbdm_laplacian: the per-window solve (K + eps I)^-1 K is
+    ill-conditioned (K = X X^T has rank 4 of (2r+1)^2), so two LAPACK builds
+    agree only to ~1e-9 of the matrix scale; tolerance 1e-8 of max |L|."""
+    g = golden("laplacians_small.npz")
+    for k in range(int(g["lbdm_n"][0])):
+        img, r = g[f"lbdm{k}_image"], int(g[f"lbdm{k}_radius"][0])
+        n = img.shape[0] * img.shape[1]
+        R = scipy.sparse.csr_matrix((g[f"lbdm{k}_data"], g[f"lbdm{k}_indices"],
+                                     g[f"lbdm{k}_indptr"]), shape=(n, n))
+        D = abs(oracle.lbdm_laplacian(img, radius=r) - R)
+        assert (D.max() if D.nnz else 0.0) <= 1e-8 * max(abs(R).max(), 1.0), k
