@@ -157,6 +157,22 @@ int pmb_lbdm_laplacian(const double* image, int h, int w, int radius, double eps
                        double* scratch, const int64_t* px, const int64_t* py, int64_t* rowptr,
                        int64_t* cols, double* vals, void* stream);
 
+/* Replace knn_laplacian(image, n_neighbors, distance_weights, kernel)
+ * (pymatting/laplacian/knn_laplacian.py): per pass p, the n_neighbors[p]
+ * nearest pixels in the float32 feature space (r, g, b, dw x, dw y) by an
+ * exact search with the insertion rule of pymatting/util/kdtree.py (equal
+ * distances resolved by index, not by tree order; O(n^2) per pass);
+ * W = sum_p B_p + B_p^T (soft != 0: weights 1 - |f_i - f_j|_1 / 5);
+ * L = I - diag(1 / rowsum(W)) W as canonical CSR. Two calls on the same
+ * scratch (pmb_knn_scratch_elems int64) and rowptr (h w + 1): the first with
+ * cols = vals = null returns the entry count in *nnz; the second fills cols
+ * and vals (*nnz entries). image: (h, w, 3) float64 on the device;
+ * n_neighbors and distance_weights: host arrays of `passes` (1..4) values. */
+int64_t pmb_knn_scratch_elems(int64_t n, int total_neighbors, int passes);
+int pmb_knn_laplacian(const double* image, int h, int w, const int* n_neighbors,
+                      const double* distance_weights, int passes, int soft, int64_t* scratch,
+                      int64_t* rowptr, int64_t* cols, double* vals, int64_t* nnz, void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

@@ -18,6 +18,7 @@ Pieces and the reference code each restates (paths inside PyMatting 1.1.15):
 * ``lkm_laplacian``      pymatting/laplacian/lkm_laplacian.py:6-76
 * ``estimate_foreground_ml`` pymatting/foreground/estimate_foreground_ml.py:5-253 (C)
 * ``estimate_foreground_ml_cupy`` pymatting/foreground/estimate_foreground_ml_cupy.py:5-230
+* ``window_laplacian``, ``lbdm_laplacian``, ``knn_laplacian`` pymatting/laplacian/*.py
 
 Parity of this restatement with the reference itself is pinned by
 ``tests/test_oracle.py`` against the fixtures in ``tests/golden/`` that
@@ -706,3 +707,47 @@ def lbdm_laplacian(image, epsilon=1e-7, radius=1):
             vals.append(T.ravel())
     return scipy.sparse.csr_matrix((np.concatenate(vals), (np.concatenate(rows),
                                                            np.concatenate(cols))), shape=(n, n))
+
+
+
+def knn(f, k):
+    """Indices of the k nearest feature rows of every row (oracle/knn.c:
+    the k-d tree's insertion rule, candidates in index order)."""
+    lib = _load()
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    n, dims = f.shape
+    out = np.zeros((n, k), dtype=np.int64)
+    lib.oracle_knn.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int64, ctypes.c_int,
+                               ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    lib.oracle_knn(_p(f, ctypes.c_float), n, dims, k, _p(out, ctypes.c_int64))
+    return out
+
+
+def knn_laplacian(image, n_neighbors=[20, 10], distance_weights=[2.0, 0.1], kernel="binary"):
+    """pymatting/laplacian/knn_laplacian.py restated with oracle.knn in place
+    of the reference's k-d tree (same neighbours except among equal
+    distances), then the reference's own scipy assembly: W = B + B^T,
+    normalize_rows, L = I - W."""
+    image = np.asarray(image, dtype=np.float64)
+    h, w = image.shape[:2]
+    r, g, b = image.reshape(-1, 3).T
+    n = w * h
+    x = np.tile(np.linspace(0, 1, w), h)
+    y = np.repeat(np.linspace(0, 1, h), w)
+    i, j, coo_data = [], [], []
+    for k, dw in zip(n_neighbors, distance_weights):
+        f = np.stack([r, g, b, dw * x, dw * y], axis=1, out=np.zeros((n, 5), dtype=np.float32))
+        nbr = knn(f, k)
+        i.append(np.repeat(np.arange(n), k))
+        j.append(nbr.ravel())
+        W_ij = np.ones(k * n)
+        if kernel == "soft":
+            W_ij -= np.abs(f[i[-1]] - f[j[-1]]).sum(axis=1) / f.shape[1]
+        coo_data.append(W_ij)
+    ij = np.concatenate(i + j)
+    ji = np.concatenate(j + i)
+    coo_data = np.concatenate(coo_data + coo_data)
+    W = scipy.sparse.csr_matrix((coo_data, (ij, ji)), (n, n))
+    rs = W.dot(np.ones(n))
+    W = scipy.sparse.diags(1.0 / rs).dot(W)
+    return scipy.sparse.identity(n) - W

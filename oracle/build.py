@@ -10,7 +10,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ["cf_laplacian.c", "ichol.c", "foreground.c"]
+SOURCES = ["cf_laplacian.c", "ichol.c", "foreground.c", "knn.c"]
 TARGET = os.path.join(HERE, "liboracle.so")
 
 

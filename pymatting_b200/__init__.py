@@ -12,7 +12,7 @@ computed by hand-written sm_100a kernels behind a C ABI
 
 from .util import trimap_split, sanity_check_image
 from .laplacian import (cf_laplacian, make_linear_system, DeviceCSRMatrix, rw_laplacian,
-                        uniform_laplacian, lbdm_laplacian)
+                        uniform_laplacian, lbdm_laplacian, knn_laplacian)
 from .preconditioner import jacobi, vcycle, ichol, CholeskyDecomposition
 from .solver import cg, CounterCallback, ProgressCallback
 from .alpha import estimate_alpha_cf, estimate_alpha
@@ -29,5 +29,5 @@ __all__ = [
     "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
     "lkm_laplacian", "estimate_alpha_lkm", "estimate_foreground_ml",
     "estimate_foreground_ml_cupy", "cutout", "load_image", "save_image", "stack_images", "blend",
-    "rw_laplacian", "uniform_laplacian", "lbdm_laplacian",
+    "rw_laplacian", "uniform_laplacian", "lbdm_laplacian", "knn_laplacian",
 ]

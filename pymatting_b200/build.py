@@ -27,6 +27,7 @@ SOURCES = {
     "foreground.cu": [],
     "foreground_jacobi.cu": [],
     "laplacians.cu": [],
+    "knn.cu": [],
     "ichol.cu": ["-fmad=false"],
     "engine.cu": [],
 }

@@ -1151,6 +1151,25 @@ PMB_API int pmb_lbdm_laplacian(const double* image, int h, int w, int radius, do
     return 0;
 }
 
+int64_t pmb_launch_knn_scratch(long long, int, int);
+int pmb_launch_knn(const double*, int, int, const int*, const double*, int, int, int64_t*,
+                   int64_t*, int64_t*, double*, int64_t*, cudaStream_t);
+
+PMB_API int64_t pmb_knn_scratch_elems(int64_t n, int total_neighbors, int passes) {
+    return pmb_launch_knn_scratch((long long)n, total_neighbors, passes);
+}
+
+PMB_API int pmb_knn_laplacian(const double* image, int h, int w, const int* n_neighbors,
+                              const double* distance_weights, int passes, int soft,
+                              int64_t* scratch, int64_t* rowptr, int64_t* cols, double* vals,
+                              int64_t* nnz, void* stream) {
+    const int rc = pmb_launch_knn(image, h, w, n_neighbors, distance_weights, passes, soft, scratch,
+                                  rowptr, cols, vals, nnz, (cudaStream_t)stream);
+    if (rc == -2) return fail(kErrArg, "pmb_knn_laplacian: bad arguments (1 to 4 passes of 1 to 64 neighbours, at most the pixel count)");
+    if (rc) return fail(kErrCuda, std::string("pmb_knn_laplacian: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, const uint8_t* is_fg,
                                int h, int w, double epsilon, double* planes, double* rhs,
                                void* stream) {

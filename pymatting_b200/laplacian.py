@@ -22,7 +22,7 @@ from . import _device as dev
 from . import _ffi
 from .util import trimap_split
 
-__all__ = ["cf_laplacian", "uniform_laplacian", "rw_laplacian", "lbdm_laplacian",
+__all__ = ["cf_laplacian", "uniform_laplacian", "rw_laplacian", "lbdm_laplacian", "knn_laplacian",
            "make_linear_system",
            "DeviceCSRMatrix", "CFSource", "device_source", "device_csr_arrays"]
 
@@ -338,3 +338,43 @@ def lbdm_laplacian(image, epsilon=1e-7, radius=1):
                                       dev.ptr(cols), dev.ptr(vals), dev.stream()),
                "pmb_lbdm_laplacian")
     return DeviceCSRMatrix(shape=(n, n), pmb_arrays=(rowptr, cols, vals))
+
+
+def knn_laplacian(image, n_neighbors=[20, 10], distance_weights=[2.0, 0.1], kernel="binary"):
+    """k-nearest-neighbour Laplacian: pymatting/laplacian/knn_laplacian.py.
+
+    For each (k, weight) pass, the k nearest pixels in the float32 feature
+    space (r, g, b, weight x, weight y) are found by an exact search on the
+    device with the reference k-d tree's insertion rule. Equal distances are
+    resolved by pixel index where the reference resolves them in its tree
+    order. The search is O(n^2) per pass. W = sum of B + B^T (binary or soft
+    weights), L = I - D^-1 W as canonical CSR on the device.
+    """
+    if kernel not in ["binary", "soft"]:
+        raise ValueError("kernel must be binary/soft, but not " + kernel + ".")
+    h, w = image.shape[:2]
+    n = h * w
+    ks = np.ascontiguousarray(list(n_neighbors), dtype=np.int32)
+    dws = np.ascontiguousarray(list(distance_weights), dtype=np.float64)
+    passes = min(len(ks), len(dws))
+    ks, dws = ks[:passes], dws[:passes]
+    lib = _ffi.lib()
+    img = _image_to_device(image)
+    elems = int(lib.pmb_knn_scratch_elems(n, int(ks.sum()), passes))
+    if elems <= 0:
+        raise ValueError("knn_laplacian: unsupported neighbour counts %r" % (list(ks),))
+    scratch = dev.empty(elems, torch.int64)
+    rowptr = dev.empty(n + 1, torch.int64)
+    nnz = np.zeros(1, dtype=np.int64)
+    soft = 1 if kernel == "soft" else 0
+    _ffi.check(lib.pmb_knn_laplacian(dev.ptr(img), h, w, ks.ctypes.data, dws.ctypes.data,
+                                     passes, soft, dev.ptr(scratch), dev.ptr(rowptr), None, None,
+                                     nnz.ctypes.data, dev.stream()), "pmb_knn_laplacian")
+    m = int(nnz[0])
+    cols = dev.empty(max(m, 1), torch.int64)
+    vals = dev.empty(max(m, 1), torch.float64)
+    _ffi.check(lib.pmb_knn_laplacian(dev.ptr(img), h, w, ks.ctypes.data, dws.ctypes.data,
+                                     passes, soft, dev.ptr(scratch), dev.ptr(rowptr),
+                                     dev.ptr(cols), dev.ptr(vals), nnz.ctypes.data, dev.stream()),
+               "pmb_knn_laplacian")
+    return DeviceCSRMatrix(shape=(n, n), pmb_arrays=(rowptr, cols[:m], vals[:m]))

@@ -388,6 +388,26 @@ def gen_laplacians(pm, root, rng):
         out[f"lbdm{k}_indptr"] = L.indptr.astype(np.int64)
         out[f"lbdm{k}_indices"] = L.indices.astype(np.int64)
         out[f"lbdm{k}_data"] = L.data
+    A, b = pm.make_linear_system(pm.knn_laplacian(image), trimap)
+    x = scipy.sparse.linalg.spsolve(A, b)
+    alpha = np.clip(x, 0, 1).reshape(trimap.shape)
+    out["lemur_knn_error"] = np.array([np.linalg.norm(np.abs(alpha - good)[is_unknown])])
+    kc = [((6, 7), "binary"), ((9, 8), "soft"), ((13, 17), "binary"), ((20, 15), "soft")]
+    out["knn_n"] = np.array([len(kc)])
+    for k, ((h, w), kern) in enumerate(kc):
+        img = rng.random((h, w, 3))
+        L = scipy.sparse.csr_matrix(pm.knn_laplacian(img, kernel=kern))
+        L.sum_duplicates()
+        L.sort_indices()
+        out[f"knn{k}_image"], out[f"knn{k}_soft"] = img, np.array([kern == "soft"])
+        out[f"knn{k}_indptr"] = L.indptr.astype(np.int64)
+        out[f"knn{k}_indices"] = L.indices.astype(np.int64)
+        out[f"knn{k}_data"] = L.data
+    L = scipy.sparse.csr_matrix(pm.knn_laplacian(image))
+    L.sum_duplicates()
+    L.sort_indices()
+    out["lemur_knn_indptr"], out["lemur_knn_indices"] = L.indptr.astype(np.int64), L.indices.astype(np.int64)
+    out["lemur_knn_data"] = L.data
     out["lemur_image"], out["lemur_trimap"], out["lemur_good"] = image, trimap, good
     np.savez_compressed(os.path.join(HERE, "laplacians_small.npz"), **out)
 

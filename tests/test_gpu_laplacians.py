@@ -102,3 +102,49 @@ def test_lbdm_larger_against_oracle_and_lemur_error(gpu):
     expected = float(g["lemur_lbdm_error"][0])
     assert (error - expected) / expected <= 0.01
     assert abs(error - expected) <= 1e-5 * expected, (error, expected)
+
+
+def _knn_ref(g, prefix, n):
+    return scipy.sparse.csr_matrix((g[prefix + "_data"], g[prefix + "_indices"],
+                                    g[prefix + "_indptr"]), shape=(n, n))
+
+
+def test_knn_matches_reference_and_oracle(gpu):
+    """Same neighbour rule and candidate order as the oracle: identical
+    matrices. Against the reference: identical on random images; on the
+    lemur image rows whose k-th neighbour is tied may differ (the reference
+    resolves ties in its k-d tree's order)."""
+    import pymatting_b200 as pm
+    g = golden("laplacians_small.npz")
+    for k in range(int(g["knn_n"][0])):
+        img = g[f"knn{k}_image"]
+        n = img.shape[0] * img.shape[1]
+        kern = "soft" if g[f"knn{k}_soft"][0] else "binary"
+        L = pm.knn_laplacian(img, kernel=kern)
+        assert _maxdiff(L, _knn_ref(g, f"knn{k}", n)) == 0.0, k
+    img = g["lemur_image"]
+    n = img.shape[0] * img.shape[1]
+    L = pm.knn_laplacian(img)
+    Lo = scipy.sparse.csr_matrix(oracle.knn_laplacian(img))
+    Lo.sum_duplicates()
+    Lo.sort_indices()
+    assert np.array_equal(L.indptr, Lo.indptr) and np.array_equal(L.indices, Lo.indices)
+    assert np.array_equal(L.data, Lo.data)
+    D = (scipy.sparse.csr_matrix(L) - _knn_ref(g, "lemur_knn", n)).tocsr()
+    D.eliminate_zeros()
+    assert np.count_nonzero(np.diff(D.indptr)) <= 5
+
+
+def test_knn_lemur_error_and_errors(gpu):
+    import scipy.sparse.linalg
+    import pymatting_b200 as pm
+    g = golden("laplacians_small.npz")
+    image, trimap, good = g["lemur_image"], g["lemur_trimap"], g["lemur_good"]
+    is_unknown = pm.trimap_split(trimap, flatten=False)[3]
+    A, b = pm.make_linear_system(pm.knn_laplacian(image), trimap)
+    x = scipy.sparse.linalg.spsolve(scipy.sparse.csr_matrix(A), b)
+    error = np.linalg.norm(np.abs(np.clip(x, 0, 1).reshape(trimap.shape) - good)[is_unknown])
+    expected = float(g["lemur_knn_error"][0])
+    assert (error - expected) / expected <= 0.01, (error, expected)
+    with pytest.raises(ValueError):
+        pm.knn_laplacian(image, kernel="gaussian")

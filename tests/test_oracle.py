@@ -249,3 +249,27 @@ def test_oracle_lbdm_matches_reference():
                                      g[f"lbdm{k}_indptr"]), shape=(n, n))
         D = abs(oracle.lbdm_laplacian(img, radius=r) - R)
         assert (D.max() if D.nnz else 0.0) <= 1e-8 * max(abs(R).max(), 1.0), k
+
+
+def test_oracle_knn_laplacian_matches_reference():
+    """The index-order search with the k-d tree's insertion rule gives the
+    reference's knn_laplacian exactly on random images (binary and soft);
+    on the lemur image only rows whose k-th neighbour is tied can differ."""
+    g = golden("laplacians_small.npz")
+
+    def ref(prefix, n):
+        return scipy.sparse.csr_matrix((g[prefix + "_data"], g[prefix + "_indices"],
+                                        g[prefix + "_indptr"]), shape=(n, n))
+
+    for k in range(int(g["knn_n"][0])):
+        img = g[f"knn{k}_image"]
+        n = img.shape[0] * img.shape[1]
+        L = oracle.knn_laplacian(img, kernel="soft" if g[f"knn{k}_soft"][0] else "binary")
+        D = abs(scipy.sparse.csr_matrix(L) - ref(f"knn{k}", n))
+        assert (D.max() if D.nnz else 0.0) == 0.0, k
+    img = g["lemur_image"]
+    n = img.shape[0] * img.shape[1]
+    L = scipy.sparse.csr_matrix(oracle.knn_laplacian(img))
+    D = (L - ref("lemur_knn", n)).tocsr()
+    D.eliminate_zeros()
+    assert np.count_nonzero(np.diff(D.indptr)) <= 5
