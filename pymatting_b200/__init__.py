@@ -15,7 +15,8 @@ from .laplacian import (cf_laplacian, make_linear_system, DeviceCSRMatrix, rw_la
                         uniform_laplacian, lbdm_laplacian, knn_laplacian)
 from .preconditioner import jacobi, vcycle, ichol, CholeskyDecomposition
 from .solver import cg, CounterCallback, ProgressCallback
-from .alpha import estimate_alpha_cf, estimate_alpha
+from .alpha import (estimate_alpha_cf, estimate_alpha, estimate_alpha_knn, estimate_alpha_lbdm,
+                    estimate_alpha_rw)
 from .autograd import cf_alpha
 from .lkm import lkm_laplacian, estimate_alpha_lkm
 from .foreground import estimate_foreground_ml, estimate_foreground_ml_cupy
@@ -29,5 +30,9 @@ __all__ = [
     "CounterCallback", "ProgressCallback", "estimate_alpha_cf", "estimate_alpha", "cf_alpha",
     "lkm_laplacian", "estimate_alpha_lkm", "estimate_foreground_ml",
     "estimate_foreground_ml_cupy", "cutout", "load_image", "save_image", "stack_images", "blend",
-    "rw_laplacian", "uniform_laplacian", "lbdm_laplacian", "knn_laplacian",
+    "rw_laplacian", "uniform_laplacian", "lbdm_laplacian", "knn_laplacian", "LAPLACIANS",
+    "estimate_alpha_knn", "estimate_alpha_lbdm", "estimate_alpha_rw",
 ]
+
+# the reference's list (pymatting/laplacian/__init__.py)
+LAPLACIANS = [cf_laplacian, knn_laplacian, lbdm_laplacian, rw_laplacian, uniform_laplacian]

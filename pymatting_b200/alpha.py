@@ -19,7 +19,8 @@ from .preconditioner import ichol
 from .solver import cg
 from .util import sanity_check_image, trimap_split
 
-__all__ = ["estimate_alpha_cf", "estimate_alpha"]
+__all__ = ["estimate_alpha_cf", "estimate_alpha", "estimate_alpha_knn", "estimate_alpha_lbdm",
+           "estimate_alpha_rw"]
 
 
 def hard_system(image, trimap, epsilon=1e-7, radius=1, is_fg=None, is_known=None):
@@ -99,3 +100,42 @@ def estimate_alpha_cf(image, trimap, preconditioner=None, laplacian_kwargs={}, c
 
 
 estimate_alpha = estimate_alpha_cf
+
+
+def _estimate_alpha_with(laplacian, default_preconditioner, image, trimap, preconditioner,
+                         laplacian_kwargs, cg_kwargs):
+    """make_linear_system(laplacian(image), trimap), preconditioned cg, clip:
+    the common body of estimate_alpha_knn / _lbdm / _rw."""
+    from .laplacian import make_linear_system
+    if preconditioner is None:
+        preconditioner = default_preconditioner
+    sanity_check_image(image)
+    A, b = make_linear_system(laplacian(image, **laplacian_kwargs), trimap)
+    x = cg(A, b, M=preconditioner(A), **cg_kwargs)
+    return np.clip(x, 0, 1).reshape(trimap.shape)
+
+
+def estimate_alpha_knn(image, trimap, preconditioner=None, laplacian_kwargs={}, cg_kwargs={}):
+    """pymatting/alpha/estimate_alpha_knn.py: knn_laplacian, Jacobi-
+    preconditioned cg (by default), clipped."""
+    from .laplacian import knn_laplacian
+    from .preconditioner import jacobi
+    return _estimate_alpha_with(knn_laplacian, jacobi, image, trimap, preconditioner,
+                                laplacian_kwargs, cg_kwargs)
+
+
+def estimate_alpha_lbdm(image, trimap, preconditioner=None, laplacian_kwargs={}, cg_kwargs={}):
+    """pymatting/alpha/estimate_alpha_lbdm.py: lbdm_laplacian, ichol-
+    preconditioned cg (by default), clipped."""
+    from .laplacian import lbdm_laplacian
+    return _estimate_alpha_with(lbdm_laplacian, ichol, image, trimap, preconditioner,
+                                laplacian_kwargs, cg_kwargs)
+
+
+def estimate_alpha_rw(image, trimap, preconditioner=None, laplacian_kwargs={}, cg_kwargs={}):
+    """pymatting/alpha/estimate_alpha_rw.py: rw_laplacian, Jacobi-
+    preconditioned cg (by default), clipped."""
+    from .laplacian import rw_laplacian
+    from .preconditioner import jacobi
+    return _estimate_alpha_with(rw_laplacian, jacobi, image, trimap, preconditioner,
+                                laplacian_kwargs, cg_kwargs)

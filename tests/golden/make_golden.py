@@ -408,6 +408,9 @@ def gen_laplacians(pm, root, rng):
     L.sort_indices()
     out["lemur_knn_indptr"], out["lemur_knn_indices"] = L.indptr.astype(np.int64), L.indices.astype(np.int64)
     out["lemur_knn_data"] = L.data
+    for name, fn in (("knn", pm.estimate_alpha_knn), ("lbdm", pm.estimate_alpha_lbdm),
+                     ("rw", pm.estimate_alpha_rw)):
+        out[f"lemur_alpha_{name}"] = fn(image, trimap)
     out["lemur_image"], out["lemur_trimap"], out["lemur_good"] = image, trimap, good
     np.savez_compressed(os.path.join(HERE, "laplacians_small.npz"), **out)
 

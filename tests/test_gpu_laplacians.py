@@ -150,3 +150,25 @@ def test_knn_lemur_error_and_errors(gpu):
     assert (error - expected) / expected <= 0.01, (error, expected)
     with pytest.raises(ValueError):
         pm.knn_laplacian(image, kernel="gaussian")
+
+
+@pytest.mark.parametrize("name,limit,tol", [("knn", 2.2, 1e-3), ("lbdm", 1.68, 1e-4),
+                                            ("rw", 6.0, 1e-4)])
+def test_other_alpha_estimators(gpu, name, limit, tol):
+    """tests/test_estimate_alpha.py of the reference (error against the good
+    alpha below its limit) and the reference's own alpha for the same lemur
+    inputs: mean difference within `tol` (CG stops at rtol 1e-7; the knn
+    matrix differs in the rows with tied neighbours)."""
+    import pymatting_b200 as pm
+    g = golden("laplacians_small.npz")
+    image, trimap, good = g["lemur_image"], g["lemur_trimap"], g["lemur_good"]
+    alpha = getattr(pm, "estimate_alpha_" + name)(image, trimap)
+    assert alpha.shape == trimap.shape
+    assert np.linalg.norm(alpha - good) < limit
+    assert np.abs(alpha - g["lemur_alpha_" + name]).mean() <= tol
+
+
+def test_laplacians_list(gpu):
+    import pymatting_b200 as pm
+    assert [f.__name__ for f in pm.LAPLACIANS] == [
+        "cf_laplacian", "knn_laplacian", "lbdm_laplacian", "rw_laplacian", "uniform_laplacian"]
