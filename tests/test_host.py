@@ -167,3 +167,31 @@ def test_foreground_level_plan_matches_oracle():
         foreground_levels(1, 1)
     with pytest.raises(ZeroDivisionError):
         oracle.fg_levels(1, 1)
+
+
+def test_window_extent_prefixes_match_brute_force():
+    """Row-pointer prefixes of the device Laplacians (host side): the
+    clamped-window widths of uniform/rw and the shared-window widths of lbdm,
+    against direct counts."""
+    from pymatting_b200.laplacian import _lbdm_extents, _window_extents
+    for n in (1, 2, 3, 5, 8, 17):
+        for r in (1, 2, 3):
+            brute = [len({min(max(v + d, 0), n - 1) for d in range(-r, r + 1)}) for v in range(n)]
+            assert list(np.diff(_window_extents(n, r))) == brute, (n, r)
+            if n > 2 * r:
+                centres = range(r, n - r)
+                brute = []
+                for v in range(n):
+                    cs = [c for c in centres if abs(c - v) <= r]
+                    brute.append(len({q for c in cs for q in range(c - r, c + r + 1)}))
+                assert list(np.diff(_lbdm_extents(n, r))) == brute, (n, r)
+
+
+def test_laplacian_argument_errors():
+    """Errors raised on the host before any device work, as in the reference."""
+    import pymatting_b200 as pm
+    img = np.zeros((6, 7, 3))
+    with pytest.raises(ValueError):
+        pm.knn_laplacian(img, kernel="gaussian")
+    with pytest.raises(NotImplementedError):
+        pm.lbdm_laplacian(img, radius=3)
