@@ -711,8 +711,8 @@ def lbdm_laplacian(image, epsilon=1e-7, radius=1):
 
 
 def knn(f, k):
-    """Indices of the k nearest feature rows of every row (oracle/knn.c:
-    the k-d tree's insertion rule, candidates in index order)."""
+    """Indices of the k nearest feature rows of every row (oracle/knn.c: the
+    k-d tree's distance, the k smallest by (distance, index))."""
     lib = _load()
     f = np.ascontiguousarray(f, dtype=np.float32)
     n, dims = f.shape

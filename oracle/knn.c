@@ -1,17 +1,17 @@
 /* ORACLE — test infrastructure, not product code.
  *
- * Exact k-nearest-neighbour search with the insertion rule of PyMatting's
- * k-d tree (pymatting/util/kdtree.py:_find_knn, :129-199): the squared
- * distance accumulates float32 squared differences in float64 (numba types
- * `distance = 0.0` as float64), is stored as float32, and a candidate is
- * inserted before the first stored distance that is strictly larger.
- * Candidates are visited in index order here; the reference visits them in
- * its tree order, which only matters among points at equal distance.
+ * Exact k-nearest-neighbour search with the distance of PyMatting's k-d
+ * tree (pymatting/util/kdtree.py:_find_knn, :129-199): float32 squared
+ * differences accumulated in float64 (numba types `distance = 0.0` as
+ * float64). The k smallest by (distance, index) are kept, which is
+ * independent of the visiting order. The reference keeps the first found
+ * among equal (and float32-equal) distances in its tree order, so the two
+ * differ only where the k-th distance is tied.
  */
 #include <stdint.h>
 
 void oracle_knn(const float* f, int64_t n, int dims, int k, int64_t* out) {
-    float D[256];
+    double D[256];
     int64_t I[256];
     for (int64_t q = 0; q < n; ++q) {
         int cnt = 0;
@@ -21,18 +21,19 @@ void oracle_knn(const float* f, int64_t n, int dims, int k, int64_t* out) {
                 float dd = f[q * dims + d] - f[c * dims + d];
                 dist += (double)(dd * dd);
             }
-            int pos = cnt;
-            for (int j = cnt - 1; j >= 0; --j)
-                if ((double)D[j] > dist) pos = j;
-            if (pos < k) {
-                for (int j = (cnt < k - 1 ? cnt : k - 1); j > pos; --j) {
-                    D[j] = D[j - 1];
-                    I[j] = I[j - 1];
+            /* keep the k smallest by (distance, index) */
+            if (cnt == k && !(dist < D[k - 1] || (dist == D[k - 1] && c < I[k - 1]))) continue;
+            int pos = cnt < k ? cnt : k - 1;
+            while (pos > 0 && (D[pos - 1] > dist || (D[pos - 1] == dist && I[pos - 1] > c))) {
+                if (pos < k) {
+                    D[pos] = D[pos - 1];
+                    I[pos] = I[pos - 1];
                 }
-                D[pos] = (float)dist;
-                I[pos] = c;
-                cnt = cnt + 1 < k ? cnt + 1 : k;
+                --pos;
             }
+            D[pos] = dist;
+            I[pos] = c;
+            if (cnt < k) ++cnt;
         }
         for (int j = 0; j < k; ++j) out[q * k + j] = I[j];
     }

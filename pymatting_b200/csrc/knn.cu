@@ -3,13 +3,12 @@
 //
 // Features per pixel: (r, g, b, dw x, dw y) in float32 with x, y the
 // numpy.linspace(0, 1, .) grids, one pass per (k, dw). Neighbours come from
-// an exact brute-force search with the reference's k-d tree insertion rule
-// (pymatting/util/kdtree.py:_find_knn): distances accumulate float32 squared
-// differences in float64, are stored as float32, and a candidate goes
-// before the first stored distance that is larger. Candidates are visited in
-// index order, so among points at exactly equal distance the lower index
-// wins, where the reference's tree visits them in tree order. The search
-// costs O(n^2) per pass.
+// an exact search with the reference k-d tree's distance
+// (pymatting/util/kdtree.py:_find_knn: float32 squared differences summed in
+// float64), keeping the k smallest by (distance, index). Candidate tiles of
+// 256 pixels whose bounding box is farther than every query's k-th distance
+// are skipped. The reference keeps the first found among equal distances in
+// its tree order, so the two differ only where the k-th distance is tied.
 //
 // W = sum over passes of B + B^T (B_ij = 1, or 1 - |f_i - f_j|_1 / 5 for the
 // soft kernel), assembled per row: the row's own neighbours, then the rows
@@ -48,45 +47,86 @@ __global__ void k_features(const double* __restrict__ image, int h, int w, doubl
 
 constexpr int kTile = 256;
 
-// One thread per query; candidates staged through shared memory in tiles.
-__global__ void __launch_bounds__(kTile) k_knn(const float* __restrict__ f, long long n, int k,
+// Bounding box of every tile of kTile consecutive feature rows: lo[5], hi[5].
+__global__ void k_tile_boxes(const float* __restrict__ f, long long n, float* __restrict__ box) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ntiles = (n + kTile - 1) / kTile;
+    if (t >= ntiles) return;
+    float lo[kDims], hi[kDims];
+    for (int d = 0; d < kDims; ++d) lo[d] = hi[d] = f[t * kTile * kDims + d];
+    const long long end = min(n, (t + 1) * kTile);
+    for (long long i = t * kTile + 1; i < end; ++i)
+        for (int d = 0; d < kDims; ++d) {
+            lo[d] = fminf(lo[d], f[i * kDims + d]);
+            hi[d] = fmaxf(hi[d], f[i * kDims + d]);
+        }
+    for (int d = 0; d < kDims; ++d) {
+        box[t * 2 * kDims + d] = lo[d];
+        box[t * 2 * kDims + kDims + d] = hi[d];
+    }
+}
+
+// One thread per query, one CTA per tile of queries. Candidate tiles are
+// visited with the query tile first; a tile is skipped when, for every
+// query of the CTA with a full list, the lower bound of the distance to the
+// tile's box exceeds the k-th distance (with a 1e-5 relative margin over the
+// float32 rounding of the computed distances). The k smallest by
+// (distance, index) are kept, so the visiting order does not change them.
+__global__ void __launch_bounds__(kTile) k_knn(const float* __restrict__ f,
+                                               const float* __restrict__ box, long long n, int k,
                                                int64_t* __restrict__ nbr) {
     __shared__ float tile[kTile * kDims];
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ntiles = (n + kTile - 1) / kTile;
     float qf[kDims];
 #pragma unroll
     for (int d = 0; d < kDims; ++d) qf[d] = q < n ? f[q * kDims + d] : 0.f;
-    float D[kMaxK];
+    double D[kMaxK];
     int64_t I[kMaxK];
     int cnt = 0;
-    for (long long t0 = 0; t0 < n; t0 += kTile) {
-        __syncthreads();
+    for (long long vt = 0; vt < ntiles; ++vt) {
+        // visiting order: own tile, then the others in index order
+        const long long tt = vt == 0 ? blockIdx.x : (vt <= blockIdx.x ? vt - 1 : vt);
+        bool need = q < n;
+        if (need && cnt == k) {
+            double lb = 0.0;
+#pragma unroll
+            for (int d = 0; d < kDims; ++d) {
+                const double lo = box[tt * 2 * kDims + d], hi = box[tt * 2 * kDims + kDims + d];
+                const double v = qf[d];
+                const double e = v < lo ? lo - v : (v > hi ? v - hi : 0.0);
+                lb += e * e;
+            }
+            need = !(lb > D[k - 1] * (1.0 + 1e-5));
+        }
+        if (!__syncthreads_or(need)) continue;
+        const long long t0 = tt * kTile;
         const int m = (int)min((long long)kTile, n - t0);
         for (int e = threadIdx.x; e < m * kDims; e += blockDim.x) tile[e] = f[t0 * kDims + e];
         __syncthreads();
-        if (q >= n) continue;
-        for (int c = 0; c < m; ++c) {
-            double dist = 0.0;
+        if (need) {
+            for (int c = 0; c < m; ++c) {
+                double dist = 0.0;
 #pragma unroll
-            for (int d = 0; d < kDims; ++d) {
-                const float dd = __fsub_rn(qf[d], tile[c * kDims + d]);
-                dist = __dadd_rn(dist, (double)__fmul_rn(dd, dd));
-            }
-            if (cnt == k && !((double)D[k - 1] > dist)) continue;
-            int pos = cnt;
-            for (int j = 0; j < cnt; ++j)
-                if ((double)D[j] > dist) {
-                    pos = j;
-                    break;
+                for (int d = 0; d < kDims; ++d) {
+                    const float dd = __fsub_rn(qf[d], tile[c * kDims + d]);
+                    dist = __dadd_rn(dist, (double)__fmul_rn(dd, dd));
                 }
-            if (pos >= k) continue;
-            for (int j = min(cnt, k - 1); j > pos; --j) {
-                D[j] = D[j - 1];
-                I[j] = I[j - 1];
+                const long long ci = t0 + c;
+                if (cnt == k && !(dist < D[k - 1] || (dist == D[k - 1] && ci < I[k - 1])))
+                    continue;
+                int pos = cnt < k ? cnt : k - 1;
+                while (pos > 0 && (D[pos - 1] > dist || (D[pos - 1] == dist && I[pos - 1] > ci))) {
+                    if (pos < k) {
+                        D[pos] = D[pos - 1];
+                        I[pos] = I[pos - 1];
+                    }
+                    --pos;
+                }
+                D[pos] = dist;
+                I[pos] = ci;
+                if (cnt < k) ++cnt;
             }
-            D[pos] = (float)dist;
-            I[pos] = t0 + c;
-            cnt = min(cnt + 1, k);
         }
     }
     if (q < n)
@@ -210,7 +250,8 @@ using namespace pmb::knn;
 int64_t pmb_launch_knn_scratch(long long n, int kt, int np) {
     if (n <= 0 || kt <= 0 || np <= 0 || np > 4) return -1;
     const long long feat = (n * kDims * np * 4 + 7) / 8;  // floats -> int64 slots
-    return feat + n * kt + 4 * (n + 1) + ((n + 1) + 1023) / 1024 + 2 + 2 * (2 * n * kt);
+    const long long boxes = (((n + kTile - 1) / kTile) * 2 * kDims * 4 + 7) / 8;
+    return feat + boxes + n * kt + 4 * (n + 1) + ((n + 1) + 1023) / 1024 + 2 + 2 * (2 * n * kt);
 }
 
 // Two calls on the same scratch and rowptr. First (cols / vals null): the
@@ -229,6 +270,8 @@ int pmb_launch_knn(const double* image, int h, int w, const int* ks, const doubl
     }
     float* feat = (float*)scratch;
     int64_t* s = scratch + (n * kDims * np * 4 + 7) / 8;
+    float* boxes = (float*)s;
+    s += (((n + kTile - 1) / kTile) * 2 * kDims * 4 + 7) / 8;
     int64_t* nbr = s;
     s += n * kt;
     int64_t* cap = s;
@@ -256,7 +299,9 @@ int pmb_launch_knn(const double* image, int h, int w, const int* ks, const doubl
     for (int p = 0; p < np; ++p) {
         float* fp = feat + (long long)p * n * kDims;
         k_features<<<blocks, 256, 0, st>>>(image, h, w, dws[p], fp);
-        k_knn<<<(unsigned)((n + kTile - 1) / kTile), kTile, 0, st>>>(fp, n, ks[p], nb);
+        const long long ntiles = (n + kTile - 1) / kTile;
+        k_tile_boxes<<<(unsigned)((ntiles + 127) / 128), 128, 0, st>>>(fp, n, boxes);
+        k_knn<<<(unsigned)ntiles, kTile, 0, st>>>(fp, boxes, n, ks[p], nb);
         P.p[p] = Pass{nb, fp, ks[p]};
         nb += n * ks[p];
     }

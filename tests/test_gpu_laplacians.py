@@ -172,3 +172,18 @@ def test_laplacians_list(gpu):
     import pymatting_b200 as pm
     assert [f.__name__ for f in pm.LAPLACIANS] == [
         "cf_laplacian", "knn_laplacian", "lbdm_laplacian", "rw_laplacian", "uniform_laplacian"]
+
+
+def test_knn_pruned_search_on_a_larger_image(gpu):
+    """96x128 pixels, 48 candidate tiles, so tile pruning is exercised:
+    identical to the oracle's brute force."""
+    import pymatting_b200 as pm
+    from pymatting_b200.synthetic import make_matting_problem
+    img, _, _, _ = make_matting_problem(96, 128, 3, sigma=2.0, band=5, unknown_fraction=0.1)
+    for kern in ("binary", "soft"):
+        L = pm.knn_laplacian(img, kernel=kern)
+        Lo = scipy.sparse.csr_matrix(oracle.knn_laplacian(img, kernel=kern))
+        Lo.sum_duplicates()
+        Lo.sort_indices()
+        assert np.array_equal(L.indptr, Lo.indptr) and np.array_equal(L.indices, Lo.indices)
+        assert np.array_equal(L.data, Lo.data)
