@@ -160,8 +160,9 @@ int pmb_lbdm_laplacian(const double* image, int h, int w, int radius, double eps
 /* Replace knn_laplacian(image, n_neighbors, distance_weights, kernel)
  * (pymatting/laplacian/knn_laplacian.py): per pass p, the n_neighbors[p]
  * nearest pixels in the float32 feature space (r, g, b, dw x, dw y) by an
- * exact search with the insertion rule of pymatting/util/kdtree.py (equal
- * distances resolved by index, not by tree order; O(n^2) per pass);
+ * exact search with the distance of pymatting/util/kdtree.py, keeping the k
+ * smallest by (distance, index) (the reference resolves equal distances in
+ * its tree order);
  * W = sum_p B_p + B_p^T (soft != 0: weights 1 - |f_i - f_j|_1 / 5);
  * L = I - diag(1 / rowsum(W)) W as canonical CSR. Two calls on the same
  * scratch (pmb_knn_scratch_elems int64) and rowptr (h w + 1): the first with

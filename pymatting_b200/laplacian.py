@@ -345,10 +345,11 @@ def knn_laplacian(image, n_neighbors=[20, 10], distance_weights=[2.0, 0.1], kern
 
     For each (k, weight) pass, the k nearest pixels in the float32 feature
     space (r, g, b, weight x, weight y) are found by an exact search on the
-    device with the reference k-d tree's insertion rule. Equal distances are
-    resolved by pixel index where the reference resolves them in its tree
-    order. The search is O(n^2) per pass. W = sum of B + B^T (binary or soft
-    weights), L = I - D^-1 W as canonical CSR on the device.
+    device with the reference k-d tree's distance, keeping the k smallest by
+    (distance, index); the reference resolves equal distances in its tree
+    order. Candidate tiles are pruned by their bounding boxes. W = sum of
+    B + B^T (binary or soft weights), L = I - D^-1 W as canonical CSR on the
+    device.
     """
     if kernel not in ["binary", "soft"]:
         raise ValueError("kernel must be binary/soft, but not " + kernel + ".")
