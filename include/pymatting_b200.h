@@ -174,6 +174,16 @@ int pmb_knn_laplacian(const double* image, int h, int w, const int* n_neighbors,
                       const double* distance_weights, int passes, int soft, int64_t* scratch,
                       int64_t* rowptr, int64_t* cols, double* vals, int64_t* nnz, void* stream);
 
+/* System matrix of estimate_foreground_cf
+ * (pymatting/foreground/estimate_foreground_cf.py) for the default
+ * neighbours: A = U^T U + diag(S, S) over 2 h w unknowns (foreground, then
+ * background) as canonical CSR. Two calls: with cols = vals = null it writes
+ * rowptr (2 h w + 1; the entry count is rowptr[2 h w]); then it fills cols
+ * and vals. alpha: (h, w) float64 on the device; scratch:
+ * (2 h w + 1023) / 1024 + 2 int64. */
+int pmb_fg_cf_system(const double* alpha, int h, int w, double regularization, int64_t* rowptr,
+                     int64_t* cols, double* vals, int64_t* scratch, void* stream);
+
 /* Hard-constraint system of estimate_alpha_cf
  * (pymatting/alpha/estimate_alpha_cf.py:64-74) on the full grid: planes of
  * L_U with identity rows for known pixels, and rhs = -R is_fg (0 on known

@@ -19,7 +19,8 @@ from .alpha import (estimate_alpha_cf, estimate_alpha, estimate_alpha_knn, estim
                     estimate_alpha_rw)
 from .autograd import cf_alpha
 from .lkm import lkm_laplacian, estimate_alpha_lkm
-from .foreground import estimate_foreground_ml, estimate_foreground_ml_cupy
+from .foreground import (estimate_foreground_ml, estimate_foreground_ml_cupy,
+                         estimate_foreground_cf)
 from .cutout import cutout, load_image, save_image, stack_images, blend
 
 __version__ = "0.1.0"
@@ -31,7 +32,7 @@ __all__ = [
     "lkm_laplacian", "estimate_alpha_lkm", "estimate_foreground_ml",
     "estimate_foreground_ml_cupy", "cutout", "load_image", "save_image", "stack_images", "blend",
     "rw_laplacian", "uniform_laplacian", "lbdm_laplacian", "knn_laplacian", "LAPLACIANS",
-    "estimate_alpha_knn", "estimate_alpha_lbdm", "estimate_alpha_rw",
+    "estimate_alpha_knn", "estimate_alpha_lbdm", "estimate_alpha_rw", "estimate_foreground_cf",
 ]
 
 # the reference's list (pymatting/laplacian/__init__.py)

@@ -47,6 +47,7 @@ _SIGNATURES = {
     "pmb_knn_scratch_elems": (c_i64, [c_i64, c_int, c_int]),
     "pmb_knn_laplacian": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp,
                                   c_vp, c_vp, c_vp]),
+    "pmb_fg_cf_system": (c_int, [c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_cf_hard_system": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_dbl, c_vp, c_vp, c_vp]),
     "pmb_scan_scratch_elems": (c_i64, [c_i64]),
     "pmb_ell_csr_rowptr": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp]),

@@ -1170,6 +1170,19 @@ PMB_API int pmb_knn_laplacian(const double* image, int h, int w, const int* n_ne
     return 0;
 }
 
+int pmb_launch_fg_cf_system(const double*, int, int, double, int64_t*, int64_t*, double*,
+                            int64_t*, cudaStream_t);
+
+PMB_API int pmb_fg_cf_system(const double* alpha, int h, int w, double regularization,
+                             int64_t* rowptr, int64_t* cols, double* vals, int64_t* scratch,
+                             void* stream) {
+    const int rc = pmb_launch_fg_cf_system(alpha, h, w, regularization, rowptr, cols, vals,
+                                           scratch, (cudaStream_t)stream);
+    if (rc == -2) return fail(kErrArg, "pmb_fg_cf_system: bad arguments");
+    if (rc) return fail(kErrCuda, std::string("pmb_fg_cf_system: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, const uint8_t* is_fg,
                                int h, int w, double epsilon, double* planes, double* rhs,
                                void* stream) {

@@ -267,3 +267,93 @@ int pmb_launch_lbdm_laplacian(const double* image, int h, int w, int r, double e
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
+
+// ---------------------------------------------------------------------------
+// System of estimate_foreground_cf (pymatting/foreground/estimate_foreground_cf.py)
+// for the default neighbours (-1,0), (1,0), (0,-1), (0,1):
+// A = U^T U + diag(S, S), U = [diag(a), diag(1 - a)],
+// S = sum_d D_d^T diag(reg + |D_d a|) D_d. For unit offsets every pair of
+// 4-neighbours p, q enters S twice (once from each direction) with weight
+// reg + |a_p - a_q|. Row p (foreground unknowns) holds its neighbours, p and
+// n + p; row n + p (background) holds p, then n + its neighbours and n + p.
+// ---------------------------------------------------------------------------
+
+namespace pmb {
+namespace fgcf {
+
+__device__ __forceinline__ int nbr_count(int y, int x, int h, int w) {
+    return (x > 0) + (x < w - 1) + (y > 0) + (y < h - 1);
+}
+
+// rowptr[r] before the scan: entries of row r (r < n: F rows, r >= n: B rows).
+__global__ void k_fgcf_count(int h, int w, int64_t* rowcnt) {
+    const long long n = (long long)h * w;
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= 2 * n) return;
+    const long long p = r < n ? r : r - n;
+    const int y = (int)(p / w), x = (int)(p % w);
+    rowcnt[r] = nbr_count(y, x, h, w) + 2;
+}
+
+__global__ void k_fgcf_fill(const double* __restrict__ a, int h, int w, double reg,
+                            const int64_t* __restrict__ rowptr, int64_t* __restrict__ cols,
+                            double* __restrict__ vals) {
+    const long long n = (long long)h * w;
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= 2 * n) return;
+    const bool brow = r >= n;
+    const long long p = brow ? r - n : r;
+    const int y = (int)(p / w), x = (int)(p % w);
+    const double ap = a[p];
+    // neighbours in ascending index order: up, left, right, down
+    long long q[4];
+    double wq[4];
+    int m = 0;
+    if (y > 0) { q[m] = p - w; ++m; }
+    if (x > 0) { q[m] = p - 1; ++m; }
+    if (x < w - 1) { q[m] = p + 1; ++m; }
+    if (y < h - 1) { q[m] = p + w; ++m; }
+    double spp = 0.0;
+    for (int t = 0; t < m; ++t) {
+        const double wt = __dadd_rn(reg, fabs(__dsub_rn(ap, a[q[t]])));
+        wq[t] = __dadd_rn(wt, wt);  // both directions of the pair
+        spp = __dadd_rn(spp, wq[t]);
+    }
+    const double a1 = __dsub_rn(1.0, ap);
+    long long o = rowptr[r];
+    if (!brow) {
+        int t = 0;
+        for (; t < m && q[t] < p; ++t, ++o) { cols[o] = q[t]; vals[o] = -wq[t]; }
+        cols[o] = p; vals[o] = __dadd_rn(__dmul_rn(ap, ap), spp); ++o;
+        for (; t < m; ++t, ++o) { cols[o] = q[t]; vals[o] = -wq[t]; }
+        cols[o] = n + p; vals[o] = __dmul_rn(ap, a1);
+    } else {
+        cols[o] = p; vals[o] = __dmul_rn(ap, a1); ++o;
+        int t = 0;
+        for (; t < m && q[t] < p; ++t, ++o) { cols[o] = n + q[t]; vals[o] = -wq[t]; }
+        cols[o] = n + p; vals[o] = __dadd_rn(__dmul_rn(a1, a1), spp); ++o;
+        for (; t < m; ++t, ++o) { cols[o] = n + q[t]; vals[o] = -wq[t]; }
+    }
+}
+
+}  // namespace fgcf
+}  // namespace pmb
+
+int pmb_scan_exclusive(int64_t* v, int64_t n, int64_t* chunk_scratch, int64_t* total,
+                       cudaStream_t s);
+
+// rowptr: 2 h w + 1; cols / vals: 2 (2 h w) + 2 * (number of neighbour pairs
+// counted per row) entries = rowptr[2 h w]; scratch: (2 h w + 1023) / 1024 + 2.
+int pmb_launch_fg_cf_system(const double* alpha, int h, int w, double reg, int64_t* rowptr,
+                            int64_t* cols, double* vals, int64_t* scratch, cudaStream_t st) {
+    if (!alpha || !rowptr || h <= 0 || w <= 0) return -2;
+    const long long n2 = 2LL * h * w;
+    const int blocks = (int)((n2 + 255) / 256);
+    if (!cols || !vals) {
+        pmb::fgcf::k_fgcf_count<<<blocks, 256, 0, st>>>(h, w, rowptr);
+        if (pmb_scan_exclusive(rowptr, n2, scratch, rowptr + n2, st)) return 1;
+        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    }
+    pmb::fgcf::k_fgcf_fill<<<blocks, 256, 0, st>>>(alpha, h, w, reg, rowptr, cols, vals);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

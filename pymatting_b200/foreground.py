@@ -25,7 +25,8 @@ import torch
 from . import _device as dev
 from . import _ffi
 
-__all__ = ["estimate_foreground_ml", "estimate_foreground_ml_cupy", "foreground_levels"]
+__all__ = ["estimate_foreground_ml", "estimate_foreground_ml_cupy", "estimate_foreground_cf",
+           "foreground_levels"]
 
 
 def foreground_levels(h, w, n_small_iterations=10, n_big_iterations=2, small_size=32):
@@ -126,3 +127,61 @@ def estimate_foreground_ml_cupy(input_image, input_alpha, regularization=1e-5,
     if return_background:
         return F, B
     return F
+
+
+def _fg_cf_matrix(alpha_t, h, w, regularization):
+    """Device CSR of A = U^T U + diag(S, S) (pmb_fg_cf_system)."""
+    from .laplacian import DeviceCSRMatrix
+    lib = _ffi.lib()
+    n2 = 2 * h * w
+    rowptr = dev.empty(n2 + 1, torch.int64)
+    scratch = dev.empty((n2 + 1023) // 1024 + 2, torch.int64)
+    _ffi.check(lib.pmb_fg_cf_system(dev.ptr(alpha_t), h, w, float(regularization),
+                                    dev.ptr(rowptr), None, None, dev.ptr(scratch), dev.stream()),
+               "pmb_fg_cf_system")
+    nnz = int(rowptr[n2].item())
+    cols = dev.empty(nnz, torch.int64)
+    vals = dev.empty(nnz, torch.float64)
+    _ffi.check(lib.pmb_fg_cf_system(dev.ptr(alpha_t), h, w, float(regularization),
+                                    dev.ptr(rowptr), dev.ptr(cols), dev.ptr(vals),
+                                    dev.ptr(scratch), dev.stream()), "pmb_fg_cf_system")
+    return DeviceCSRMatrix(shape=(n2, n2), pmb_arrays=(rowptr, cols, vals))
+
+
+def estimate_foreground_cf(image, alpha, regularization=1e-5, rtol=1e-5,
+                           neighbors=[(-1, 0), (1, 0), (0, -1), (0, 1)],
+                           return_background=False, foreground_guess=None,
+                           background_guess=None, ichol_kwargs={}, cg_kwargs={}):
+    """Closed-form foreground / background estimation:
+    pymatting/foreground/estimate_foreground_cf.py. The 2 h w system
+    A = U^T U + diag(S, S) is assembled on the device (default neighbours),
+    preconditioned with the device ``ichol`` and solved per colour channel
+    with the device ``cg`` from the image (or the guesses). Results are
+    clipped to [0, 1]; numpy arrays like the reference."""
+    from .preconditioner import ichol
+    from .solver import cg
+    if sorted(tuple(d) for d in neighbors) != [(-1, 0), (0, -1), (0, 1), (1, 0)]:
+        raise NotImplementedError("estimate_foreground_cf on the device supports the default "
+                                  "4-neighbourhood")
+    image = np.asarray(image)
+    h, w, d = image.shape
+    alpha = np.asarray(alpha)
+    assert alpha.shape == (h, w)
+    n = h * w
+    a = alpha.astype(np.float64).ravel()
+    A = _fg_cf_matrix(dev.to_device(a, torch.float64), h, w, regularization)
+    precondition = ichol(A, **ichol_kwargs)
+    foreground = (image if foreground_guess is None else foreground_guess).copy()
+    background = (image if background_guess is None else background_guess).copy()
+    for channel in range(d):
+        image_channel = image[:, :, channel].ravel()
+        b = np.concatenate([a * image_channel, (1 - a) * image_channel])
+        fb = np.concatenate([foreground[:, :, channel].ravel(), background[:, :, channel].ravel()])
+        fb = cg(A, b, x0=fb, M=precondition, rtol=rtol, **cg_kwargs)
+        foreground[:, :, channel] = fb[:n].reshape(h, w)
+        background[:, :, channel] = fb[n:].reshape(h, w)
+    foreground = np.clip(foreground, 0, 1)
+    background = np.clip(background, 0, 1)
+    if return_background:
+        return foreground, background
+    return foreground

@@ -312,6 +312,28 @@ def gen_foreground(pm, root, rng):
     finally:
         os.chdir(cwd)
     F, B = estimate_foreground_ml(image, alpha, return_background=True)
+    Fc, Bc = pm.estimate_foreground_cf(image, alpha, return_background=True)
+    out["lemur_F_cf"], out["lemur_B_cf"] = Fc, Bc
+    # the system matrix of estimate_foreground_cf on a small image
+    import scipy.sparse
+    rs = np.random.default_rng(12)
+    a_small = np.clip(rs.random((5, 7)) * 1.4 - 0.2, 0.0, 1.0)
+    n_s = a_small.size
+    S = None
+    for dx, dy in [(-1, 0), (1, 0), (0, -1), (0, 1)]:
+        from pymatting.util.util import sparse_conv_matrix_with_offsets
+        D = sparse_conv_matrix_with_offsets(7, 5, [1.0, -1.0], [0, dx], [0, dy])
+        S2 = D.T.dot(scipy.sparse.diags(1e-5 + np.abs(D.dot(a_small.ravel())))).dot(D)
+        S = S2 if S is None else S + S2
+    V = scipy.sparse.bmat([[S, None], [None, S]])
+    a_f = a_small.ravel()
+    U = scipy.sparse.bmat([[scipy.sparse.diags(a_f), scipy.sparse.diags(1 - a_f)]])
+    A = (U.T.dot(U) + V).tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    out["cf_small_alpha"] = a_small
+    out["cf_small_indptr"], out["cf_small_indices"] = A.indptr.astype(np.int64), A.indices.astype(np.int64)
+    out["cf_small_data"] = A.data
     out["lemur_image"], out["lemur_alpha"], out["lemur_trimap"] = image, alpha, trimap
     out["lemur_expected"], out["lemur_F"], out["lemur_B"] = expected, F, B
     np.savez_compressed(os.path.join(HERE, "foreground_small.npz"), **out)

@@ -192,3 +192,37 @@ def test_jacobi_device_output_and_errors(gpu):
         pm.estimate_foreground_ml_cupy(np.zeros((1, 1, 3)), np.zeros((1, 1)))
     with pytest.raises(AssertionError):
         pm.estimate_foreground_ml_cupy(np.zeros((4, 4, 4)), np.zeros((4, 4)))
+
+
+# --- closed-form foreground (estimate_foreground_cf) ---
+
+def test_foreground_cf_system_matches_reference(gpu):
+    """A = U^T U + diag(S, S) assembled on the device against the matrix
+    the reference builds with scipy (same entries; values within 1e-15,
+    the reference sums the same terms in its sparse-product order)."""
+    import scipy.sparse
+    from pymatting_b200.foreground import _fg_cf_matrix
+    import pymatting_b200._device as dev
+    import torch
+    g = golden("foreground_small.npz")
+    a = g["cf_small_alpha"]
+    h, w = a.shape
+    A = _fg_cf_matrix(dev.to_device(a.ravel(), torch.float64), h, w, 1e-5)
+    R = scipy.sparse.csr_matrix((g["cf_small_data"], g["cf_small_indices"], g["cf_small_indptr"]),
+                                shape=A.shape)
+    assert np.array_equal(A.indptr, R.indptr) and np.array_equal(A.indices, R.indices)
+    assert np.abs(A.data - R.data).max() <= 1e-15
+
+
+def test_foreground_cf_lemur(gpu):
+    """The reference test's check (mse <= 0.022) and closeness to the
+    reference's own result (CG to rtol 1e-5 from the image, ichol
+    preconditioner)."""
+    import pymatting_b200 as pm
+    g = golden("foreground_small.npz")
+    image, alpha, trimap = g["lemur_image"], g["lemur_alpha"], g["lemur_trimap"]
+    F, B = pm.estimate_foreground_cf(image, alpha, return_background=True)
+    unknown = (trimap > 0.1) & (trimap < 0.9)
+    mse = np.mean((alpha[:, :, None] * np.abs(F - g["lemur_expected"]))[unknown])
+    assert mse <= 0.022
+    assert np.abs(F - g["lemur_F_cf"]).mean() <= 1e-3 and np.abs(B - g["lemur_B_cf"]).mean() <= 1e-3

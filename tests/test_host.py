@@ -195,3 +195,9 @@ def test_laplacian_argument_errors():
         pm.knn_laplacian(img, kernel="gaussian")
     with pytest.raises(NotImplementedError):
         pm.lbdm_laplacian(img, radius=3)
+
+
+def test_foreground_cf_neighbour_sets():
+    import pymatting_b200 as pm
+    with pytest.raises(NotImplementedError):
+        pm.estimate_foreground_cf(np.zeros((4, 4, 3)), np.zeros((4, 4)), neighbors=[(1, 1)])
