@@ -285,14 +285,19 @@ __device__ __forceinline__ int nbr_count(int y, int x, int h, int w) {
     return (x > 0) + (x < w - 1) + (y > 0) + (y < h - 1);
 }
 
+// The coupling entry a (1 - a) of rows p and n + p exists only when it is
+// non-zero: the reference builds U from diags(a) and diags(1 - a), whose
+// zero entries scipy drops.
+__device__ __forceinline__ bool has_coupling(double ap) { return ap != 0.0 && ap != 1.0; }
+
 // rowptr[r] before the scan: entries of row r (r < n: F rows, r >= n: B rows).
-__global__ void k_fgcf_count(int h, int w, int64_t* rowcnt) {
+__global__ void k_fgcf_count(const double* __restrict__ a, int h, int w, int64_t* rowcnt) {
     const long long n = (long long)h * w;
     const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (r >= 2 * n) return;
     const long long p = r < n ? r : r - n;
     const int y = (int)(p / w), x = (int)(p % w);
-    rowcnt[r] = nbr_count(y, x, h, w) + 2;
+    rowcnt[r] = nbr_count(y, x, h, w) + 1 + (has_coupling(a[p]) ? 1 : 0);
 }
 
 __global__ void k_fgcf_fill(const double* __restrict__ a, int h, int w, double reg,
@@ -326,9 +331,9 @@ __global__ void k_fgcf_fill(const double* __restrict__ a, int h, int w, double r
         for (; t < m && q[t] < p; ++t, ++o) { cols[o] = q[t]; vals[o] = -wq[t]; }
         cols[o] = p; vals[o] = __dadd_rn(__dmul_rn(ap, ap), spp); ++o;
         for (; t < m; ++t, ++o) { cols[o] = q[t]; vals[o] = -wq[t]; }
-        cols[o] = n + p; vals[o] = __dmul_rn(ap, a1);
+        if (has_coupling(ap)) { cols[o] = n + p; vals[o] = __dmul_rn(ap, a1); }
     } else {
-        cols[o] = p; vals[o] = __dmul_rn(ap, a1); ++o;
+        if (has_coupling(ap)) { cols[o] = p; vals[o] = __dmul_rn(ap, a1); ++o; }
         int t = 0;
         for (; t < m && q[t] < p; ++t, ++o) { cols[o] = n + q[t]; vals[o] = -wq[t]; }
         cols[o] = n + p; vals[o] = __dadd_rn(__dmul_rn(a1, a1), spp); ++o;
@@ -342,15 +347,15 @@ __global__ void k_fgcf_fill(const double* __restrict__ a, int h, int w, double r
 int pmb_scan_exclusive(int64_t* v, int64_t n, int64_t* chunk_scratch, int64_t* total,
                        cudaStream_t s);
 
-// rowptr: 2 h w + 1; cols / vals: 2 (2 h w) + 2 * (number of neighbour pairs
-// counted per row) entries = rowptr[2 h w]; scratch: (2 h w + 1023) / 1024 + 2.
+// rowptr: 2 h w + 1; cols / vals: rowptr[2 h w] entries (written by the
+// first call); scratch: (2 h w + 1023) / 1024 + 2.
 int pmb_launch_fg_cf_system(const double* alpha, int h, int w, double reg, int64_t* rowptr,
                             int64_t* cols, double* vals, int64_t* scratch, cudaStream_t st) {
     if (!alpha || !rowptr || h <= 0 || w <= 0) return -2;
     const long long n2 = 2LL * h * w;
     const int blocks = (int)((n2 + 255) / 256);
     if (!cols || !vals) {
-        pmb::fgcf::k_fgcf_count<<<blocks, 256, 0, st>>>(h, w, rowptr);
+        pmb::fgcf::k_fgcf_count<<<blocks, 256, 0, st>>>(alpha, h, w, rowptr);
         if (pmb_scan_exclusive(rowptr, n2, scratch, rowptr + n2, st)) return 1;
         return cudaGetLastError() == cudaSuccess ? 0 : 1;
     }
