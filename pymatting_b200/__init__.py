@@ -1,13 +1,24 @@
-"""pymatting_b200 — PyMatting's closed-form alpha path on NVIDIA B200.
+"""pymatting_b200 — PyMatting's matting paths on NVIDIA B200.
 
-Drop-in replacements for ``cf_laplacian``, ``lkm_laplacian``, ``make_linear_system``, ``cg``
-(with ``CounterCallback`` / ``ProgressCallback``), the ``jacobi`` /
-``vcycle`` / ``ichol`` preconditioner factories, ``estimate_alpha_cf`` and
-``estimate_alpha_lkm``,
-computed by hand-written sm_100a kernels behind a C ABI
-(``include/pymatting_b200.h``). Extensions without a reference counterpart:
-``solve_alpha`` (batched, mixed-precision soft-constraint solves) and
-``cf_alpha`` (alpha differentiable with respect to the image).
+Drop-in replacements, computed by hand-written sm_100a kernels behind a C ABI
+(``include/pymatting_b200.h``):
+
+* the closed-form alpha path: ``cf_laplacian``, ``make_linear_system``, ``cg``
+  (with ``CounterCallback`` / ``ProgressCallback``), the ``jacobi`` /
+  ``vcycle`` / ``ichol`` preconditioner factories and ``estimate_alpha_cf``;
+* the other Laplacians and their estimators: ``lkm_laplacian``,
+  ``uniform_laplacian``, ``rw_laplacian``, ``lbdm_laplacian``,
+  ``knn_laplacian`` (``LAPLACIANS``), ``estimate_alpha_lkm`` / ``_knn`` /
+  ``_lbdm`` / ``_rw``;
+* foreground estimation: ``estimate_foreground_ml`` (the reference's sweep
+  order), ``estimate_foreground_ml_cupy`` (its GPU backend's Jacobi variant)
+  and ``estimate_foreground_cf``;
+* ``cutout`` with ``load_image`` / ``save_image`` / ``stack_images`` /
+  ``blend``.
+
+Extensions without a reference counterpart: ``solve_alpha`` (batched,
+mixed-precision soft-constraint solves) and ``cf_alpha`` (alpha
+differentiable with respect to the image).
 """
 
 from .util import trimap_split, sanity_check_image
