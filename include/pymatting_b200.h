@@ -124,7 +124,8 @@ int pmb_fg_levels(int h, int w, int n_small_iterations, int n_big_iterations, in
  * after the swaps). image (h, w, 3), alpha (h, w), F and B (h, w, 3)
  * float32 on the device (B may be null). Fused multiply-adds are allowed as
  * in the reference's NVRTC build, so results agree to float32 rounding.
- * Returns -4 for a 1x1 image (the reference divides by zero). */
+ * Sides up to 65535 and h w 3 < 2^31. Returns -4 for a 1x1 image (the
+ * reference divides by zero). */
 int64_t pmb_fg_jacobi_workspace_bytes(int h, int w);
 int pmb_fg_ml_jacobi(const float* image, const float* alpha, int h, int w, float regularization,
                      int n_small_iterations, int n_big_iterations, int small_size, float* F,
@@ -138,7 +139,7 @@ int pmb_fg_ml_jacobi(const float* image, const float* alpha, int h, int w, float
  * image: (h, w, 3) float64 (mode 1 only). px: w + 1 and py: h + 1 int64
  * prefix sums of the clamped window width per column and height per row;
  * the result is canonical CSR with rowptr (h w + 1), cols and vals
- * (py[h] * px[w] entries), all on the device. */
+ * (py[h] * px[w] entries), all on the device. h w < 2^31. */
 int pmb_window_laplacian(int mode, const double* image, int h, int w, int radius,
                          double regularization, const int64_t* px, const int64_t* py,
                          int64_t* rowptr, int64_t* cols, double* vals, void* stream);

@@ -176,8 +176,9 @@ int64_t pmb_launch_fgj_workspace(int h, int w) {
 int pmb_launch_fgj(const float* image, const float* alpha, int h0, int w0, float reg, int n_small,
                    int n_big, int small_size, float* outF, float* outB, void* workspace,
                    int64_t ws_bytes, cudaStream_t st) {
+    // pixel and value indices are 32-bit in the kernels
     if (!image || !alpha || !outF || !workspace || h0 <= 0 || w0 <= 0 || h0 > 65535 ||
-        w0 > 65535 || n_small < 0 || n_big < 0)
+        w0 > 65535 || (long long)h0 * w0 * 3 >= (1LL << 31) || n_small < 0 || n_big < 0)
         return -2;
     const int m0 = std::max(w0, h0) - 1;
     int n_levels = 0;

@@ -115,6 +115,7 @@ int pmb_launch_window_laplacian(int mode, const double* image, int h, int w, int
                                 const int64_t* px, const int64_t* py, int64_t* rowptr,
                                 int64_t* cols, double* vals, cudaStream_t st) {
     if (h <= 0 || w <= 0 || r < 0 || !px || !py || !rowptr || !cols || !vals) return -2;
+    if ((long long)h * w >= (1LL << 31)) return -2;  // pixel indices are 32-bit in the kernel
     if (mode == kRandomWalk && !image) return -2;
     Args A{image, h, w, r, reg, px, py, rowptr, cols, vals};
     const long long n = (long long)h * w;
