@@ -2,30 +2,38 @@
 """Benchmark of the closed-form alpha solve on B200.
 
 Metric: Mpix/s of soft-constraint closed-form alpha solves, each to FP64
-relative residual 1e-7, on the 1920x1080 synthetic workload (one image per
-GPU): assembly of the matting Laplacian, V-cycle hierarchy setup and the
-preconditioned CG solve, from image + trimap resident in HBM to alpha
-resident in HBM. ``value`` is the mixed-precision path (FP32 inner V-cycle
-PCG inside FP64 iterative refinement); the plain FP64 path is reported
-beside it. ``e2e`` is the same metric through the public ``solve_alpha`` API
-with host numpy buffers (uploads and the alpha download inside the timed
-region). ``--impl reference`` times the CPU restatement of PyMatting's own
-path (cf_laplacian + make_linear_system + vcycle + cg) on host cores.
+relative residual 1e-7. The default workload is the mixed batch: 64 images
+with sizes drawn from {256x256, 640x480, 1024x768, 1280x720, 1920x1080,
+2048x1536} and unknown fractions from 5-25 %, seeded synthetic images
+(``pymatting_b200.synthetic``), solved together in one batched engine. One
+step goes from images + trimaps resident in HBM to alphas resident in HBM:
+Laplacian assembly, V-cycle hierarchy setup and the preconditioned CG solve.
+``value`` is the mixed-precision path (FP32 inner V-cycle PCG inside FP64
+iterative refinement); the plain FP64 path is reported beside it as
+``fp64_value``. ``e2e`` is the same metric through the public API with
+pinned host buffers: uploads, the solve, the gather of every rank's alphas
+to rank 0 and their download are inside the timed region.
 
-``--workload foreground`` instead times estimate_foreground_ml (the step
-after alpha in PyMatting's cutout) on a 1920x1080 image and matte: the
-multi-level Gauss-Seidel sweeps in the reference's exact order, bit-identical
-to it for equal seed colours; its reference arm is the oracle's C
-restatement on one host core.
+``--impl reference`` times the CPU restatement of PyMatting's own path
+(cf_laplacian + make_linear_system + vcycle + cg, one solve per image) on
+the same workload: the batch's own images at full size, in batch order, one
+image per step, spread over the host cores by a process pool.
+
+Other workloads: ``1080p`` (one 1920x1080 image per GPU), ``4096`` (one
+4096x4096 image), ``foreground`` (estimate_foreground_ml on a 1920x1080
+image and matte).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-Multi-GPU: launched by torch.distributed.run, one rank per GPU; every rank
-solves its own image (weak scaling, no collective on the data path).
+Multi-GPU: with --gpus N > 1 and no torch.distributed environment, bench.py
+starts N ranks itself through torch.distributed.run (one per GPU). The batch
+is sharded over the ranks by pixel count (no collective in the solve); the
+time is the max over ranks and ``value`` counts the pixels of all ranks.
 """
 
 import argparse
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -39,6 +47,7 @@ sys.path.insert(0, HERE)
 
 METRIC = "Mpix/s of cf alpha solves at FP64 rel-residual 1e-7: mixed vs FP64 GPU; % HBM"
 L2_FLUSH_BYTES = 256 << 20
+BATCH_SEED = 1000
 
 
 def parse():
@@ -47,49 +56,239 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["1080p", "4096", "batch64", "foreground"],
-                    default="1080p",
-                    help="foreground: estimate_foreground_ml on a 1920x1080 image + matte")
+    ap.add_argument("--workload", choices=["batch64", "1080p", "4096", "foreground"],
+                    default="batch64",
+                    help="batch64 (default): the 64-image mixed batch; 1080p / 4096: one "
+                         "image per GPU; foreground: estimate_foreground_ml on a 1920x1080 "
+                         "image + matte")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", choices=["auto", "none"], default="none",
                     help="auto: run the launch-shape autotuner before timing; none (default): "
-                         "the built-in launch shapes, which matched or beat the tuner's "
-                         "picks at 1080p with L2 flushed between steps")
+                         "the built-in launch shapes")
     ap.add_argument("--profile", choices=["apply", "solve", "solve-fp64", "solve-mixed"],
                     default=None,
                     help="profiling case: a few operator applies, or one solve per precision "
-                         "(or of one precision)")
+                         "(or of one precision); prints no bench line")
+    ap.add_argument("--plumbing-check", action="store_true",
+                    help="CPU only (gloo): run the rank launch, the sharding of the batch and "
+                         "the gather to rank 0 with a stand-in result per image (no solve, no "
+                         "timing) and print what rank 0 received")
     return ap.parse_args()
 
 
 WORKLOADS = {
-    # name: list of (h, w, seed offset, unknown fraction)
+    # name: list of (h, w, unknown fraction)
     "1080p": dict(sizes=[(1080, 1920, 0.08)], sigma=3.0, band=10),
     "4096": dict(sizes=[(4096, 4096, 0.15)], sigma=3.0, band=10),
 }
 
 
-def make_inputs(workload, rank):
-    from pymatting_b200.synthetic import make_matting_problem, batch_sizes
+def workload_spec(workload):
+    """All images of a workload: ``[(h, w, unknown fraction, seed)]``, sigma, band."""
+    from pymatting_b200.synthetic import batch_sizes
     if workload == "batch64":
-        spec = [(h, w, frac, seed) for (h, w, frac, seed) in batch_sizes(64, 1000)]
-        from pymatting_b200.shard import shard_sizes
-        world = int(os.environ.get("WORLD_SIZE", "1"))
-        mine = shard_sizes([(h, w) for h, w, _, _ in spec], world)[rank]
-        spec = [spec[k] for k in mine]
-        sigma, band = 3.0, 10
+        return list(batch_sizes(64, BATCH_SEED)), 3.0, 10
+    wl = WORKLOADS[workload]
+    return [(h, w, frac, 100) for (h, w, frac) in wl["sizes"]], wl["sigma"], wl["band"]
+
+
+def make_image(spec_k, sigma, band):
+    from pymatting_b200.synthetic import make_matting_problem
+    h, w, frac, seed = spec_k
+    img, tri, _a, real = make_matting_problem(h, w, seed, sigma=sigma, band=band,
+                                              unknown_fraction=frac)
+    return img, tri, real
+
+
+def _gen_image(job):
+    spec_k, sigma, band = job
+    return make_image(spec_k, sigma, band)
+
+
+def generate_images(specs, sigma, band):
+    """The synthetic images of ``specs``, generated by a process pool over the
+    host cores (spawned workers, before this process touches the GPU)."""
+    import multiprocessing as mp
+    jobs = [(sp, sigma, band) for sp in specs]
+    workers = max(1, min(os.cpu_count() or 1, len(jobs)))
+    if workers == 1:
+        return [_gen_image(j) for j in jobs]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_gen_image, jobs, chunksize=1)
+
+
+def rank_images(workload, rank, world):
+    """This rank's images: batch64 is sharded by pixel count; a single-image
+    workload gives every rank its own image (seed 100 + rank)."""
+    from pymatting_b200.shard import shard_sizes
+    spec, sigma, band = workload_spec(workload)
+    if workload == "batch64":
+        parts = shard_sizes([(h, w) for h, w, _f, _s in spec], world)
     else:
-        wl = WORKLOADS[workload]
-        spec = [(h, w, frac, 100 + rank) for (h, w, frac) in wl["sizes"]]
-        sigma, band = wl["sigma"], wl["band"]
-    imgs, tris, fracs = [], [], []
-    for h, w, frac, seed in spec:
-        img, tri, _a, real = make_matting_problem(h, w, seed, sigma=sigma, band=band,
-                                                  unknown_fraction=frac)
-        imgs.append(img)
-        tris.append(tri)
-        fracs.append(real)
-    return imgs, tris, fracs
+        spec = [(h, w, f, s + r) for r in range(world) for (h, w, f, s) in spec]
+        parts = [[r] for r in range(world)]
+    mine = parts[rank]
+    made = generate_images([spec[k] for k in mine], sigma, band)
+    imgs = [m[0] for m in made]
+    tris = [m[1] for m in made]
+    fracs = [m[2] for m in made]
+    sizes = [(h, w) for h, w, _f, _s in spec]
+    return imgs, tris, fracs, mine, parts, sizes
+
+
+def free_port():
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_ranks(args):
+    """Start ``--gpus`` ranks through torch.distributed.run (one process per
+    GPU) with this command line; rank 0 prints the line. Returns the exit code."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(args.gpus), "--master-addr", "127.0.0.1",
+           "--master-port", str(free_port()), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def plumbing_check(args, rank, world):
+    """Launch + shard + gather on CPU (gloo) with a stand-in per-image result:
+    image k of the batch holds k + j / n at element j. Rank 0 checks that every
+    image arrived, in batch order, and prints one line."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from pymatting_b200.shard import gather_images, shard_sizes
+    spec, _s, _b = workload_spec("batch64")
+    # Sizes scaled down 16x per side: the check is about order and plumbing.
+    sizes = [(max(h // 16, 1), max(w // 16, 1)) for h, w, _f, _s in spec]
+    if world > 1:
+        dist.init_process_group("gloo", timeout=timedelta(seconds=120))
+    parts = shard_sizes(sizes, world)
+
+    def standin(k):
+        n = sizes[k][0] * sizes[k][1]
+        return k + torch.arange(n, dtype=torch.float64) / n
+
+    local = [standin(k) for k in parts[rank]]
+    out = gather_images(local, sizes, parts, rank, world, torch.device("cpu"))
+    if rank == 0:
+        ok = all(torch.equal(out[k], standin(k)) for k in range(len(sizes)))
+        print(json.dumps({"plumbing": "shard + gather to rank 0, gloo, stand-in results",
+                          "n_gpus": world, "images": len(out), "order_ok": bool(ok),
+                          "images_per_rank": [len(p) for p in parts]}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------
+# Reference arm: the CPU restatement of the reference path on host cores
+# --------------------------------------------------------------------------
+
+def _reference_prepare(job):
+    """Generate one image of the workload into ``folder`` (worker process)."""
+    k, spec_k, sigma, band, folder = job
+    img, tri, _real = make_image(spec_k, sigma, band)
+    np.save(os.path.join(folder, "img%d.npy" % k), img)
+    np.save(os.path.join(folder, "tri%d.npy" % k), tri)
+    return k
+
+
+def _reference_solve(job):
+    """One image of the workload through the CPU restatement (worker process)."""
+    import oracle
+    k, folder = job
+    img = np.load(os.path.join(folder, "img%d.npy" % k))
+    tri = np.load(os.path.join(folder, "tri%d.npy" % k))
+    t0 = time.perf_counter()
+    x, iters = oracle.solve_soft(img, tri, preconditioner="vcycle", rtol=1e-7)
+    dt = time.perf_counter() - t0
+    return tri.size, dt, iters
+
+
+def reference_workers(count):
+    """Worker processes for the reference arm: every host core, bounded by
+    the host memory a full-size solve needs (about 5 GB for 2048x1536)."""
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        mem = psutil.virtual_memory().available
+        cores = max(1, min(cores, int(mem // (5 << 30))))
+    except ImportError:
+        pass
+    return max(1, min(cores, count))
+
+
+def run_reference(args, rank, world):
+    """PyMatting's path (CPU restatement) on this workload, rank 0 only.
+
+    Each step solves one image of the workload at full size, in workload
+    order (image s mod n for step s); the warm-up images come first. The
+    images are generated beforehand (outside the timing) into a scratch
+    folder; the timed steps are solved concurrently by a process pool over
+    the host cores, each worker with an equal share of the BLAS threads;
+    value = their pixels / the wall time of the timed region.
+    """
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    import shutil
+    import tempfile
+    spec, sigma, band = workload_spec(args.workload)
+    n = len(spec)
+    warm = [s % n for s in range(max(args.warmup, 1))]
+    timed = [(args.warmup + s) % n for s in range(args.steps)]
+    workers = reference_workers(len(timed))
+    threads = str(max(1, (os.cpu_count() or 1) // workers))
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = threads
+    root = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    folder = tempfile.mkdtemp(prefix="pmb_ref_", dir=root)
+    try:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(workers) as pool:
+            pool.map(_reference_prepare, [(k, spec[k], sigma, band, folder)
+                                          for k in sorted(set(warm + timed))], chunksize=1)
+            pool.map(_reference_solve, [(k, folder) for k in warm], chunksize=1)
+            t0 = time.perf_counter()
+            res = pool.map(_reference_solve, [(k, folder) for k in timed], chunksize=1)
+            wall = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(folder, ignore_errors=True)
+    npx = sum(r[0] for r in res)
+    value = npx / wall / 1e6
+    per_solve = sum(r[0] for r in res) / sum(r[1] for r in res) / 1e6
+    images = ["%dx%d" % (spec[k][1], spec[k][0]) for k in timed]
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / len(timed), "higher_is_better": True,
+        "scaling": "weak" if args.workload != "batch64" else "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": workload_name(args.workload),
+                   "images": images, "image_indices": timed,
+                   "path": "cf_laplacian + make_linear_system + vcycle + cg, rel-res 1e-7 "
+                           "(CPU restatement, one solve per image)",
+                   "same_config": True},
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": workers, "kind": "port",
+                         "sample": "%d images of the workload at full size (%.1f Mpix), one "
+                                   "per step, %d worker processes x %s BLAS threads; one "
+                                   "solve on one core: %.3f Mpix/s"
+                                   % (len(timed), npx / 1e6, workers, threads, per_solve)},
+        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "iters": [r[2] for r in res],
+    }
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def workload_name(workload):
+    return {"batch64": "cf_alpha_soft_vcycle_rtol1e-7_batch64_mixed_sizes",
+            "1080p": "cf_alpha_soft_vcycle_rtol1e-7_1080p",
+            "4096": "cf_alpha_soft_vcycle_rtol1e-7_4096x4096"}[workload]
 
 
 class ClockSampler:
@@ -171,63 +370,6 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def traffic_per_launch(kind, npx):
-    """DRAM bytes per apply launch from the committed ncu summary, scaled."""
-    path = os.path.join(HERE, "profiles", "apply_traffic.json")
-    if not os.path.exists(path):
-        return None
-    with open(path) as f:
-        d = json.load(f)
-    e = d.get(kind)
-    if not e:
-        return None
-    return float(e["dram_bytes"]) * npx / float(e["pixels"])
-
-
-def run_reference(args, rank, world):
-    """CPU restatement of the reference path on host cores (rank 0 only)."""
-    if rank != 0:
-        return None
-    import oracle
-    imgs, tris, fracs = make_inputs(args.workload if args.workload != "batch64" else "1080p", 0)
-    img, tri = imgs[0], tris[0]
-    h, w = tri.shape
-    # Bound the run to a few minutes: full image for short runs, a crop
-    # otherwise (throughput per pixel is close to size-independent).
-    steps = args.steps + args.warmup
-    if steps > 6:
-        hh, ww = h // 2, w // 2
-        y0, x0 = (h - hh) // 2, (w - ww) // 2
-        img, tri = img[y0:y0 + hh, x0:x0 + ww].copy(), tri[y0:y0 + hh, x0:x0 + ww].copy()
-    sample = "%dx%d soft system from the %s workload" % (tri.shape[1], tri.shape[0], args.workload)
-    times = []
-    for s in range(steps):
-        t0 = time.perf_counter()
-        x, iters = oracle.solve_soft(img, tri, preconditioner="vcycle", rtol=1e-7)
-        dt = time.perf_counter() - t0
-        if s >= args.warmup:
-            times.append(dt)
-    npx = tri.size
-    value = npx * len(times) / sum(times) / 1e6
-    line = {
-        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": "cf_alpha_soft_vcycle_rtol1e-7_" + args.workload,
-                   "image": "%dx%d" % (tri.shape[1], tri.shape[0]),
-                   "path": "cf_laplacian + make_linear_system + vcycle + cg (CPU restatement)"},
-        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": 1, "kind": "port",
-                         "sample": sample},
-        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-        "iters": iters,
-    }
-    print(json.dumps(line), flush=True)
-    return line
 
 
 FG_METRIC = "Mpix/s of estimate_foreground_ml (reference sweep order, bit-exact for equal seeds)"
@@ -413,15 +555,63 @@ def run_foreground(args, rank, world, local):
         dist.destroy_process_group()
 
 
-def cpu_baseline(img, tri):
+
+
+# --------------------------------------------------------------------------
+# Our arm: the batched stencil engine
+# --------------------------------------------------------------------------
+
+# Algorithmic bytes per level-0 pixel of the level-0 kernels of one inner CG
+# iteration, in elements of the inner precision (s = 4 FP32, 8 FP64). Each
+# counts the 13 half-stencil planes once where the kernel reads them, every
+# vector read or written once, and the quarter-size coarse vector.
+KERNEL_ELEMS = {
+    "cg_apply": (17.0, "13 planes + z + p_old in, p + Ap out"),
+    "cg_update": (6.0, "x, r, p, Ap in, x, r out"),
+    "vc_down_l0": (14.25, "13 planes + r in, coarse b (1/4) out"),
+    "vc_up_l0": (15.25, "13 planes + r + coarse x (1/4) in, z out"),
+}
+
+
+def cpu_sample(imgs, tris, budget_s=15.0):
+    """The oracle's solve (CPU restatement of the reference path, one core) of
+    this rank's first images, in batch order, until about ``budget_s`` of
+    CPU time: the cpu_baseline sample and the reference alphas the GPU
+    results are compared with."""
     import oracle
-    t0 = time.perf_counter()
-    x, iters = oracle.solve_soft(img, tri, preconditioner="vcycle", rtol=1e-7)
-    dt = time.perf_counter() - t0
-    return {"value": tri.size / dt / 1e6, "unit": "Mpix/s", "cores": 1, "kind": "port",
-            "sample": "one %dx%d soft-constraint vcycle CG solve to rtol 1e-7 (oracle: C "
-                      "cf_laplacian, scipy make_linear_system / vcycle / cg), %d iterations, "
-                      "%.1f s" % (tri.shape[1], tri.shape[0], iters, dt)}, x
+    out, spent = [], 0.0
+    for k, (img, tri) in enumerate(zip(imgs, tris)):
+        t0 = time.perf_counter()
+        x, iters = oracle.solve_soft(img, tri, preconditioner="vcycle", rtol=1e-7)
+        dt = time.perf_counter() - t0
+        out.append((k, x, dt, iters))
+        spent += dt
+        if spent >= budget_s:
+            break
+    return out
+
+
+def kernel_roofline(batches, npx, peak, peak_kind):
+    """Per-kernel HBM fraction of the level-0 kernels of one inner iteration,
+    from CUDA-event durations of each launch inside live solve iterations
+    (``StencilSystem.profile_kernels``)."""
+    out = {}
+    for precision, es in [("mixed", 4), ("fp64", 8)]:
+        prof = batches[precision].system.profile_kernels(iters=8)
+        rows = {}
+        for name, (elems, what) in KERNEL_ELEMS.items():
+            ms = prof.get(name)
+            if not ms:
+                continue
+            nbytes = npx * elems * es
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            rows[name] = {"ms": ms, "bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak,
+                          "bytes_formula": "pixels x %.2f x %d B (%s)" % (elems, es, what)}
+        total = sum(prof.values())
+        rows["iteration_ms"] = total
+        rows["iteration_share"] = {k: v / total for k, v in prof.items() if total > 0}
+        out[precision] = rows
+    return out
 
 
 def run_profile_case(args, imgs_d, tris_d, npx):
@@ -446,10 +636,16 @@ def run_profile_case(args, imgs_d, tris_d, npx):
 
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    env_world = os.environ.get("WORLD_SIZE")
+    if env_world is None and args.gpus > 1:
+        sys.exit(launch_ranks(args))
+    world = int(env_world or "1")
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.plumbing_check:
+        plumbing_check(args, rank, world)
+        return
     if args.workload == "foreground":
         if args.impl == "reference":
             run_foreground_reference(args, rank)
@@ -472,9 +668,11 @@ def main():
 
     import pymatting_b200  # noqa: F401
     from pymatting_b200.batch import AlphaBatch, solve_alpha
+    from pymatting_b200.shard import gather_images
 
-    imgs, tris, fracs = make_inputs(args.workload, rank)
+    imgs, tris, fracs, mine, parts, sizes = rank_images(args.workload, rank, world)
     npx = sum(t.size for t in tris)
+    npx_all = sum(h * w for k, (h, w) in enumerate(sizes) if any(k in p for p in parts))
     imgs_d = [torch.as_tensor(i, device=dev) for i in imgs]
     tris_d = [torch.as_tensor(t, device=dev) for t in tris]
     if args.profile:
@@ -486,8 +684,7 @@ def main():
     def device_step(precision):
         batch = AlphaBatch(imgs_d, tris_d, precision=precision, tune="cached")
         x = batch.solve()
-        alphas = batch.alphas(x)
-        return batch, x, alphas
+        return batch, x
 
     def timed(fn, steps):
         times, info = [], None
@@ -531,55 +728,61 @@ def main():
         barrier()
         total_ms = max_over_ranks(sum(times))
         batch = info[0]
-        launches = sum(batch.system.launch_count() for _ in [0]) + 4 * len(imgs)
+        launches = batch.system.launch_count() + 4 * len(imgs)
         results[precision] = dict(total_ms=total_ms, batch=batch, x=info[1],
                                   launches_per_step=launches)
 
-    # FP64 relative residual of the mixed result, measured with the FP64
-    # operator of an FP64 system on the same inputs.
-    b64 = results["fp64"]["batch"]
-    ax = b64.system.apply(results["mixed"]["x"])
-    rel_mixed = float(torch.linalg.norm(b64.b - ax) / torch.linalg.norm(b64.b))
-    ax = b64.system.apply(results["fp64"]["x"])
-    rel_fp64 = float(torch.linalg.norm(b64.b - ax) / torch.linalg.norm(b64.b))
-    alpha_diff = float((torch.clamp(results["mixed"]["x"], 0, 1) -
-                        torch.clamp(results["fp64"]["x"], 0, 1)).abs().max())
-    # Error of both results against a tight FP64 solve (rel-res 1e-12) of the
-    # same system, outside the timed region: at rel-res 1e-7 weakly
-    # constrained unknown regions still move, in either precision.
-    stats_timed = {p: results[p]["batch"].stats()[0] for p in ["fp64", "mixed"]}
-    x_tight = AlphaBatch(imgs_d, tris_d, precision="fp64").solve(rtol=1e-12)
-    alpha_err = {p: float((torch.clamp(results[p]["x"], 0, 1) - torch.clamp(x_tight, 0, 1))
-                          .abs().max()) for p in ["fp64", "mixed"]}
-
-    # End to end through the public API with host buffers: pinned CPU
-    # tensors in, alphas back in host memory, both copies inside the timing.
+    # End to end through the public API with host buffers: pinned host
+    # tensors in, every rank's alphas gathered to rank 0 and downloaded there.
     imgs_h = [torch.from_numpy(i).pin_memory() for i in imgs]
     tris_h = [torch.from_numpy(t).pin_memory() for t in tris]
+    out_h = torch.empty(npx_all, dtype=torch.float64).pin_memory() if rank == 0 else None
+
+    def e2e_step():
+        im = [t.to(dev, non_blocking=True) for t in imgs_h]
+        tr = [t.to(dev, non_blocking=True) for t in tris_h]
+        alphas = solve_alpha(im, tr, precision="mixed", tune="cached")
+        allv = gather_images(alphas, sizes, parts, rank, world, dev)
+        if rank == 0:
+            out_h.copy_(torch.cat([a.reshape(-1) for a in allv if a is not None]))
+        return None
+
     for _ in range(max(1, args.warmup)):
-        solve_alpha(imgs_h, tris_h, precision="mixed", tune="cached")
+        e2e_step()
     barrier()
-    e2e_times, _ = timed(lambda: solve_alpha(imgs_h, tris_h, precision="mixed", tune="cached"),
-                         args.steps)
+    e2e_times, _ = timed(e2e_step, args.steps)
     e2e_ms = max_over_ranks(sum(e2e_times))
     clock_rec = clocks.stop()
 
-    # Roofline of the Laplacian apply (the operator kernel of the solve).
+    # Accuracy, outside the timed regions. FP64 relative residual of both
+    # results with the FP64 operator of the same inputs.
+    b64 = results["fp64"]["batch"]
+    rel = {}
+    for p in ["fp64", "mixed"]:
+        ax = b64.system.apply(results[p]["x"])
+        rel[p] = float(torch.linalg.norm(b64.b - ax) / torch.linalg.norm(b64.b))
+    stats_timed = {p: results[p]["batch"].stats() for p in ["fp64", "mixed"]}
+    alpha = {p: results[p]["batch"].alphas(results[p]["x"]) for p in ["fp64", "mixed"]}
+    alpha_diff = max(float((a - b).abs().max()) for a, b in zip(alpha["mixed"], alpha["fp64"]))
+    # Both results against a tight FP64 solve (rel-res 1e-12) of the same
+    # systems: at rel-res 1e-7 weakly constrained unknown regions still move,
+    # in either precision.
+    tight = AlphaBatch(imgs_d, tris_d, precision="fp64")
+    alpha_tight = tight.alphas(tight.solve(rtol=1e-12))
+    alpha_err = {p: max(float((a - b).abs().max()) for a, b in zip(alpha[p], alpha_tight))
+                 for p in ["fp64", "mixed"]}
+
     peak, peak_kind = measured_peaks()
-    apply = {}
-    for precision, es in [("mixed", 4), ("fp64", 8)]:
-        ms = results[precision]["batch"].system.time_apply(50)
-        bytes_alg = npx * 15 * es
-        apply[precision] = dict(ms=ms, bytes=bytes_alg, gbs=bytes_alg / (ms * 1e-3) / 1e9)
-    traffic = traffic_per_launch("fp32", npx)
+    batches = {p: results[p]["batch"] for p in ["fp64", "mixed"]}
+    kernels = kernel_roofline(batches, npx, peak, peak_kind)
 
     if rank == 0:
         k = args.steps
-        value = world * npx * k / (results["mixed"]["total_ms"] * 1e-3) / 1e6
-        value64 = world * npx * k / (results["fp64"]["total_ms"] * 1e-3) / 1e6
-        e2e_value = world * npx * k / (e2e_ms * 1e-3) / 1e6
-        st_m = stats_timed["mixed"]
-        st_d = stats_timed["fp64"]
+        value = npx_all * k / (results["mixed"]["total_ms"] * 1e-3) / 1e6
+        value64 = npx_all * k / (results["fp64"]["total_ms"] * 1e-3) / 1e6
+        e2e_value = npx_all * k / (e2e_ms * 1e-3) / 1e6
+        km = kernels["mixed"]
+        dom = max((n for n in KERNEL_ELEMS if n in km), key=lambda n: km[n]["ms"])
         line = {
             "metric": METRIC,
             "value": value,
@@ -589,51 +792,65 @@ def main():
             "warmup": args.warmup,
             "ms_per_step": results["mixed"]["total_ms"] / k,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "weak" if args.workload != "batch64" else "strong",
             "vs_baseline": None,
             "dtype": "f32 inner / f64 refinement",
             "data": "synthetic",
             "config": {
-                "workload": "cf_alpha_soft_vcycle_rtol1e-7_" + args.workload,
+                "workload": workload_name(args.workload),
+                "images": len(sizes) if args.workload == "batch64" else world,
                 "images_per_gpu": len(imgs),
-                "image": "x".join(str(s) for s in (tris[0].shape[1], tris[0].shape[0])),
-                "unknown_fraction": round(float(np.mean(fracs)), 4),
+                "megapixels": round(npx_all / 1e6, 3),
+                "unknown_fraction_mean": round(float(np.mean(fracs)), 4),
                 "lambda": 100.0, "epsilon": 1e-7, "preconditioner": "vcycle",
                 "precision": "mixed (FP32 inner rtol 1e-4, FP64 refinement)",
                 "l2": "flushed between steps (256 MB write); planes exceed L2",
-                "parallelism": "weak: one image per GPU, no collective",
+                "parallelism": ("batch sharded over ranks by pixel count, no collective in "
+                                "the solve" if args.workload == "batch64" else
+                                "one image per GPU, no collective"),
                 "launch_shapes": {p: (t or {}).get("knobs") for p, t in tunings.items()},
             },
             "fp64_value": value64,
             "mixed_over_fp64": value / value64,
-            "iters": {"mixed_inner_total": st_m.iters, "mixed_outer": st_m.outer_iters,
-                      "fp64": st_d.iters},
-            "rel_residual_fp64": {"mixed": rel_mixed, "fp64": rel_fp64},
+            "iters": {"mixed_inner": [s.iters for s in stats_timed["mixed"]],
+                      "mixed_outer": [s.outer_iters for s in stats_timed["mixed"]],
+                      "fp64": [s.iters for s in stats_timed["fp64"]]},
+            "rel_residual_fp64": rel,
             "alpha_maxabs_mixed_vs_fp64": alpha_diff,
             "alpha_maxabs_vs_fp64_rtol1e-12": alpha_err,
-            "roofline": {
-                "bound": "hbm",
-                "kernel": "half-stencil Laplacian apply y = (L + lambda D) x, FP32",
-                "achieved": apply["mixed"]["gbs"],
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": apply["mixed"]["gbs"] / peak,
-                "peak_source": peak_kind,
-                "traffic": traffic,
-                "bytes_per_launch": apply["mixed"]["bytes"],
-                "bytes_formula": "pixels x 15 values (13 half-stencil planes + x + y) x 4 B",
-                "fp64": {"achieved": apply["fp64"]["gbs"], "frac": apply["fp64"]["gbs"] / peak,
-                         "bytes_per_launch": apply["fp64"]["bytes"]},
-            },
+            "roofline": dict({"bound": "hbm", "kernel": dom + " (FP32, level 0)",
+                              "achieved": km[dom]["achieved_gbs"], "peak": peak,
+                              "unit": "GB/s", "frac": km[dom]["frac"],
+                              "peak_source": peak_kind, "traffic": None,
+                              "bytes_per_launch": km[dom]["bytes"],
+                              "bytes_formula": km[dom]["bytes_formula"]},
+                             kernels=kernels),
             "e2e": {"value": e2e_value, "unit": "Mpix/s",
-                    "h2d_bytes_per_step": int(npx * (24 + 8)),
-                    "d2h_bytes_per_step": int(npx * 8)},
+                    "h2d_bytes_per_step": int(npx_all * (24 + 8)),
+                    "d2h_bytes_per_step": int(npx_all * 8)},
             "gpu_launches": int(results["mixed"]["launches_per_step"] * k),
             "clocks": clock_rec,
         }
-        if world == 1 and not args.no_cpu_baseline and args.workload == "1080p":
-            cb, _x = cpu_baseline(imgs[0], tris[0])
-            line["cpu_baseline"] = cb
+        if world == 1 and not args.no_cpu_baseline:
+            sample = cpu_sample(imgs, tris)
+            px = sum(tris[kk].size for kk, _x, _dt, _it in sample)
+            secs = sum(dt for _k, _x, dt, _it in sample)
+            line["cpu_baseline"] = {
+                "value": px / secs / 1e6, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                "sample": "the first %d images of the workload at full size (%.2f Mpix), one "
+                          "soft-constraint vcycle CG solve each to rtol 1e-7 (oracle: C "
+                          "cf_laplacian, scipy make_linear_system / vcycle / cg), %.1f s"
+                          % (len(sample), px / 1e6, secs)}
+            errs = {}
+            for p in ["fp64", "mixed"]:
+                errs[p] = max(float(np.abs(alpha[p][kk].cpu().numpy().reshape(-1) -
+                                           np.clip(x, 0, 1)).max())
+                              for kk, x, _dt, _it in sample)
+            line["alpha_maxabs_vs_reference"] = dict(
+                errs, images=[kk for kk, _x, _dt, _it in sample],
+                note="against the reference path's own CPU solve (CPU restatement) at "
+                     "rel-res 1e-7; both sides stop at 1e-7, so weakly constrained regions "
+                     "differ by the solver tolerance")
         print(json.dumps(line), flush=True)
     if world > 1:
         barrier()

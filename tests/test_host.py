@@ -107,6 +107,84 @@ def test_shard_ranks_agree_without_communication():
     assert not set(gathered[0]) & set(gathered[1])
 
 
+def _gather_worker(rank, world, port, out):
+    """Shard the 64-image batch, 'solve' each image with a CPU stand-in
+    (alpha = clipped trimap of a small synthetic image of that seed), gather
+    the alphas and a statistics row per image to rank 0 over gloo."""
+    import torch
+    from pymatting_b200.shard import STAT_FIELDS, gather_images
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    spec = batch_sizes(64, 1000)
+    sizes = [(h // 32, w // 32) for h, w, _f, _s in spec]
+    parts = shard_sizes(sizes, world)
+
+    def standin(k):
+        h, w = sizes[k]
+        _i, tri, _a, _f = make_matting_problem(h, w, spec[k][3], sigma=1.0, band=1,
+                                               unknown_fraction=0.2)
+        return torch.from_numpy(np.clip(tri, 0, 1)).reshape(-1)
+
+    alphas = [standin(k) for k in parts[rank]]
+    stats = [torch.tensor([float(k), 1.0, 1e-3, 1.0, float(rank)], dtype=torch.float64)
+             for k in parts[rank]]
+    cpu = torch.device("cpu")
+    got = gather_images(alphas, sizes, parts, rank, world, cpu)
+    got_st = gather_images(stats, [len(STAT_FIELDS)] * len(sizes), parts, rank, world, cpu)
+    if rank == 0:
+        ok = all(torch.equal(got[k], standin(k)) for k in range(len(sizes)))
+        order = [int(s[0]) for s in got_st]
+        owner = [int(s[4]) for s in got_st]
+        out.put((ok, order, owner, [list(p) for p in parts]))
+    else:
+        assert got is None and got_st is None
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_gather_to_rank0_in_batch_order():
+    """The final gather of per-image alphas and statistics (gloo, 2 ranks):
+    rank 0 receives every image once, in batch order, from the rank that
+    owns it."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 31500 + (os.getpid() % 2000)
+    procs = [ctx.Process(target=_gather_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    ok, order, owner, parts = q.get(timeout=180)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert ok
+    assert order == list(range(64))
+    for r, part in enumerate(parts):
+        assert all(owner[k] == r for k in part)
+
+
+def test_bench_starts_its_own_ranks():
+    """bench.py --gpus 2 without a torch.distributed environment starts two
+    ranks itself; its CPU plumbing check shards the batch and gathers it to
+    rank 0, which prints the line."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2",
+                          "--plumbing-check"], capture_output=True, text=True, timeout=300,
+                         env=env, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    rec = json.loads(lines[0])
+    assert rec["n_gpus"] == 2 and rec["images"] == 64 and rec["order_ok"]
+    assert sum(rec["images_per_rank"]) == 64
+
+
 def _write_png(path, arr):
     from PIL import Image
     Image.fromarray(arr).save(path)
