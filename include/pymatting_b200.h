@@ -245,6 +245,15 @@ int pmb_stencil_tuning(const pmb_stencil* s, int knob);
  * precision), timed with CUDA events on the solver's stream over `iters`
  * launches. Benchmark hook; no reference counterpart. */
 int pmb_stencil_time_apply(pmb_stencil* s, int iters, double* ms, void* stream);
+/* Milliseconds per iteration in each kind of launch over `iters` live solve
+ * iterations of A x = b (b: concatenated per-image vectors), CUDA events on
+ * the solver's stream after every launch. ms_out holds 10 values: CG apply,
+ * CG update, mixed-precision refinement, restriction from level 0,
+ * restriction from coarser levels, coarse-level tail, direct coarsest
+ * solves, prolongation at coarser levels, prolongation at level 0, other.
+ * Measurement only: no reference counterpart (it times the loop of
+ * pymatting/solver/cg.py:82-113 with vcycle.py:46-100 as M). */
+int pmb_stencil_profile(pmb_stencil* s, const double* b, int iters, double* ms_out, void* stream);
 
 /* ---- Sparse-format helpers (device arrays, int64 indices) ---------------- */
 
@@ -258,15 +267,27 @@ int pmb_ell_csr_rowptr(const double* values, int h, int w, int radius, int64_t* 
                        int64_t* scratch, void* stream);
 int pmb_ell_csr_fill(const double* values, int h, int w, int radius, const int64_t* rowptr,
                      int64_t* indices, double* data, void* stream);
-/* Canonical CSR of A + diag(c) for a general CSR A with rows of at most 64
- * entries (make_linear_system on a matrix not assembled by this library,
- * pymatting/laplacian/laplacian.py:50-55). *overflow = 1 for longer rows. */
+/* Canonical CSR of A + diag(c) for a general CSR A of any row length
+ * (make_linear_system on a matrix not assembled by this library,
+ * pymatting/laplacian/laplacian.py:50-55): columns ascending, duplicates
+ * summed in stored order, explicit zeros dropped. *overflow is set to 0 (kept
+ * for callers of the earlier row-length limit). */
 int pmb_csr_add_diag_rowptr(int64_t n, const int64_t* indptr, const int64_t* indices,
                             const double* data, const double* c, int64_t* rowptr, int* overflow,
                             int64_t* scratch, void* stream);
 int pmb_csr_add_diag_fill(int64_t n, const int64_t* indptr, const int64_t* indices,
                           const double* data, const double* c, const int64_t* rowptr,
                           int64_t* out_indices, double* out_data, void* stream);
+/* Half-stencil planes (13 x h x pitch doubles, the stencil engine's layout)
+ * of an (h w) x (h w) CSR matrix of a pixel grid whose entries lie within
+ * the 5x5 neighbourhood of their row's pixel, so that vcycle runs on any
+ * such matrix (pymatting/preconditioner/vcycle.py:103-153 accepts any A of
+ * shape (h w, h w)). back: 12 x h x pitch doubles of scratch. bad[0] = entries
+ * outside the 5x5 neighbourhood, bad[1] = pairs A[i, j] / A[j, i] that differ
+ * by more than rel_tol relative (the engine needs a symmetric A). */
+int pmb_csr_to_planes(const int64_t* indptr, const int64_t* indices, const double* data, int h,
+                      int w, double* planes, double* back, double rel_tol,
+                      unsigned long long* bad, void* stream);
 
 /* ---- Trimap and hard-constraint system --------------------------------- */
 
@@ -290,12 +311,13 @@ int pmb_unknown_index(const uint8_t* is_known, int64_t n, int64_t* cidx, int64_t
 #define PMB_UNKNOWN_INDEX_STATIC_MAX_N 33553407
 int pmb_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t* cidx, void* stream);
 /* L_U = L[U, :][:, U] and b_U = -L[U, :][:, K] is_fg[K] from the ELL of the
- * Laplacian assembled with is_known (estimate_alpha_cf.py:64-74). */
-int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, const int64_t* cidx,
+ * Laplacian of window radius `radius` assembled with is_known (ELL rows of
+ * (4 radius + 1)^2 slots; estimate_alpha_cf.py:55, 64-74). */
+int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, int radius, const int64_t* cidx,
                        int64_t n_unknown, int64_t* rowptr, int64_t* scratch, void* stream);
 int pmb_hard_lu_fill(const double* ell_values, const uint8_t* is_known, const uint8_t* is_fg,
-                     int h, int w, const int64_t* cidx, const int64_t* rowptr, int64_t* indices,
-                     double* data, double* rhs, void* stream);
+                     int h, int w, int radius, const int64_t* cidx, const int64_t* rowptr,
+                     int64_t* indices, double* data, double* rhs, void* stream);
 /* alpha = clip(trimap on known pixels, x_U on unknown ones) to [0, 1]
  * (estimate_alpha_cf.py:72-76). */
 int pmb_alpha_compose(const double* trimap, const uint8_t* is_known, const int64_t* cidx,

@@ -55,9 +55,9 @@ _SIGNATURES = {
     "pmb_trimap_masks": (c_int, [c_vp, c_i64, c_dbl, c_dbl, c_vp, c_vp, c_vp, c_vp]),
     "pmb_unknown_index": (c_int, [c_vp, c_i64, c_vp, c_vp, c_vp]),
     "pmb_unknown_index_static": (c_int, [c_vp, c_i64, c_vp, c_vp]),
-    "pmb_hard_lu_rowptr": (c_int, [c_vp, c_int, c_int, c_vp, c_i64, c_vp, c_vp, c_vp]),
-    "pmb_hard_lu_fill": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
-                                 c_vp]),
+    "pmb_hard_lu_rowptr": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "pmb_hard_lu_fill": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp,
+                                 c_vp, c_vp]),
     "pmb_alpha_compose": (c_int, [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp]),
     "pmb_stencil_create": (c_int, [c_int, c_vp, c_vp, c_int, c_int, c_int, c_int, c_dbl, c_int,
                                    ctypes.POINTER(c_vp)]),
@@ -76,6 +76,7 @@ _SIGNATURES = {
                                   ctypes.POINTER(c_int)]),
     "pmb_stencil_launch_count": (c_i64, [c_vp]),
     "pmb_stencil_time_apply": (c_int, [c_vp, c_int, ctypes.POINTER(c_dbl), c_vp]),
+    "pmb_stencil_profile": (c_int, [c_vp, c_vp, c_int, c_vp, c_vp]),
     "pmb_stencil_destroy": (c_int, [c_vp]),
     "pmb_stencil_tune": (c_int, [c_vp, c_int, c_int]),
     "pmb_stencil_tuning": (c_int, [c_vp, c_int]),
@@ -108,6 +109,8 @@ _SIGNATURES = {
     "pmb_ichol_destroy": (c_int, [c_vp]),
     "pmb_planes_inv_diag": (c_int, [c_vp, c_int, c_int, c_vp, c_vp]),
     "pmb_csr_add_diag_rowptr": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_csr_to_planes": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_dbl, c_vp,
+                                  c_vp]),
     "pmb_csr_add_diag_fill": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_dense_solve": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_mask_scale": (c_int, [c_vp, c_i64, c_dbl, c_vp, c_vp]),

@@ -25,19 +25,20 @@ __all__ = ["estimate_alpha_cf", "estimate_alpha", "estimate_alpha_knn", "estimat
 
 def hard_system(image, trimap, epsilon=1e-7, radius=1, is_fg=None, is_known=None):
     """Device ``(L_U, b_U, context)`` of the hard-constraint system."""
-    if radius != 1:
-        raise NotImplementedError("estimate_alpha_cf on the device supports radius=1")
+    if int(radius) != radius or radius < 1:
+        raise ValueError("radius must be a positive integer")
+    radius = int(radius)
     lib = _ffi.lib()
     h, w = trimap.shape[:2]
     n = h * w
     image_t = _image_to_device(image)
     known_t = _mask_to_device(is_known, h, w).reshape(-1)
     fg_t = _mask_to_device(is_fg, h, w).reshape(-1)
-    S = 25
+    S = (4 * radius + 1) ** 2
     values = dev.empty(n * S, torch.float64)
     indices = dev.empty(n * S, torch.int64)
     indptr = dev.empty(n + 1, torch.int64)
-    _ffi.check(lib.pmb_cf_laplacian_ell(dev.ptr(image_t), dev.ptr(known_t), h, w, 1,
+    _ffi.check(lib.pmb_cf_laplacian_ell(dev.ptr(image_t), dev.ptr(known_t), h, w, radius,
                                         float(epsilon), None, 0.0, dev.ptr(values),
                                         dev.ptr(indices), dev.ptr(indptr), dev.stream()),
                "cf_laplacian")
@@ -49,15 +50,16 @@ def hard_system(image, trimap, epsilon=1e-7, radius=1, is_fg=None, is_known=None
     nu = int(cidx[n].item())
     rowptr = dev.empty(nu + 1, torch.int64)
     scratch_u = dev.empty(int(lib.pmb_scan_scratch_elems(nu + 1)), torch.int64)
-    _ffi.check(lib.pmb_hard_lu_rowptr(dev.ptr(known_t), h, w, dev.ptr(cidx), nu, dev.ptr(rowptr),
-                                      dev.ptr(scratch_u), dev.stream()), "L_U rowptr")
+    _ffi.check(lib.pmb_hard_lu_rowptr(dev.ptr(known_t), h, w, radius, dev.ptr(cidx), nu,
+                                      dev.ptr(rowptr), dev.ptr(scratch_u), dev.stream()),
+               "L_U rowptr")
     nnz = int(rowptr[nu].item())
     cols = dev.empty(max(nnz, 1), torch.int64)
     data = dev.empty(max(nnz, 1), torch.float64)
     rhs = dev.empty(max(nu, 1), torch.float64)
     _ffi.check(lib.pmb_hard_lu_fill(dev.ptr(values), dev.ptr(known_t), dev.ptr(fg_t), h, w,
-                                    dev.ptr(cidx), dev.ptr(rowptr), dev.ptr(cols), dev.ptr(data),
-                                    dev.ptr(rhs), dev.stream()), "L_U fill")
+                                    radius, dev.ptr(cidx), dev.ptr(rowptr), dev.ptr(cols),
+                                    dev.ptr(data), dev.ptr(rhs), dev.stream()), "L_U fill")
     L_U = DeviceCSRMatrix(shape=(nu, nu), pmb_arrays=(rowptr, cols[:nnz], data[:nnz]))
     return L_U, rhs[:nu], (known_t, cidx, n)
 

@@ -244,7 +244,7 @@ int pmb_launch_cf_ell(const double* image, const uint8_t* known, int h, int w, i
     if (r == 1) cf_assemble_kernel<1, kModeEll><<<grid, kAT * kAT, 0, s>>>(a);
     else if (r == 2) cf_assemble_kernel<2, kModeEll><<<grid, kAT * kAT, 0, s>>>(a);
     else return -1;
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_cf_half(const double* image, const uint8_t* known, int h, int w, double eps,
@@ -255,7 +255,7 @@ int pmb_launch_cf_half(const double* image, const uint8_t* known, int h, int w, 
     a.planes = planes; a.pitch = pitch; a.diag_mask = diag_mask; a.diag_value = diag_value;
     dim3 grid((w + kAT - 1) / kAT, (h + kAT - 1) / kAT);
     cf_assemble_kernel<1, kModeHalf><<<grid, kAT * kAT, 0, s>>>(a);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_cf_hard(const double* image, const uint8_t* known, const uint8_t* fg, int h,
@@ -266,7 +266,7 @@ int pmb_launch_cf_hard(const double* image, const uint8_t* known, const uint8_t*
     a.planes = planes; a.pitch = pitch; a.fg = fg; a.rhs = rhs;
     dim3 grid((w + kAT - 1) / kAT, (h + kAT - 1) / kAT);
     cf_assemble_kernel<1, kModeHard><<<grid, kAT * kAT, 0, s>>>(a);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 // --------------------------------------------------------------------------
@@ -354,14 +354,14 @@ __global__ void k_flag_unknown(const uint8_t* __restrict__ known, int64_t n, int
 // Row counts of L_U = L[U, :][:, U] (estimate_alpha_cf.py:66): in-image
 // slots whose column is unknown. cidx holds the compact index of every
 // pixel (exclusive scan of the unknown flags).
-__global__ void k_lu_count(const uint8_t* __restrict__ known, int h, int w, int64_t* counts_u,
-                           const int64_t* __restrict__ cidx) {
+__global__ void k_lu_count(const uint8_t* __restrict__ known, int h, int w, int r,
+                           int64_t* counts_u, const int64_t* __restrict__ cidx) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= (int64_t)h * w || known[i]) return;
     const int y = (int)(i / w), x = (int)(i % w);
     int64_t c = 0;
-    for (int dy = -2; dy <= 2; ++dy)
-        for (int dx = -2; dx <= 2; ++dx) {
+    for (int dy = -2 * r; dy <= 2 * r; ++dy)
+        for (int dx = -2 * r; dx <= 2 * r; ++dx) {
             const int yj = y + dy, xj = x + dx;
             if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
             if (!known[(int64_t)yj * w + xj]) ++c;
@@ -372,21 +372,22 @@ __global__ void k_lu_count(const uint8_t* __restrict__ known, int h, int w, int6
 // Fill L_U (CSR, compact indices) and b_U = -R m with m = is_fg on the known
 // columns, summed in column order (estimate_alpha_cf.py:66-74).
 __global__ void k_lu_fill(const double* __restrict__ values, const uint8_t* __restrict__ known,
-                          const uint8_t* __restrict__ fg, int h, int w,
+                          const uint8_t* __restrict__ fg, int h, int w, int r,
                           const int64_t* __restrict__ cidx, const int64_t* __restrict__ rowptr,
                           int64_t* indices, double* data, double* rhs) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= (int64_t)h * w || known[i]) return;
     const int y = (int)(i / w), x = (int)(i % w);
+    const int S = 4 * r + 1;   // ELL row: an S x S block of offsets
     const int64_t ci = cidx[i];
     int64_t k = rowptr[ci];
     double sum = 0.0;
-    for (int dy = -2; dy <= 2; ++dy)
-        for (int dx = -2; dx <= 2; ++dx) {
+    for (int dy = -2 * r; dy <= 2 * r; ++dy)
+        for (int dx = -2 * r; dx <= 2 * r; ++dx) {
             const int yj = y + dy, xj = x + dx;
             if (yj < 0 || yj >= h || xj < 0 || xj >= w) continue;
             const int64_t j = (int64_t)yj * w + xj;
-            const double v = values[i * 25 + (dy + 2) * 5 + (dx + 2)];
+            const double v = values[i * S * S + (dy + 2 * r) * S + (dx + 2 * r)];
             if (known[j]) {
                 sum += v * (fg[j] ? 1.0 : 0.0);
             } else {
@@ -438,61 +439,61 @@ int pmb_scan_exclusive(int64_t* v, int64_t n, int64_t* chunk_scratch, int64_t* t
                        cudaStream_t s) {
     const int64_t nchunks = (n + 1023) / 1024;
     if (n <= 0) {
-        return cudaMemsetAsync(total, 0, sizeof(int64_t), s) == cudaSuccess ? 0 : -2;
+        return launch_status(cudaMemsetAsync(total, 0, sizeof(int64_t), s));
     }
     k_scan_chunks<<<(unsigned)nchunks, 1024, 0, s>>>(v, n, chunk_scratch);
     k_scan_totals<<<1, 32, 0, s>>>(chunk_scratch, nchunks, total);
     k_scan_add<<<(unsigned)nchunks, 1024, 0, s>>>(v, n, chunk_scratch);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_ell_count(const double* values, int h, int w, int r, int64_t* counts, cudaStream_t s) {
     const int64_t n = (int64_t)h * w;
     k_ell_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, h, w, r, counts);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_ell_fill(const double* values, int h, int w, int r, const int64_t* rowptr,
                         int64_t* indices, double* data, cudaStream_t s) {
     const int64_t n = (int64_t)h * w;
     k_ell_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, h, w, r, rowptr, indices, data);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_flag_unknown(const uint8_t* known, int64_t n, int64_t* flag, cudaStream_t s) {
     k_flag_unknown<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(known, n, flag);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
-int pmb_launch_lu_count(const uint8_t* known, int h, int w, int64_t* counts_u, const int64_t* cidx,
-                        cudaStream_t s) {
+int pmb_launch_lu_count(const uint8_t* known, int h, int w, int r, int64_t* counts_u,
+                        const int64_t* cidx, cudaStream_t s) {
     const int64_t n = (int64_t)h * w;
-    k_lu_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(known, h, w, counts_u, cidx);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    k_lu_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(known, h, w, r, counts_u, cidx);
+    return launch_status();
 }
 
 int pmb_launch_lu_fill(const double* values, const uint8_t* known, const uint8_t* fg, int h, int w,
-                       const int64_t* cidx, const int64_t* rowptr, int64_t* indices, double* data,
-                       double* rhs, cudaStream_t s) {
+                       int r, const int64_t* cidx, const int64_t* rowptr, int64_t* indices,
+                       double* data, double* rhs, cudaStream_t s) {
     const int64_t n = (int64_t)h * w;
-    k_lu_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, known, fg, h, w, cidx, rowptr,
+    k_lu_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(values, known, fg, h, w, r, cidx, rowptr,
                                                           indices, data, rhs);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_alpha_compose(const double* trimap, const uint8_t* known, const int64_t* cidx,
                              const double* xu, int64_t n, double* alpha, cudaStream_t s) {
     k_alpha_compose<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(trimap, known, cidx, xu, n, alpha);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 int pmb_launch_trimap_masks(const double* trimap, int64_t n, double fg_thr, double bg_thr,
                             uint8_t* is_fg, uint8_t* is_known, unsigned long long* counts,
                             cudaStream_t s) {
-    if (cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess) return -2;
+    if (launch_status(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s))) return -2;
     k_trimap_masks<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(trimap, n, fg_thr, bg_thr, is_fg,
                                                                is_known, counts);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }
 
 // --------------------------------------------------------------------------
@@ -548,7 +549,7 @@ int pmb_launch_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t*
     int64_t* scratch = nullptr;
     if (int rc = static_scan_address(&scratch)) return rc;
     const int64_t nchunks = (n + 1 + 1023) / 1024;
-    if (cudaMemsetAsync(cidx + n, 0, sizeof(int64_t), s) != cudaSuccess) return -2;
+    if (launch_status(cudaMemsetAsync(cidx + n, 0, sizeof(int64_t), s))) return -2;
     if (pmb_launch_flag_unknown(is_known, n, cidx, s)) return -2;
     return pmb_scan_exclusive(cidx, n + 1, scratch, scratch + nchunks, s);
 }
@@ -702,5 +703,5 @@ int pmb_launch_cf_vjp(const double* image, const uint8_t* known, int h, int w, d
                       const double* x, const double* mu, double* grad, cudaStream_t s) {
     const dim3 grid((w + pmb::kAT - 1) / pmb::kAT, (h + pmb::kAT - 1) / pmb::kAT);
     pmb::cf_vjp_kernel<<<grid, pmb::kAT * pmb::kAT, 0, s>>>(image, known, h, w, eps, x, mu, grad);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return launch_status();
 }

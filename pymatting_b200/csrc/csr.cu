@@ -278,7 +278,8 @@ constexpr int kRowMax = 64;
 // column, duplicates summed in stored order, c_i added to the diagonal and
 // explicit zeros dropped (what L + scipy.sparse.diags(c) followed by tocsr()
 // and sum_duplicates() yields, pymatting/laplacian/laplacian.py:50-55).
-// Returns the number of entries, or -1 if the row is longer than kRowMax.
+// Rows of fewer than kRowMax stored entries only (longer rows take
+// canonical_row_long); returns the number of entries.
 __device__ int canonical_row(const CsrMat& A, int64_t i, const double* __restrict__ c,
                              int64_t* cols, double* vals) {
     int m = 0;
@@ -335,19 +336,69 @@ __device__ int canonical_row(const CsrMat& A, int64_t i, const double* __restric
     return z;
 }
 
+// The same canonical row for rows longer than kRowMax, without a row buffer:
+// the distinct columns are visited in ascending order by repeated selection
+// of the next larger column (O(m^2) per row), each column's stored entries
+// are summed in stored order, then c_i is added on the diagonal and zeros
+// are dropped — the arithmetic of canonical_row. Writes the entries to
+// out_cols / out_vals when they are given; returns the entry count.
+__device__ int64_t canonical_row_long(const CsrMat& A, int64_t i, const double* __restrict__ c,
+                                      int64_t* out_cols, double* out_vals) {
+    const int64_t k0 = A.indptr[i], k1 = A.indptr[i + 1];
+    int64_t count = 0;
+    int64_t last = INT64_MIN;
+    bool diag_done = false;
+    auto emit = [&](int64_t col, double v) {
+        if (v == 0.0) return;
+        if (out_cols) {
+            out_cols[count] = col;
+            out_vals[count] = v;
+        }
+        ++count;
+    };
+    for (;;) {
+        int64_t col = INT64_MAX;
+        for (int64_t k = k0; k < k1; ++k) {
+            const int64_t q = A.indices[k];
+            if (q > last && q < col) col = q;
+        }
+        // The diagonal comes in its place even if the row does not store it.
+        if (!diag_done && i > last && i < col && c[i] != 0.0) {
+            emit(i, c[i]);
+            diag_done = true;
+            last = i;
+            continue;
+        }
+        if (col == INT64_MAX) break;
+        double v = 0.0;
+        bool first = true;
+        for (int64_t k = k0; k < k1; ++k)
+            if (A.indices[k] == col) {
+                v = first ? A.data[k] : v + A.data[k];
+                first = false;
+            }
+        if (col == i) {
+            v = v + c[i];
+            diag_done = true;
+        }
+        emit(col, v);
+        last = col;
+    }
+    return count;
+}
+
 __global__ void k_add_diag_count(CsrMat A, int64_t n, const double* __restrict__ c, int64_t* counts,
                                  int* overflow) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    (void)overflow;
+    if (A.indptr[i + 1] - A.indptr[i] >= kRowMax) {
+        counts[i] = canonical_row_long(A, i, c, nullptr, nullptr);
+        return;
+    }
     int64_t cols[kRowMax];
     double vals[kRowMax];
-    const int m = canonical_row(A, i, c, cols, vals);
-    if (m < 0) {
-        atomicExch(overflow, 1);
-        counts[i] = 0;
-    } else {
-        counts[i] = m;
-    }
+    counts[i] = canonical_row(A, i, c, cols, vals);
 }
 
 __global__ void k_add_diag_fill(CsrMat A, int64_t n, const double* __restrict__ c,
@@ -355,14 +406,84 @@ __global__ void k_add_diag_fill(CsrMat A, int64_t n, const double* __restrict__ 
                                 double* out_vals) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int64_t at = rowptr[i];
+    if (A.indptr[i + 1] - A.indptr[i] >= kRowMax) {
+        canonical_row_long(A, i, c, out_cols + at, out_vals + at);
+        return;
+    }
     int64_t cols[kRowMax];
     double vals[kRowMax];
     const int m = canonical_row(A, i, c, cols, vals);
-    const int64_t at = rowptr[i];
     for (int q = 0; q < m; ++q) {
         out_cols[at + q] = cols[q];
         out_vals[at + q] = vals[q];
     }
+}
+
+// Grid matrix -> half-stencil planes. Row i = (y, x) of an (h w) x (h w)
+// matrix: an entry at column j = (yj, xj) with d = (yj - y, xj - x) inside
+// the 5x5 block is a forward entry (stored in plane half_index(d) at pixel
+// i) or a backward one (kept in `back` at pixel j for the symmetry check);
+// duplicates are summed. Entries with |dy| > 2 or |dx| > 2 are counted in
+// bad[0]. planes and back must be zero on entry.
+__global__ void k_csr_to_planes(CsrMat A, int h, int w, int pitch, double* planes, double* back,
+                                unsigned long long* bad) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)h * w;
+    if (i >= n) return;
+    const int y = (int)(i / w), x = (int)(i % w);
+    const int64_t ps = (int64_t)h * pitch;
+    unsigned long long nbad = 0;
+    for (int64_t k = A.indptr[i]; k < A.indptr[i + 1]; ++k) {
+        const int64_t j = A.indices[k];
+        const int yj = (int)(j / w), xj = (int)(j % w);
+        const int dy = yj - y, dx = xj - x;
+        if (j < 0 || j >= n || dy < -2 || dy > 2 || dx < -2 || dx > 2) {
+            ++nbad;
+            continue;
+        }
+        const int p = half_index(dy, dx);
+        if (p >= 0) planes[p * ps + (int64_t)y * pitch + x] += A.data[k];
+        else back[(half_index(-dy, -dx) - 1) * ps + (int64_t)yj * pitch + xj] += A.data[k];
+    }
+    if (nbad) atomicAdd(&bad[0], nbad);
+}
+
+// Symmetry: A[i, i + d] (plane p at pixel i) against A[i + d, i] (kept in
+// back at pixel i), within rel_tol of |A_ii| + |A_jj| + both values (a
+// Laplacian assembled window by window is symmetric up to rounding, and
+// entries that are sums of cancelling terms keep rounding of the diagonal's
+// size). Pairs whose partner pixel lies outside the grid must be zero.
+__global__ void k_planes_symmetric(int h, int w, int pitch, const double* planes,
+                                   const double* back, double rel_tol, unsigned long long* bad) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)h * w) return;
+    const int y = (int)(i / w), x = (int)(i % w);
+    const int64_t ps = (int64_t)h * pitch;
+    unsigned long long nbad = 0;
+    for (int p = 1; p < kNH; ++p) {
+        const double f = planes[p * ps + (int64_t)y * pitch + x];
+        const double b = back[(p - 1) * ps + (int64_t)y * pitch + x];
+        const int yj = y + half_dy(p), xj = x + half_dx(p);
+        const bool inside = yj >= 0 && yj < h && xj >= 0 && xj < w;
+        if (!inside) {
+            if (f != 0.0 || b != 0.0) ++nbad;
+            continue;
+        }
+        const double di = planes[(int64_t)y * pitch + x];
+        const double dj = planes[(int64_t)yj * pitch + xj];
+        if (fabs(f - b) > rel_tol * (fabs(f) + fabs(b) + fabs(di) + fabs(dj))) ++nbad;
+    }
+    if (nbad) atomicAdd(&bad[1], nbad);
+}
+
+void csr_launch_to_planes(const CsrMat& A, int h, int w, int pitch, double* planes, double* back,
+                          double rel_tol, unsigned long long* bad, cudaStream_t s) {
+    const int64_t n = (int64_t)h * w;
+    if (n <= 0) return;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    k_csr_to_planes<<<g, 256, 0, s>>>(A, h, w, pitch, planes, back, bad);
+    k_planes_symmetric<<<g, 256, 0, s>>>(h, w, pitch, planes, back, rel_tol, bad);
 }
 
 void csr_launch_add_diag_count(const CsrMat& A, int64_t n, const double* c, int64_t* counts,

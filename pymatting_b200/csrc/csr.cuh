@@ -39,5 +39,10 @@ void csr_launch_add_diag_count(const CsrMat& A, int64_t n, const double* c, int6
                                int* overflow, cudaStream_t s);
 void csr_launch_add_diag_fill(const CsrMat& A, int64_t n, const double* c, const int64_t* rowptr,
                               int64_t* cols, double* vals, cudaStream_t s);
+// Half-stencil planes (pitched, 13 planes) of a grid matrix given as CSR,
+// and the counts of entries outside the 5x5 pattern (bad[0]) and of
+// forward/backward pairs that differ by more than rel_tol (bad[1]).
+void csr_launch_to_planes(const CsrMat& A, int h, int w, int pitch, double* planes, double* back,
+                          double rel_tol, unsigned long long* bad, cudaStream_t s);
 
 }  // namespace pmb

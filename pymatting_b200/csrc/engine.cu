@@ -35,9 +35,9 @@ int pmb_launch_ell_count(const double*, int, int, int, int64_t*, cudaStream_t);
 int pmb_launch_ell_fill(const double*, int, int, int, const int64_t*, int64_t*, double*,
                         cudaStream_t);
 int pmb_launch_flag_unknown(const uint8_t*, int64_t, int64_t*, cudaStream_t);
-int pmb_launch_lu_count(const uint8_t*, int, int, int64_t*, const int64_t*, cudaStream_t);
-int pmb_launch_lu_fill(const double*, const uint8_t*, const uint8_t*, int, int, const int64_t*,
-                       const int64_t*, int64_t*, double*, double*, cudaStream_t);
+int pmb_launch_lu_count(const uint8_t*, int, int, int, int64_t*, const int64_t*, cudaStream_t);
+int pmb_launch_lu_fill(const double*, const uint8_t*, const uint8_t*, int, int, int,
+                       const int64_t*, const int64_t*, int64_t*, double*, double*, cudaStream_t);
 int pmb_launch_alpha_compose(const double*, const uint8_t*, const int64_t*, const double*, int64_t,
                              double*, cudaStream_t);
 int pmb_launch_trimap_masks(const double*, int64_t, double, double, uint8_t*, uint8_t*,
@@ -64,6 +64,26 @@ static int fail(int code, const std::string& msg) {
     } while (0)
 
 enum : int { kErrArg = -1, kErrCuda = -2, kErrState = -3, kErrZeroDiv = -4 };
+
+static thread_local cudaError_t t_launch_error = cudaSuccess;
+int launch_status(cudaError_t e) {
+    if (e == cudaSuccess) return 0;
+    t_launch_error = e;
+    return -2;
+}
+cudaError_t take_launch_error() {
+    const cudaError_t e = t_launch_error;
+    t_launch_error = cudaSuccess;
+    return e;
+}
+
+// Text of the CUDA error behind a failed launch helper (the error the helper
+// recorded, else the pending one; "bad arguments or sizes" if there is none).
+static const char* launch_error_text() {
+    cudaError_t e = take_launch_error();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e != cudaSuccess ? cudaGetErrorString(e) : "bad arguments or sizes";
+}
 
 static inline int pitch_for(int w) { return ((w + 31) / 32) * 32; }
 
@@ -186,6 +206,9 @@ struct Stencil {
     bool bound = false, setup_done = false;
     // last solve
     int64_t launches = 0;
+    // Kernel profile (pmb_stencil_profile): when set, every launch of an
+    // iteration is followed by an event tagged with the launch's kind.
+    std::vector<std::pair<int, cudaEvent_t>>* prof = nullptr;
 
     template <typename T> T* at(size_t off) const { return reinterpret_cast<T*>(ws + off); }
     InstState* state() const { return at<InstState>(o_state); }
@@ -729,6 +752,29 @@ template <typename T> static const DirectDesc* direct_dev(Stencil& S);
 template <> const DirectDesc* direct_dev<double>(Stencil& S) { return S.at<DirectDesc>(S.o_direct64); }
 template <> const DirectDesc* direct_dev<float>(Stencil& S) { return S.at<DirectDesc>(S.o_direct32); }
 
+// Kinds of launches told apart by pmb_stencil_profile (index into its output).
+enum : int {
+    kPkApply = 0,   // CG apply p = z + beta p, Ap, p.Ap
+    kPkUpdate,      // CG vector update x, r, |r|
+    kPkRefine,      // mixed: FP64 correction and residual replacement
+    kPkDown0,       // V-cycle restriction from level 0
+    kPkDown,        // restriction from levels >= 1
+    kPkTail,        // shared-memory tail of the small levels
+    kPkDirect,      // dense coarsest solves outside a tail
+    kPkUp,          // prolongation + post sweep at levels >= 1
+    kPkUp0,         // prolongation + post sweep at level 0 (z, r.z, beta)
+    kPkOther,       // extra smoothing sweeps, separate r.z
+    kPkCount
+};
+
+static void prof_mark(Stencil& S, int kind) {
+    if (!S.prof) return;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, S.stream);
+    S.prof->push_back({kind, e});
+}
+
 // V-cycle z = M r (vcycle.py:46-100) at level 0 with r = b0 (the level-0 b
 // buffer) and z = z0 (the level-0 x buffer). With st != null the level-0
 // pass also reduces r . z and finishes beta.
@@ -753,12 +799,14 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
             launch_vc_smooth<T>(LaunchCfg{persistent_grid(f)}, f.wl, S.maps(), -1, lvl_P<T>(S, l),
                                 B(l), a, om, st, S.err(), s);
             ++S.launches;
+            prof_mark(S, kPkOther);
             bool in_a = true;
             for (int k = 1; k < pre; ++k) {
                 launch_vc_smooth<T>(LaunchCfg{persistent_grid(f)}, f.wl, S.maps(),
                                     in_a ? kMapXAF : kMapXBF, lvl_P<T>(S, l), B(l), in_a ? bb : a,
                                     om, st, S.err(), s);
                 ++S.launches;
+                prof_mark(S, kPkOther);
                 in_a = !in_a;
             }
             xs_slot_f[l] = in_a ? kMapXAF : kMapXBF;
@@ -767,12 +815,14 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
         launch_vc_down<T>(pre, LaunchCfg{persistent_grid(c)}, c.wl, c.partner_dev, S.maps(),
                           xs_slot_d[l], B(l + 1), om, st, S.err(), s);
         ++S.launches;
+        prof_mark(S, l == 0 ? kPkDown0 : kPkDown);
     }
     // Small levels of the images that have a tail, in one clustered launch.
     if (!S.tail_images.empty()) {
         launch_vc_tail<T>(S.at<TailDesc<T>>(S.o_tail), (int)S.tail_images.size(), S.tail_smem, st,
                           om, S.err(), s);
         ++S.launches;
+        prof_mark(S, kPkTail);
     }
     // Coarsest solves of the other images, whatever their depth.
     for (size_t i = 0; i < S.direct64.size(); ++i) {
@@ -782,6 +832,7 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
         const bool z_out = (l == 0);
         launch_vc_direct<T>(direct_dev<T>(S) + i, 1, B(l), X(l), st, z_out && st != nullptr, s);
         ++S.launches;
+        prof_mark(S, kPkDirect);
     }
     for (int l = L - 2; l >= 0; --l) {
         HostList& f = S.levels[l].fine;
@@ -796,12 +847,14 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
                         first_out, om, st, reduce_here ? 1 : 0, dr, reorth, S.partials(), S.err(),
                         s);
         ++S.launches;
+        prof_mark(S, l == 0 ? kPkUp0 : kPkUp);
         bool cur_x = first_in_x;
         for (int k = 0; k < extra; ++k) {
             T* nxt = cur_x ? lvl_xa<T>(S, l) : X(l);
             launch_vc_smooth<T>(Lf, f.wl, S.maps(), cur_x ? kMapXF : kMapXAF, lvl_P<T>(S, l), B(l),
                                 nxt, om, st, S.err(), s);
             ++S.launches;
+            prof_mark(S, kPkOther);
             cur_x = !cur_x;
         }
         if (l == 0 && st && extra > 0) {
@@ -810,6 +863,7 @@ static void run_vcycle(Stencil& S, const T* b0, T* z0, InstState* st, const T* d
             launch_cg_rz<T>(LaunchCfg{persistent_grid(S.levels[0].flat)}, S.levels[0].flat.wl, b0,
                             z0, dr, reorth, st, S.partials(), s);
             ++S.launches;
+            prof_mark(S, kPkOther);
         }
     }
 }
@@ -824,10 +878,12 @@ static void cg_iteration(Stencil& S, int reorth) {
     const int zslot = S.precond == kPrecNone ? kMapBF : kMapZF;
     launch_cg_apply<T>(S.vec_apply, LaunchCfg{persistent_grid(S.fine0)}, S.fine0.wl, S.maps(), zslot,
                        v.p0, v.p1, v.ap, st, S.partials(), S.err(), s);
+    prof_mark(S, kPkApply);
     const bool mixed = S.precision == 1;
     launch_cg_update<T>(S.precond, LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, v.P, v.x, v.r,
                         v.z, v.p0, v.p1, v.ap, v.dr, reorth, mixed ? 1 : 0, S.err() + kPendingSlot, st,
                         S.partials(), s);
+    prof_mark(S, kPkUpdate);
     S.launches += 2;
     if (mixed) {
         // Residual replacement for the images whose FP32 phase just ended.
@@ -840,6 +896,7 @@ static void cg_iteration(Stencil& S, int reorth) {
                                S.at<float>(S.o_xin32), S.at<float>(S.o_z32), S.outer(), st,
                                S.partials(), 0.0, 0.0, S.delta, 0, S.max_outer, S.err(), s);
         S.launches += 2;
+        prof_mark(S, kPkRefine);
     }
     if (S.precond == kPrecVcycle) run_vcycle<T>(S, v.r, v.z, st, v.dr, reorth);
 }
@@ -900,8 +957,8 @@ static int iterate(Stencil& S, int reorth, int maxiter) {
     return check_err(S);
 }
 
-static int solve_fp64(Stencil& S, const double* x0, double atol, double rtol, int maxiter,
-                      int reorth) {
+// Initial residual and first preconditioner apply of an FP64 solve.
+static void start_fp64(Stencil& S, const double* x0, double atol, double rtol, int maxiter) {
     cudaStream_t s = S.stream;
     CgVecs<double> v = cg_vecs<double>(S);
     HostList& a = S.fine0;
@@ -913,11 +970,18 @@ static int solve_fp64(Stencil& S, const double* x0, double atol, double rtol, in
                            S.partials(), atol, rtol, maxiter, S.err(), s);
     S.launches += 1;
     if (S.precond == kPrecVcycle) run_vcycle<double>(S, v.r, v.z, S.state(), v.dr, 0);
+}
+
+static int solve_fp64(Stencil& S, const double* x0, double atol, double rtol, int maxiter,
+                      int reorth) {
+    start_fp64(S, x0, atol, rtol, maxiter);
     return iterate<double>(S, reorth, maxiter);
 }
 
-static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, int maxiter,
-                       int reorth, double inner_rtol, int max_outer) {
+// First FP64 residual, outer state and first preconditioner apply of a
+// mixed-precision solve.
+static int start_mixed(Stencil& S, const double* x0, double atol, double rtol, int maxiter,
+                       double inner_rtol, int max_outer) {
     cudaStream_t s = S.stream;
     CgVecs<float> v = cg_vecs<float>(S);
     HostList& a = S.fine0;
@@ -944,10 +1008,18 @@ static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, i
                            S.partials(), atol, rtol, inner_rtol, maxiter, max_outer, S.err(), s);
     S.launches += 1;
     if (S.precond == kPrecVcycle) run_vcycle<float>(S, v.r, v.z, S.state(), v.dr, 0);
+    return 0;
+}
+
+static int solve_mixed(Stencil& S, const double* x0, double atol, double rtol, int maxiter,
+                       int reorth, double inner_rtol, int max_outer) {
+    CgVecs<float> v = cg_vecs<float>(S);
+    double* x64 = S.at<double>(S.o_x64);
+    if (int rc = start_mixed(S, x0, atol, rtol, maxiter, inner_rtol, max_outer)) return rc;
     if (int rc = iterate<float>(S, reorth, maxiter)) return rc;
     // Fold the last FP32 correction into x64 (zero for converged images).
     launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, x64, v.x, nullptr,
-                          S.err() + kPendingSlot, s);
+                          S.err() + kPendingSlot, S.stream);
     S.launches += 1;
     if (int rc = read_states(S, true)) return rc;
     return check_err(S);
@@ -979,7 +1051,7 @@ PMB_API int pmb_cf_laplacian_ell(const double* image, const uint8_t* is_known, i
     int rc = pmb_launch_cf_ell(image, is_known, h, w, radius, epsilon, diag_mask, diag_value,
                                values, indices, indptr, (cudaStream_t)stream);
     if (rc == -1) return fail(kErrArg, "pmb_cf_laplacian_ell: radius must be 1 or 2");
-    if (rc) return fail(kErrCuda, std::string("cf_laplacian launch: ") + cudaGetErrorString(cudaGetLastError()));
+    if (rc) return fail(kErrCuda, std::string("cf_laplacian launch: ") + launch_error_text());
     return 0;
 }
 
@@ -990,7 +1062,7 @@ PMB_API int pmb_cf_laplacian_planes(const double* image, const uint8_t* is_known
         return fail(kErrArg, "pmb_cf_laplacian_planes: bad arguments");
     if (pmb_launch_cf_half(image, is_known, h, w, epsilon, planes, pitch_for(w), diag_mask,
                            diag_value, (cudaStream_t)stream))
-        return fail(kErrCuda, std::string("cf planes launch: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(kErrCuda, std::string("cf planes launch: ") + launch_error_text());
     return 0;
 }
 
@@ -1011,7 +1083,7 @@ PMB_API int pmb_lkm_setup(const double* image, int h, int w, int radius, double 
     if (!image || !windows || !scratch || radius < 0 || h <= 2 * radius || w <= 2 * radius)
         return fail(kErrArg, "pmb_lkm_setup: bad arguments (the image must exceed 2 radius)");
     if (pmb_launch_lkm_setup(image, h, w, radius, epsilon, windows, scratch, (cudaStream_t)stream))
-        return fail(kErrCuda, std::string("lkm setup: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(kErrCuda, std::string("lkm setup: ") + launch_error_text());
     return 0;
 }
 
@@ -1023,7 +1095,7 @@ PMB_API int pmb_lkm_apply(const double* image, int h, int w, int radius, const d
         return fail(kErrArg, "pmb_lkm_apply: bad arguments");
     if (pmb_launch_lkm_apply(image, h, w, radius, windows, diag_add, p, out, scratch,
                              (cudaStream_t)stream))
-        return fail(kErrCuda, std::string("lkm apply: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(kErrCuda, std::string("lkm apply: ") + launch_error_text());
     return 0;
 }
 
@@ -1035,7 +1107,7 @@ PMB_API int pmb_lkm_diagonal(const double* image, int h, int w, int radius, cons
         return fail(kErrArg, "pmb_lkm_diagonal: bad arguments");
     if (pmb_launch_lkm_diag(image, h, w, radius, windows, diag_add, diag, inv_diag, scratch,
                             (cudaStream_t)stream))
-        return fail(kErrCuda, std::string("lkm diagonal: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(kErrCuda, std::string("lkm diagonal: ") + launch_error_text());
     return 0;
 }
 
@@ -1049,7 +1121,7 @@ PMB_API int pmb_cf_laplacian_vjp(const double* image, const uint8_t* is_known, i
         return fail(kErrArg, "pmb_cf_laplacian_vjp: bad arguments");
     if (pmb_launch_cf_vjp(image, is_known, h, w, epsilon, x, mu, grad, (cudaStream_t)stream))
         return fail(kErrCuda, std::string("cf_laplacian_vjp launch: ") +
-                                  cudaGetErrorString(cudaGetLastError()));
+                                  launch_error_text());
     return 0;
 }
 
@@ -1127,7 +1199,7 @@ PMB_API int pmb_window_laplacian(int mode, const double* image, int h, int w, in
                                                rowptr, cols, vals, (cudaStream_t)stream);
     if (rc == -2) return fail(kErrArg, "pmb_window_laplacian: bad arguments");
     if (rc) return fail(kErrCuda, std::string("pmb_window_laplacian launch: ") +
-                                      cudaGetErrorString(cudaGetLastError()));
+                                      launch_error_text());
     return 0;
 }
 
@@ -1147,7 +1219,7 @@ PMB_API int pmb_lbdm_laplacian(const double* image, int h, int w, int radius, do
                                              cols, vals, (cudaStream_t)stream);
     if (rc == -2) return fail(kErrArg, "pmb_lbdm_laplacian: bad arguments (radius 1 or 2, image larger than 2 radius)");
     if (rc) return fail(kErrCuda, std::string("pmb_lbdm_laplacian launch: ") +
-                                      cudaGetErrorString(cudaGetLastError()));
+                                      launch_error_text());
     return 0;
 }
 
@@ -1166,7 +1238,7 @@ PMB_API int pmb_knn_laplacian(const double* image, int h, int w, const int* n_ne
     const int rc = pmb_launch_knn(image, h, w, n_neighbors, distance_weights, passes, soft, scratch,
                                   rowptr, cols, vals, nnz, (cudaStream_t)stream);
     if (rc == -2) return fail(kErrArg, "pmb_knn_laplacian: bad arguments (1 to 4 passes of 1 to 64 neighbours, at most the pixel count)");
-    if (rc) return fail(kErrCuda, std::string("pmb_knn_laplacian: ") + cudaGetErrorString(cudaGetLastError()));
+    if (rc) return fail(kErrCuda, std::string("pmb_knn_laplacian: ") + launch_error_text());
     return 0;
 }
 
@@ -1179,7 +1251,7 @@ PMB_API int pmb_fg_cf_system(const double* alpha, int h, int w, double regulariz
     const int rc = pmb_launch_fg_cf_system(alpha, h, w, regularization, rowptr, cols, vals,
                                            scratch, (cudaStream_t)stream);
     if (rc == -2) return fail(kErrArg, "pmb_fg_cf_system: bad arguments");
-    if (rc) return fail(kErrCuda, std::string("pmb_fg_cf_system: ") + cudaGetErrorString(cudaGetLastError()));
+    if (rc) return fail(kErrCuda, std::string("pmb_fg_cf_system: ") + launch_error_text());
     return 0;
 }
 
@@ -1190,7 +1262,7 @@ PMB_API int pmb_cf_hard_system(const double* image, const uint8_t* is_known, con
         return fail(kErrArg, "pmb_cf_hard_system: bad arguments");
     if (pmb_launch_cf_hard(image, is_known, is_fg, h, w, epsilon, planes, pitch_for(w), rhs,
                            (cudaStream_t)stream))
-        return fail(kErrCuda, std::string("cf hard launch: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(kErrCuda, std::string("cf hard launch: ") + launch_error_text());
     return 0;
 }
 
@@ -1199,8 +1271,7 @@ PMB_API int64_t pmb_scan_scratch_elems(int64_t n) { return (n + 1023) / 1024 + 2
 #define PMB_LAUNCHED(expr, what)                                                      \
     do {                                                                              \
         if ((expr) != 0)                                                              \
-            return fail(kErrCuda, std::string(what) + ": " +                          \
-                                      cudaGetErrorString(cudaGetLastError()));        \
+            return fail(kErrCuda, std::string(what) + ": " + launch_error_text());   \
     } while (0)
 
 PMB_API int pmb_ell_csr_rowptr(const double* values, int h, int w, int radius, int64_t* rowptr,
@@ -1260,30 +1331,31 @@ PMB_API int pmb_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t
     const int rc = pmb_launch_unknown_index_static(is_known, n, cidx, (cudaStream_t)stream);
     if (rc == -3) return fail(kErrCuda, "pmb_unknown_index_static: scratch address lookup failed");
     if (rc) return fail(kErrCuda, std::string("pmb_unknown_index_static: ") +
-                                      cudaGetErrorString(cudaGetLastError()));
+                                      launch_error_text());
     return 0;
 }
 
-PMB_API int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, const int64_t* cidx,
-                               int64_t n_unknown, int64_t* rowptr, int64_t* scratch, void* stream) {
-    if (!is_known || !cidx || !rowptr || !scratch || h <= 0 || w <= 0)
+PMB_API int pmb_hard_lu_rowptr(const uint8_t* is_known, int h, int w, int radius,
+                               const int64_t* cidx, int64_t n_unknown, int64_t* rowptr,
+                               int64_t* scratch, void* stream) {
+    if (!is_known || !cidx || !rowptr || !scratch || h <= 0 || w <= 0 || radius < 1)
         return fail(kErrArg, "pmb_hard_lu_rowptr: bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
     PMB_CUDA(cudaMemsetAsync(rowptr, 0, sizeof(int64_t) * (n_unknown + 1), s));
-    PMB_LAUNCHED(pmb_launch_lu_count(is_known, h, w, rowptr, cidx, s), "L_U count");
+    PMB_LAUNCHED(pmb_launch_lu_count(is_known, h, w, radius, rowptr, cidx, s), "L_U count");
     PMB_LAUNCHED(pmb_scan_exclusive(rowptr, n_unknown + 1, scratch,
                                     scratch + (n_unknown + 1023) / 1024 + 1, s), "scan");
     return 0;
 }
 
 PMB_API int pmb_hard_lu_fill(const double* ell_values, const uint8_t* is_known,
-                             const uint8_t* is_fg, int h, int w, const int64_t* cidx,
+                             const uint8_t* is_fg, int h, int w, int radius, const int64_t* cidx,
                              const int64_t* rowptr, int64_t* indices, double* data, double* rhs,
                              void* stream) {
-    if (!ell_values || !is_known || !is_fg || !cidx || !rowptr || !rhs)
+    if (!ell_values || !is_known || !is_fg || !cidx || !rowptr || !rhs || radius < 1)
         return fail(kErrArg, "pmb_hard_lu_fill: bad arguments");
-    PMB_LAUNCHED(pmb_launch_lu_fill(ell_values, is_known, is_fg, h, w, cidx, rowptr, indices, data,
-                                    rhs, (cudaStream_t)stream), "L_U fill");
+    PMB_LAUNCHED(pmb_launch_lu_fill(ell_values, is_known, is_fg, h, w, radius, cidx, rowptr,
+                                    indices, data, rhs, (cudaStream_t)stream), "L_U fill");
     return 0;
 }
 
@@ -2092,6 +2164,27 @@ PMB_API int pmb_csr_add_diag_fill(int64_t n, const int64_t* indptr, const int64_
     return 0;
 }
 
+// Half-stencil planes of an (h w) x (h w) CSR matrix of a pixel grid (the
+// form vcycle needs, pymatting/preconditioner/vcycle.py:103-153 takes any A
+// of that shape). planes: 13 h pitch doubles, back: 12 h pitch doubles of
+// scratch; bad[0] counts entries outside the 5x5 neighbourhood, bad[1] the
+// forward/backward pairs that differ by more than rel_tol (relative).
+PMB_API int pmb_csr_to_planes(const int64_t* indptr, const int64_t* indices, const double* data,
+                              int h, int w, double* planes, double* back, double rel_tol,
+                              unsigned long long* bad, void* stream) {
+    if (!indptr || !planes || !back || !bad || h <= 0 || w <= 0)
+        return fail(kErrArg, "pmb_csr_to_planes: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t ps = (int64_t)h * pitch_for(w);
+    PMB_CUDA(cudaMemsetAsync(planes, 0, sizeof(double) * kNH * ps, s));
+    PMB_CUDA(cudaMemsetAsync(back, 0, sizeof(double) * (kNH - 1) * ps, s));
+    PMB_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), s));
+    csr_launch_to_planes(CsrMat{indptr, indices, data}, h, w, pitch_for(w), planes, back, rel_tol,
+                         bad, s);
+    PMB_CUDA(cudaGetLastError());
+    return 0;
+}
+
 // x = A^-1 b for a small square CSR matrix (n <= 4096). scratch: n*n
 // doubles; x holds b on entry; *singular set to 1 for a zero pivot.
 PMB_API int pmb_dense_solve(int64_t n, const int64_t* indptr, const int64_t* indices,
@@ -2141,6 +2234,52 @@ PMB_API int pmb_clip01(const double* x, int64_t n, double* out, void* stream) {
 // back-to-back launches on the solver's stream, timed with CUDA events on
 // that stream. The solver's inner precision decides FP64 or FP32. Used by
 // the benchmark to relate the Laplacian apply to the HBM roofline.
+// Milliseconds per iteration spent in each kind of launch (kPkCount values:
+// CG apply, CG update, refinement, restriction from level 0, restriction
+// from coarser levels, tail, direct solves, prolongation at coarser levels,
+// prolongation at level 0, other), over `iters` live iterations of a solve
+// of A x = b. Each launch is followed by an event on the solver's stream and
+// charged with the time since the previous event. The iterations run one by
+// one (not from the captured graph), so launch gaps are included; images
+// that converge within `iters` make later launches cheaper. Leaves the
+// solver mid-solve (the next solve starts afresh).
+PMB_API int pmb_stencil_profile(pmb_stencil* p, const double* b, int iters, double* ms_out,
+                                void* stream) {
+    if (!p || !b || !ms_out || iters <= 0) return fail(kErrArg, "pmb_stencil_profile: bad arguments");
+    Stencil& S = p->S;
+    if (!S.bound) return fail(kErrState, "pmb_stencil_profile: not bound");
+    return on_stream(S, (cudaStream_t)stream, [&]() -> int {
+        if (!S.setup_done) {
+            if (int rc = setup_stencil(S)) return rc;
+        }
+        HostList& a = S.fine0;
+        cudaStream_t s = S.stream;
+        launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), b,
+                                    S.at<double>(S.o_b64), S.user_total, s);
+        if (S.precision == 0) start_fp64(S, nullptr, 0.0, 1e-30, 1 << 30);
+        else if (int rc = start_mixed(S, nullptr, 0.0, 1e-30, 1 << 30, 1e-4, 1 << 20)) return rc;
+        std::vector<std::pair<int, cudaEvent_t>> marks;
+        S.prof = &marks;
+        prof_mark(S, -1);
+        for (int i = 0; i < iters; ++i) {
+            if (S.precision == 0) cg_iteration<double>(S, 0);
+            else cg_iteration<float>(S, 0);
+        }
+        S.prof = nullptr;
+        cudaError_t e = cudaStreamSynchronize(s);
+        for (int k = 0; k < kPkCount; ++k) ms_out[k] = 0.0;
+        for (size_t i = 1; i < marks.size() && e == cudaSuccess; ++i) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, marks[i - 1].second, marks[i].second) == cudaSuccess)
+                ms_out[marks[i].first] += (double)t / iters;
+        }
+        for (auto& m : marks) cudaEventDestroy(m.second);
+        PMB_CUDA(e);
+        PMB_CUDA(cudaGetLastError());
+        return check_err(S);
+    });
+}
+
 PMB_API int pmb_stencil_time_apply(pmb_stencil* p, int iters, double* ms, void* stream) {
     if (!p || iters <= 0 || !ms) return fail(kErrArg, "pmb_stencil_time_apply: bad arguments");
     Stencil& S = p->S;

@@ -16,6 +16,8 @@
 // fixed order, and the row is normalised: L = I - diag(1 / rowsum(W)) W.
 
 #include <cuda_runtime.h>
+
+#include "pm_common.cuh"
 #include <stdint.h>
 
 int pmb_scan_exclusive(int64_t* v, int64_t n, int64_t* chunk_scratch, int64_t* total,
@@ -290,7 +292,7 @@ int pmb_launch_knn(const double* image, int h, int w, const int* ks, const doubl
     const int blocks = (int)((n + 255) / 256);
     if (cols && vals) {
         k_normalize<<<blocks, 256, 0, st>>>(n, off, rowptr, wcols, wvals, cols, vals);
-        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+        return pmb::launch_status() ? 1 : 0;
     }
     Passes P{};
     P.np = np;
@@ -319,5 +321,5 @@ int pmb_launch_knn(const double* image, int h, int w, const int* ks, const doubl
     cudaMemcpyAsync(&nnz, rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return 1;
     if (nnz_out) *nnz_out = nnz;
-    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    return pmb::launch_status() ? 1 : 0;
 }

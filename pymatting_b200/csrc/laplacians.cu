@@ -12,6 +12,8 @@
 // order (the order scipy's sparse product leaves the row in).
 
 #include <cuda_runtime.h>
+
+#include "pm_common.cuh"
 #include <math.h>
 #include <stdint.h>
 
@@ -123,7 +125,7 @@ int pmb_launch_window_laplacian(int mode, const double* image, int h, int w, int
     if (mode == kUniform) k_window_laplacian<kUniform><<<blocks, 256, 0, st>>>(A);
     else if (mode == kRandomWalk) k_window_laplacian<kRandomWalk><<<blocks, 256, 0, st>>>(A);
     else return -2;
-    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    return pmb::launch_status() ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -266,7 +268,7 @@ int pmb_launch_lbdm_laplacian(const double* image, int h, int w, int r, double e
         pmb::lbdm::k_lbdm_windows<2><<<wb, 128, 0, st>>>(image, h, w, eps, T);
         pmb::lbdm::k_lbdm_rows<2><<<rb, 256, 0, st>>>(h, w, T, px, py, rowptr, cols, vals);
     }
-    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    return pmb::launch_status() ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -358,8 +360,8 @@ int pmb_launch_fg_cf_system(const double* alpha, int h, int w, double reg, int64
     if (!cols || !vals) {
         pmb::fgcf::k_fgcf_count<<<blocks, 256, 0, st>>>(alpha, h, w, rowptr);
         if (pmb_scan_exclusive(rowptr, n2, scratch, rowptr + n2, st)) return 1;
-        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+        return pmb::launch_status() ? 1 : 0;
     }
     pmb::fgcf::k_fgcf_fill<<<blocks, 256, 0, st>>>(alpha, h, w, reg, rowptr, cols, vals);
-    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    return pmb::launch_status() ? 1 : 0;
 }

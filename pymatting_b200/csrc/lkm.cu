@@ -21,6 +21,8 @@
 
 #include <cuda_runtime.h>
 
+#include "pm_common.cuh"
+
 namespace pmb {
 
 constexpr int kSeg = 64;         // outputs per thread of a box pass
@@ -70,7 +72,7 @@ static int box_pass(const double* src, double* dst, int nlines, int n_in, int n_
     if (total <= 0) return 0;
     k_box_pass<K><<<(unsigned)((total + kBoxThreads - 1) / kBoxThreads), kBoxThreads, 0, s>>>(
         src, dst, nlines, n_in, n_out, line_in, line_out, stride_in, stride_out, r, lo);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return pmb::launch_status();
 }
 
 // 2-D box filter of an (h, w, K) array: rows then columns.
@@ -233,7 +235,7 @@ int pmb_launch_lkm_setup(const double* image, int h, int w, int r, double eps, d
     if (int rc = box2d<6>(outer, tmp, s2, h, w, r, false, s)) return rc;
     k_lkm_windows<<<blocks(nw), 256, 0, s>>>(s1, s2, nw, (double)((2 * r + 1) * (2 * r + 1)), eps,
                                               win);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return pmb::launch_status();
 }
 
 int pmb_launch_lkm_apply(const double* image, int h, int w, int r, const double* win,
@@ -251,7 +253,7 @@ int pmb_launch_lkm_apply(const double* image, int h, int w, int r, const double*
     k_lkm_window_apply<<<blocks(nw), 256, 0, s>>>(sums, win, nw, t);
     if (int rc = box2d<4>(t, tmp, B, hv, wv, r, true, s)) return rc;
     k_lkm_finish<<<blocks(n), 256, 0, s>>>(image, p, B, add, h, w, r, out);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return pmb::launch_status();
 }
 
 int pmb_launch_lkm_diag(const double* image, int h, int w, int r, const double* win,
@@ -265,5 +267,5 @@ int pmb_launch_lkm_diag(const double* image, int h, int w, int r, const double* 
     k_lkm_diag_src<<<blocks(nw), 256, 0, s>>>(win, nw, d10);
     if (int rc = box2d<10>(d10, tmp, B, hv, wv, r, true, s)) return rc;
     k_lkm_diag<<<blocks(n), 256, 0, s>>>(image, B, n, add, diag, inv);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    return pmb::launch_status();
 }

@@ -15,6 +15,14 @@
 
 namespace pmb {
 
+// Launch helpers return 0 or -2. On -2 they record the CUDA error they saw
+// (cudaGetLastError clears it) so that the C ABI can report its text;
+// take_launch_error() returns and clears it (cudaSuccess if the helper
+// failed an argument check instead).
+int launch_status(cudaError_t e);
+inline int launch_status() { return launch_status(cudaGetLastError()); }
+cudaError_t take_launch_error();
+
 constexpr int kRS = 2;       // stencil radius of the stored operator
 constexpr int kNH = 13;      // stored planes (centre + 12 forward offsets)
 constexpr int kTX = 64;      // fine tile width

@@ -19,7 +19,7 @@ from .systems import (FP64, PREC_JACOBI, PREC_VCYCLE, CsrSystem, IcholFactor, St
                       csc_profile)
 
 __all__ = ["jacobi", "vcycle", "ichol", "CholeskyDecomposition", "JacobiPreconditioner",
-           "VCyclePreconditioner"]
+           "VCyclePreconditioner", "GridPlanes"]
 
 
 def _vec_in(r):
@@ -105,6 +105,60 @@ class _DenseDirect:
         return x
 
 
+class GridPlanes:
+    """Half-stencil planes of a grid matrix this package did not assemble.
+
+    ``A`` is any ``(h w, h w)`` matrix (scipy sparse, dense, or device CSR)
+    whose entries couple each pixel only with pixels at most two rows and two
+    columns away — the pattern of the radius-1 matting Laplacian and of
+    ``make_linear_system``'s matrix, whatever computed them. The conversion
+    runs on the device; matrices outside that pattern, or not symmetric
+    (the stencil engine stores one triangle), raise ``NotImplementedError``.
+    Stands in for a CFSource in the stencil solver.
+    """
+
+    radius = 1
+
+    def __init__(self, A, h, w, rel_tol=1e-10):
+        indptr, indices, data, n, m = to_device_csr(A)
+        if n != m or n != h * w:
+            raise ValueError("A must be square with h * w rows")
+        self.h, self.w = int(h), int(w)
+        lib = _ffi.lib()
+        self.pitch = int(lib.pmb_grid_pitch(self.w))
+        ps = self.h * self.pitch
+        self._planes = dev.empty(13 * ps, torch.float64)
+        back = dev.empty(12 * ps, torch.float64)
+        bad = dev.zeros(2, torch.int64)
+        _ffi.check(lib.pmb_csr_to_planes(dev.ptr(indptr), dev.ptr(indices), dev.ptr(data),
+                                         self.h, self.w, dev.ptr(self._planes), dev.ptr(back),
+                                         float(rel_tol), dev.ptr(bad), dev.stream()),
+                   "pmb_csr_to_planes")
+        outside, asym = (int(v) for v in bad.cpu())
+        if outside:
+            raise NotImplementedError(
+                "vcycle on the device needs a matrix whose entries couple pixels at most two "
+                "rows and columns apart (%d entries are farther)" % outside)
+        if asym:
+            raise NotImplementedError(
+                "vcycle on the device needs a symmetric matrix (%d entry pairs differ)" % asym)
+
+    @property
+    def n(self):
+        return self.h * self.w
+
+    @property
+    def plane_elems(self):
+        return 13 * self.h * self.pitch
+
+    def planes(self):
+        return self._planes
+
+    def assemble_planes(self, out):
+        out.copy_(self._planes)
+        return out
+
+
 class VCyclePreconditioner:
     """Geometric multigrid V-cycle (pymatting/preconditioner/vcycle.py).
 
@@ -128,10 +182,11 @@ class VCyclePreconditioner:
         h, w = self.shape
         if h * w <= direct_solve_size:
             self._direct = _DenseDirect(A)
-        elif self.source is None or self.source.radius != 1 or (self.source.h, self.source.w) != self.shape:
-            raise NotImplementedError(
-                "vcycle on the device needs the radius-1 matting system assembled by this "
-                "package (cf_laplacian / make_linear_system) for the given shape")
+        elif (self.source is None or self.source.radius != 1 or
+              (self.source.h, self.source.w) != self.shape):
+            # Any other matrix of the grid (a host scipy matrix, another
+            # Laplacian): converted to the stencil planes on the device.
+            self.source = GridPlanes(A, h, w)
 
     @property
     def system(self):

@@ -25,7 +25,7 @@ import torch
 
 from . import _device as dev
 from .laplacian import DeviceCSRMatrix, device_source
-from .preconditioner import (CholeskyDecomposition, JacobiPreconditioner,
+from .preconditioner import (CholeskyDecomposition, GridPlanes, JacobiPreconditioner,
                              VCyclePreconditioner)
 from .sparse import to_device_csr
 from .systems import (FP64, M_EXTERNAL, M_ICHOL, M_JACOBI, M_MATRIX, M_NONE, PREC_JACOBI,
@@ -57,6 +57,10 @@ class ProgressCallback:
 
 def _stencil_system(A, src, M):
     """The stencil engine to use for (A, M), or None if (A, M) does not fit."""
+    if (src is None and isinstance(M, VCyclePreconditioner) and M.A is A and
+            M._direct is None and isinstance(M.source, GridPlanes)):
+        # A matrix from elsewhere that vcycle already turned into planes.
+        return M.system
     if src is None or src.radius != 1:
         return None
     if M is None:

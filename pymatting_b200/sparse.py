@@ -48,9 +48,6 @@ def add_diagonal(L, c):
     _ffi.check(lib.pmb_csr_add_diag_rowptr(n, dev.ptr(indptr), dev.ptr(indices), dev.ptr(data),
                                            dev.ptr(c_t), dev.ptr(rowptr), dev.ptr(overflow),
                                            dev.ptr(scratch), dev.stream()), "add_diagonal")
-    if int(overflow.item()):
-        raise NotImplementedError(
-            "make_linear_system on the device supports rows of at most 64 stored entries")
     nnz = int(rowptr[n].item())
     cols = dev.empty(max(nnz, 1), torch.int64)
     vals = dev.empty(max(nnz, 1), torch.float64)

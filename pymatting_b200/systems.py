@@ -125,6 +125,21 @@ class StencilSystem:
         """Kernel launches issued by this system so far (graph replays included)."""
         return int(_ffi.lib().pmb_stencil_launch_count(self._h))
 
+    PROFILE_KINDS = ("cg_apply", "cg_update", "refine", "vc_down_l0", "vc_down", "vc_tail",
+                     "vc_direct", "vc_up", "vc_up_l0", "other")
+
+    def profile_kernels(self, b=None, iters=8):
+        """Milliseconds per iteration in each kind of launch (``PROFILE_KINDS``)
+        over ``iters`` live iterations of a solve with right-hand side ``b``
+        (default: all ones), CUDA events after every launch."""
+        if b is None:
+            b = torch.ones(self.n_user, dtype=torch.float64, device=dev.device())
+        out = np.zeros(len(self.PROFILE_KINDS), dtype=np.float64)
+        _ffi.check(_ffi.lib().pmb_stencil_profile(self._h, dev.ptr(b.reshape(-1)), int(iters),
+                                                  out.ctypes.data, dev.stream()),
+                   "pmb_stencil_profile")
+        return {k: float(v) for k, v in zip(self.PROFILE_KINDS, out) if v > 0}
+
     def time_apply(self, iters=20):
         """Average milliseconds of one level-0 operator apply (CUDA events on
         the solver's stream)."""
