@@ -16,9 +16,10 @@ Drop-in replacements, computed by hand-written sm_100a kernels behind a C ABI
 * ``cutout`` with ``load_image`` / ``save_image`` / ``stack_images`` /
   ``blend``.
 
-Extensions without a reference counterpart: ``solve_alpha`` (batched,
-mixed-precision soft-constraint solves) and ``cf_alpha`` (alpha
-differentiable with respect to the image).
+Extensions without a reference counterpart: ``solve_alpha`` / ``AlphaBatch``
+(batched, mixed-precision soft-constraint solves), ``solve_alpha_sharded``
+(a batch split over GPUs, results gathered to rank 0) and ``cf_alpha``
+(alpha differentiable with respect to the image).
 """
 
 from .util import trimap_split, sanity_check_image
@@ -29,6 +30,8 @@ from .solver import cg, CounterCallback, ProgressCallback
 from .alpha import (estimate_alpha_cf, estimate_alpha, estimate_alpha_knn, estimate_alpha_lbdm,
                     estimate_alpha_rw)
 from .autograd import cf_alpha
+from .batch import AlphaBatch, solve_alpha
+from .shard import solve_alpha_sharded
 from .lkm import lkm_laplacian, estimate_alpha_lkm
 from .foreground import (estimate_foreground_ml, estimate_foreground_ml_cupy,
                          estimate_foreground_cf)
@@ -44,6 +47,7 @@ __all__ = [
     "estimate_foreground_ml_cupy", "cutout", "load_image", "save_image", "stack_images", "blend",
     "rw_laplacian", "uniform_laplacian", "lbdm_laplacian", "knn_laplacian", "LAPLACIANS",
     "estimate_alpha_knn", "estimate_alpha_lbdm", "estimate_alpha_rw", "estimate_foreground_cf",
+    "AlphaBatch", "solve_alpha", "solve_alpha_sharded",
 ]
 
 # the reference's list (pymatting/laplacian/__init__.py)

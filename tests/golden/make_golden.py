@@ -437,8 +437,34 @@ def gen_laplacians(pm, root, rng):
     np.savez_compressed(os.path.join(HERE, "laplacians_small.npz"), **out)
 
 
+def gen_layout(pm):
+    """reference_layout.json: for every loaded pymatting module, which of its
+    attributes are bound to a function the integration replaces, named by
+    (defining module, name). Pins the re-export structure the integration
+    stub has to rebind."""
+    import json
+    from pymatting_b200.integration import HOT_PATH, NEXT_ROWS
+    targets = {}
+    for mod, name in HOT_PATH + NEXT_ROWS:
+        m = sys.modules.get(mod)
+        if m is not None and hasattr(m, name):
+            targets[id(getattr(m, name))] = [mod, name]
+    layout = {}
+    for mname in sorted(k for k in sys.modules if k == "pymatting" or k.startswith("pymatting.")):
+        m = sys.modules[mname]
+        if m is None:
+            continue
+        hits = {attr: targets[id(v)] for attr, v in vars(m).items() if id(v) in targets}
+        if hits:
+            layout[mname] = hits
+    with open(os.path.join(HERE, "reference_layout.json"), "w") as f:
+        json.dump(layout, f, indent=1, sort_keys=True)
+
+
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <pymatting source tree> [fixture names]")
+    root = sys.argv[1]
     pm = import_reference(root)
     rng = np.random.default_rng(2024)
     only = sys.argv[2:]
@@ -448,7 +474,8 @@ def main():
                      ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77))),
                      ("foreground", lambda: gen_foreground(pm, root, np.random.default_rng(91))),
                      ("cutout", lambda: gen_cutout(pm, root)),
-                     ("laplacians", lambda: gen_laplacians(pm, root, np.random.default_rng(5)))]:
+                     ("laplacians", lambda: gen_laplacians(pm, root, np.random.default_rng(5))),
+                     ("layout", lambda: gen_layout(pm))]:
         if not only or name in only:
             fn()
     for f in sorted(os.listdir(HERE)):

@@ -185,6 +185,53 @@ def test_bench_starts_its_own_ranks():
     assert sum(rec["images_per_rank"]) == 64
 
 
+def test_integration_rebinds_every_reexport():
+    """The integration stub on PyMatting's own module layout
+    (tests/golden/reference_layout.json, recorded from the imported
+    reference): every module attribute bound to a replaced function — the
+    defining module, the package re-exports under submodule names, and the
+    names other modules imported — resolves to pymatting_b200 afterwards.
+    Stand-in module objects carry the layout; no kernel is called."""
+    import json
+    import types
+    import pymatting_b200 as b200
+    from pymatting_b200 import integration
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_layout.json")) as f:
+        layout = json.load(f)
+    originals = {}
+
+    def original(defmod, name):
+        key = (defmod, name)
+        if key not in originals:
+            originals[key] = type(name, (), {}) if name[0].isupper() else (lambda *a: None)
+        return originals[key]
+
+    mods = {}
+    for mname, attrs in layout.items():
+        m = types.ModuleType(mname)
+        for attr, (defmod, name) in attrs.items():
+            setattr(m, attr, original(defmod, name))
+        mods[mname] = m
+    hot = {tuple(r) for r in integration.HOT_PATH}
+    n_hot = sum(1 for attrs in layout.values() for v in attrs.values() if tuple(v) in hot)
+    assert integration.install(include_next=False, modules=mods) == n_hot
+    integration.uninstall()
+    assert all(getattr(mods[m], a) is original(*v) for m, attrs in layout.items()
+               for a, v in attrs.items())
+    total = sum(len(a) for a in layout.values())
+    assert integration.install(modules=mods) == total
+    for mname, attrs in layout.items():
+        for attr, (defmod, name) in attrs.items():
+            assert getattr(mods[mname], attr) is getattr(b200, name), (mname, attr)
+    # The bindings the reference's own call sites go through.
+    assert mods["pymatting.laplacian"].cf_laplacian is b200.cf_laplacian
+    assert mods["pymatting.preconditioner"].vcycle is b200.vcycle
+    assert mods["pymatting"].make_linear_system is b200.make_linear_system
+    ecf = mods["pymatting.alpha.estimate_alpha_cf"]
+    assert ecf.cf_laplacian is b200.cf_laplacian and ecf.cg is b200.cg and ecf.ichol is b200.ichol
+    integration.uninstall()
+
+
 def _write_png(path, arr):
     from PIL import Image
     Image.fromarray(arr).save(path)
