@@ -278,6 +278,16 @@ int pmb_csr_add_diag_rowptr(int64_t n, const int64_t* indptr, const int64_t* ind
 int pmb_csr_add_diag_fill(int64_t n, const int64_t* indptr, const int64_t* indices,
                           const double* data, const double* c, const int64_t* rowptr,
                           int64_t* out_indices, double* out_data, void* stream);
+/* Bounded-wait self-test (no reference counterpart; it tests the failure
+ * convention that every device wait of this library ends with an error
+ * status instead of spinning, as the reference's solvers end with errors:
+ * pymatting/solver/cg.py:115-117, pymatting/preconditioner/ichol.py:259-296).
+ * which = 0: the mbarrier wait of the TMA kernels, limit in polls; which = 1:
+ * the epoch poll of the foreground sweep, limit in nanoseconds. Each waits
+ * on a barrier or word that nothing completes; *timed_out = 1 when the wait
+ * gave up and reported it. scratch: 64 bytes of device memory. */
+int pmb_selftest_wait(int which, int64_t limit, void* scratch, int* timed_out, void* stream);
+
 /* Half-stencil planes (13 x h x pitch doubles, the stencil engine's layout)
  * of an (h w) x (h w) CSR matrix of a pixel grid whose entries lie within
  * the 5x5 neighbourhood of their row's pixel, so that vcycle runs on any
@@ -306,8 +316,11 @@ int pmb_unknown_index(const uint8_t* is_known, int64_t n, int64_t* cidx, int64_t
  * device that loads it until the process exits; n is limited to
  * PMB_UNKNOWN_INDEX_STATIC_MAX_N (larger n fails with status -1). The first
  * call on a device looks up the array's device address; make that first
- * call before any stream capture. Calls share the array, so calls whose work
- * overlaps on the GPU race; order them on one stream. */
+ * call before any stream capture. After a device reset the library is loaded
+ * into a new context and the array moves: the first call in the new context
+ * looks the address up again (make that call, too, before any capture).
+ * Calls share the array, so calls whose work overlaps on the GPU race; order
+ * them on one stream. */
 #define PMB_UNKNOWN_INDEX_STATIC_MAX_N 33553407
 int pmb_unknown_index_static(const uint8_t* is_known, int64_t n, int64_t* cidx, void* stream);
 /* L_U = L[U, :][:, U] and b_U = -L[U, :][:, K] is_fg[K] from the ELL of the

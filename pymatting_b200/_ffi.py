@@ -109,6 +109,7 @@ _SIGNATURES = {
     "pmb_ichol_destroy": (c_int, [c_vp]),
     "pmb_planes_inv_diag": (c_int, [c_vp, c_int, c_int, c_vp, c_vp]),
     "pmb_csr_add_diag_rowptr": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_selftest_wait": (c_int, [c_int, c_i64, c_vp, ctypes.POINTER(c_int), c_vp]),
     "pmb_csr_to_planes": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_dbl, c_vp,
                                   c_vp]),
     "pmb_csr_add_diag_fill": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

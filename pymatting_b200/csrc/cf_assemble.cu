@@ -521,20 +521,45 @@ static __device__ __align__(256) int64_t g_static_scan[kStaticScanElems];
 // plus one slot for the total.
 int64_t pmb_static_scan_max_n() { return (pmb::kStaticScanElems - 1) * 1024 - 1; }
 
+// The driver's current context, as an opaque key (null if unavailable).
+typedef int (*CtxGetCurrentFn)(void**);
+static void* current_context() {
+    static CtxGetCurrentFn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+        looked = true;
+    }
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
 // Device address of the array on the current device. Host code only knows a
 // host-side stand-in for g_static_scan, so the address is looked up with
-// cudaGetSymbolAddress, once per device (the first call on a device does it).
+// cudaGetSymbolAddress, once per device and context: the first call on a
+// device does it, and a call after the caller reset the device (a new
+// primary context, where the module and its array are loaded again) looks
+// it up anew.
 static int static_scan_address(int64_t** out) {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
     static int64_t* addr[kMaxDevices] = {};
+    static void* ctx_of[kMaxDevices] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -2;
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (!addr[dev] || !ctx || ctx_of[dev] != ctx) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, pmb::g_static_scan) != cudaSuccess || !p) return -3;
         addr[dev] = static_cast<int64_t*>(p);
+        // The lookup makes the runtime's context current if it was not yet.
+        ctx_of[dev] = ctx ? ctx : current_context();
     }
     *out = addr[dev];
     return 0;

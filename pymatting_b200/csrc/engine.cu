@@ -2164,6 +2164,38 @@ PMB_API int pmb_csr_add_diag_fill(int64_t n, const int64_t* indptr, const int64_
     return 0;
 }
 
+int pmb_launch_selftest_poll(void*, unsigned long long, int*, cudaStream_t);
+
+// Bounded-wait self-test: which = 0 runs the mbarrier wait of the TMA
+// kernels with a limit of `limit` polls, which = 1 the epoch poll of the
+// foreground sweep with a deadline of `limit` nanoseconds, each on a barrier
+// or word that nothing completes. *timed_out = 1 when the wait gave up and
+// reported it (every waiting thread, for the mbarrier). scratch: 64 bytes of
+// device memory.
+PMB_API int pmb_selftest_wait(int which, int64_t limit, void* scratch, int* timed_out,
+                              void* stream) {
+    if (!scratch || !timed_out || limit <= 0 || (which != 0 && which != 1))
+        return fail(kErrArg, "pmb_selftest_wait: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    *timed_out = 0;
+    if (which == 1) {
+        const int rc = pmb_launch_selftest_poll(scratch, (unsigned long long)limit, timed_out, s);
+        if (rc) return fail(kErrCuda, std::string("poll self-test: ") +
+                                          cudaGetErrorString((cudaError_t)rc));
+        return 0;
+    }
+    if (limit > 0x7fffffff) return fail(kErrArg, "pmb_selftest_wait: poll limit too large");
+    int* gave_up = static_cast<int*>(scratch);
+    PMB_CUDA(cudaMemsetAsync(gave_up, 0, sizeof(int), s));
+    launch_selftest_mbar((uint32_t)limit, gave_up, s);
+    PMB_CUDA(cudaGetLastError());
+    int h = 0;
+    PMB_CUDA(cudaMemcpyAsync(&h, gave_up, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PMB_CUDA(cudaStreamSynchronize(s));
+    *timed_out = h == 64 ? 1 : 0;
+    return 0;
+}
+
 // Half-stencil planes of an (h w) x (h w) CSR matrix of a pixel grid (the
 // form vcycle needs, pymatting/preconditioner/vcycle.py:103-153 takes any A
 // of that shape). planes: 13 h pitch doubles, back: 12 h pitch doubles of

@@ -120,7 +120,8 @@ __device__ __forceinline__ unsigned long long now_ns() {
 // Poll until both words of *p carry `want` and return them. Bounded: gives
 // up (returning the last read) when the error word is set or after
 // kTimeoutNs, which it reports.
-__device__ __noinline__ ulonglong2 poll_epoch(const ulonglong2* p, uint32_t want, int* err) {
+__device__ __noinline__ ulonglong2 poll_epoch(const ulonglong2* p, uint32_t want, int* err,
+                                              unsigned long long timeout_ns = kTimeoutNs) {
     unsigned long long t0 = 0;
     ulonglong2 v = make_ulonglong2(0, 0);
     for (uint32_t n = 0;; ++n) {
@@ -128,7 +129,7 @@ __device__ __noinline__ ulonglong2 poll_epoch(const ulonglong2* p, uint32_t want
             if (ld_err(err)) return v;
             if (n == 0) {
                 t0 = now_ns();
-            } else if (now_ns() - t0 > kTimeoutNs) {
+            } else if (now_ns() - t0 > timeout_ns) {
                 atomicCAS(err, 0, kErrTimeout);
                 return v;
             }
@@ -602,10 +603,35 @@ static Layout layout(int h0, int w0, int depth) {
     return l;
 }
 
+// Self-test of the bounded poll: one thread waits with poll_epoch for epoch
+// 1 in a word that holds epoch 0 and that nothing writes, with a deadline of
+// timeout_ns. The poll must give up and leave kErrTimeout in *err.
+__global__ void k_selftest_poll(const ulonglong2* word, int* err, unsigned long long timeout_ns) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) (void)poll_epoch(word, 1u, err, timeout_ns);
+}
+
 }  // namespace fg
 }  // namespace pmb
 
 using namespace pmb::fg;
+
+// scratch: 64 bytes of device memory. Returns 0 and sets *timed_out (1 if
+// the poll gave up and reported it), or a CUDA error code.
+int pmb_launch_selftest_poll(void* scratch, unsigned long long timeout_ns, int* timed_out,
+                             cudaStream_t st) {
+    ulonglong2* word = static_cast<ulonglong2*>(scratch);
+    int* err = reinterpret_cast<int*>(static_cast<char*>(scratch) + 32);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 64, st);
+    if (e != cudaSuccess) return (int)e;
+    k_selftest_poll<<<1, 32, 0, st>>>(word, err, timeout_ns);
+    int h = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return (int)e;
+    *timed_out = h == kErrTimeout ? 1 : 0;
+    return 0;
+}
 
 int64_t pmb_launch_fg_workspace(int h, int w, int depth) {
     if (h <= 0 || w <= 0 || depth < 1 || depth > kMaxDepth) return -1;

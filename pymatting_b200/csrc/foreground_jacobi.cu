@@ -9,9 +9,10 @@
 // single CTA with a barrier between iterations. The buffer handling is the
 // reference's: flat buffers F, F_prev, B, B_prev swapped after every
 // iteration, F and B seeded with the colour of pixel (0, 0), each level
-// resized from the buffer named F, and F returned. This file is compiled
-// with fused multiply-adds allowed, as NVRTC compiles the reference's
-// kernel by default; the per-pixel expressions keep the reference's order.
+// resized from the buffer named F, and F returned. The per-pixel update is
+// this file's own formulation of the 2x2 normal equations (below); it
+// agrees with the reference's to float32 rounding, and the tests pin it
+// against the oracle's restatement of the reference.
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -26,48 +27,83 @@ constexpr int kSmallThreads = 1024;
 constexpr int kSmallPixels = 8192;  // levels this small run in one CTA
 constexpr int kMaxLevels = 40;
 
-// One Jacobi update of pixel (x, y): estimate_foreground_ml_cupy.py:34-107.
-__device__ __forceinline__ void jacobi_pixel(int x, int y, int w, int h, float reg,
-                                             const float* __restrict__ img,
-                                             const float* __restrict__ al,
-                                             const float* __restrict__ Fp,
-                                             const float* __restrict__ Bp, float* __restrict__ F,
-                                             float* __restrict__ B) {
-    const int i = x + y * w;
-    const float a0 = al[i];
-    const float a1 = 1.0f - a0;
-    float b00 = a0 * img[i * 3 + 0];
-    float b01 = a0 * img[i * 3 + 1];
-    float b02 = a0 * img[i * 3 + 2];
-    float b10 = a1 * img[i * 3 + 0];
-    float b11 = a1 * img[i * 3 + 1];
-    float b12 = a1 * img[i * 3 + 2];
-    const int js[4] = {max(0, x - 1) + y * w, min(w - 1, x + 1) + y * w,
-                       x + max(0, y - 1) * w, x + min(h - 1, y + 1) * w};
-    float a_sum = 0.0f;
+// Per pixel, the cost (a F + (1 - a) B - I)^2 + sum_j w_j (|F - F_j|^2 +
+// |B - B_j|^2) over the four neighbours j (clamped at the border), with
+// w_j = reg + |a - a_j|, is minimised channel by channel with the
+// neighbours' previous F_j, B_j held fixed (a Jacobi step;
+// estimate_foreground_ml_cupy.py:34-107 is the reference's kernel). With
+// S = sum_j w_j the normal equations are
+//   [a^2 + S   a(1-a)  ] [F]   [a I + sum_j w_j F_j    ]
+//   [a(1-a)    (1-a)^2+S] [B] = [(1-a) I + sum_j w_j B_j],
+// whose determinant is S (a^2 + (1-a)^2 + S) (the a^2 (1-a)^2 terms cancel
+// exactly, so it is formed without that cancellation). The solution is
+// clamped to [0, 1].
+struct FBSums {
+    float S;         // sum of the weights
+    float f[3];      // sum of w_j F_j per channel
+    float b[3];      // sum of w_j B_j per channel
+};
+
+__device__ __forceinline__ void fb_add(FBSums& q, float a, float aj, float reg, const float* Fj,
+                                       const float* Bj, int stride) {
+    const float wj = reg + fabsf(a - aj);
+    q.S += wj;
 #pragma unroll
-    for (int d = 0; d < 4; d++) {
-        const int j = js[d];
-        const float da = reg + fabsf(a0 - al[j]);
-        a_sum += da;
-        b00 += da * Fp[j * 3 + 0];
-        b01 += da * Fp[j * 3 + 1];
-        b02 += da * Fp[j * 3 + 2];
-        b10 += da * Bp[j * 3 + 0];
-        b11 += da * Bp[j * 3 + 1];
-        b12 += da * Bp[j * 3 + 2];
+    for (int c = 0; c < 3; ++c) {
+        q.f[c] += wj * Fj[c * stride];
+        q.b[c] += wj * Bj[c * stride];
     }
-    const float a00 = a0 * a0 + a_sum;
-    const float a11 = a1 * a1 + a_sum;
-    const float a01 = a0 * a1;
-    const float inv_det = 1.0f / (a00 * a11 - a01 * a01);
-    F[i * 3 + 0] = fmaxf(0.0f, fminf(1.0f, inv_det * (a11 * b00 - a01 * b10)));
-    F[i * 3 + 1] = fmaxf(0.0f, fminf(1.0f, inv_det * (a11 * b01 - a01 * b11)));
-    F[i * 3 + 2] = fmaxf(0.0f, fminf(1.0f, inv_det * (a11 * b02 - a01 * b12)));
-    B[i * 3 + 0] = fmaxf(0.0f, fminf(1.0f, inv_det * (a00 * b10 - a01 * b00)));
-    B[i * 3 + 1] = fmaxf(0.0f, fminf(1.0f, inv_det * (a00 * b11 - a01 * b01)));
-    B[i * 3 + 2] = fmaxf(0.0f, fminf(1.0f, inv_det * (a00 * b12 - a01 * b02)));
 }
+
+__device__ __forceinline__ void fb_solve(const FBSums& q, float a, const float* I, float* F,
+                                         float* B) {
+    const float na = 1.0f - a;
+    const float pF = a * a + q.S;      // F-F entry
+    const float pB = na * na + q.S;    // B-B entry
+    const float m = a * na;            // coupling
+    const float inv = 1.0f / (q.S * (a * a + na * na + q.S));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float rF = a * I[c] + q.f[c];
+        const float rB = na * I[c] + q.b[c];
+        // min first: a NaN (S = 0, only with reg = 0) clamps to 1, as in
+        // the reference
+        F[c] = fmaxf(fminf((pB * rF - m * rB) * inv, 1.0f), 0.0f);
+        B[c] = fmaxf(fminf((pF * rB - m * rF) * inv, 1.0f), 0.0f);
+    }
+}
+
+// One pixel read straight from global memory (the one-CTA small levels).
+__device__ __forceinline__ void jacobi_global(int x, int y, int w, int h, float reg,
+                                              const float* __restrict__ img,
+                                              const float* __restrict__ al,
+                                              const float* __restrict__ Fp,
+                                              const float* __restrict__ Bp, float* __restrict__ F,
+                                              float* __restrict__ B) {
+    const int i = x + y * w;
+    const float a = al[i];
+    FBSums q{0.0f, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    const int nb[4] = {max(x - 1, 0) + y * w, min(x + 1, w - 1) + y * w,
+                       x + max(y - 1, 0) * w, x + min(y + 1, h - 1) * w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) fb_add(q, a, al[nb[k]], reg, Fp + 3 * nb[k], Bp + 3 * nb[k], 1);
+    float I[3] = {img[3 * i], img[3 * i + 1], img[3 * i + 2]};
+    float f[3], b[3];
+    fb_solve(q, a, I, f, b);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        F[3 * i + c] = f[c];
+        B[3 * i + c] = b[c];
+    }
+}
+
+// Tiles of the large levels: kJX x kJY pixels per CTA, one per thread. The
+// tile's alpha and previous F / B with a one-pixel halo (coordinates clamped
+// to the image, which makes the halo hold exactly the neighbours the border
+// pixels use) are staged in shared memory, F and B split into channel
+// planes; rows of the interleaved global arrays are read contiguously.
+constexpr int kJX = 32, kJY = 8;
+constexpr int kHX = kJX + 2, kHY = kJY + 2;
 
 __device__ __forceinline__ int src_of(int v, int n_src, int n_dst) {
     return min((int)((unsigned)v * (unsigned)n_src / (unsigned)n_dst), n_src - 1);
@@ -120,12 +156,46 @@ struct IterArgs {
     float reg;
 };
 
-__global__ void __launch_bounds__(256) k_fgj_iter(IterArgs A) {
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(kJX * kJY) k_fgj_iter(IterArgs A) {
+    __shared__ float s_a[kHY][kHX];
+    __shared__ float s_f[3][kHY][kHX];
+    __shared__ float s_b[3][kHY][kHX];
+    const int x0 = blockIdx.x * kJX, y0 = blockIdx.y * kJY;
+    // Stage: halo row r is image row clamp(y0 - 1 + r); element e of that row
+    // is channel e % 3 of column clamp(x0 - 1 + e / 3).
+    for (int q = threadIdx.x; q < kHY * kHX * 3; q += kJX * kJY) {
+        const int r = q / (kHX * 3), e = q - r * (kHX * 3);
+        const int hx = e / 3, c = e - hx * 3;
+        const int y = min(max(y0 - 1 + r, 0), A.h - 1);
+        const int x = min(max(x0 - 1 + hx, 0), A.w - 1);
+        const int g = (y * A.w + x) * 3 + c;
+        s_f[c][r][hx] = A.F_prev[g];
+        s_b[c][r][hx] = A.B_prev[g];
+        if (c == 0) s_a[r][hx] = A.alpha_level[y * A.w + x];
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % kJX, ty = threadIdx.x / kJX;
+    const int x = x0 + tx, y = y0 + ty;
     if (x >= A.w || y >= A.h) return;
-    jacobi_pixel(x, y, A.w, A.h, A.reg, A.image_level, A.alpha_level, A.F_prev, A.B_prev, A.F,
-                 A.B);
+    const int cx = tx + 1, cy = ty + 1;
+    const float a = s_a[cy][cx];
+    FBSums q{0.0f, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    constexpr int ps = kHY * kHX;   // channel-plane stride
+    // Neighbours left, right, up, down (the halo already holds the clamp).
+    fb_add(q, a, s_a[cy][cx - 1], A.reg, &s_f[0][cy][cx - 1], &s_b[0][cy][cx - 1], ps);
+    fb_add(q, a, s_a[cy][cx + 1], A.reg, &s_f[0][cy][cx + 1], &s_b[0][cy][cx + 1], ps);
+    fb_add(q, a, s_a[cy - 1][cx], A.reg, &s_f[0][cy - 1][cx], &s_b[0][cy - 1][cx], ps);
+    fb_add(q, a, s_a[cy + 1][cx], A.reg, &s_f[0][cy + 1][cx], &s_b[0][cy + 1][cx], ps);
+    const int i = y * A.w + x;
+    const float I[3] = {A.image_level[3 * i], A.image_level[3 * i + 1],
+                        A.image_level[3 * i + 2]};
+    float f[3], b[3];
+    fb_solve(q, a, I, f, b);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        A.F[3 * i + c] = f[c];
+        A.B[3 * i + c] = b[c];
+    }
 }
 
 // A whole small level in one CTA: the resizes, then n_iter iterations with
@@ -139,8 +209,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_fgj_small(ResizeArgs R, float
     __syncthreads();
     for (int it = 0; it < n_iter; ++it) {
         for (int p = threadIdx.x; p < m; p += blockDim.x)
-            jacobi_pixel(p % R.w, p / R.w, R.w, R.h, reg, R.image_level, R.alpha_level, F_prev,
-                         B_prev, F, B);
+            jacobi_global(p % R.w, p / R.w, R.w, R.h, reg, R.image_level, R.alpha_level, F_prev,
+                          B_prev, F, B);
         __syncthreads();
         float* t = F;
         F = F_prev;
@@ -214,9 +284,10 @@ int pmb_launch_fgj(const float* image, const float* alpha, int h0, int w0, float
         } else {
             const dim3 grid((w + 31) / 32, (h + 7) / 8);
             k_fgj_resize<<<grid, 256, 0, st>>>(R);
+            const dim3 tiles((w + kJX - 1) / kJX, (h + kJY - 1) / kJY);
             for (int it = 0; it < n_iter; ++it) {
                 IterArgs I{image_level, alpha_level, F_prev, B_prev, F, B, h, w, reg};
-                k_fgj_iter<<<grid, 256, 0, st>>>(I);
+                k_fgj_iter<<<tiles, kJX * kJY, 0, st>>>(I);
                 std::swap(F, F_prev);
                 std::swap(B, B_prev);
             }

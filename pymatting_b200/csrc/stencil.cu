@@ -132,11 +132,22 @@ struct Pipe {
         }
         __syncthreads();
     }
-    __device__ bool wait(int b) {
-        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1u);
+    // Wait for buffer b. The outcome is made uniform over the CTA: false in
+    // every thread if any thread's wait gave up. Then thread 0 sets the error
+    // flag and waits once more, again bounded, for the loads that may still
+    // be in flight into buffer b and (other_issued) the other buffer, so the
+    // CTA does not exit while a copy into its shared memory is pending.
+    __device__ bool wait(int b, bool other_issued) {
+        const uint32_t par = (phase >> b) & 1u;
+        const bool ok = mbar_wait(&bar[b], par);
         phase ^= 1u << b;
-        if (!ok && err) atomicExch(err, 1);
-        return ok;
+        if (!__syncthreads_or(!ok)) return true;
+        if (threadIdx.x == 0) {
+            if (err) atomicExch(err, 1);
+            if (!ok) mbar_wait(&bar[b], par);
+            if (other_issued) mbar_wait(&bar[b ^ 1], (phase >> (b ^ 1)) & 1u);
+        }
+        return false;
     }
 };
 
@@ -197,7 +208,7 @@ __device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* s
         __syncthreads();
         const Meta m = s_m[b];
         if (m.run) {
-            if (!pipe.wait(b)) return;
+            if (!pipe.wait(b, tn < wl.total && s_m[b ^ 1].run)) return;
             body(m, s_g[b], b);
             ++mine;
             const bool last_of_image = (tn >= wl.total) || (s_m[b ^ 1].inst != m.inst);
@@ -1020,8 +1031,13 @@ k_galerkin_t(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtenso
         tma_load_3d(s_pl, map_of(maps, gf, kMapPlG), 2 * X0 - 6, 2 * Y0 - 1, 0, &s_bar);
     }
     __syncthreads();
-    if (!mbar_wait(&s_bar, 0)) {
-        if (threadIdx.x == 0) atomicExch(err, 1);
+    const bool ok = mbar_wait(&s_bar, 0);
+    if (__syncthreads_or(!ok)) {
+        // Report, and wait (bounded) for the copy still in flight.
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            if (!ok) mbar_wait(&s_bar, 0);
+        }
         return;
     }
     const int ly = threadIdx.x / kGTX, lx = threadIdx.x % kGTX;
@@ -1676,6 +1692,29 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
 
 
 // --------------------------------------------------------------------------
+// Self-test of the bounded mbarrier wait
+// --------------------------------------------------------------------------
+//
+// Thread 0 arms a barrier for 16 bytes of transaction that no copy will ever
+// deliver (nothing is issued, so nothing is in flight), then every thread
+// waits for it with a limit of `polls`; each thread whose wait gave up adds
+// one to *gave_up. Used to show on the device that the waits of the TMA
+// kernels end with an error status instead of spinning.
+__global__ void k_selftest_mbar(uint32_t polls, int* gave_up) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, 16);
+    }
+    __syncthreads();
+    if (!mbar_wait(&bar, 0, polls)) atomicAdd(gave_up, 1);
+}
+
+void launch_selftest_mbar(uint32_t polls, int* gave_up, cudaStream_t s) {
+    k_selftest_mbar<<<1, 64, 0, s>>>(polls, gave_up);
+}
+
+// --------------------------------------------------------------------------
 // Coarse-level tail: one CTA per image, shared-memory resident
 // --------------------------------------------------------------------------
 //
@@ -1767,9 +1806,14 @@ k_vc_tail(const TailDesc<T>* __restrict__ descs, const InstState* st, double ome
                   (uint32_t)(g0.pstride * sizeof(T)), &s_bar);
     }
     __syncthreads();
-    if (!mbar_wait(&s_bar, 0)) {
-        if (threadIdx.x == 0) atomicExch(err, 1);
-        return;   // every thread saw the same timeout
+    const bool ok = mbar_wait(&s_bar, 0);
+    if (__syncthreads_or(!ok)) {
+        // Report, and wait (bounded) for the copies still in flight.
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            if (!ok) mbar_wait(&s_bar, 0);
+        }
+        return;
     }
     auto planes = [&](int l) { return sm + s_off[l]; };
     auto vb = [&](int l) { return sm + s_off[l] + kNH * D.lev[l].g.pstride; };

@@ -61,6 +61,10 @@ template <typename T> int down_box_width();
 // Raise the dynamic shared-memory limits once (before any graph capture).
 void stencil_prepare();
 
+// Self-test: 64 threads wait `polls` polls for an mbarrier that never
+// completes; each gives up and adds one to *gave_up.
+void launch_selftest_mbar(uint32_t polls, int* gave_up, cudaStream_t s);
+
 template <typename T>
 void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
                     const T* P, const T* b, T* x, bool have_x0, T* r, T* z, InstState* st,

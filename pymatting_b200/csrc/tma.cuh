@@ -36,10 +36,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // Wait for phase `parity` of the barrier to complete. Returns false if the
-// poll limit was reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// poll limit (`limit` polls, kSpinLimit by default) was reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t limit = kSpinLimit) {
     const uint32_t a = smem_addr(bar);
-    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
