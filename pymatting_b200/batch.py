@@ -29,7 +29,7 @@ def _device_masks(trimap_t):
     n = trimap_t.numel()
     fg = dev.empty(n, torch.uint8)
     known = dev.empty(n, torch.uint8)
-    counts = dev.zeros(2, torch.int64)
+    counts = dev.empty(2, torch.int64)     # zeroed by pmb_trimap_masks
     _ffi.check(_ffi.lib().pmb_trimap_masks(dev.ptr(trimap_t), n, 0.9, 0.1, dev.ptr(fg),
                                            dev.ptr(known), dev.ptr(counts), dev.stream()),
                "trimap masks")
@@ -57,8 +57,8 @@ class AlphaBatch:
             sources.append(src)
             fgs.append(fg)
         if check_trimaps:
-            for cnt in counts:
-                nf, nb = (int(v) for v in cnt.cpu())
+            # one device-to-host read for every image's counts
+            for nf, nb in torch.stack(counts).cpu().tolist():
                 if nb == 0:
                     raise ValueError("Trimap did not contain background values (values <= %f)" % 0.1)
                 if nf == 0:

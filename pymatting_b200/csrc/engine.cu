@@ -616,7 +616,9 @@ static int bind_stencil(Stencil& S, void* ws, const double* P0) {
     S.direct32 = S.direct64;
     for (size_t i = 0; i < S.direct64.size(); ++i) {
         S.direct64[i].inv = S.at<double>(S.o_inv) + S.direct_inv_off[i];
+        S.direct64[i].P = planes64(S, S.coarsest[S.direct64[i].g.inst]);
         S.direct32[i].inv = S.direct64[i].inv;
+        S.direct32[i].P = S.direct64[i].P;
     }
     if (!S.direct64.empty()) {
         PMB_CUDA(cudaMemcpyAsync(S.ws + S.o_direct64, S.direct64.data(),
@@ -658,9 +660,8 @@ static int setup_stencil(Stencil& S) {
         ++S.launches;
     }
     PMB_CUDA(cudaMemsetAsync(S.ws + S.o_status, 0, sizeof(int), s));
-    for (size_t i = 0; i < S.direct64.size(); ++i) {
-        const int l = S.coarsest[S.direct64[i].g.inst];
-        launch_dense_inverse(S.at<DirectDesc>(S.o_direct64) + i, 1, planes64(S, l),
+    if (!S.direct64.empty()) {
+        launch_dense_inverse(S.at<DirectDesc>(S.o_direct64), (int)S.direct64.size(),
                              S.at<double>(S.o_invwork), S.at<int>(S.o_status), s);
         ++S.launches;
     }

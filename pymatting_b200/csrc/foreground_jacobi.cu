@@ -35,14 +35,18 @@ constexpr int kMaxLevels = 40;
 // S = sum_j w_j the normal equations are
 //   [a^2 + S   a(1-a)  ] [F]   [a I + sum_j w_j F_j    ]
 //   [a(1-a)    (1-a)^2+S] [B] = [(1-a) I + sum_j w_j B_j],
-// whose determinant is S (a^2 + (1-a)^2 + S) (the a^2 (1-a)^2 terms cancel
-// exactly, so it is formed without that cancellation). The solution is
-// clamped to [0, 1].
+// solved by Cramer's rule and clamped to [0, 1]. The right-hand sides are
+// accumulated from the data term on, neighbour by neighbour.
 struct FBSums {
     float S;         // sum of the weights
-    float f[3];      // sum of w_j F_j per channel
-    float b[3];      // sum of w_j B_j per channel
+    float f[3];      // a I + sum of w_j F_j per channel
+    float b[3];      // (1 - a) I + sum of w_j B_j per channel
 };
+
+__device__ __forceinline__ FBSums fb_start(float a, const float* I) {
+    const float na = 1.0f - a;
+    return FBSums{0.0f, {a * I[0], a * I[1], a * I[2]}, {na * I[0], na * I[1], na * I[2]}};
+}
 
 __device__ __forceinline__ void fb_add(FBSums& q, float a, float aj, float reg, const float* Fj,
                                        const float* Bj, int stride) {
@@ -55,21 +59,18 @@ __device__ __forceinline__ void fb_add(FBSums& q, float a, float aj, float reg, 
     }
 }
 
-__device__ __forceinline__ void fb_solve(const FBSums& q, float a, const float* I, float* F,
-                                         float* B) {
+__device__ __forceinline__ void fb_solve(const FBSums& q, float a, float* F, float* B) {
     const float na = 1.0f - a;
     const float pF = a * a + q.S;      // F-F entry
     const float pB = na * na + q.S;    // B-B entry
     const float m = a * na;            // coupling
-    const float inv = 1.0f / (q.S * (a * a + na * na + q.S));
+    const float inv = 1.0f / (pF * pB - m * m);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float rF = a * I[c] + q.f[c];
-        const float rB = na * I[c] + q.b[c];
         // min first: a NaN (S = 0, only with reg = 0) clamps to 1, as in
         // the reference
-        F[c] = fmaxf(fminf((pB * rF - m * rB) * inv, 1.0f), 0.0f);
-        B[c] = fmaxf(fminf((pF * rB - m * rF) * inv, 1.0f), 0.0f);
+        F[c] = fmaxf(fminf((pB * q.f[c] - m * q.b[c]) * inv, 1.0f), 0.0f);
+        B[c] = fmaxf(fminf((pF * q.b[c] - m * q.f[c]) * inv, 1.0f), 0.0f);
     }
 }
 
@@ -82,14 +83,14 @@ __device__ __forceinline__ void jacobi_global(int x, int y, int w, int h, float 
                                               float* __restrict__ B) {
     const int i = x + y * w;
     const float a = al[i];
-    FBSums q{0.0f, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    const float I[3] = {img[3 * i], img[3 * i + 1], img[3 * i + 2]};
+    FBSums q = fb_start(a, I);
     const int nb[4] = {max(x - 1, 0) + y * w, min(x + 1, w - 1) + y * w,
                        x + max(y - 1, 0) * w, x + min(y + 1, h - 1) * w};
 #pragma unroll
     for (int k = 0; k < 4; ++k) fb_add(q, a, al[nb[k]], reg, Fp + 3 * nb[k], Bp + 3 * nb[k], 1);
-    float I[3] = {img[3 * i], img[3 * i + 1], img[3 * i + 2]};
     float f[3], b[3];
-    fb_solve(q, a, I, f, b);
+    fb_solve(q, a, f, b);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         F[3 * i + c] = f[c];
@@ -179,18 +180,18 @@ __global__ void __launch_bounds__(kJX * kJY) k_fgj_iter(IterArgs A) {
     if (x >= A.w || y >= A.h) return;
     const int cx = tx + 1, cy = ty + 1;
     const float a = s_a[cy][cx];
-    FBSums q{0.0f, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    const int i = y * A.w + x;
+    const float I[3] = {A.image_level[3 * i], A.image_level[3 * i + 1],
+                        A.image_level[3 * i + 2]};
+    FBSums q = fb_start(a, I);
     constexpr int ps = kHY * kHX;   // channel-plane stride
     // Neighbours left, right, up, down (the halo already holds the clamp).
     fb_add(q, a, s_a[cy][cx - 1], A.reg, &s_f[0][cy][cx - 1], &s_b[0][cy][cx - 1], ps);
     fb_add(q, a, s_a[cy][cx + 1], A.reg, &s_f[0][cy][cx + 1], &s_b[0][cy][cx + 1], ps);
     fb_add(q, a, s_a[cy - 1][cx], A.reg, &s_f[0][cy - 1][cx], &s_b[0][cy - 1][cx], ps);
     fb_add(q, a, s_a[cy + 1][cx], A.reg, &s_f[0][cy + 1][cx], &s_b[0][cy + 1][cx], ps);
-    const int i = y * A.w + x;
-    const float I[3] = {A.image_level[3 * i], A.image_level[3 * i + 1],
-                        A.image_level[3 * i + 2]};
     float f[3], b[3];
-    fb_solve(q, a, I, f, b);
+    fb_solve(q, a, f, b);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         A.F[3 * i + c] = f[c];

@@ -90,33 +90,6 @@ struct Meta {
     double beta;          // CG: current beta
 };
 
-template <int H, int W, int GATE = kGateRunning>
-__device__ __forceinline__ void make_meta(const WorkList& wl, int t, const InstState* st,
-                                          Meta& m, GridDesc& gd) {
-    m.t = t;
-    m.g = find_grid(wl, t);
-    gd = wl.grids[m.g];
-    m.t0 = wl.tile_start[m.g];
-    m.t1 = wl.tile_start[m.g + 1];
-    const int local = t - m.t0;
-    const int tiles_x = (gd.w + W - 1) / W;
-    const int ty = local / tiles_x;
-    m.y0 = ty * H;
-    m.x0 = (local - ty * tiles_x) * W;
-    m.inst = gd.inst;
-    m.run = 1;
-    m.par = 0;
-    m.first = 0;
-    m.beta = 0.0;
-    if (st) {
-        const InstState& s = st[gd.inst];
-        m.run = s.status == kRunning && (GATE == kGateRunning || (s.flags & kUpdate) != 0);
-        m.par = s.iters & 1;
-        m.first = (s.flags & kFirst) != 0;
-        m.beta = s.beta;
-    }
-}
-
 // Two mbarriers (one per pipeline buffer) and their phase bits.
 struct Pipe {
     uint64_t* bar;
@@ -132,24 +105,80 @@ struct Pipe {
         }
         __syncthreads();
     }
-    // Wait for buffer b. The outcome is made uniform over the CTA: false in
-    // every thread if any thread's wait gave up. Then thread 0 sets the error
-    // flag and waits once more, again bounded, for the loads that may still
-    // be in flight into buffer b and (other_issued) the other buffer, so the
-    // CTA does not exit while a copy into its shared memory is pending.
-    __device__ bool wait(int b, bool other_issued) {
-        const uint32_t par = (phase >> b) & 1u;
-        const bool ok = mbar_wait(&bar[b], par);
+    // Wait for buffer b (bounded). Returns false if this thread gave up; the
+    // caller records that and acts on it at its next block barrier.
+    __device__ bool wait(int b) {
+        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1u);
         phase ^= 1u << b;
-        if (!__syncthreads_or(!ok)) return true;
-        if (threadIdx.x == 0) {
-            if (err) atomicExch(err, 1);
-            if (!ok) mbar_wait(&bar[b], par);
-            if (other_issued) mbar_wait(&bar[b ^ 1], (phase >> (b ^ 1)) & 1u);
-        }
-        return false;
+        return ok;
+    }
+    // After a wait that gave up (seen by the whole CTA at a barrier): thread
+    // 0 sets the error flag and waits once more, again bounded, for the loads
+    // that may still be in flight into buffer b (waited on last) and, if
+    // other_issued, into the other buffer, so that the CTA does not exit
+    // while a copy into its shared memory is pending.
+    __device__ void drain(int b, bool other_issued) {
+        if (threadIdx.x != 0) return;
+        if (err) atomicExch(err, 1);
+        mbar_wait(&bar[b], ((phase >> b) & 1u) ^ 1u);
+        if (other_issued) mbar_wait(&bar[b ^ 1], (phase >> (b ^ 1)) & 1u);
     }
 };
+
+// Per-CTA directory of a work list in shared memory: tile starts, grid
+// descriptors and the fields of each grid's image that the tile loops read
+// (gate, CG parity, first-pass flag, beta). Loaded once per launch, so that
+// the thread that prepares the next tile does no dependent global loads
+// (a binary search over tile_start in global memory costs one L2 round trip
+// per level). The image fields are stable for a launch: a kernel's own
+// finaliser changes an image's fields only after all of that image's tiles
+// are done. Lists of more than kDirGrids grids use global lookups.
+constexpr int kDirGrids = 64;
+struct TileDir {
+    int n;                              // grids held (0: use the global list)
+    int start[kDirGrids + 1];
+    int run[kDirGrids];
+    int par[kDirGrids];
+    int first[kDirGrids];
+    double beta[kDirGrids];
+    GridDesc g[kDirGrids];
+};
+
+template <int GATE>
+__device__ __forceinline__ void dir_load(TileDir& D, const WorkList& wl, const InstState* st) {
+    const bool fits = wl.ngrids <= kDirGrids;
+    if (fits) {
+        for (int i = threadIdx.x; i <= wl.ngrids; i += blockDim.x) D.start[i] = wl.tile_start[i];
+        for (int i = threadIdx.x; i < wl.ngrids; i += blockDim.x) {
+            const GridDesc g = wl.grids[i];
+            D.g[i] = g;
+            int run = 1, par = 0, first = 0;
+            double beta = 0.0;
+            if (st) {
+                const InstState& q = st[g.inst];
+                run = q.status == kRunning && (GATE == kGateRunning || (q.flags & kUpdate) != 0);
+                par = q.iters & 1;
+                first = (q.flags & kFirst) != 0;
+                beta = q.beta;
+            }
+            D.run[i] = run;
+            D.par[i] = par;
+            D.first[i] = first;
+            D.beta[i] = beta;
+        }
+    }
+    if (threadIdx.x == 0) D.n = fits ? wl.ngrids : 0;
+    __syncthreads();
+}
+
+__device__ __forceinline__ int dir_find(const TileDir& D, int t) {
+    int lo = 0, hi = D.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (D.start[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
 
 __device__ __forceinline__ const CUtensorMap* map_of(const CUtensorMap* maps, const GridDesc& g,
                                                      int slot) {
@@ -181,43 +210,129 @@ __device__ __forceinline__ T stencil_at(const T* P, int ph, const T* X, int r, i
 //   issue(meta, gd, buf)            thread 0 only
 //   body(meta, gd, buf)             all threads; returns nothing
 //   flush(meta, mine)               all threads, after an image's last tile
+// First tile >= t of this CTA's sequence (t = blockIdx.x mod gridDim.x)
+// whose image is running (every image when st is null), or wl.total; *gout
+// = its grid. Every tile of an image that is not running is skipped in one
+// step per image.
+template <int GATE>
+__device__ __forceinline__ int next_running_tile(const TileDir& D, const WorkList& wl,
+                                                 const InstState* st, int t, int* gout) {
+    const int G = gridDim.x;
+    while (t < wl.total) {
+        int g, nxt;
+        bool run;
+        if (D.n) {
+            g = dir_find(D, t);
+            run = D.run[g] != 0;
+            nxt = D.start[g + 1];
+        } else {
+            g = find_grid(wl, t);
+            run = true;
+            if (st) {
+                const InstState& q = st[wl.grids[g].inst];
+                run = q.status == kRunning && (GATE == kGateRunning || (q.flags & kUpdate) != 0);
+            }
+            nxt = wl.tile_start[g + 1];
+        }
+        if (run) {
+            *gout = g;
+            return t;
+        }
+        t += ((nxt - t + G - 1) / G) * G;
+    }
+    *gout = -1;
+    return wl.total;
+}
+
+// Meta of tile t of grid g (from the directory when it holds the list).
+template <int H, int W>
+__device__ __forceinline__ void dir_meta(const TileDir& D, const WorkList& wl, const InstState* st,
+                                         int t, int g, Meta& m, GridDesc& gd) {
+    m.t = t;
+    m.g = g;
+    m.run = 1;
+    if (D.n) {
+        gd = D.g[g];
+        m.t0 = D.start[g];
+        m.t1 = D.start[g + 1];
+        m.par = D.par[g];
+        m.first = D.first[g];
+        m.beta = D.beta[g];
+    } else {
+        gd = wl.grids[g];
+        m.t0 = wl.tile_start[g];
+        m.t1 = wl.tile_start[g + 1];
+        m.par = 0;
+        m.first = 0;
+        m.beta = 0.0;
+        if (st) {
+            const InstState& q = st[gd.inst];
+            m.par = q.iters & 1;
+            m.first = (q.flags & kFirst) != 0;
+            m.beta = q.beta;
+        }
+    }
+    const int local = t - m.t0;
+    const int tiles_x = (gd.w + W - 1) / W;
+    const int ty = local / tiles_x;
+    m.y0 = ty * H;
+    m.x0 = (local - ty * tiles_x) * W;
+    m.inst = gd.inst;
+}
+
 template <int H, int W, int GATE = kGateRunning, typename Issue, typename Body, typename Flush>
 __device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* st, Pipe& pipe,
                                           Meta* s_m, GridDesc* s_g, Issue issue, Body body,
                                           Flush flush) {
-    const int G = gridDim.x;
-    int t = blockIdx.x;
+    // Thread 0 walks the CTA's tiles through the directory, skipping every
+    // tile of an image that is not running; the tile after the current one
+    // is passed through s_t. A wait that gave up is recorded in s_abort and
+    // acted on at the barrier that ends the tile.
+    __shared__ TileDir D;
+    __shared__ int s_t[2], s_abort;
+    if (threadIdx.x == 0) s_abort = 0;
+    dir_load<GATE>(D, wl, st);
     int b = 0;
     unsigned int mine = 0;
-    if (threadIdx.x == 0 && t < wl.total) {
-        make_meta<H, W, GATE>(wl, t, st, s_m[0], s_g[0]);
-        if (s_m[0].run) {
+    if (threadIdx.x == 0) {
+        int g0;
+        const int t0 = next_running_tile<GATE>(D, wl, st, blockIdx.x, &g0);
+        s_t[0] = t0;
+        if (t0 < wl.total) {
+            dir_meta<H, W>(D, wl, st, t0, g0, s_m[0], s_g[0]);
             fence_proxy_async();
             issue(s_m[0], s_g[0], 0);
         }
     }
+    __syncthreads();
+    int t = s_t[0];
     while (t < wl.total) {
-        const int tn = t + G;
-        if (threadIdx.x == 0 && tn < wl.total) {
-            make_meta<H, W, GATE>(wl, tn, st, s_m[b ^ 1], s_g[b ^ 1]);
-            if (s_m[b ^ 1].run) {
+        if (threadIdx.x == 0) {
+            int gn;
+            const int tn = next_running_tile<GATE>(D, wl, st, t + (int)gridDim.x, &gn);
+            s_t[b ^ 1] = tn;
+            if (tn < wl.total) {
+                dir_meta<H, W>(D, wl, st, tn, gn, s_m[b ^ 1], s_g[b ^ 1]);
                 fence_proxy_async();
                 issue(s_m[b ^ 1], s_g[b ^ 1], b ^ 1);
             }
         }
         __syncthreads();
+        const int tn = s_t[b ^ 1];
         const Meta m = s_m[b];
-        if (m.run) {
-            if (!pipe.wait(b, tn < wl.total && s_m[b ^ 1].run)) return;
-            body(m, s_g[b], b);
-            ++mine;
-            const bool last_of_image = (tn >= wl.total) || (s_m[b ^ 1].inst != m.inst);
-            if (last_of_image) {
-                flush(m, mine);
-                mine = 0;
-            }
+        if (!pipe.wait(b)) s_abort = 1;
+        body(m, s_g[b], b);
+        ++mine;
+        const bool last_of_image = (tn >= wl.total) || (s_m[b ^ 1].inst != m.inst);
+        if (last_of_image) {
+            flush(m, mine);
+            mine = 0;
         }
         __syncthreads();
+        if (s_abort) {
+            pipe.drain(b, tn < wl.total);
+            return;
+        }
         b ^= 1;
         t = tn;
     }
@@ -415,38 +530,39 @@ k_cg_apply(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap,
 template <int GATE = kGateRunning, typename Body, typename Flush>
 __device__ __forceinline__ void flat_loop(const WorkList& wl, const InstState* st, Body body,
                                           Flush flush) {
-    __shared__ int s_inst[2], s_run, s_t0, s_t1;
+    // Thread 0 walks the CTA's chunks through the list's directory,
+    // skipping every chunk of an image that is not running.
+    __shared__ TileDir D;
+    __shared__ int s_inst[2], s_t0, s_t1, s_next, s_gnext;
     __shared__ GridDesc s_gd;
-    const int G = gridDim.x;
+    dir_load<GATE>(D, wl, st);
     unsigned int mine = 0;
-    for (int t = blockIdx.x; t < wl.total; t += G) {
-        const int tn = t + G;
+    if (threadIdx.x == 0) s_next = next_running_tile<GATE>(D, wl, st, blockIdx.x, &s_gnext);
+    __syncthreads();
+    for (int t = s_next; t < wl.total; t = s_next) {
+        __syncthreads();
         if (threadIdx.x == 0) {
-            const int g = find_grid(wl, t);
-            s_gd = wl.grids[g];
-            s_t0 = wl.tile_start[g];
-            s_t1 = wl.tile_start[g + 1];
+            const int g = s_gnext;
+            s_gd = D.n ? D.g[g] : wl.grids[g];
+            s_t0 = D.n ? D.start[g] : wl.tile_start[g];
+            s_t1 = D.n ? D.start[g + 1] : wl.tile_start[g + 1];
             s_inst[0] = s_gd.inst;
-            s_inst[1] = tn < wl.total ? wl.grids[find_grid(wl, tn)].inst : -1;
-            if (st) {
-                const InstState& q = st[s_gd.inst];
-                s_run = q.status == kRunning && (GATE == kGateRunning || (q.flags & kUpdate) != 0);
-            } else {
-                s_run = 1;
-            }
+            int gn;
+            const int tn = next_running_tile<GATE>(D, wl, st, t + (int)gridDim.x, &gn);
+            s_next = tn;
+            s_gnext = gn;
+            s_inst[1] = tn < wl.total ? (D.n ? D.g[gn].inst : wl.grids[gn].inst) : -1;
         }
         __syncthreads();
-        if (s_run) {
-            const GridDesc g = s_gd;
-            const int64_t n = (int64_t)g.h * g.pitch;
-            const int64_t e0 = (int64_t)(t - s_t0) * kFlat;
-            const int64_t e1 = min(e0 + kFlat, n);
-            body(g, e0, e1);
-            ++mine;
-            if (s_inst[1] != s_inst[0]) {
-                flush(s_inst[0], s_t0, s_t1, mine);
-                mine = 0;
-            }
+        const GridDesc g = s_gd;
+        const int64_t n = (int64_t)g.h * g.pitch;
+        const int64_t e0 = (int64_t)(t - s_t0) * kFlat;
+        const int64_t e1 = min(e0 + kFlat, n);
+        body(g, e0, e1);
+        ++mine;
+        if (s_inst[1] != s_inst[0]) {
+            flush(s_inst[0], s_t0, s_t1, mine);
+            mine = 0;
         }
         __syncthreads();
     }
@@ -1049,10 +1165,10 @@ k_galerkin_t(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtenso
 // Dense inverse of the coarsest operator by Gauss-Jordan elimination with
 // partial pivoting. One CTA per image; n <= kMaxDirect. *status is raised to
 // 2 on an exactly zero pivot and to 1 on a non-finite one.
-__global__ void k_dense_inverse(const DirectDesc* dd, int count, const double* __restrict__ Pc,
-                                double* work, int* status) {
+__global__ void k_dense_inverse(const DirectDesc* dd, int count, double* work, int* status) {
     if ((int)blockIdx.x >= count) return;
     const DirectDesc d = dd[blockIdx.x];
+    const double* __restrict__ Pc = d.P;
     const GridDesc g = d.g;
     const int n = g.h * g.w;
     double* A = work + d.work_off;
@@ -1325,8 +1441,16 @@ __device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int
         for (int j = 0; j < 3; ++j) loadx(r - 2 + k, c0 - V + j * V, &xr[k][j * V]);
     T pc[V];
     ldv<T, V>(P + r * BW + c0, pc);
+    // FP32: forward and backward terms in two independent chains (half the
+    // dependent-FMA latency per pixel). FP64 keeps one chain in the original
+    // order, which its iteration-count parity with the reference rests on.
+    constexpr bool kSplit = sizeof(T) == 4;
+    T accb[V];
 #pragma unroll
-    for (int v = 0; v < V; ++v) acc[v] = pc[v] * xr[2][V + v];
+    for (int v = 0; v < V; ++v) {
+        acc[v] = pc[v] * xr[2][V + v];
+        accb[v] = T(0);
+    }
 #pragma unroll
     for (int p = 1; p < kNH; ++p) {
         const int dy = half_dy(p), dx = half_dx(p);
@@ -1341,9 +1465,22 @@ __device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             acc[v] += pf[v] * xr[2 + dy][V + v + dx];
-            acc[v] += pb[(dx > 0 ? V : 0) + v - dx] * xr[2 - dy][V + v - dx];
+            if (kSplit) accb[v] += pb[(dx > 0 ? V : 0) + v - dx] * xr[2 - dy][V + v - dx];
+            else acc[v] += pb[(dx > 0 ? V : 0) + v - dx] * xr[2 - dy][V + v - dx];
         }
     }
+    if (kSplit) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] += accb[v];
+    }
+}
+
+// Division in the smoothing sweeps: IEEE in FP64; __fdividef in FP32, where
+// the V-cycle is the inner preconditioner of the mixed solve (convergence is
+// judged on the FP64 residual).
+template <typename T> __device__ __forceinline__ T smooth_div(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float smooth_div<float>(float a, float b) {
+    return __fdividef(a, b);
 }
 
 // y = A x (pitched vectors, no reductions). Plane box: rows y0-2 .. y0+7
@@ -1528,8 +1665,8 @@ k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensor
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const int fx = bx + col + v;
-                o[v] = (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w) ? (T)omega * bv[v] / dv[v]
-                                                                       : T(0);
+                o[v] = (fy >= 0 && fy < gf.h && fx >= 0 && fx < gf.w)
+                           ? smooth_div<T>((T)omega * bv[v], dv[v]) : T(0);
             }
             stv<T, V>(sX + rr * DW + col, o);
         }
@@ -1625,26 +1762,22 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
                 const int x = bx + col + v;
                 T val = T(0);
                 if (y >= 0 && y < gf.h && x >= 0 && x < gf.w) {
-                    const T x1 = (T)omega * bv[v] / dv[v];
+                    const T x1 = smooth_div<T>((T)omega * bv[v], dv[v]);
                     // Coarse pixels whose 3x3 support holds (y, x), in raster
-                    // order: even coordinates have one parent (weight 2), odd
-                    // ones two (weight 1); parents outside the grid add nothing.
-                    const int Ya = (y - 1) >> 1, Xa = (x - 1) >> 1;
-                    const bool ey = (y & 1) == 0, ex = (x & 1) == 0;
+                    // order: an even coordinate has one parent (weight 2), an
+                    // odd one two (weight 1). Written without branches: the
+                    // second parent of an even coordinate gets weight 0, and
+                    // parents outside the coarse grid read the zeros the TMA
+                    // box is filled with there, so both add exactly nothing.
+                    const int oy = y & 1, ox = x & 1;
+                    const T* c00 = C + (((y - oy) >> 1) - cy0) * kCBW + (((x - ox) >> 1) - cx0);
+                    const T wy0 = T(2 - oy), wy1 = T(oy), wx0 = T(2 - ox), wx1 = T(ox);
+                    const T s16 = T(0.0625);
                     T sum = T(0);
-#pragma unroll
-                    for (int jy = 0; jy < 2; ++jy) {
-                        const int Y = ey ? (y >> 1) : Ya + jy;
-                        if ((ey && jy == 1) || Y >= gc.h) continue;
-                        const double wy = ey ? 2.0 : 1.0;
-#pragma unroll
-                        for (int jx = 0; jx < 2; ++jx) {
-                            const int Xc = ex ? (x >> 1) : Xa + jx;
-                            if ((ex && jx == 1) || Xc >= gc.w) continue;
-                            const double wx = ex ? 2.0 : 1.0;
-                            sum += (T)(wx * wy / 16.0) * C[(Y - cy0) * kCBW + (Xc - cx0)];
-                        }
-                    }
+                    sum += (wx0 * wy0 * s16) * c00[0];
+                    sum += (wx1 * wy0 * s16) * c00[ox];
+                    sum += (wx0 * wy1 * s16) * c00[oy * kCBW];
+                    sum += (wx1 * wy1 * s16) * c00[oy * kCBW + ox];
                     val = x1 + sum;
                 }
                 o[v] = val;
@@ -1667,7 +1800,7 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 if (xx + v < gf.w) {
-                    x3[v] = x2[v] + (T)omega * (bv[v] - ax[v]) / dv[v];
+                    x3[v] = x2[v] + smooth_div<T>((T)omega * (bv[v] - ax[v]), dv[v]);
                     if (level0) {
                         acc2[0] += (double)bv[v] * (double)x3[v];
                         if (reorth) acc2[1] += (double)dr[i + v] * (double)x3[v];
@@ -2151,9 +2284,9 @@ void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrid
     k_galerkin<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(fine_g, coarse_g, ngrids, Pf, Pc, total);
 }
 
-void launch_dense_inverse(const DirectDesc* dd, int count, const double* Pc, double* work,
-                          int* status, cudaStream_t s) {
-    if (count > 0) k_dense_inverse<<<count, 256, 0, s>>>(dd, count, Pc, work, status);
+void launch_dense_inverse(const DirectDesc* dd, int count, double* work, int* status,
+                          cudaStream_t s) {
+    if (count > 0) k_dense_inverse<<<count, 256, 0, s>>>(dd, count, work, status);
 }
 
 void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s) {

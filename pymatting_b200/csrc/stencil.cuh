@@ -18,6 +18,7 @@ struct DirectDesc {
     GridDesc g;
     double* inv;        // n x n inverse
     int64_t work_off;   // n x n scratch used while inverting (setup only)
+    const double* P;    // FP64 planes of the grid's level (grid at P + g.poff)
 };
 
 // Coarse-level tail (one CTA per image, shared-memory resident; k_vc_tail).
@@ -115,8 +116,9 @@ void launch_galerkin_t(const WorkList& wl, const GridDesc* fine, const CUtensorM
                        double* Pc, int* err, cudaStream_t s);
 void launch_galerkin(const GridDesc* fine_g, const GridDesc* coarse_g, int ngrids, const double* Pf,
                      double* Pc, int64_t total, cudaStream_t s);
-void launch_dense_inverse(const DirectDesc* dd, int count, const double* Pc, double* work,
-                          int* status, cudaStream_t s);
+// Dense inverses of every coarsest grid in one launch (one CTA per grid).
+void launch_dense_inverse(const DirectDesc* dd, int count, double* work, int* status,
+                          cudaStream_t s);
 void launch_convert_f32(const double* src, float* dst, int64_t n, cudaStream_t s);
 void launch_refine_residual(int prec, int first, const LaunchCfg& L, const WorkList& wl,
                             const CUtensorMap* maps, const float* P32, const double* b,
