@@ -730,7 +730,7 @@ def main():
         batch = info[0]
         launches = batch.system.launch_count() + 4 * len(imgs)
         results[precision] = dict(total_ms=total_ms, batch=batch, x=info[1],
-                                  launches_per_step=launches)
+                                  launches_per_step=launches, step_ms=times)
 
     # End to end through the public API with host buffers: pinned host
     # tensors in, every rank's alphas gathered to rank 0 and downloaded there.
@@ -812,6 +812,7 @@ def main():
             },
             "fp64_value": value64,
             "mixed_over_fp64": value / value64,
+            "step_ms": {p: [round(t, 2) for t in results[p]["step_ms"]] for p in ["mixed", "fp64"]},
             "iters": {"mixed_inner": [s.iters for s in stats_timed["mixed"]],
                       "mixed_outer": [s.outer_iters for s in stats_timed["mixed"]],
                       "fp64": [s.iters for s in stats_timed["fp64"]]},

@@ -15,6 +15,8 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -533,61 +535,91 @@ static int encode_map(CUtensorMap* out, const void* base, const GridDesc& g, boo
 
 // Fill every grid's descriptor block. Slots that a configuration never
 // reads are left zero.
-static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
-    maps.assign((size_t)S.nmaps * kMapsPerGrid, CUtensorMap{});
+// Descriptors of one grid of level l (the block at g.map_base).
+static int encode_grid_maps(Stencil& S, int l, const GridDesc& g, CUtensorMap* m) {
     const bool mixed = S.precision == 1;
     const int DH = 2 * S.cy + 5;
     const int DWV = mixed ? down_box_width<float>() : down_box_width<double>();
-    for (int l = 0; l < (int)S.levels.size(); ++l) {
-        Level& lv = S.levels[l];
-        const void* P = mixed ? (const void*)planes32(S, l) : (const void*)planes64(S, l);
-        const void* B; const void* X; const void* XA = nullptr; const void* XB = nullptr;
-        if (l == 0) {
-            B = mixed ? (const void*)S.at<float>(S.o_r32) : (const void*)S.at<double>(S.o_r64);
-            X = mixed ? (const void*)S.at<float>(S.o_z32) : (const void*)S.at<double>(S.o_z64);
-        } else {
-            B = mixed ? (const void*)S.at<float>(lv.b32) : (const void*)S.at<double>(lv.b64);
-            X = mixed ? (const void*)S.at<float>(lv.x32) : (const void*)S.at<double>(lv.x64);
-        }
-        if (S.precond == kPrecVcycle && (S.pre > 1 || S.post > 1)) {
-            XA = mixed ? (const void*)S.at<float>(lv.xa32) : (const void*)S.at<double>(lv.xa64);
-            XB = mixed ? (const void*)S.at<float>(lv.xb32) : (const void*)S.at<double>(lv.xb64);
-        }
-        for (const GridDesc& g : lv.grids) {
-            if (g.w <= 0 || g.h <= 0) continue;
-            CUtensorMap* m = &maps[(size_t)g.map_base * kMapsPerGrid];
-            int rc = 0;
-            rc |= encode_map(m + kMapPlF, P, g, true, mixed, kBW, kBH);
-            rc |= encode_map(m + kMapPlD, P, g, true, mixed, kBW, DH);
-            rc |= encode_map(m + kMapBF, B, g, false, mixed, kBW, kBH);
-            rc |= encode_map(m + kMapBD, B, g, false, mixed, kBW, DH);
-            rc |= encode_map(m + kMapXC, X, g, false, mixed, kCBW, kCBH);
-            rc |= encode_map(m + kMapXF, X, g, false, mixed, kBW, kBH);
-            rc |= encode_map(m + kMapPlS, P, g, true, mixed, kBW, kPH);
-            rc |= encode_map(m + kMapPlDV, P, g, true, mixed, DWV, DH);
-            rc |= encode_map(m + kMapBDV, B, g, false, mixed, DWV, DH);
-            rc |= encode_map(m + kMapPlG, planes64(S, l), g, true, false, kGCols, kGRows);
-            if (XA) {
-                rc |= encode_map(m + kMapXAF, XA, g, false, mixed, kBW, kBH);
-                rc |= encode_map(m + kMapXAD, XA, g, false, mixed, kBW, DH);
-                rc |= encode_map(m + kMapXBF, XB, g, false, mixed, kBW, kBH);
-                rc |= encode_map(m + kMapXBD, XB, g, false, mixed, kBW, DH);
-            }
-            if (l == 0) {
-                const void* Z = X;
-                const void* Q0 = mixed ? (const void*)S.at<float>(S.o_p032) : (const void*)S.at<double>(S.o_p064);
-                const void* Q1 = mixed ? (const void*)S.at<float>(S.o_p132) : (const void*)S.at<double>(S.o_p164);
-                rc |= encode_map(m + kMapZF, Z, g, false, mixed, kBW, kBH);
-                rc |= encode_map(m + kMapP0F, Q0, g, false, mixed, kBW, kBH);
-                rc |= encode_map(m + kMapP1F, Q1, g, false, mixed, kBW, kBH);
-                if (mixed) {
-                    rc |= encode_map(m + kMapX64F, S.at<double>(S.o_x64), g, false, false, kBW, kBH);
-                    rc |= encode_map(m + kMapP64F, S.P0, g, true, false, kBW, kBH);
-                }
-            }
-            if (rc) return rc;
+    Level& lv = S.levels[l];
+    const void* P = mixed ? (const void*)planes32(S, l) : (const void*)planes64(S, l);
+    const void* B; const void* X; const void* XA = nullptr; const void* XB = nullptr;
+    if (l == 0) {
+        B = mixed ? (const void*)S.at<float>(S.o_r32) : (const void*)S.at<double>(S.o_r64);
+        X = mixed ? (const void*)S.at<float>(S.o_z32) : (const void*)S.at<double>(S.o_z64);
+    } else {
+        B = mixed ? (const void*)S.at<float>(lv.b32) : (const void*)S.at<double>(lv.b64);
+        X = mixed ? (const void*)S.at<float>(lv.x32) : (const void*)S.at<double>(lv.x64);
+    }
+    if (S.precond == kPrecVcycle && (S.pre > 1 || S.post > 1)) {
+        XA = mixed ? (const void*)S.at<float>(lv.xa32) : (const void*)S.at<double>(lv.xa64);
+        XB = mixed ? (const void*)S.at<float>(lv.xb32) : (const void*)S.at<double>(lv.xb64);
+    }
+    int rc = 0;
+    rc |= encode_map(m + kMapPlF, P, g, true, mixed, kBW, kBH);
+    rc |= encode_map(m + kMapPlD, P, g, true, mixed, kBW, DH);
+    rc |= encode_map(m + kMapBF, B, g, false, mixed, kBW, kBH);
+    rc |= encode_map(m + kMapBD, B, g, false, mixed, kBW, DH);
+    rc |= encode_map(m + kMapXC, X, g, false, mixed, kCBW, kCBH);
+    rc |= encode_map(m + kMapXF, X, g, false, mixed, kBW, kBH);
+    rc |= encode_map(m + kMapPlS, P, g, true, mixed, kBW, kPH);
+    rc |= encode_map(m + kMapPlDV, P, g, true, mixed, DWV, DH);
+    rc |= encode_map(m + kMapBDV, B, g, false, mixed, DWV, DH);
+    rc |= encode_map(m + kMapPlG, planes64(S, l), g, true, false, kGCols, kGRows);
+    if (XA) {
+        rc |= encode_map(m + kMapXAF, XA, g, false, mixed, kBW, kBH);
+        rc |= encode_map(m + kMapXAD, XA, g, false, mixed, kBW, DH);
+        rc |= encode_map(m + kMapXBF, XB, g, false, mixed, kBW, kBH);
+        rc |= encode_map(m + kMapXBD, XB, g, false, mixed, kBW, DH);
+    }
+    if (l == 0) {
+        const void* Z = X;
+        const void* Q0 = mixed ? (const void*)S.at<float>(S.o_p032) : (const void*)S.at<double>(S.o_p064);
+        const void* Q1 = mixed ? (const void*)S.at<float>(S.o_p132) : (const void*)S.at<double>(S.o_p164);
+        rc |= encode_map(m + kMapZF, Z, g, false, mixed, kBW, kBH);
+        rc |= encode_map(m + kMapP0F, Q0, g, false, mixed, kBW, kBH);
+        rc |= encode_map(m + kMapP1F, Q1, g, false, mixed, kBW, kBH);
+        if (mixed) {
+            rc |= encode_map(m + kMapX64F, S.at<double>(S.o_x64), g, false, false, kBW, kBH);
+            rc |= encode_map(m + kMapP64F, S.P0, g, true, false, kBW, kBH);
         }
     }
+    return rc;
+}
+
+// Fill every grid's descriptor block (host work: thousands of descriptors
+// for a large batch), spread over up to 8 host threads. Slots that a
+// configuration never reads are left zero.
+static int encode_maps(Stencil& S, std::vector<CUtensorMap>& maps) {
+    maps.assign((size_t)S.nmaps * kMapsPerGrid, CUtensorMap{});
+    if (!encode_fn()) return fail(kErrCuda, "cuTensorMapEncodeTiled is not available");
+    std::vector<std::pair<int, GridDesc>> work;
+    for (int l = 0; l < (int)S.levels.size(); ++l)
+        for (const GridDesc& g : S.levels[l].grids)
+            if (g.w > 0 && g.h > 0) work.push_back({l, g});
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<size_t>({(size_t)8, (size_t)hw, (work.size() + 63) / 64});
+    std::atomic<int> bad{0};
+    int device = 0;
+    PMB_CUDA(cudaGetDevice(&device));
+    auto run = [&](int k) {
+        // The encoder needs the caller's context current in this thread.
+        if (k > 0 && cudaSetDevice(device) != cudaSuccess) {
+            bad.store(1);
+            return;
+        }
+        for (size_t q = (size_t)k; q < work.size(); q += (size_t)std::max(nt, 1)) {
+            const GridDesc& g = work[q].second;
+            if (encode_grid_maps(S, work[q].first, g, &maps[(size_t)g.map_base * kMapsPerGrid]))
+                bad.store(1);
+        }
+    };
+    // Share 0 on the calling thread (its context is current), the others on
+    // helper threads.
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) th.emplace_back(run, k);
+    run(0);
+    for (auto& t : th) t.join();
+    if (bad.load()) return fail(kErrCuda, "cuTensorMapEncodeTiled failed");
     return 0;
 }
 
