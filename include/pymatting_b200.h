@@ -237,8 +237,11 @@ int pmb_stencil_destroy(pmb_stencil* s);
  * only for the FP32 inner solve), 1 the same for the prolongation, 2/3/4
  * resident CTAs per SM of the level-0 tile kernels / prolongation /
  * restriction (up to the shared-memory limit), 5 CTAs per SM of the
- * element-wise kernels, 6 CG iterations per graph replay. Returns the value
- * applied (after clamping) or a negative status. */
+ * element-wise kernels, 6 CG iterations per graph replay, 7 buffers of the
+ * CG apply, restriction and prolongation kernels (1, the default: half the
+ * shared memory, so twice the CTAs per SM; 2: a tile in flight per CTA;
+ * setting it resets knobs 2, 3 and 4 to the new residency limit). Returns
+ * the value applied (after clamping) or a negative status. */
 int pmb_stencil_tune(pmb_stencil* s, int knob, int value);
 int pmb_stencil_tuning(const pmb_stencil* s, int knob);
 /* Average milliseconds of one level-0 operator apply y = A x (inner

@@ -10,7 +10,12 @@ The knobs (``pmb_stencil_tune`` in the C ABI):
   their shared memory);
 * ``ctas_flat`` — CTAs per SM of the element-wise kernels;
 * ``chunk`` — CG iterations per CUDA-graph replay (the host reads the
-  per-image status once per replay).
+  per-image status once per replay);
+* ``stages`` — buffers of the CG apply, restriction and prolongation
+  kernels: 1 (the default: half the shared memory, so twice the CTAs per SM)
+  or 2 (one tile in flight per CTA while another is computed). Setting it
+  resets ``ctas_fine`` / ``ctas_up`` / ``ctas_down`` to the new residency
+  limit, so it is walked first.
 
 ``autotune(batch)`` times full solves of the batch's own system with CUDA
 events and walks the knobs one at a time (coordinate descent, two passes),
@@ -30,9 +35,9 @@ from . import _ffi
 
 __all__ = ["KNOBS", "tuning", "apply_tuning", "autotune", "cache_key", "cached"]
 
-KNOBS = {"vec_apply": 0, "vec_up": 1, "ctas_fine": 2, "ctas_up": 3, "ctas_down": 4,
-         "ctas_flat": 5, "chunk": 6}
-CANDIDATES = {"vec_apply": [2, 4], "vec_up": [2, 4], "ctas_fine": [1, 2, 3, 4],
+KNOBS = {"stages": 7, "vec_apply": 0, "vec_up": 1, "ctas_fine": 2, "ctas_up": 3,
+         "ctas_down": 4, "ctas_flat": 5, "chunk": 6}
+CANDIDATES = {"stages": [1, 2], "vec_apply": [2, 4], "vec_up": [2, 4], "ctas_fine": [1, 2, 3, 4],
               "ctas_up": [1, 2, 3, 4], "ctas_down": [1, 2, 3, 4], "ctas_flat": [2, 4, 8, 16],
               "chunk": [2, 4, 8]}
 _MARGIN = 0.02          # a change must win by 2 %

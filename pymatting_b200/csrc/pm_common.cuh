@@ -70,6 +70,10 @@ enum : int {
     kMapPlDV,      // planes, register-blocked restriction box
     kMapBDV,       // b, register-blocked restriction box
     kMapPlG,       // FP64 planes, Galerkin box (42 x 21 x 13)
+    kMapPlD0,      // plane 0, register-blocked restriction box (1 plane)
+    kMapPlD1,      // planes 1..12, restriction box two rows shorter (loaded at plane 1)
+    kMapPlU0,      // plane 0, prolongation box kBW x kBH (1 plane)
+    kMapPlU1,      // planes 1..12, kBW x kPH (loaded at plane 1)
     kMapsPerGrid
 };
 

@@ -338,6 +338,55 @@ __device__ __forceinline__ void tile_loop(const WorkList& wl, const InstState* s
     }
 }
 
+// Single-buffer variant of tile_loop: the tile's loads are issued when the
+// previous tile is done, so a CTA has at most one tile in flight and needs
+// half the shared memory; several CTAs per SM then overlap each other's
+// loads and compute.
+template <int H, int W, int GATE = kGateRunning, typename Issue, typename Body, typename Flush>
+__device__ __forceinline__ void tile_loop1(const WorkList& wl, const InstState* st, Pipe& pipe,
+                                           Meta* s_m, GridDesc* s_g, Issue issue, Body body,
+                                           Flush flush) {
+    __shared__ TileDir D;
+    __shared__ int s_tn, s_gn, s_ninst, s_abort;   // the tile after the current one
+    if (threadIdx.x == 0) s_abort = 0;
+    dir_load<GATE>(D, wl, st);
+    unsigned int mine = 0;
+    if (threadIdx.x == 0) s_tn = next_running_tile<GATE>(D, wl, st, blockIdx.x, &s_gn);
+    __syncthreads();
+    int t = s_tn;
+    int g = s_gn;
+    __syncthreads();
+    while (t < wl.total) {
+        if (threadIdx.x == 0) {
+            dir_meta<H, W>(D, wl, st, t, g, s_m[0], s_g[0]);
+            fence_proxy_async();
+            issue(s_m[0], s_g[0], 0);
+            int gn;
+            const int tn = next_running_tile<GATE>(D, wl, st, t + (int)gridDim.x, &gn);
+            s_tn = tn;
+            s_gn = gn;
+            s_ninst = tn < wl.total ? (D.n ? D.g[gn].inst : wl.grids[gn].inst) : -1;
+        }
+        __syncthreads();
+        const Meta m = s_m[0];
+        const int tn = s_tn, gn = s_gn, ninst = s_ninst;
+        if (!pipe.wait(0)) s_abort = 1;
+        body(m, s_g[0], 0);
+        ++mine;
+        if (ninst != m.inst) {
+            flush(m, mine);
+            mine = 0;
+        }
+        __syncthreads();
+        if (s_abort) {
+            pipe.drain(0, false);
+            return;
+        }
+        t = tn;
+        g = gn;
+    }
+}
+
 struct NoFlush {
     __device__ void operator()(const Meta&, unsigned int) const {}
 };
@@ -1431,16 +1480,18 @@ constexpr int kDownThreads = 256;
 // row 0 = two rows above the first output row of the tile; loadx(row, col, o)
 // loads V operand values at an aligned box position. Needs rows r-2 .. r+2 of
 // the operand, r-2 .. r of the planes, columns c0 - V .. c0 + 2V - 1.
+// Plane 0 and planes 1..12 may lie in separate boxes with the same first
+// row: plane 0 at P0, plane p >= 1 at P1 + (p - 1) ps1 (BW-wide rows).
 template <typename T, int V, int BW, typename LoadX>
-__device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int r, int c0,
-                                            T (&acc)[V]) {
+__device__ __forceinline__ void stencil_split(const T* P0, const T* P1, int ps1, LoadX loadx,
+                                              int r, int c0, T (&acc)[V]) {
     T xr[5][3 * V];
 #pragma unroll
     for (int k = 0; k < 5; ++k)
 #pragma unroll
         for (int j = 0; j < 3; ++j) loadx(r - 2 + k, c0 - V + j * V, &xr[k][j * V]);
     T pc[V];
-    ldv<T, V>(P + r * BW + c0, pc);
+    ldv<T, V>(P0 + r * BW + c0, pc);
     // FP32: forward and backward terms in two independent chains (half the
     // dependent-FMA latency per pixel). FP64 keeps one chain in the original
     // order, which its iteration-count parity with the reference rests on.
@@ -1454,14 +1505,15 @@ __device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int
 #pragma unroll
     for (int p = 1; p < kNH; ++p) {
         const int dy = half_dy(p), dx = half_dx(p);
+        const T* Pp = P1 + (p - 1) * ps1;
         T pf[V];
-        ldv<T, V>(P + p * ps + r * BW + c0, pf);
+        ldv<T, V>(Pp + r * BW + c0, pf);
         // Backward entries A[i, i - d] = plane p at (r - dy, c - dx): an
         // aligned window of one or two vectors around c0 - dx.
         T pb[2 * V];
         const int cb = dx > 0 ? c0 - V : c0;
-        ldv<T, V>(P + p * ps + (r - dy) * BW + cb, pb);
-        if (dx != 0) ldv<T, V>(P + p * ps + (r - dy) * BW + cb + V, pb + V);
+        ldv<T, V>(Pp + (r - dy) * BW + cb, pb);
+        if (dx != 0) ldv<T, V>(Pp + (r - dy) * BW + cb + V, pb + V);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             acc[v] += pf[v] * xr[2 + dy][V + v + dx];
@@ -1473,6 +1525,12 @@ __device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int
 #pragma unroll
         for (int v = 0; v < V; ++v) acc[v] += accb[v];
     }
+}
+
+template <typename T, int V, int BW, typename LoadX>
+__device__ __forceinline__ void stencil_vec(const T* P, int ps, LoadX loadx, int r, int c0,
+                                            T (&acc)[V]) {
+    stencil_split<T, V, BW>(P, P + ps, ps, loadx, r, c0, acc);
 }
 
 // Division in the smoothing sweeps: IEEE in FP64; __fdividef in FP32, where
@@ -1529,7 +1587,7 @@ k_apply_v(WorkList wl, const CUtensorMap* maps, T* y, int* err) {
 // p_new = z + beta p_old (z on the first pass), Ap = A p_new, p_new . Ap;
 // finaliser alpha = rz / (p . Ap) (cg.py:85-90, 111-113). p_new is formed
 // in registers from the z and p_old boxes.
-template <typename T, int V>
+template <typename T, int V, int NST>
 __global__ void __launch_bounds__(tile_threads_v<V>())
 k_cg_apply_v(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap, InstState* st,
              double* partials, int* err) {
@@ -1542,10 +1600,15 @@ k_cg_apply_v(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* A
     T* sP_[2];
     T* sZ_[2];
     T* sQ_[2];
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < NST; ++k) {
         sP_[k] = sc.take<T>(kNH * kPH * kBW);
         sZ_[k] = sc.take<T>(kBH * kBW);
         sQ_[k] = sc.take<T>(kBH * kBW);
+    }
+    if (NST == 1) {
+        sP_[1] = sP_[0];
+        sZ_[1] = sZ_[0];
+        sQ_[1] = sQ_[0];
     }
     const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
     const Buf2<T> sZ{sZ_[0], sZ_[1] - sZ_[0]};
@@ -1602,7 +1665,8 @@ k_cg_apply_v(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* A
             s->flags &= ~kFirst;
         });
     };
-    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
+    if (NST == 2) tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
+    else tile_loop1<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
 }
 
 // Restriction box of the register-blocked restriction kernel: fine columns
@@ -1621,7 +1685,11 @@ template <typename T, int VV> struct DownBox {
 // (vcycle.py:33-36, 77-80; same arithmetic as k_vc_down<T, 1>):
 //   x1 = omega b / d on the box, res = b - A x1 on the fine rows
 //   2 Y0 - 1 .. 2 Y0 + 2 CY - 1, b_coarse = R res.
-template <typename T, int V>
+// NST: 2 buffers (a tile in flight while the previous one is computed) or 1
+// (half the shared memory, twice the CTAs per SM). Plane 0 (the diagonal of
+// the sweep over the whole box) is loaded on DH rows, planes 1..12 (only
+// the residual rows' backward entries) on DH - 2.
+template <typename T, int V, int NST>
 __global__ void __launch_bounds__(kDownThreads)
 k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensorMap* maps, T* bc,
             double omega, const InstState* st, int* err) {
@@ -1632,13 +1700,21 @@ k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensor
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP_[2];
+    T* sP0_[2];
+    T* sP1_[2];
     T* sB_[2];
-    for (int k = 0; k < 2; ++k) {
-        sP_[k] = sc.take<T>(kNH * DH * DW);
+    for (int k = 0; k < NST; ++k) {
+        sP0_[k] = sc.take<T>(DH * DW);
+        sP1_[k] = sc.take<T>((kNH - 1) * (DH - 2) * DW);
         sB_[k] = sc.take<T>(DH * DW);
     }
-    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    if (NST == 1) {
+        sP0_[1] = sP0_[0];
+        sP1_[1] = sP1_[0];
+        sB_[1] = sB_[0];
+    }
+    const Buf2<T> sP0{sP0_[0], sP0_[1] - sP0_[0]};
+    const Buf2<T> sP1{sP1_[0], sP1_[1] - sP1_[0]};
     const Buf2<T> sB{sB_[0], sB_[1] - sB_[0]};
     T* sX = sc.take<T>(DH * DW);
     T* sR = sc.take<T>(RH * RW);
@@ -1647,15 +1723,17 @@ k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensor
     auto issue = [&](const Meta& m, const GridDesc& gc, int bb) {
         const GridDesc gf = fine[m.g];
         const int bx = 2 * m.x0 - D::DOFF, by = 2 * m.y0 - 3;
-        mbar_expect_tx(&pipe.bar[bb], (kNH + 1) * DH * DW * sizeof(T));
-        tma_load_3d(sP[bb], map_of(maps, gf, kMapPlDV), bx, by, 0, &pipe.bar[bb]);
+        mbar_expect_tx(&pipe.bar[bb], (2 * DH + (kNH - 1) * (DH - 2)) * DW * sizeof(T));
+        tma_load_3d(sP0[bb], map_of(maps, gf, kMapPlD0), bx, by, 0, &pipe.bar[bb]);
+        tma_load_3d(sP1[bb], map_of(maps, gf, kMapPlD1), bx, by, 1, &pipe.bar[bb]);
         tma_load_2d(sB[bb], map_of(maps, gf, kMapBDV), bx, by, &pipe.bar[bb]);
     };
     auto body = [&](const Meta& m, const GridDesc& gc, int bb) {
         const GridDesc gf = fine[m.g];
         const int bx = 2 * m.x0 - D::DOFF, by = 2 * m.y0 - 3;
         const T* B = sB[bb];
-        const T* P = sP[bb];
+        const T* P = sP0[bb];
+        const T* P1 = sP1[bb];
         for (int q = threadIdx.x; q < DH * XV; q += kDownThreads) {
             const int rr = q / XV, col = (q - rr * XV) * V;
             const int fy = by + rr;
@@ -1676,9 +1754,9 @@ k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensor
             const int br = rr + 2, bcol = D::DOFF - V + cv * V;
             const int fy = by + br;
             T acc[V], bv[V], o[V];
-            stencil_vec<T, V, DW>(P, DH * DW,
-                               [&](int r2, int c2, T* out) { ldv<T, V>(sX + r2 * DW + c2, out); },
-                               br, bcol, acc);
+            stencil_split<T, V, DW>(P, P1, (DH - 2) * DW,
+                                    [&](int r2, int c2, T* out) { ldv<T, V>(sX + r2 * DW + c2, out); },
+                                    br, bcol, acc);
             ldv<T, V>(B + br * DW + bcol, bv);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
@@ -1703,14 +1781,18 @@ k_vc_down_v(WorkList wl /* coarse tiles */, const GridDesc* fine, const CUtensor
             }
         }
     };
-    tile_loop<CY, kCX>(wl, st, pipe, s_m, s_g, issue, body, NoFlush());
+    if (NST == 2) tile_loop<CY, kCX>(wl, st, pipe, s_m, s_g, issue, body, NoFlush());
+    else tile_loop1<CY, kCX>(wl, st, pipe, s_m, s_g, issue, body, NoFlush());
 }
 
 // Prolongation and one post-smoothing sweep (same arithmetic as
 // k_vc_up<T, 1, 1>): x2 = x1 + P xc on the 72 x 12 box into shared memory,
 // then x3 = x2 + omega (b - A x2) / d for the tile; at level 0 also r . z
 // (and (r - r_old) . z) with beta.
-template <typename T, int V>
+// NST as in k_vc_down_v. Plane 0 (the diagonal of the first sweep over the
+// whole box) is loaded on kBH rows, planes 1..12 (the post sweep's backward
+// entries) on kPH.
+template <typename T, int V, int NST>
 __global__ void __launch_bounds__(tile_threads_v<V>())
 k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMap* maps,
           const T* __restrict__ b, T* xout, double omega, InstState* st, int level0,
@@ -1721,15 +1803,24 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
     __shared__ Meta s_m[2];
     __shared__ GridDesc s_g[2];
     SmemCarve sc(g_smem);
-    T* sP_[2];
+    T* sP0_[2];
+    T* sP1_[2];
     T* sB_[2];
     T* sC_[2];
-    for (int k = 0; k < 2; ++k) {
-        sP_[k] = sc.take<T>(kNH * kBH * kBW);
+    for (int k = 0; k < NST; ++k) {
+        sP0_[k] = sc.take<T>(kBH * kBW);
+        sP1_[k] = sc.take<T>((kNH - 1) * kPH * kBW);
         sB_[k] = sc.take<T>(kBH * kBW);
         sC_[k] = sc.take<T>(kCBH * kCBW);
     }
-    const Buf2<T> sP{sP_[0], sP_[1] - sP_[0]};
+    if (NST == 1) {
+        sP0_[1] = sP0_[0];
+        sP1_[1] = sP1_[0];
+        sB_[1] = sB_[0];
+        sC_[1] = sC_[0];
+    }
+    const Buf2<T> sP0{sP0_[0], sP0_[1] - sP0_[0]};
+    const Buf2<T> sP1{sP1_[0], sP1_[1] - sP1_[0]};
     const Buf2<T> sB{sB_[0], sB_[1] - sB_[0]};
     const Buf2<T> sC{sC_[0], sC_[1] - sC_[0]};
     T* sX = sc.take<T>(kBH * kBW);
@@ -1738,8 +1829,10 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
     double acc2[2] = {0.0, 0.0};
     auto issue = [&](const Meta& m, const GridDesc& gf, int bb) {
         const GridDesc gc = coarse[m.g];
-        mbar_expect_tx(&pipe.bar[bb], ((kNH + 1) * kBH * kBW + kCBH * kCBW) * sizeof(T));
-        tma_load_3d(sP[bb], map_of(maps, gf, kMapPlF), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        mbar_expect_tx(&pipe.bar[bb],
+                       ((2 * kBH + (kNH - 1) * kPH) * kBW + kCBH * kCBW) * sizeof(T));
+        tma_load_3d(sP0[bb], map_of(maps, gf, kMapPlU0), m.x0 - kBOX, m.y0 - 2, 0, &pipe.bar[bb]);
+        tma_load_3d(sP1[bb], map_of(maps, gf, kMapPlU1), m.x0 - kBOX, m.y0 - 2, 1, &pipe.bar[bb]);
         tma_load_2d(sB[bb], map_of(maps, gf, kMapBF), m.x0 - kBOX, m.y0 - 2, &pipe.bar[bb]);
         tma_load_2d(sC[bb], map_of(maps, gc, kMapXC), (m.x0 >> 1) - 4, (m.y0 >> 1) - 2,
                     &pipe.bar[bb]);
@@ -1748,7 +1841,8 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
         const GridDesc gc = coarse[m.g];
         const int bx = m.x0 - kBOX, by = m.y0 - 2;
         const int cx0 = (m.x0 >> 1) - 4, cy0 = (m.y0 >> 1) - 2;
-        const T* P = sP[bb];
+        const T* P = sP0[bb];
+        const T* P1 = sP1[bb];
         const T* B = sB[bb];
         const T* C = sC[bb];
         for (int q = threadIdx.x; q < kBH * XV; q += NT) {
@@ -1790,9 +1884,9 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
         if (yy < gf.h && xx < gf.w) {
             const int r = ty + 2, c0 = kBOX + V * tx;
             T ax[V], x2[V], bv[V], dv[V], x3[V];
-            stencil_vec<T, V, kBW>(P, kBH * kBW,
-                                [&](int r2, int c2, T* out) { ldv<T, V>(sX + r2 * kBW + c2, out); },
-                                r, c0, ax);
+            stencil_split<T, V, kBW>(P, P1, kPH * kBW,
+                                     [&](int r2, int c2, T* out) { ldv<T, V>(sX + r2 * kBW + c2, out); },
+                                     r, c0, ax);
             ldv<T, V>(sX + r * kBW + c0, x2);
             ldv<T, V>(B + r * kBW + c0, bv);
             ldv<T, V>(P + r * kBW + c0, dv);
@@ -1820,7 +1914,8 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
             else finish_beta(s, sum[0]);
         });
     };
-    tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
+    if (NST == 2) tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
+    else tile_loop1<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
 }
 
 
@@ -2088,8 +2183,8 @@ template <typename T> size_t smem_up(int pre) {
     return 2 * per + 128;
 }
 
-template <typename T> size_t smem_apply_v() {
-    return 2 * (rup(kNH * kPH * kBW * sizeof(T)) + 2 * rup(kBH * kBW * sizeof(T))) + 128;
+template <typename T> size_t smem_apply_v(int nst) {
+    return nst * (rup(kNH * kPH * kBW * sizeof(T)) + 2 * rup(kBH * kBW * sizeof(T))) + 128;
 }
 // Vector widths of the register-blocked kernels, measured on B200 at
 // 1920x1080 and 4096x4096: the plain apply is fastest with 4 FP32 pixels per
@@ -2101,17 +2196,18 @@ template <typename T> constexpr int kVSolve = 2;
 // and the prolongation): 4 in FP32, 2 in FP64.
 template <typename T> constexpr int kVWide = sizeof(T) == 8 ? 2 : 4;
 
-template <typename T, int V> static size_t smem_down_vv() {
+template <typename T, int V> static size_t smem_down_vv(int nst) {
     using D = DownBox<T, V>;
-    return 2 * (rup(kNH * D::DH * D::DW * sizeof(T)) + rup(D::DH * D::DW * sizeof(T))) +
+    return nst * (rup(D::DH * D::DW * sizeof(T)) +
+                  rup((kNH - 1) * (D::DH - 2) * D::DW * sizeof(T)) + rup(D::DH * D::DW * sizeof(T))) +
            rup(D::DH * D::DW * sizeof(T)) + rup(D::RH * D::RW * sizeof(T)) + 128;
 }
-template <typename T> size_t smem_up_v() {
-    return 2 * (rup(kNH * kBH * kBW * sizeof(T)) + rup(kBH * kBW * sizeof(T)) +
-                rup(kCBH * kCBW * sizeof(T))) +
+template <typename T> size_t smem_up_v(int nst) {
+    return nst * (rup(kBH * kBW * sizeof(T)) + rup((kNH - 1) * kPH * kBW * sizeof(T)) +
+                  rup(kBH * kBW * sizeof(T)) + rup(kCBH * kCBW * sizeof(T))) +
            rup(kBH * kBW * sizeof(T)) + 128;
 }
-template <typename T> size_t smem_down_v() { return smem_down_vv<T, kVSolve<T>>(); }
+template <typename T> size_t smem_down_v(int nst) { return smem_down_vv<T, kVSolve<T>>(nst); }
 template <typename T> int down_box_width() { return DownBox<T, kVSolve<T>>::DW; }
 
 // Raise the dynamic shared-memory limit of a kernel. Done once for every
@@ -2145,17 +2241,23 @@ void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUte
 }
 
 template <typename T>
-void launch_cg_apply(int vec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
-                     int zslot, T* p0, T* p1, T* Ap, InstState* st, double* part, int* err,
-                     cudaStream_t s) {
-    const size_t sm = smem_apply_v<T>();
+void launch_cg_apply(int vec, int stages, const LaunchCfg& L, const WorkList& wl,
+                     const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap, InstState* st,
+                     double* part, int* err, cudaStream_t s) {
+    const int ns = stages <= 1 ? 1 : 2;
+    const size_t sm = smem_apply_v<T>(ns);
     constexpr int V4 = kVWide<T>;
-    if (vec == 4 && V4 == 4)
-        k_cg_apply_v<T, V4><<<L.grid, tile_threads_v<V4>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, st,
-                                                                     part, err);
-    else
-        k_cg_apply_v<T, 2><<<L.grid, tile_threads_v<2>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, st,
-                                                                   part, err);
+#define PMB_CGA(VV, NS)                                                                       \
+    k_cg_apply_v<T, VV, NS><<<L.grid, tile_threads_v<VV>(), sm, s>>>(wl, maps, zslot, p0, p1, Ap, \
+                                                                     st, part, err)
+    if (vec == 4 && V4 == 4) {
+        if (ns == 1) PMB_CGA(V4, 1);
+        else PMB_CGA(V4, 2);
+    } else {
+        if (ns == 1) PMB_CGA(2, 1);
+        else PMB_CGA(2, 2);
+    }
+#undef PMB_CGA
 }
 
 template <typename T>
@@ -2176,14 +2278,18 @@ void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z
 }
 
 template <typename T>
-void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridDesc* fine,
-                    const CUtensorMap* maps, int xs_slot, T* bc, double omega,
-                    const InstState* st, int* err, cudaStream_t s) {
+void launch_vc_down(int pre, int stages, const LaunchCfg& L, const WorkList& wl,
+                    const GridDesc* fine, const CUtensorMap* maps, int xs_slot, T* bc,
+                    double omega, const InstState* st, int* err, cudaStream_t s) {
     const int pk = pre > 1 ? 2 : pre;
     if (pk == 1) {
         constexpr int V = kVSolve<T>;
-        k_vc_down_v<T, V><<<L.grid, kDownThreads, smem_down_v<T>(), s>>>(wl, fine, maps, bc, omega,
-                                                                          st, err);
+        if (stages == 1)
+            k_vc_down_v<T, V, 1><<<L.grid, kDownThreads, smem_down_v<T>(1), s>>>(
+                wl, fine, maps, bc, omega, st, err);
+        else
+            k_vc_down_v<T, V, 2><<<L.grid, kDownThreads, smem_down_v<T>(2), s>>>(
+                wl, fine, maps, bc, omega, st, err);
         return;
     }
     const size_t sm = smem_down<T>(pk);
@@ -2199,20 +2305,25 @@ void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridD
 }
 
 template <typename T>
-void launch_vc_up(int vec, int pre, int post, const LaunchCfg& L, const WorkList& wl, const GridDesc* coarse,
-                  const CUtensorMap* maps, int xs_slot, const T* b, T* xout, double omega,
-                  InstState* st, int level0, const T* dr, int reorth, double* part, int* err,
-                  cudaStream_t s) {
+void launch_vc_up(int vec, int stages, int pre, int post, const LaunchCfg& L, const WorkList& wl,
+                  const GridDesc* coarse, const CUtensorMap* maps, int xs_slot, const T* b,
+                  T* xout, double omega, InstState* st, int level0, const T* dr, int reorth,
+                  double* part, int* err, cudaStream_t s) {
     const int pk = pre > 1 ? 2 : pre;
     const int qk = post > 0 ? 1 : 0;
     if (pk == 1 && qk == 1) {
         constexpr int V4 = kVWide<T>;
-        if (vec == 4 && V4 == 4)
-            k_vc_up_v<T, V4><<<L.grid, tile_threads_v<V4>(), smem_up_v<T>(), s>>>(
-                wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err);
-        else
-            k_vc_up_v<T, 2><<<L.grid, tile_threads_v<2>(), smem_up_v<T>(), s>>>(
-                wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err);
+#define PMB_UPV(VV, NS)                                                                       \
+    k_vc_up_v<T, VV, NS><<<L.grid, tile_threads_v<VV>(), smem_up_v<T>(NS), s>>>(               \
+        wl, coarse, maps, b, xout, omega, st, level0, dr, reorth, part, err)
+        if (vec == 4 && V4 == 4) {
+            if (stages == 1) PMB_UPV(V4, 1);
+            else PMB_UPV(V4, 2);
+        } else {
+            if (stages == 1) PMB_UPV(2, 1);
+            else PMB_UPV(2, 2);
+        }
+#undef PMB_UPV
         return;
     }
     const size_t sm = smem_up<T>(pk);
@@ -2248,7 +2359,7 @@ void launch_vc_direct(const DirectDesc* dd, int count, const T* b, T* x, InstSta
 template <typename T>
 void launch_apply(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps, T* y, int* err,
                   cudaStream_t s) {
-    const size_t sm = smem_apply_v<T>();
+    const size_t sm = smem_apply_v<T>(2);
     constexpr int V = kVApply<T>;
     k_apply_v<T, V><<<L.grid, tile_threads_v<V>(), sm, s>>>(wl, maps, y, err);
 }
@@ -2343,13 +2454,18 @@ static void prepare_type() {
     allow_smem(k_vc_up<T, 2, 1>, smem_up<T>(2));
     allow_smem(k_vc_smooth<T>, smem_init<T>());
     allow_smem(k_apply<T>, smem_init<T>());
-    allow_smem(k_apply_v<T, kVApply<T>>, smem_apply_v<T>());
+    allow_smem(k_apply_v<T, kVApply<T>>, smem_apply_v<T>(2));
     allow_smem(k_vc_tail<T>, kTailSmem);
-    allow_smem(k_cg_apply_v<T, 2>, smem_apply_v<T>());
-    allow_smem(k_cg_apply_v<T, kVWide<T>>, smem_apply_v<T>());
-    allow_smem(k_vc_up_v<T, kVWide<T>>, smem_up_v<T>());
-    allow_smem(k_vc_down_v<T, kVSolve<T>>, smem_down_v<T>());
-    allow_smem(k_vc_up_v<T, kVSolve<T>>, smem_up_v<T>());
+    allow_smem(k_cg_apply_v<T, 2, 2>, smem_apply_v<T>(2));
+    allow_smem(k_cg_apply_v<T, 2, 1>, smem_apply_v<T>(1));
+    allow_smem(k_cg_apply_v<T, kVWide<T>, 2>, smem_apply_v<T>(2));
+    allow_smem(k_cg_apply_v<T, kVWide<T>, 1>, smem_apply_v<T>(1));
+    allow_smem(k_vc_up_v<T, kVWide<T>, 2>, smem_up_v<T>(2));
+    allow_smem(k_vc_up_v<T, kVWide<T>, 1>, smem_up_v<T>(1));
+    allow_smem(k_vc_down_v<T, kVSolve<T>, 2>, smem_down_v<T>(2));
+    allow_smem(k_vc_down_v<T, kVSolve<T>, 1>, smem_down_v<T>(1));
+    allow_smem(k_vc_up_v<T, kVSolve<T>, 2>, smem_up_v<T>(2));
+    allow_smem(k_vc_up_v<T, kVSolve<T>, 1>, smem_up_v<T>(1));
 }
 
 void stencil_prepare() {
@@ -2371,19 +2487,20 @@ void stencil_prepare() {
     template void launch_cg_init<T>(int, const LaunchCfg&, const WorkList&, const CUtensorMap*,   \
                                     const T*, const T*, T*, bool, T*, T*, InstState*, double*,    \
                                     double, double, int, int*, cudaStream_t);                     \
-    template void launch_cg_apply<T>(int, const LaunchCfg&, const WorkList&, const CUtensorMap*, int,  \
-                                     T*, T*, T*, InstState*, double*, int*, cudaStream_t);        \
+    template void launch_cg_apply<T>(int, int, const LaunchCfg&, const WorkList&,                 \
+                                     const CUtensorMap*, int, T*, T*, T*, InstState*, double*,    \
+                                     int*, cudaStream_t);                                         \
     template void launch_cg_update<T>(int, const LaunchCfg&, const WorkList&, const T*, T*, T*,   \
                                       T*, const T*, const T*, const T*, T*, int, int, int*,      \
                                       InstState*, double*, cudaStream_t);                        \
     template void launch_cg_rz<T>(const LaunchCfg&, const WorkList&, const T*, const T*,          \
                                   const T*, int, InstState*, double*, cudaStream_t);             \
-    template void launch_vc_down<T>(int, const LaunchCfg&, const WorkList&, const GridDesc*,      \
+    template void launch_vc_down<T>(int, int, const LaunchCfg&, const WorkList&, const GridDesc*, \
                                     const CUtensorMap*, int, T*, double, const InstState*, int*, \
                                     cudaStream_t);                                               \
-    template void launch_vc_up<T>(int, int, int, const LaunchCfg&, const WorkList&, const GridDesc*,   \
-                                  const CUtensorMap*, int, const T*, T*, double, InstState*, int, \
-                                  const T*, int, double*, int*, cudaStream_t);                   \
+    template void launch_vc_up<T>(int, int, int, int, const LaunchCfg&, const WorkList&,         \
+                                  const GridDesc*, const CUtensorMap*, int, const T*, T*, double, \
+                                  InstState*, int, const T*, int, double*, int*, cudaStream_t);  \
     template void launch_vc_smooth<T>(const LaunchCfg&, const WorkList&, const CUtensorMap*, int, \
                                       const T*, const T*, T*, double, const InstState*, int*,    \
                                       cudaStream_t);                                             \
@@ -2395,9 +2512,9 @@ void stencil_prepare() {
     template size_t smem_init<T>();                                                               \
     template size_t smem_down<T>(int);                                                            \
     template size_t smem_up<T>(int);                                                              \
-    template size_t smem_apply_v<T>();                                                            \
-    template size_t smem_down_v<T>();                                                             \
-    template size_t smem_up_v<T>();                                                               \
+    template size_t smem_apply_v<T>(int);                                                         \
+    template size_t smem_down_v<T>(int);                                                          \
+    template size_t smem_up_v<T>(int);                                                            \
     template int down_box_width<T>();
 
 PMB_INST(double)

@@ -53,9 +53,10 @@ template <typename T> size_t smem_init();
 template <typename T> size_t smem_down(int pre);
 template <typename T> size_t smem_up(int pre);
 // ... of the register-blocked kernels (default one pre- and one post-sweep).
-template <typename T> size_t smem_apply_v();
-template <typename T> size_t smem_down_v();
-template <typename T> size_t smem_up_v();
+template <typename T> size_t smem_apply_v(int nst);
+// nst: 2 buffers (a tile in flight while one is computed) or 1.
+template <typename T> size_t smem_down_v(int nst);
+template <typename T> size_t smem_up_v(int nst);
 // Width of the register-blocked restriction box (its TMA maps).
 template <typename T> int down_box_width();
 
@@ -71,9 +72,9 @@ void launch_cg_init(int prec, const LaunchCfg& L, const WorkList& wl, const CUte
                     const T* P, const T* b, T* x, bool have_x0, T* r, T* z, InstState* st,
                     double* part, double atol, double rtol, int maxiter, int* err, cudaStream_t s);
 template <typename T>
-void launch_cg_apply(int vec, const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
-                     int zslot, T* p0, T* p1, T* Ap, InstState* st, double* part, int* err,
-                     cudaStream_t s);
+void launch_cg_apply(int vec, int stages, const LaunchCfg& L, const WorkList& wl,
+                     const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap, InstState* st,
+                     double* part, int* err, cudaStream_t s);
 template <typename T>
 void launch_cg_update(int prec, const LaunchCfg& L, const WorkList& wl, const T* P, T* x, T* r,
                       T* z, const T* p0, const T* p1, const T* Ap, T* dr, int reorth, int reliable,
@@ -82,14 +83,14 @@ template <typename T>
 void launch_cg_rz(const LaunchCfg& L, const WorkList& wl, const T* r, const T* z, const T* dr,
                   int reorth, InstState* st, double* part, cudaStream_t s);
 template <typename T>
-void launch_vc_down(int pre, const LaunchCfg& L, const WorkList& wl, const GridDesc* fine,
-                    const CUtensorMap* maps, int xs_slot, T* bc, double omega,
-                    const InstState* st, int* err, cudaStream_t s);
+void launch_vc_down(int pre, int stages, const LaunchCfg& L, const WorkList& wl,
+                    const GridDesc* fine, const CUtensorMap* maps, int xs_slot, T* bc,
+                    double omega, const InstState* st, int* err, cudaStream_t s);
 template <typename T>
-void launch_vc_up(int vec, int pre, int post, const LaunchCfg& L, const WorkList& wl,
-                  const GridDesc* coarse, const CUtensorMap* maps, int xs_slot, const T* b, T* xout,
-                  double omega, InstState* st, int level0, const T* dr, int reorth, double* part,
-                  int* err, cudaStream_t s);
+void launch_vc_up(int vec, int stages, int pre, int post, const LaunchCfg& L, const WorkList& wl,
+                  const GridDesc* coarse, const CUtensorMap* maps, int xs_slot, const T* b,
+                  T* xout, double omega, InstState* st, int level0, const T* dr, int reorth,
+                  double* part, int* err, cudaStream_t s);
 template <typename T>
 void launch_vc_smooth(const LaunchCfg& L, const WorkList& wl, const CUtensorMap* maps,
                       int xin_slot, const T* P, const T* b, T* xout, double omega,

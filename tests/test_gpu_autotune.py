@@ -37,7 +37,8 @@ def test_every_setting_gives_the_same_solution(problem, precision):
     batch = AlphaBatch([img], [tri], precision=precision)
     ref = batch.solve().clone()
     for knobs in [{"vec_apply": 4, "vec_up": 4}, {"ctas_fine": 1, "ctas_up": 1, "ctas_down": 1},
-                  {"ctas_flat": 2, "chunk": 8}, {"chunk": 1, "ctas_fine": 3}]:
+                  {"ctas_flat": 2, "chunk": 8}, {"chunk": 1, "ctas_fine": 3},
+                  {"stages": 1}, {"stages": 1, "vec_up": 4, "ctas_up": 2}, {"stages": 2}]:
         autotune.apply_tuning(batch.system, knobs)
         x = batch.solve()
         assert batch.stats()[0].status == 1
