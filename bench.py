@@ -690,6 +690,9 @@ def main():
         times, info = [], None
         t_start = time.time()
         for _ in range(steps):
+            # Release the previous step's solver (its multi-GB workspace goes
+            # back to torch's cache) before the next one allocates its own.
+            info = None
             flush.fill_(1.0)
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -724,6 +727,7 @@ def main():
         for _ in range(args.warmup):
             device_step(precision)
         barrier()
+        results.pop(precision, None)
         times, info = timed(lambda: device_step(precision), args.steps)
         barrier()
         total_ms = max_over_ranks(sum(times))
