@@ -79,3 +79,21 @@ def test_solve_alpha_host_tensor_io(problems):
     for a, r in zip(out, ref):
         assert isinstance(a, torch.Tensor) and not a.is_cuda
         assert np.array_equal(a.numpy(), r)
+
+
+def test_sharded_solve_on_one_rank(problems):
+    """solve_alpha_sharded with one rank: the shard is the whole batch, the
+    gather returns every image in batch order, equal to solve_alpha's."""
+    import torch
+    from pymatting_b200 import solve_alpha, solve_alpha_sharded
+    from pymatting_b200.shard import STAT_FIELDS
+    imgs = [p[0] for p in problems]
+    tris = [p[1] for p in problems]
+    alphas, stats = solve_alpha_sharded(imgs, tris, 0, 1, torch.device("cuda", 0),
+                                        precision="fp64")
+    ref = solve_alpha(imgs, tris, precision="fp64")
+    assert len(alphas) == len(ref) and stats.shape == (len(ref), len(STAT_FIELDS))
+    for a, r, t in zip(alphas, ref, tris):
+        assert a.shape == t.shape
+        np.testing.assert_allclose(a.cpu().numpy(), r, rtol=0, atol=1e-12)
+    assert bool((stats[:, 1] == 1).all())
