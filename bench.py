@@ -573,6 +573,20 @@ KERNEL_ELEMS = {
 }
 
 
+def level0_traffic(kernel, npx):
+    """DRAM bytes per launch of a level-0 FP32 kernel on this workload: the
+    committed ncu capture's bytes scaled by level-0 pixels, or None."""
+    path = os.path.join(HERE, "profiles", "level0_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(kernel)
+    if not e:
+        return None
+    return float(e["dram_bytes"]) * npx / float(d["pixels"])
+
+
 def cpu_sample(imgs, tris, budget_s=15.0):
     """The oracle's solve (CPU restatement of the reference path, one core) of
     this rank's first images, in batch order, until about ``budget_s`` of
@@ -787,6 +801,7 @@ def main():
         e2e_value = npx_all * k / (e2e_ms * 1e-3) / 1e6
         km = kernels["mixed"]
         dom = max((n for n in KERNEL_ELEMS if n in km), key=lambda n: km[n]["ms"])
+        traffic = level0_traffic(dom, npx)
         line = {
             "metric": METRIC,
             "value": value,
@@ -826,7 +841,7 @@ def main():
             "roofline": dict({"bound": "hbm", "kernel": dom + " (FP32, level 0)",
                               "achieved": km[dom]["achieved_gbs"], "peak": peak,
                               "unit": "GB/s", "frac": km[dom]["frac"],
-                              "peak_source": peak_kind, "traffic": None,
+                              "peak_source": peak_kind, "traffic": traffic,
                               "bytes_per_launch": km[dom]["bytes"],
                               "bytes_formula": km[dom]["bytes_formula"]},
                              kernels=kernels),
