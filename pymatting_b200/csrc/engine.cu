@@ -235,6 +235,12 @@ static int blocks_per_sm(size_t smem) {
 
 constexpr int kMaxCtasPerSm = 16;   // bound of every list's per_sm (tile kernels: 4)
 
+// Grid of a launch over list L by a kernel whose CTAs use `smem` bytes of
+// dynamic shared memory (its own residency, not the list's).
+static int grid_for(const HostList& L, size_t smem) {
+    return std::max(1, std::min(L.wl.total, 148 * blocks_per_sm(smem)));
+}
+
 static int persistent_grid(const HostList& L) {
     return std::max(1, std::min(L.wl.total, 148 * std::min(L.per_sm, kMaxCtasPerSm)));
 }
@@ -342,14 +348,15 @@ static int plan_stencil(Stencil& S) {
     S.nmaps = map_base;
     // Work lists and the residency of the kernels that walk them.
     const bool vec_up = S.pre == 1 && S.post == 1, vec_down = S.pre == 1;
-    const int per_fine = blocks_per_sm(mixed ? smem_apply_v<float>(S.stages)
-                                             : smem_apply_v<double>(S.stages));
-    const int per_up = blocks_per_sm(
-        vec_up ? (mixed ? smem_up_v<float>(S.stages) : smem_up_v<double>(S.stages))
-               : (mixed ? smem_up<float>(S.pre) : smem_up<double>(S.pre)));
-    const int per_down = blocks_per_sm(
-        vec_down ? (mixed ? smem_down_v<float>(S.stages) : smem_down_v<double>(S.stages))
-                 : (mixed ? smem_down<float>(S.pre) : smem_down<double>(S.pre)));
+    const int per_fine = mixed ? resident_cg_apply<float>(S.vec_apply, S.stages)
+                               : resident_cg_apply<double>(S.vec_apply, S.stages);
+    const int per_up =
+        vec_up ? (mixed ? resident_up<float>(S.vec_up, S.stages)
+                        : resident_up<double>(S.vec_up, S.stages))
+               : blocks_per_sm(mixed ? smem_up<float>(S.pre) : smem_up<double>(S.pre));
+    const int per_down =
+        vec_down ? (mixed ? resident_down<float>(S.stages) : resident_down<double>(S.stages))
+                 : blocks_per_sm(mixed ? smem_down<float>(S.pre) : smem_down<double>(S.pre));
     S.max_fine = per_fine;
     S.max_up = per_up;
     S.max_down = per_down;
@@ -936,7 +943,8 @@ static void cg_iteration(Stencil& S, int reorth) {
         launch_refine_correct(LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl,
                               S.at<double>(S.o_x64), S.at<float>(S.o_xin32), st,
                               S.err() + kPendingSlot, s);
-        launch_refine_residual(S.precond, 0, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(),
+        launch_refine_residual(S.precond, 0, LaunchCfg{grid_for(a, smem_init<double>())}, a.wl,
+                               S.maps(),
                                S.at<float>(S.o_P032), S.at<double>(S.o_b64), S.at<float>(S.o_r32),
                                S.at<float>(S.o_xin32), S.at<float>(S.o_z32), S.outer(), st,
                                S.partials(), 0.0, 0.0, S.delta, 0, S.max_outer, S.err(), s);
@@ -1010,7 +1018,7 @@ static void start_fp64(Stencil& S, const double* x0, double atol, double rtol, i
     if (x0)
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), x0, v.p0,
                                     S.user_total, s);
-    launch_cg_init<double>(S.precond, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), v.P,
+    launch_cg_init<double>(S.precond, LaunchCfg{grid_for(a, smem_init<double>())}, a.wl, S.maps(), v.P,
                            S.at<double>(S.o_b64), v.x, x0 != nullptr, v.r, v.z, S.state(),
                            S.partials(), atol, rtol, maxiter, S.err(), s);
     S.launches += 1;
@@ -1048,7 +1056,7 @@ static int start_mixed(Stencil& S, const double* x0, double atol, double rtol, i
     }
     PMB_CUDA(cudaMemcpyAsync(S.outer(), init.data(), sizeof(InstState) * S.nimg,
                              cudaMemcpyHostToDevice, s));
-    launch_refine_residual(S.precond, 1, LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), v.P,
+    launch_refine_residual(S.precond, 1, LaunchCfg{grid_for(a, smem_init<double>())}, a.wl, S.maps(), v.P,
                            S.at<double>(S.o_b64), v.r, v.x, v.z, S.outer(), S.state(),
                            S.partials(), atol, rtol, inner_rtol, maxiter, max_outer, S.err(), s);
     S.launches += 1;
@@ -1528,7 +1536,7 @@ PMB_API int pmb_stencil_precondition(pmb_stencil* p, const double* r, double* z,
             run_vcycle<double>(S, v.r, v.z, nullptr, nullptr, 0);
         } else if (S.precond == kPrecJacobi) {
             // z = r / diag: the first Jacobi sweep from zero with omega = 1.
-            launch_vc_smooth<double>(LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), -1, S.P0, v.r,
+            launch_vc_smooth<double>(LaunchCfg{grid_for(a, smem_init<double>())}, a.wl, S.maps(), -1, S.P0, v.r,
                                      v.z, 1.0, nullptr, S.err(), s);
         } else {
             PMB_CUDA(cudaMemcpyAsync(v.z, v.r, sizeof(double) * S.levels[0].vec_elems,
@@ -1553,7 +1561,8 @@ PMB_API int pmb_stencil_apply(pmb_stencil* p, const double* x, double* y, void* 
         double* ty = S.at<double>(S.o_ap64);
         launch_pack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), x, tx,
                                     S.user_total, s);
-        launch_apply<double>(LaunchCfg{persistent_grid(a)}, a.wl, S.maps(), ty, S.err(), s);
+        launch_apply<double>(LaunchCfg{grid_for(a, smem_apply_v<double>(2))}, a.wl, S.maps(), ty,
+                             S.err(), s);
         launch_unpack<double, double>(a.wl.grids, a.wl.ngrids, S.at<int64_t>(S.o_uoff), ty, y,
                                       S.user_total, s);
         PMB_CUDA(cudaGetLastError());
@@ -1591,8 +1600,20 @@ PMB_API int pmb_stencil_tune(pmb_stencil* p, int knob, int value) {
     auto clampi = [](int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); };
     int applied;
     switch (knob) {
-    case 0: applied = S.vec_apply = (value >= 4 ? wide : 2); break;
-    case 1: applied = S.vec_up = (value >= 4 ? wide : 2); break;
+    case 0:
+        applied = S.vec_apply = (value >= 4 ? wide : 2);
+        S.max_fine = S.precision == 1 ? resident_cg_apply<float>(S.vec_apply, S.stages)
+                                      : resident_cg_apply<double>(S.vec_apply, S.stages);
+        S.fine0.per_sm = std::min(S.fine0.per_sm, S.max_fine);
+        break;
+    case 1:
+        applied = S.vec_up = (value >= 4 ? wide : 2);
+        if (S.pre == 1 && S.post == 1) {
+            S.max_up = S.precision == 1 ? resident_up<float>(S.vec_up, S.stages)
+                                        : resident_up<double>(S.vec_up, S.stages);
+            for (auto& lv : S.levels) lv.fine.per_sm = std::min(lv.fine.per_sm, S.max_up);
+        }
+        break;
     case 2:
         applied = clampi(value, 1, S.max_fine);
         S.fine0.per_sm = applied;
@@ -1616,15 +1637,17 @@ PMB_API int pmb_stencil_tune(pmb_stencil* p, int knob, int value) {
         // SM follow the shared memory of the choice.
         applied = S.stages = value <= 1 ? 1 : 2;
         const bool mixed = S.precision == 1;
-        S.max_fine = blocks_per_sm(mixed ? smem_apply_v<float>(S.stages)
-                                         : smem_apply_v<double>(S.stages));
+        S.max_fine = mixed ? resident_cg_apply<float>(S.vec_apply, S.stages)
+                           : resident_cg_apply<double>(S.vec_apply, S.stages);
         S.fine0.per_sm = S.max_fine;
-        S.max_up = blocks_per_sm(mixed ? smem_up_v<float>(S.stages) : smem_up_v<double>(S.stages));
-        S.max_down = blocks_per_sm(mixed ? smem_down_v<float>(S.stages)
-                                         : smem_down_v<double>(S.stages));
-        for (auto& lv : S.levels) {
-            lv.fine.per_sm = S.max_up;
-            lv.coarse.per_sm = S.max_down;
+        if (S.pre == 1 && S.post == 1) {
+            S.max_up = mixed ? resident_up<float>(S.vec_up, S.stages)
+                             : resident_up<double>(S.vec_up, S.stages);
+            S.max_down = mixed ? resident_down<float>(S.stages) : resident_down<double>(S.stages);
+            for (auto& lv : S.levels) {
+                lv.fine.per_sm = S.max_up;
+                lv.coarse.per_sm = S.max_down;
+            }
         }
         break;
     }
@@ -2387,7 +2410,8 @@ PMB_API int pmb_stencil_time_apply(pmb_stencil* p, int iters, double* ms, void* 
         PMB_CUDA(cudaEventCreate(&e0));
         PMB_CUDA(cudaEventCreate(&e1));
         HostList& a = S.fine0;
-        const LaunchCfg L{persistent_grid(a)};
+        const LaunchCfg L{grid_for(a, S.precision == 0 ? smem_apply_v<double>(2)
+                                                      : smem_apply_v<float>(2))};
         auto launch = [&]() {
             if (S.precision == 0)
                 launch_apply<double>(L, a.wl, S.maps(), S.at<double>(S.o_ap64), S.err(), S.stream);

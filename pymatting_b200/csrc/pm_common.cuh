@@ -47,7 +47,15 @@ constexpr int kCX = 32;
 constexpr int kCBW = 40;
 constexpr int kCBH = 8;
 
-template <typename T> struct Coarse { static constexpr int CY = 3; };
+#ifndef PMB_CY_FP32
+#define PMB_CY_FP32 3
+#endif
+#ifndef PMB_CY_FP64
+#define PMB_CY_FP64 3
+#endif
+template <typename T> struct Coarse {
+    static constexpr int CY = sizeof(T) == 4 ? PMB_CY_FP32 : PMB_CY_FP64;
+};
 
 // TMA descriptor slots of one grid (see engine.cu for what each maps).
 enum : int {

@@ -1838,7 +1838,6 @@ k_vc_up_v(WorkList wl /* fine tiles */, const GridDesc* coarse, const CUtensorMa
                     &pipe.bar[bb]);
     };
     auto body = [&](const Meta& m, const GridDesc& gf, int bb) {
-        const GridDesc gc = coarse[m.g];
         const int bx = m.x0 - kBOX, by = m.y0 - 2;
         const int cx0 = (m.x0 >> 1) - 4, cy0 = (m.y0 >> 1) - 2;
         const T* P = sP0[bb];
@@ -2468,6 +2467,48 @@ static void prepare_type() {
     allow_smem(k_vc_up_v<T, kVSolve<T>, 1>, smem_up_v<T>(1));
 }
 
+// Resident CTAs per SM of the register-blocked kernels as the occupancy
+// calculator gives them (registers, static and dynamic shared memory,
+// threads), at least 1. The shared-memory limits must be raised first
+// (stencil_prepare).
+template <typename K>
+static int occupancy_of(K kernel, int threads, size_t smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+template <typename T> int resident_cg_apply(int vec, int stages) {
+    stencil_prepare();
+    constexpr int V4 = kVWide<T>;
+    const int ns = stages <= 1 ? 1 : 2;
+    const size_t sm = smem_apply_v<T>(ns);
+    if (vec == 4 && V4 == 4)
+        return ns == 1 ? occupancy_of(k_cg_apply_v<T, V4, 1>, tile_threads_v<V4>(), sm)
+                       : occupancy_of(k_cg_apply_v<T, V4, 2>, tile_threads_v<V4>(), sm);
+    return ns == 1 ? occupancy_of(k_cg_apply_v<T, 2, 1>, tile_threads_v<2>(), sm)
+                   : occupancy_of(k_cg_apply_v<T, 2, 2>, tile_threads_v<2>(), sm);
+}
+template <typename T> int resident_down(int stages) {
+    stencil_prepare();
+    constexpr int V = kVSolve<T>;
+    return stages <= 1 ? occupancy_of(k_vc_down_v<T, V, 1>, kDownThreads, smem_down_v<T>(1))
+                       : occupancy_of(k_vc_down_v<T, V, 2>, kDownThreads, smem_down_v<T>(2));
+}
+template <typename T> int resident_up(int vec, int stages) {
+    stencil_prepare();
+    constexpr int V4 = kVWide<T>;
+    const int ns = stages <= 1 ? 1 : 2;
+    if (vec == 4 && V4 == 4)
+        return ns == 1 ? occupancy_of(k_vc_up_v<T, V4, 1>, tile_threads_v<V4>(), smem_up_v<T>(1))
+                       : occupancy_of(k_vc_up_v<T, V4, 2>, tile_threads_v<V4>(), smem_up_v<T>(2));
+    return ns == 1 ? occupancy_of(k_vc_up_v<T, 2, 1>, tile_threads_v<2>(), smem_up_v<T>(1))
+                   : occupancy_of(k_vc_up_v<T, 2, 2>, tile_threads_v<2>(), smem_up_v<T>(2));
+}
+
 void stencil_prepare() {
     static bool done = false;
     if (done) return;
@@ -2513,6 +2554,9 @@ void stencil_prepare() {
     template size_t smem_down<T>(int);                                                            \
     template size_t smem_up<T>(int);                                                              \
     template size_t smem_apply_v<T>(int);                                                         \
+    template int resident_cg_apply<T>(int, int);                                                  \
+    template int resident_down<T>(int);                                                           \
+    template int resident_up<T>(int, int);                                                        \
     template size_t smem_down_v<T>(int);                                                          \
     template size_t smem_up_v<T>(int);                                                            \
     template int down_box_width<T>();

@@ -57,6 +57,11 @@ template <typename T> size_t smem_apply_v(int nst);
 // nst: 2 buffers (a tile in flight while one is computed) or 1.
 template <typename T> size_t smem_down_v(int nst);
 template <typename T> size_t smem_up_v(int nst);
+// Resident CTAs per SM of the register-blocked CG apply, restriction and
+// prolongation kernels for a vector width and buffer count (occupancy API).
+template <typename T> int resident_cg_apply(int vec, int stages);
+template <typename T> int resident_down(int stages);
+template <typename T> int resident_up(int vec, int stages);
 // Width of the register-blocked restriction box (its TMA maps).
 template <typename T> int down_box_width();
 
