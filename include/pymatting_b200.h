@@ -286,9 +286,11 @@ int pmb_csr_add_diag_fill(int64_t n, const int64_t* indptr, const int64_t* indic
  * status instead of spinning, as the reference's solvers end with errors:
  * pymatting/solver/cg.py:115-117, pymatting/preconditioner/ichol.py:259-296).
  * which = 0: the mbarrier wait of the TMA kernels, limit in polls; which = 1:
- * the epoch poll of the foreground sweep, limit in nanoseconds. Each waits
- * on a barrier or word that nothing completes; *timed_out = 1 when the wait
- * gave up and reported it. scratch: 64 bytes of device memory. */
+ * the epoch poll of the foreground sweep, limit in nanoseconds; which = 2:
+ * the chunk wait of the streamed ichol solve, limit in polls (a solve whose
+ * wait gives up returns NaN). Each waits on a barrier or word that nothing
+ * completes; *timed_out = 1 when the wait gave up and reported it.
+ * scratch: 64 bytes of device memory. */
 int pmb_selftest_wait(int which, int64_t limit, void* scratch, int* timed_out, void* stream);
 
 /* Half-stencil planes (13 x h x pitch doubles, the stencil engine's layout)
@@ -406,6 +408,10 @@ int pmb_ichol_factor(pmb_ichol* f, const int64_t* Ap, const int64_t* Ar, const d
                      int64_t* result, void* stream);
 /* Dependency levels of the factor (length of the triangular-solve schedule). */
 int pmb_ichol_levels(const pmb_ichol* f);
+/* CTAs of the cluster that held the factorisation's band front in
+ * distributed shared memory in the last pmb_ichol_factor (1..8), 0 when the
+ * front was in global memory (bandwidth too wide), -1 before any factor. */
+int pmb_ichol_cluster(const pmb_ichol* f);
 /* Device pointers of the CSC factor (values, row indices, column pointers). */
 int pmb_ichol_factor_arrays(pmb_ichol* f, void** Lv, void** Lr, void** Lp);
 /* x = L^-T L^-1 b (CholeskyDecomposition.__call__, ichol.py:175-181). */

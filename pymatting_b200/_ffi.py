@@ -103,6 +103,7 @@ _SIGNATURES = {
     "pmb_ichol_factor": (c_int, [c_vp, c_vp, c_vp, c_vp, c_dbl, c_dbl, c_i64, c_dbl, c_int,
                                  ctypes.POINTER(c_i64), c_vp]),
     "pmb_ichol_levels": (c_int, [c_vp]),
+    "pmb_ichol_cluster": (c_int, [c_vp]),
     "pmb_ichol_factor_arrays": (c_int, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp),
                                         ctypes.POINTER(c_vp)]),
     "pmb_ichol_apply": (c_int, [c_vp, c_vp, c_vp, c_vp]),

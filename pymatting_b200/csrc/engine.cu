@@ -1707,6 +1707,11 @@ struct Ichol {
     char* ws = nullptr;
     int64_t nnz = -1;
     int nlevels = 0;
+    int cluster = -1;     // CTAs holding the front in the last factorisation (0: global memory)
+    // Streamed solves (n <= kStreamMaxRows): chunk blocks of both sweeps.
+    size_t o_blob = 0, o_prow = 0, o_pch = 0, blob_cap = 0;
+    int stream_total = 0;  // chunks of both sweeps; 0: level-barrier solves
+    StreamFirst first{};
     template <typename T> T* at(size_t off) const { return reinterpret_cast<T*>(ws + off); }
 };
 
@@ -1735,7 +1740,85 @@ static void plan_ichol(Ichol& I) {
     I.o_Rc = c.take<int64_t>(cap);
     I.o_Rv = c.take<double>(cap);
     I.o_scan = c.take<int64_t>((n + 2 + 1023) / 1024 + 4);
+    if (n <= kStreamMaxRows) {
+        // At most one chunk per row and sweep; entries of both sweeps are the
+        // factor's off-diagonal entries, padded to 4 per chunk.
+        I.blob_cap = (size_t)(200 * n + 24 * cap);
+        I.o_blob = c.take<unsigned char>((int64_t)I.blob_cap);
+        I.o_prow = c.take<StreamPackRow>(2 * n);
+        I.o_pch = c.take<StreamPackChunk>(2 * n);
+    }
     I.ws_bytes = c.off + 256;
+}
+
+// Chunk plan of the streamed solves (ichol.cu), built on the host from the
+// level schedule and the row / column pointers, then packed on the device.
+// Leaves stream_total = 0 (level-barrier solves) when a row has more entries
+// than a chunk holds.
+static int build_stream(Ichol& I, cudaStream_t s) {
+    I.stream_total = 0;
+    if (!I.o_blob) return 0;
+    const int64_t n = I.n;
+    const int nl = I.nlevels;
+    std::vector<int> order(n);
+    std::vector<int64_t> lptr(nl + 1), Rp(n + 1), Lp(n + 1);
+    PMB_CUDA(cudaMemcpyAsync(order.data(), I.ws + I.o_order, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    PMB_CUDA(cudaMemcpyAsync(lptr.data(), I.ws + I.o_lcnt, sizeof(int64_t) * (nl + 1),
+                             cudaMemcpyDeviceToHost, s));
+    PMB_CUDA(cudaMemcpyAsync(Rp.data(), I.ws + I.o_Rp, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+    PMB_CUDA(cudaMemcpyAsync(Lp.data(), I.ws + I.o_Lp, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+    PMB_CUDA(cudaStreamSynchronize(s));
+    std::vector<StreamPackRow> recs;
+    std::vector<StreamPackChunk> chunks;
+    recs.reserve(2 * n);
+    int64_t off = 0;
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        const bool bwd = sweep == 1;
+        for (int li = 0; li < nl; ++li) {
+            const int l = bwd ? nl - 1 - li : li;
+            int64_t q = lptr[l];
+            while (q < lptr[l + 1]) {
+                const size_t first_rec = recs.size();
+                int used = 0, rows = 0;
+                while (q < lptr[l + 1] && rows < kStreamRowsMax) {
+                    const int i = order[q];
+                    const int64_t src = bwd ? Lp[i] + 1 : Rp[i];
+                    const int64_t cnt = bwd ? Lp[i + 1] - Lp[i] - 1 : Rp[i + 1] - Rp[i];
+                    if (cnt > kStreamEntsMax) return 0;
+                    if (used + cnt > kStreamEntsMax) break;
+                    recs.push_back(StreamPackRow{off, src, i, rows, used, (int)cnt, 0, 0, bwd ? 1 : 0, 0});
+                    used += (int)cnt;
+                    ++rows;
+                    ++q;
+                }
+                const int ents = (used + 3) & ~3;
+                const int bytes = (int)(sizeof(StreamHead) + rows * sizeof(StreamRow)) + 12 * ents;
+                for (size_t k = first_rec; k < recs.size(); ++k) {
+                    recs[k].rows = rows;
+                    recs[k].ents = ents;
+                }
+                chunks.push_back(StreamPackChunk{off, bytes, rows, ents, used});
+                off += bytes;
+            }
+        }
+    }
+    if ((size_t)off > I.blob_cap || (int64_t)chunks.size() > 2 * n) return 0;
+    PMB_CUDA(cudaMemcpyAsync(I.ws + I.o_prow, recs.data(), sizeof(StreamPackRow) * recs.size(),
+                             cudaMemcpyHostToDevice, s));
+    PMB_CUDA(cudaMemcpyAsync(I.ws + I.o_pch, chunks.data(), sizeof(StreamPackChunk) * chunks.size(),
+                             cudaMemcpyHostToDevice, s));
+    ichol_launch_stream_pack((int)recs.size(), I.at<StreamPackRow>(I.o_prow), (int)chunks.size(),
+                             I.at<StreamPackChunk>(I.o_pch), I.at<int64_t>(I.o_Rc), I.at<double>(I.o_Rv),
+                             I.at<int64_t>(I.o_Lr), I.at<double>(I.o_Lv), I.at<int64_t>(I.o_Lp),
+                             I.at<unsigned char>(I.o_blob), s);
+    PMB_CUDA(cudaGetLastError());
+    PMB_CUDA(cudaStreamSynchronize(s));    // the host plan arrays are released on return
+    for (int q = 0; q < kStreamStages; ++q) {
+        I.first.off[q] = q < (int)chunks.size() ? chunks[q].off : 0;
+        I.first.bytes[q] = q < (int)chunks.size() ? chunks[q].bytes : 0;
+    }
+    I.stream_total = (int)chunks.size();
+    return 0;
 }
 
 // Row profile of a CSC matrix's lower part: bandwidth max(i - j) over
@@ -1831,7 +1914,7 @@ PMB_API int pmb_ichol_factor(pmb_ichol* p, const int64_t* Ap, const int64_t* Ar,
     PMB_CUDA(cudaMemsetAsync(I.ws + I.o_pat, 0, (size_t)(W * W), s));
     ichol_launch_init(n, Ap, Ar, Av, shift, I.at<double>(I.o_d), I.at<double>(I.o_rsum),
                       I.at<int>(I.o_level), I.at<unsigned long long>(I.o_band), s);
-    ichol_launch_factor(n, W, Ap, Ar, Av, I.at<double>(I.o_d), I.at<double>(I.o_rsum),
+    I.cluster = ichol_launch_factor(n, W, Ap, Ar, Av, I.at<double>(I.o_d), I.at<double>(I.o_rsum),
                         I.at<int>(I.o_level), I.at<double>(I.o_F), I.at<uint8_t>(I.o_pat),
                         I.at<int>(I.o_cand), I.at<double>(I.o_keptv), I.at<int64_t>(I.o_kepti),
                         I.at<int64_t>(I.o_Lp), I.at<int64_t>(I.o_Lr), I.at<double>(I.o_Lv), I.cap,
@@ -1872,10 +1955,12 @@ PMB_API int pmb_ichol_factor(pmb_ichol* p, const int64_t* Ap, const int64_t* Ar,
                           I.at<int64_t>(I.o_rfill), I.at<int64_t>(I.o_Rc), I.at<double>(I.o_Rv),
                           I.at<int64_t>(I.o_Rp), s);
     PMB_CUDA(cudaGetLastError());
-    return 0;
+    return build_stream(I, s);
 }
 
 PMB_API int pmb_ichol_levels(const pmb_ichol* p) { return p ? p->I.nlevels : -1; }
+
+PMB_API int pmb_ichol_cluster(const pmb_ichol* p) { return p ? p->I.cluster : -1; }
 
 PMB_API int pmb_ichol_factor_arrays(pmb_ichol* p, void** Lv, void** Lr, void** Lp) {
     if (!p || !p->I.ws || p->I.nnz < 0) return fail(kErrState, "pmb_ichol_factor_arrays: no factor");
@@ -1886,6 +1971,11 @@ PMB_API int pmb_ichol_factor_arrays(pmb_ichol* p, void** Lv, void** Lr, void** L
 }
 
 static int ichol_apply(Ichol& I, const double* b, double* x, const InstState* st, cudaStream_t s) {
+    if (I.stream_total > 0) {
+        ichol_launch_solve_stream(I.n, I.stream_total, I.first, I.at<unsigned char>(I.o_blob), b, x, st,
+                                  kStreamSpinLimit, s);
+        return 0;
+    }
     ichol_launch_solve(I.n, I.nlevels, I.at<int64_t>(I.o_lcnt), I.at<int>(I.o_order),
                        I.at<int64_t>(I.o_Lp), I.at<int64_t>(I.o_Lr), I.at<double>(I.o_Lv),
                        I.at<int64_t>(I.o_Rp), I.at<int64_t>(I.o_Rc), I.at<double>(I.o_Rv), b, x, st, s);
@@ -2254,16 +2344,33 @@ int pmb_launch_selftest_poll(void*, unsigned long long, int*, cudaStream_t);
 
 // Bounded-wait self-test: which = 0 runs the mbarrier wait of the TMA
 // kernels with a limit of `limit` polls, which = 1 the epoch poll of the
-// foreground sweep with a deadline of `limit` nanoseconds, each on a barrier
-// or word that nothing completes. *timed_out = 1 when the wait gave up and
-// reported it (every waiting thread, for the mbarrier). scratch: 64 bytes of
-// device memory.
+// foreground sweep with a deadline of `limit` nanoseconds, which = 2 the
+// chunk wait of the streamed ichol solve (`limit` polls) on a chunk whose
+// copy is never issued; each waits on a barrier or word that nothing
+// completes. *timed_out = 1 when the wait gave up and reported it (every
+// waiting thread, for the mbarrier; a NaN result, for the solve). scratch:
+// 64 bytes of device memory.
 PMB_API int pmb_selftest_wait(int which, int64_t limit, void* scratch, int* timed_out,
                               void* stream) {
-    if (!scratch || !timed_out || limit <= 0 || (which != 0 && which != 1))
+    if (!scratch || !timed_out || limit <= 0 || which < 0 || which > 2)
         return fail(kErrArg, "pmb_selftest_wait: bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
     *timed_out = 0;
+    if (which == 2) {
+        if (limit > 0x7fffffff) return fail(kErrArg, "pmb_selftest_wait: poll limit too large");
+        ichol_prepare();
+        double* v = static_cast<double*>(scratch);
+        PMB_CUDA(cudaMemsetAsync(v, 0, 8 * sizeof(double), s));
+        StreamFirst first{};    // one chunk, never fetched
+        ichol_launch_solve_stream(4, 1, first, static_cast<const unsigned char*>(scratch), v, v + 4,
+                                  nullptr, (uint32_t)limit, s);
+        PMB_CUDA(cudaGetLastError());
+        double h = 0.0;
+        PMB_CUDA(cudaMemcpyAsync(&h, v + 4, sizeof(double), cudaMemcpyDeviceToHost, s));
+        PMB_CUDA(cudaStreamSynchronize(s));
+        *timed_out = std::isnan(h) ? 1 : 0;
+        return 0;
+    }
     if (which == 1) {
         const int rc = pmb_launch_selftest_poll(scratch, (unsigned long long)limit, timed_out, s);
         if (rc) return fail(kErrCuda, std::string("poll self-test: ") +

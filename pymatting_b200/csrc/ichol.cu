@@ -25,8 +25,11 @@
 // rows subtract their terms in the reference's order, levels separated by
 // block barriers (single CTA: the systems this preconditioner is used on
 // are the compressed unknown regions, tens of thousands of rows).
+#include <cooperative_groups.h>
+
 #include "pm_common.cuh"
 #include "ichol.cuh"
+#include "tma.cuh"
 
 namespace pmb {
 
@@ -231,6 +234,324 @@ k_ichol_factor(int64_t n, int64_t W, const int64_t* __restrict__ Ap,
     if (threadIdx.x == 0) *result = s_fail ? (int64_t)s_fail : s_nnz;
 }
 
+// ---------------------------------------------------------------------------
+// The same factorisation with the front on chip: a cluster of C CTAs keeps the
+// W x W front in distributed shared memory, CTA r owning the contiguous slots
+// [r S, r S + S) (S = ceil(W / C)) with their FP64 values, pattern bytes, ring
+// entries of the diagonal d and of the dependency level. Per column j:
+//
+//   phase F  warp 0 of EVERY CTA reads slot j from its owner (one DSMEM round
+//            trip) and runs the serial part of the column (pivot, threshold,
+//            compaction) on identical data with identical instructions, so all
+//            CTAs hold the same kept list and take the same control path; the
+//            owner writes the column of L. Meanwhile the last warp recycles the
+//            slot of column j - 1 for column j - 1 + W from registers it loaded
+//            one column earlier (A's entries) and two columns earlier (A's
+//            column pointers), so no global load latency is on the chain.
+//   phase P  each CTA applies the pair updates F[ib][ia - ib] -= L_ia L_ib whose
+//            target column ib it owns, and the diagonal and level updates of
+//            the rows it owns: every write is CTA-local.
+//
+// One cluster barrier per column orders phase P of column j before phase F of
+// column j + 1 in every CTA. Updates land in the same order as in
+// k_ichol_factor (column order, one pair per front entry per column), so the
+// two kernels produce identical factors.
+// ---------------------------------------------------------------------------
+
+constexpr int kClThreads = 512;
+constexpr int kClMaxChunks = 14;      // offsets 1 .. W - 1 in chunks of 32: W <= 449
+constexpr int kClMaxCluster = 8;      // portable cluster size
+constexpr size_t kClSmemLimit = 227 * 1024 - 256;
+
+struct ClLayout {
+    int64_t Wp, S;
+    size_t o_F, o_d, o_kv, o_cL, o_lev, o_ki, o_ci, o_own, o_pat, bytes;
+};
+
+__host__ __device__ inline ClLayout cl_layout(int64_t W, int C) {
+    ClLayout L;
+    L.Wp = (W + 7) & ~(int64_t)7;
+    L.S = (W + C - 1) / C;
+    size_t o = 0;
+    L.o_F = o;   o += (size_t)(L.S * L.Wp) * sizeof(double);
+    L.o_d = o;   o += (size_t)L.S * sizeof(double);
+    L.o_kv = o;  o += (size_t)W * sizeof(double);
+    L.o_cL = o;  o += (size_t)W * sizeof(double);
+    L.o_lev = o; o += (size_t)L.S * sizeof(int);
+    L.o_ki = o;  o += (size_t)W * sizeof(int);
+    L.o_ci = o;  o += (size_t)W * sizeof(int);
+    L.o_own = o; o += (size_t)W * sizeof(int);
+    L.o_pat = o; o += (size_t)(L.S * L.Wp);
+    L.bytes = (o + 15) & ~(size_t)15;
+    return L;
+}
+
+// Smallest cluster size whose per-CTA share of the front fits in shared
+// memory; 0 when none up to the portable limit does (or W is too wide for
+// the register chunks of phase F).
+int ichol_cluster_size(int64_t W) {
+    if (W < 1 || W - 1 > 32 * kClMaxChunks) return 0;
+    for (int C = 1; C <= kClMaxCluster; ++C)
+        if (cl_layout(W, C).bytes <= kClSmemLimit) return C;
+    return 0;
+}
+
+// NCH: 32-offset chunks of a front column held in registers by phase F
+// (ceil((W - 1) / 32) rounded up to 2, 4, 8 or 14). Slots are tracked
+// incrementally in 32-bit arithmetic; phase F computes every chunk's
+// quotient and keep decision before the ballots so the divisions overlap.
+template <int NCH>
+__global__ void __launch_bounds__(kClThreads, 1)
+k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
+                       const int64_t* __restrict__ Ar, const double* __restrict__ Av,
+                       const double* __restrict__ d0, const double* __restrict__ rsum,
+                       int* level, int64_t* Lp, int64_t* Lr, double* Lv, int64_t cap,
+                       double discard, int64_t max_nnz, double rel_discard, int diag_keep,
+                       int64_t* result) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char cl_smem[];
+    __shared__ int64_t s_nnz;
+    __shared__ int s_m, s_cn, s_nown, s_levj, s_fail;
+    const ClLayout Ly = cl_layout(W, C);
+    const int S = (int)Ly.S, Wp = (int)Ly.Wp;
+    double* F = reinterpret_cast<double*>(cl_smem + Ly.o_F);
+    double* dl = reinterpret_cast<double*>(cl_smem + Ly.o_d);
+    double* kv = reinterpret_cast<double*>(cl_smem + Ly.o_kv);
+    double* cL = reinterpret_cast<double*>(cl_smem + Ly.o_cL);
+    int* lev = reinterpret_cast<int*>(cl_smem + Ly.o_lev);
+    int* ki = reinterpret_cast<int*>(cl_smem + Ly.o_ki);
+    int* ci = reinterpret_cast<int*>(cl_smem + Ly.o_ci);
+    int* own = reinterpret_cast<int*>(cl_smem + Ly.o_own);
+    uint8_t* pat = cl_smem + Ly.o_pat;
+    const int r = (int)cluster.block_rank();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int lo = r * S, hi = min(lo + S, W);             // slots owned here: [lo, hi)
+
+    // Initial front: columns 0 .. min(W, n) - 1 sit in slots 0 .. W - 1.
+    for (int q = threadIdx.x; q < S * Wp; q += blockDim.x) {
+        F[q] = 0.0;
+        pat[q] = 0;
+    }
+    __syncthreads();
+    for (int ls = warp; lo + ls < hi; ls += nw) {
+        const int64_t c = lo + ls;
+        if (c >= n) continue;
+        for (int64_t k = Ap[c] + lane; k < Ap[c + 1]; k += 32) {
+            const int64_t i = Ar[k];
+            const double v = Av[k];
+            if (i > c && v != 0.0) {
+                F[ls * Wp + (int)(i - c)] = v;
+                pat[ls * Wp + (int)(i - c)] = 1;
+            }
+        }
+        if (lane == 0) {
+            dl[ls] = d0[c];
+            lev[ls] = 0;
+        }
+    }
+    if (threadIdx.x == 0) {
+        s_nnz = 0;
+        s_fail = 0;
+        if (r == 0) Lp[0] = 0;
+    }
+    cluster.sync();
+
+    // Last warp: A's column pointers of column j + W (loaded a column ahead)
+    // and entries of column j - 1 + W (loaded at the previous column).
+    int64_t pk0 = 0, pk1 = 0, ebeg = 0, eend = 0;
+    int64_t ei[2] = {-1, -1};
+    double ev[2] = {0.0, 0.0}, ed0 = 0.0;
+    if (warp == nw - 1 && W < n) {
+        pk0 = Ap[W];
+        pk1 = Ap[W + 1];
+    }
+    double rs_next = (warp == 0) ? rsum[0] : 0.0;
+    int slot = 0, pslot = W - 1;      // j % W and (j - 1) % W
+
+    for (int64_t j = 0; j < n; ++j) {
+        if (warp == 0) {
+            const int f = slot / S, lsj = slot - f * S;
+            const double rs = rs_next;
+            if (j + 1 < n) rs_next = rsum[j + 1];
+            const double* Fj = cluster.map_shared_rank(F, f) + lsj * Wp;
+            const uint8_t* Pj = cluster.map_shared_rank(pat, f) + lsj * Wp;
+            const double dj = cluster.map_shared_rank(dl, f)[lsj];
+            const int levj = cluster.map_shared_rank(lev, f)[lsj];
+            // Offsets o = 1 + lane + 32 k: lane order is ascending rows, the
+            // order in which the reference sorts its candidates (ichol.py:87-89).
+            double a[NCH];
+            bool flag[NCH];
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) {
+                const int o = 1 + lane + 32 * k;
+                const bool in = o < W && j + o < n;
+                a[k] = in ? Fj[o] : 0.0;
+                flag[k] = in && Pj[o] != 0;
+            }
+            unsigned fm[NCH];
+            int cn = 0;
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) {
+                fm[k] = __ballot_sync(0xffffffffu, flag[k]);
+                cn += __popc(fm[k]);
+            }
+            const int64_t nnz = s_nnz;
+            int fail = 0;
+            if (!(dj > 0.0)) fail = -1;                                         // ichol.py:80-81
+            else if (nnz + 1 + cn > max_nnz || nnz + 1 + cn > cap) fail = -2;   // ichol.py:82-83
+            const bool owner = f == r;
+            const int64_t nnz0 = nnz + 1;
+            int kept = 0, nown = 0;
+            if (!fail) {
+                const double sj = sqrt(dj);
+                const double rel = rel_discard * rs;
+                if (owner && lane == 0) {
+                    Lv[nnz] = sj;
+                    Lr[nnz] = j;
+                    level[j] = levj;
+                }
+                bool keep[NCH], mine[NCH];
+#pragma unroll
+                for (int k = 0; k < NCH; ++k) {
+                    // Lanes without a candidate divide 1.0: a zero numerator
+                    // would take the division's slow path on every lane.
+                    const double q = (flag[k] ? a[k] : 1.0) / sj;
+                    const double L = flag[k] ? q : 0.0;
+                    keep[k] = flag[k] && fabs(L) > discard && fabs(a[k]) > rel;
+                    a[k] = L;
+                    int sl = slot + 1 + lane + 32 * k;
+                    if (sl >= W) sl -= W;
+                    mine[k] = keep[k] && sl >= lo && sl < hi;
+                }
+                int cpos = 0;
+#pragma unroll
+                for (int k = 0; k < NCH; ++k) {
+                    const int o = 1 + lane + 32 * k;
+                    const unsigned km = __ballot_sync(0xffffffffu, keep[k]);
+                    const unsigned om = __ballot_sync(0xffffffffu, mine[k]);
+                    if (flag[k]) {
+                        const int q = cpos + __popc(fm[k] & lt);
+                        cL[q] = a[k];
+                        ci[q] = keep[k] ? o : -o;
+                    }
+                    if (keep[k]) {
+                        const int pos = kept + __popc(km & lt);
+                        kv[pos] = a[k];
+                        ki[pos] = o;
+                        if (owner) {
+                            Lv[nnz0 + pos] = a[k];
+                            Lr[nnz0 + pos] = j + o;
+                        }
+                        if (mine[k]) own[nown + __popc(om & lt)] = pos;
+                    }
+                    cpos += __popc(fm[k]);
+                    kept += __popc(km);
+                    nown += __popc(om);
+                }
+            }
+            if (lane == 0) {
+                s_fail = fail;
+                if (!fail) {
+                    s_m = kept;
+                    s_cn = cn;
+                    s_nown = nown;
+                    s_levj = levj;
+                    s_nnz = nnz0 + kept;
+                    if (owner) Lp[j + 1] = nnz0 + kept;
+                }
+            }
+        } else if (warp == nw - 1) {
+            // Recycle slot (j - 1) % W for column c = j - 1 + W (its readers
+            // all passed the barrier of column j - 1).
+            const int64_t c = j - 1 + W;
+            if (j >= 1 && c < n && pslot >= lo && pslot < hi) {
+                double* Fc = F + (pslot - lo) * Wp;
+                uint8_t* Pc = pat + (pslot - lo) * Wp;
+                for (int o = lane; o < W; o += 32) {
+                    Fc[o] = 0.0;
+                    Pc[o] = 0;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int64_t k = ebeg + lane + 32 * e;
+                    if (k < eend && ei[e] > c && ev[e] != 0.0) {
+                        Fc[ei[e] - c] = ev[e];
+                        Pc[ei[e] - c] = 1;
+                    }
+                }
+                for (int64_t k = ebeg + 64 + lane; k < eend; k += 32) {   // rows longer than 64
+                    const int64_t i = Ar[k];
+                    const double v = Av[k];
+                    if (i > c && v != 0.0) {
+                        Fc[i - c] = v;
+                        Pc[i - c] = 1;
+                    }
+                }
+                if (lane == 0) {
+                    dl[pslot - lo] = ed0;
+                    lev[pslot - lo] = 0;
+                }
+            }
+            // Entries of column j + W for the next column's recycle.
+            if (j + W < n) {
+                ebeg = pk0;
+                eend = pk1;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int64_t k = pk0 + lane + 32 * e;
+                    ei[e] = k < pk1 ? Ar[k] : -1;
+                    ev[e] = k < pk1 ? Av[k] : 0.0;
+                }
+                ed0 = d0[j + W];
+            }
+            // Column pointers of column j + 1 + W.
+            if (j + 1 + W < n) {
+                pk0 = Ap[j + 1 + W];
+                pk1 = Ap[j + 2 + W];
+            }
+        }
+        __syncthreads();
+        if (s_fail) break;
+        // Phase P: CTA-local updates of the rows and front columns owned here.
+        const int m = s_m, nown = s_nown, cn = s_cn, lj = s_levj + 1;
+        for (int t = warp; t < nown; t += nw) {
+            const int pb = own[t];
+            const int ob = ki[pb];
+            int sl = slot + ob;
+            if (sl >= W) sl -= W;
+            double* Fb = F + (sl - lo) * Wp;
+            uint8_t* Pb = pat + (sl - lo) * Wp;
+            const double Lb = kv[pb];
+            for (int q = pb + 1 + lane; q < m; q += 32) {
+                const int o = ki[q] - ob;
+                Fb[o] -= kv[q] * Lb;
+                Pb[o] = 1;
+            }
+        }
+        for (int q = threadIdx.x; q < cn; q += blockDim.x) {
+            const int code = ci[q];
+            int sl = slot + (code < 0 ? -code : code);
+            if (sl >= W) sl -= W;
+            if (sl < lo || sl >= hi || (!diag_keep && code < 0)) continue;
+            dl[sl - lo] -= cL[q] * cL[q];
+        }
+        for (int t = threadIdx.x; t < nown; t += blockDim.x) {
+            int sl = slot + ki[own[t]];
+            if (sl >= W) sl -= W;
+            if (lev[sl - lo] < lj) lev[sl - lo] = lj;
+        }
+        pslot = slot;
+        slot = slot + 1 == W ? 0 : slot + 1;
+        cluster.sync();
+    }
+    // No CTA leaves while another may still read its shared memory.
+    cluster.sync();
+    if (r == 0 && threadIdx.x == 0) *result = s_fail ? (int64_t)s_fail : s_nnz;
+}
+
 // Level histogram / order of rows, and the row (CSR) view of L used by the
 // forward solve. All small single-purpose kernels.
 __global__ void k_level_count(int64_t n, const int* __restrict__ level, int64_t* cnt,
@@ -423,6 +744,183 @@ k_ichol_solve_smem(int64_t n, int nlevels, const int64_t* __restrict__ lptr,
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = s_x[i];
 }
 
+// ---------------------------------------------------------------------------
+// Streamed level-scheduled solves (n <= kStreamMaxRows). Both sweeps run in
+// one CTA with x in shared memory. The rows of each sweep, in level order,
+// are packed at factorisation time into chunks (one level, or a part of a
+// level, of at most kStreamRowsMax rows and kStreamEntsMax entries), each a
+// contiguous 16-byte-aligned block:
+//
+//   StreamHead   own row and entry counts, and the offset / size of the
+//                block kStreamStages chunks later (the next one to fetch
+//                into this stage)
+//   StreamRow[rows]   row index, first entry, entry count, diagonal
+//   double[ents]      L values of the row terms
+//   int[ents]         their x indices       (ents padded to a multiple of 4)
+//
+// One thread keeps kStreamStages chunks in flight with bulk copies into a
+// shared-memory ring (completion on one mbarrier per stage); every chunk
+// ends with the block barrier that separates levels and frees the stage.
+// The data of a chunk never depends on x, so the copies run ahead of the
+// dependency chain and no global-load latency sits on it. Within a row the
+// terms are summed lane-strided and reduced across the warp, as in
+// k_ichol_solve_smem, and x_i = (x_i - sum) / L_ii as the reference's
+// back substitutions (ichol.py:116-145).
+// ---------------------------------------------------------------------------
+
+constexpr int kStreamThreads = 256;
+constexpr size_t kStreamStageBytes =
+    sizeof(StreamHead) + kStreamRowsMax * sizeof(StreamRow) + kStreamEntsMax * 12;
+static_assert(kStreamStageBytes % 16 == 0, "stages are 16-byte aligned");
+
+size_t ichol_stream_smem(int64_t n) {
+    return kStreamStages * kStreamStageBytes + (size_t)n * sizeof(double);
+}
+
+__global__ void __launch_bounds__(kStreamThreads)
+k_ichol_solve_stream(int64_t n, int total, StreamFirst first, const unsigned char* __restrict__ blob,
+                     const double* __restrict__ b, double* x, const InstState* st, uint32_t limit) {
+    extern __shared__ __align__(16) unsigned char ss_smem[];
+    __shared__ uint64_t full[kStreamStages];
+    __shared__ int s_bad;
+    if (st && st->status != kRunning) return;
+    double* sx = reinterpret_cast<double*>(ss_smem + kStreamStages * kStreamStageBytes);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        s_bad = 0;
+        for (int q = 0; q < kStreamStages; ++q) mbar_init(&full[q], 1);
+        for (int q = 0; q < kStreamStages && q < total; ++q) {
+            if (first.bytes[q] <= 0) continue;
+            mbar_expect_tx(&full[q], (uint32_t)first.bytes[q]);
+            bulk_load(ss_smem + q * kStreamStageBytes, blob + first.off[q], (uint32_t)first.bytes[q],
+                      &full[q]);
+        }
+    }
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) sx[i] = b[i];
+    __syncthreads();
+    int c = 0;
+    for (; c < total; ++c) {
+        const int q = c % kStreamStages;
+        unsigned char* stage = ss_smem + q * kStreamStageBytes;
+        if (!mbar_wait(&full[q], (uint32_t)(c / kStreamStages) & 1u, limit)) {
+            s_bad = 1;
+        } else {
+            const StreamHead* h = reinterpret_cast<const StreamHead*>(stage);
+            const StreamRow* rec = reinterpret_cast<const StreamRow*>(stage + sizeof(StreamHead));
+            const int rows = h->rows, ents = h->ents;
+            const double* val = reinterpret_cast<const double*>(stage + sizeof(StreamHead) +
+                                                                rows * sizeof(StreamRow));
+            const int* col = reinterpret_cast<const int*>(val + ents);
+            for (int k = warp; k < rows; k += nw) {
+                const StreamRow rw = rec[k];
+                double acc = 0.0;
+                for (int e = lane; e < rw.count; e += 32)
+                    acc += val[rw.start + e] * sx[col[rw.start + e]];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (lane == 0) sx[rw.row] = (sx[rw.row] - acc) / rw.diag;
+            }
+        }
+        __syncthreads();          // level barrier; the stage is free again
+        if (s_bad) break;
+        // The last warp refills the stage: rows go to warps in order, so it
+        // only has rows of its own in chunks of more than nw - 1 rows.
+        if (threadIdx.x == blockDim.x - 32) {
+            const StreamHead* h = reinterpret_cast<const StreamHead*>(stage);
+            const int64_t off = h->next_off;
+            const int bytes = h->next_bytes;
+            if (bytes > 0) {
+                fence_proxy_async();
+                mbar_expect_tx(&full[q], (uint32_t)bytes);
+                bulk_load(stage, blob + off, (uint32_t)bytes, &full[q]);
+            }
+        }
+    }
+    if (s_bad) {
+        // A copy did not complete: the result is NaN, and copies still in
+        // flight are waited for (bounded) before the CTA leaves.
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = __longlong_as_double(0x7ff8000000000000ll);
+        if (threadIdx.x == blockDim.x - 32) {
+            for (int k = c; k < c + kStreamStages && k < total; ++k)
+                mbar_wait(&full[k % kStreamStages], (uint32_t)(k / kStreamStages) & 1u, limit);
+        }
+        __syncthreads();
+        return;
+    }
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = sx[i];
+}
+
+// Pack the chunk blocks of both sweeps. One warp per row record: its entries
+// (x indices narrowed to int) and its record; one thread per chunk writes the
+// head and zeroes the entry padding.
+__global__ void k_stream_pack_rows(int nrec, const StreamPackRow* __restrict__ recs,
+                                   const int64_t* __restrict__ Rc, const double* __restrict__ Rv,
+                                   const int64_t* __restrict__ Lr, const double* __restrict__ Lv,
+                                   const int64_t* __restrict__ Lp, unsigned char* blob) {
+    const int w = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= nrec) return;
+    const StreamPackRow R = recs[w];
+    unsigned char* chunk = blob + R.chunk_off;
+    StreamRow* rec = reinterpret_cast<StreamRow*>(chunk + sizeof(StreamHead)) + R.slot;
+    double* val = reinterpret_cast<double*>(chunk + sizeof(StreamHead) + R.rows * sizeof(StreamRow));
+    int* col = reinterpret_cast<int*>(val + R.ents);
+    const int64_t* ci = R.backward ? Lr : Rc;
+    const double* cv = R.backward ? Lv : Rv;
+    for (int e = lane; e < R.count; e += 32) {
+        val[R.start + e] = cv[R.src + e];
+        col[R.start + e] = (int)ci[R.src + e];
+    }
+    if (lane == 0) {
+        StreamRow rw;
+        rw.row = R.row;
+        rw.start = R.start;
+        rw.count = R.count;
+        rw.pad = 0;
+        rw.diag = Lv[Lp[R.row]];
+        rw.pad2 = 0.0;
+        *rec = rw;
+    }
+}
+
+__global__ void k_stream_pack_heads(int nchunks, const StreamPackChunk* __restrict__ ch,
+                                    unsigned char* blob) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    const StreamPackChunk C = ch[c];
+    StreamHead h;
+    h.next_off = c + kStreamStages < nchunks ? ch[c + kStreamStages].off : 0;
+    h.next_bytes = c + kStreamStages < nchunks ? ch[c + kStreamStages].bytes : 0;
+    h.rows = C.rows;
+    h.ents = C.ents;
+    h.pad[0] = h.pad[1] = h.pad[2] = 0;
+    *reinterpret_cast<StreamHead*>(blob + C.off) = h;
+    double* val = reinterpret_cast<double*>(blob + C.off + sizeof(StreamHead) + C.rows * sizeof(StreamRow));
+    int* col = reinterpret_cast<int*>(val + C.ents);
+    for (int e = C.used; e < C.ents; ++e) {
+        val[e] = 0.0;
+        col[e] = 0;
+    }
+}
+
+void ichol_launch_stream_pack(int nrec, const StreamPackRow* recs, int nchunks,
+                              const StreamPackChunk* chunks, const int64_t* Rc, const double* Rv,
+                              const int64_t* Lr, const double* Lv, const int64_t* Lp,
+                              unsigned char* blob, cudaStream_t s) {
+    if (nrec > 0)
+        k_stream_pack_rows<<<(unsigned)((nrec * 32 + 255) / 256), 256, 0, s>>>(nrec, recs, Rc, Rv, Lr,
+                                                                               Lv, Lp, blob);
+    if (nchunks > 0)
+        k_stream_pack_heads<<<(unsigned)((nchunks + 127) / 128), 128, 0, s>>>(nchunks, chunks, blob);
+}
+
+void ichol_launch_solve_stream(int64_t n, int total, const StreamFirst& first,
+                               const unsigned char* blob, const double* b, double* x,
+                               const InstState* st, uint32_t limit, cudaStream_t s) {
+    k_ichol_solve_stream<<<1, kStreamThreads, ichol_stream_smem(n), s>>>(n, total, first, blob, b, x,
+                                                                         st, limit);
+}
+
 // The forward sweep above overwrites x in place: y lives in x. For the
 // forward pass to read y_j of earlier levels and b_i of its own row, b and
 // x may alias (the reference also works in place on a copy of b).
@@ -433,14 +931,46 @@ void ichol_launch_init(int64_t n, const int64_t* Ap, const int64_t* Ar, const do
     if (n > 0) k_ichol_init<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Ap, Ar, Av, shift, d, rsum, level, band);
 }
 
-void ichol_launch_factor(int64_t n, int64_t W, const int64_t* Ap, const int64_t* Ar,
-                         const double* Av, double* d, const double* rsum, int* level, double* F,
-                         uint8_t* pat, int* cand, double* keptv, int64_t* kepti, int64_t* Lp,
-                         int64_t* Lr, double* Lv, int64_t cap, double discard, int64_t max_nnz,
-                         double rel, int diag_keep, int64_t* result, cudaStream_t s) {
+int ichol_launch_factor(int64_t n, int64_t W, const int64_t* Ap, const int64_t* Ar,
+                        const double* Av, double* d, const double* rsum, int* level, double* F,
+                        uint8_t* pat, int* cand, double* keptv, int64_t* kepti, int64_t* Lp,
+                        int64_t* Lr, double* Lv, int64_t cap, double discard, int64_t max_nnz,
+                        double rel, int diag_keep, int64_t* result, cudaStream_t s) {
+    // Front on chip when a cluster of at most 8 CTAs holds it and such a
+    // cluster can be resident; otherwise the front lives in global memory.
+    const int C = ichol_cluster_size(W);
+    if (C > 0) {
+        const ClLayout L = cl_layout(W, C);
+        const int chunks = (int)((W - 1 + 31) / 32);
+        auto kern = chunks <= 2 ? k_ichol_factor_cluster<2>
+                  : chunks <= 4 ? k_ichol_factor_cluster<4>
+                  : chunks <= 8 ? k_ichol_factor_cluster<8> : k_ichol_factor_cluster<kClMaxChunks>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)C);
+        cfg.blockDim = dim3(kClThreads);
+        cfg.dynamicSmemBytes = L.bytes;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)C;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) == cudaSuccess && clusters >= 1) {
+            if (cudaLaunchKernelEx(&cfg, kern, n, (int)W, C, Ap, Ar, Av, (const double*)d, rsum,
+                                   level, Lp, Lr, Lv, cap, discard, max_nnz, rel, diag_keep,
+                                   result) == cudaSuccess)
+                return C;
+        }
+        cudaGetLastError();
+    }
     k_ichol_factor<<<1, kIcholThreads, 0, s>>>(n, W, Ap, Ar, Av, d, rsum, level, F, pat, cand, keptv,
                                                kepti, Lp, Lr, Lv, cap, discard, max_nnz, rel,
                                                diag_keep, result);
+    return 0;
 }
 
 void ichol_launch_levels(int64_t n, const int* level, int64_t* cnt, int* maxlevel, cudaStream_t s) {
@@ -472,6 +1002,8 @@ void ichol_launch_row_fill(int64_t n, const int64_t* Lp, const int64_t* Lr, cons
 void ichol_prepare() {
     cudaFuncSetAttribute(k_ichol_solve_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(kIcholSmemRows * sizeof(double)));
+    cudaFuncSetAttribute(k_ichol_solve_stream, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)ichol_stream_smem(kStreamMaxRows));
 }
 
 void ichol_launch_solve(int64_t n, int nlevels, const int64_t* lptr, const int* order,

@@ -266,6 +266,11 @@ class IcholFactor:
     def levels(self):
         return int(_ffi.lib().pmb_ichol_levels(self._h))
 
+    def cluster(self):
+        """CTAs that held the band front on chip in the last factorisation
+        (0: the front was in global memory)."""
+        return int(_ffi.lib().pmb_ichol_cluster(self._h))
+
     def apply(self, b):
         x = dev.empty(self.n, torch.float64)
         _ffi.check(_ffi.lib().pmb_ichol_apply(self._h, dev.ptr(b), dev.ptr(x), dev.stream()),

@@ -61,11 +61,29 @@ def test_foreground_epoch_poll_gives_up(lib):
     _normal_calls_still_work()
 
 
+@pytest.mark.parametrize("polls", [1, 1000])
+def test_ichol_stream_wait_gives_up(lib, polls):
+    """The streamed ichol solve's chunk wait (limit in polls; the solve uses
+    2^24): a chunk whose copy is never issued makes it give up, the result is
+    NaN, and an ichol factor and solve on the same context still match the
+    oracle."""
+    import scipy.sparse
+    import pymatting_b200 as pm
+    assert _selftest(lib, 2, polls) == 1
+    _normal_calls_still_work()
+    g = np.random.default_rng(5)
+    n = 300
+    B = scipy.sparse.random(n, n, density=0.02, random_state=5) + scipy.sparse.eye(n) * 4.0
+    A = scipy.sparse.csc_matrix(B @ B.T)
+    rhs = g.standard_normal(n)
+    np.testing.assert_allclose(pm.ichol(A)(rhs), oracle.ichol(A)(rhs), rtol=1e-9, atol=1e-12)
+
+
 def test_selftest_rejects_bad_arguments(lib):
     import torch
     scratch = torch.empty(64, dtype=torch.uint8, device="cuda")
     out = ctypes.c_int()
-    assert lib.pmb_selftest_wait(2, 10, ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(out),
+    assert lib.pmb_selftest_wait(3, 10, ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(out),
                                  None) == -1
     assert lib.pmb_selftest_wait(0, 0, ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(out),
                                  None) == -1
