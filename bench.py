@@ -21,7 +21,9 @@ image per step, spread over the host cores by a process pool.
 
 Other workloads: ``1080p`` (one 1920x1080 image per GPU), ``4096`` (one
 4096x4096 image), ``foreground`` (estimate_foreground_ml on a 1920x1080
-image and matte).
+image and matte), ``hard320`` (estimate_alpha_cf with hard constraints and
+the default ichol preconditioner on a 320x240 image: the reference's
+CPU-runnable configuration).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: with --gpus N > 1 and no torch.distributed environment, bench.py
@@ -56,11 +58,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch64", "1080p", "4096", "foreground"],
+    ap.add_argument("--workload", choices=["batch64", "1080p", "4096", "foreground", "hard320"],
                     default="batch64",
                     help="batch64 (default): the 64-image mixed batch; 1080p / 4096: one "
                          "image per GPU; foreground: estimate_foreground_ml on a 1920x1080 "
-                         "image + matte")
+                         "image + matte; hard320: estimate_alpha_cf (hard constraints, ichol) "
+                         "on a 320x240 image")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", choices=["auto", "none"], default="none",
                     help="auto: run the launch-shape autotuner before timing; none (default): "
@@ -555,6 +558,190 @@ def run_foreground(args, rank, world, local):
         dist.destroy_process_group()
 
 
+HARD_METRIC = ("Mpix/s of estimate_alpha_cf (hard constraints, default ichol preconditioner, "
+               "cg rtol 1e-7)")
+
+
+def hard_inputs(rank):
+    """The 320x240 image of the reference's CPU-runnable configuration (seed 1 + rank)."""
+    from pymatting_b200.synthetic import make_matting_problem
+    img, tri, _a, _f = make_matting_problem(240, 320, 1 + rank, sigma=2.0, band=7,
+                                            unknown_fraction=0.12)
+    return img, tri
+
+
+def run_hard_reference(args, rank):
+    """The oracle's restatement of estimate_alpha_cf (C ichol, scipy), rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    img, tri = hard_inputs(0)
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.estimate_alpha_cf(img, tri)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    npx = tri.size
+    value = npx * len(times) / sum(times) / 1e6
+    line = {"metric": HARD_METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "estimate_alpha_cf_hard_ichol_320x240",
+                       "path": "oracle restatement of estimate_alpha_cf (C _ichol), 1 core"},
+            "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                             "sample": "one full 320x240 estimate_alpha_cf per step"},
+            "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def count_library_launches(fn):
+    """Kernels of this library launched by one call of fn (torch profiler's
+    CUDA activity, kernels named pmb::...); None when the profiler is
+    unavailable."""
+    try:
+        import torch
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        return sum(1 for e in prof.events()
+                   if e.device_type.name == "CUDA" and "pmb::" in e.name)
+    except Exception:       # noqa: BLE001 - reporting only
+        return None
+
+
+def run_hard(args, rank, world, local):
+    """estimate_alpha_cf on the 320x240 hard-constraint image, one image per GPU."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import pymatting_b200 as pm
+    from pymatting_b200.preconditioner import ichol
+    img, tri = hard_inputs(rank)
+    npx = tri.size
+    img_d = torch.as_tensor(img, device=dev)
+    tri_d = torch.as_tensor(tri, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    factors = []
+
+    def keep_ichol(A):
+        M = ichol(A)
+        factors.append((M, A))
+        return M
+
+    def step():
+        return pm.estimate_alpha_cf(img_d, tri_d, preconditioner=keep_ichol)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world > 1:
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    t0 = time.time()
+    times, fms = [], []
+    for _ in range(args.steps):
+        factors.clear()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        alpha_d = step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        fms.append(factors[-1][0].factor.factor_ms())
+    clocks.window(t0, time.time())
+    barrier()
+    ms = max_over_ranks(sum(times) / len(times))
+    # end to end through the public API with host numpy buffers
+    e2e_times = []
+    for s in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        alpha_h = pm.estimate_alpha_cf(img, tri)
+        dt = time.perf_counter() - t1
+        if s >= args.warmup:
+            e2e_times.append(dt)
+    e2e_ms = max_over_ranks(1e3 * sum(e2e_times) / len(e2e_times))
+    clock_rec = clocks.stop()
+    launches = count_library_launches(step)
+    if rank == 0:
+        from pymatting_b200.laplacian import device_csr_arrays
+        peak, peak_kind = measured_peaks()
+        M, A = factors[-1]
+        n = M.factor.n
+        nnz_a = int(device_csr_arrays(A)[1].numel())
+        nnz_l = int(M.factor.nnz)
+        alg_bytes = 16 * (nnz_a + nnz_l) + 36 * n
+        f_ms = sum(fms) / len(fms)
+        gbs = alg_bytes / (f_ms * 1e-3) / 1e9
+        line = {
+            "metric": HARD_METRIC, "value": world * npx / (ms * 1e-3) / 1e6, "unit": "Mpix/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "estimate_alpha_cf_hard_ichol_320x240", "image": "320x240x3",
+                       "unknowns": n, "factor_nnz": nnz_l, "levels": M.factor.levels(),
+                       "cluster_ctas": M.factor.cluster(),
+                       "l2": "flushed between steps (256 MB write)",
+                       "parallelism": "weak: one image per GPU, no collective"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / peak, "peak_source": peak_kind, "traffic": None,
+                         "kernel": "k_ichol_factor_cluster", "kernel_ms": f_ms,
+                         "bytes_per_launch": alg_bytes,
+                         "note": "latency-bound: the factor is a chain of one dependent "
+                                 "column per unknown (front on chip in a CTA cluster); bytes "
+                                 "are A's lower part in and L out"},
+            "e2e": {"value": world * npx / (e2e_ms * 1e-3) / 1e6, "unit": "Mpix/s",
+                    "h2d_bytes_per_step": int(img.nbytes + tri.nbytes),
+                    "d2h_bytes_per_step": int(npx * 8)},
+            "gpu_launches": None if launches is None else int(launches * args.steps),
+            "clocks": clock_rec,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            ref = None
+            spent, calls = 0.0, 0
+            while spent < 10.0 or calls < 3:
+                t1 = time.perf_counter()
+                ref = oracle.estimate_alpha_cf(img, tri)
+                spent += time.perf_counter() - t1
+                calls += 1
+            line["cpu_baseline"] = {"value": npx * calls / spent / 1e6, "unit": "Mpix/s",
+                                    "cores": 1, "kind": "port",
+                                    "sample": "%d full 320x240 estimate_alpha_cf calls "
+                                              "(oracle restatement, C ichol), %.1f s"
+                                              % (calls, spent)}
+            line["alpha_maxabs_vs_oracle"] = float(np.abs(alpha_h - ref).max())
+            line["alpha_maxabs_device_vs_host_call"] = float(
+                np.abs(alpha_d.cpu().numpy() - alpha_h).max())
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        barrier()
+        dist.destroy_process_group()
 
 
 # --------------------------------------------------------------------------
@@ -665,6 +852,12 @@ def main():
             run_foreground_reference(args, rank)
         else:
             run_foreground(args, rank, world, local)
+        return
+    if args.workload == "hard320":
+        if args.impl == "reference":
+            run_hard_reference(args, rank)
+        else:
+            run_hard(args, rank, world, local)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -412,6 +412,9 @@ int pmb_ichol_levels(const pmb_ichol* f);
  * distributed shared memory in the last pmb_ichol_factor (1..8), 0 when the
  * front was in global memory (bandwidth too wide), -1 before any factor. */
 int pmb_ichol_cluster(const pmb_ichol* f);
+/* Device time (CUDA events on the factor's stream) of the factorisation
+ * kernel in the last pmb_ichol_factor, in milliseconds; -1 before any. */
+float pmb_ichol_factor_ms(const pmb_ichol* f);
 /* Device pointers of the CSC factor (values, row indices, column pointers). */
 int pmb_ichol_factor_arrays(pmb_ichol* f, void** Lv, void** Lr, void** Lp);
 /* x = L^-T L^-1 b (CholeskyDecomposition.__call__, ichol.py:175-181). */

@@ -104,6 +104,7 @@ _SIGNATURES = {
                                  ctypes.POINTER(c_i64), c_vp]),
     "pmb_ichol_levels": (c_int, [c_vp]),
     "pmb_ichol_cluster": (c_int, [c_vp]),
+    "pmb_ichol_factor_ms": (ctypes.c_float, [c_vp]),
     "pmb_ichol_factor_arrays": (c_int, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp),
                                         ctypes.POINTER(c_vp)]),
     "pmb_ichol_apply": (c_int, [c_vp, c_vp, c_vp, c_vp]),

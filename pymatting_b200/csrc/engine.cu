@@ -1708,6 +1708,8 @@ struct Ichol {
     int64_t nnz = -1;
     int nlevels = 0;
     int cluster = -1;     // CTAs holding the front in the last factorisation (0: global memory)
+    cudaEvent_t ev_f0 = nullptr, ev_f1 = nullptr;   // around the factor kernel
+    float factor_ms = -1.0f;
     // Streamed solves (n <= kStreamMaxRows): chunk blocks of both sweeps.
     size_t o_blob = 0, o_prow = 0, o_pch = 0, blob_cap = 0;
     int stream_total = 0;  // chunks of both sweeps; 0: level-barrier solves
@@ -1914,6 +1916,11 @@ PMB_API int pmb_ichol_factor(pmb_ichol* p, const int64_t* Ap, const int64_t* Ar,
     PMB_CUDA(cudaMemsetAsync(I.ws + I.o_pat, 0, (size_t)(W * W), s));
     ichol_launch_init(n, Ap, Ar, Av, shift, I.at<double>(I.o_d), I.at<double>(I.o_rsum),
                       I.at<int>(I.o_level), I.at<unsigned long long>(I.o_band), s);
+    if (!I.ev_f0) {
+        PMB_CUDA(cudaEventCreate(&I.ev_f0));
+        PMB_CUDA(cudaEventCreate(&I.ev_f1));
+    }
+    PMB_CUDA(cudaEventRecord(I.ev_f0, s));
     I.cluster = ichol_launch_factor(n, W, Ap, Ar, Av, I.at<double>(I.o_d), I.at<double>(I.o_rsum),
                         I.at<int>(I.o_level), I.at<double>(I.o_F), I.at<uint8_t>(I.o_pat),
                         I.at<int>(I.o_cand), I.at<double>(I.o_keptv), I.at<int64_t>(I.o_kepti),
@@ -1921,9 +1928,11 @@ PMB_API int pmb_ichol_factor(pmb_ichol* p, const int64_t* Ap, const int64_t* Ar,
                         discard_threshold, max_nnz, relative_discard_threshold, diag_keep_discarded,
                         I.at<int64_t>(I.o_result), s);
     PMB_CUDA(cudaGetLastError());
+    PMB_CUDA(cudaEventRecord(I.ev_f1, s));
     int64_t res = 0;
     PMB_CUDA(cudaMemcpyAsync(&res, I.ws + I.o_result, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     PMB_CUDA(cudaStreamSynchronize(s));
+    PMB_CUDA(cudaEventElapsedTime(&I.factor_ms, I.ev_f0, I.ev_f1));
     *result = res;
     I.nnz = res;
     if (res < 0) return 0;
@@ -1962,6 +1971,8 @@ PMB_API int pmb_ichol_levels(const pmb_ichol* p) { return p ? p->I.nlevels : -1;
 
 PMB_API int pmb_ichol_cluster(const pmb_ichol* p) { return p ? p->I.cluster : -1; }
 
+PMB_API float pmb_ichol_factor_ms(const pmb_ichol* p) { return p ? p->I.factor_ms : -1.0f; }
+
 PMB_API int pmb_ichol_factor_arrays(pmb_ichol* p, void** Lv, void** Lr, void** Lp) {
     if (!p || !p->I.ws || p->I.nnz < 0) return fail(kErrState, "pmb_ichol_factor_arrays: no factor");
     if (Lv) *Lv = p->I.ws + p->I.o_Lv;
@@ -1991,6 +2002,10 @@ PMB_API int pmb_ichol_apply(pmb_ichol* p, const double* b, double* x, void* stre
 }
 
 PMB_API int pmb_ichol_destroy(pmb_ichol* p) {
+    if (p && p->I.ev_f0) {
+        cudaEventDestroy(p->I.ev_f0);
+        cudaEventDestroy(p->I.ev_f1);
+    }
     delete p;
     return 0;
 }

@@ -236,9 +236,10 @@ k_ichol_factor(int64_t n, int64_t W, const int64_t* __restrict__ Ap,
 
 // ---------------------------------------------------------------------------
 // The same factorisation with the front on chip: a cluster of C CTAs keeps the
-// W x W front in distributed shared memory, CTA r owning the contiguous slots
-// [r S, r S + S) (S = ceil(W / C)) with their FP64 values, pattern bytes, ring
-// entries of the diagonal d and of the dependency level. Per column j:
+// W x W front in distributed shared memory, CTA r owning the slots s with
+// s mod C = r (at most S = ceil(W / C) of them) with their FP64 values,
+// pattern bytes, ring entries of the diagonal d and of the dependency level.
+// Per column j:
 //
 //   phase F  warp 0 of EVERY CTA reads slot j from its owner (one DSMEM round
 //            trip) and runs the serial part of the column (pivot, threshold,
@@ -265,7 +266,7 @@ constexpr size_t kClSmemLimit = 227 * 1024 - 256;
 
 struct ClLayout {
     int64_t Wp, S;
-    size_t o_F, o_d, o_kv, o_cL, o_lev, o_ki, o_ci, o_own, o_pat, bytes;
+    size_t o_F, o_d, o_kv, o_cL, o_lev, o_ki, o_ci, o_own, o_pre, o_pat, bytes;
 };
 
 __host__ __device__ inline ClLayout cl_layout(int64_t W, int C) {
@@ -281,6 +282,7 @@ __host__ __device__ inline ClLayout cl_layout(int64_t W, int C) {
     L.o_ki = o;  o += (size_t)W * sizeof(int);
     L.o_ci = o;  o += (size_t)W * sizeof(int);
     L.o_own = o; o += (size_t)W * sizeof(int);
+    L.o_pre = o; o += (size_t)W * sizeof(int);
     L.o_pat = o; o += (size_t)(L.S * L.Wp);
     L.bytes = (o + 15) & ~(size_t)15;
     return L;
@@ -298,8 +300,10 @@ int ichol_cluster_size(int64_t W) {
 
 // NCH: 32-offset chunks of a front column held in registers by phase F
 // (ceil((W - 1) / 32) rounded up to 2, 4, 8 or 14). Slots are tracked
-// incrementally in 32-bit arithmetic; phase F computes every chunk's
-// quotient and keep decision before the ballots so the divisions overlap.
+// incrementally in 32-bit arithmetic. Phase F compacts the column's
+// candidates first and divides only those, lane-strided: an FP64 division
+// costs about 130 cycles of latency (about 300 with a zero numerator), and
+// a column has a quarter of its offsets as candidates or fewer.
 template <int NCH>
 __global__ void __launch_bounds__(kClThreads, 1)
 k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
@@ -312,7 +316,8 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char cl_smem[];
     __shared__ int64_t s_nnz;
-    __shared__ int s_m, s_cn, s_nown, s_levj, s_fail;
+    __shared__ int s_cn, s_nown, s_np, s_levj, s_kept, s_owner, s_fail;
+    __shared__ double s_sj;
     const ClLayout Ly = cl_layout(W, C);
     const int S = (int)Ly.S, Wp = (int)Ly.Wp;
     double* F = reinterpret_cast<double*>(cl_smem + Ly.o_F);
@@ -323,11 +328,16 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
     int* ki = reinterpret_cast<int*>(cl_smem + Ly.o_ki);
     int* ci = reinterpret_cast<int*>(cl_smem + Ly.o_ci);
     int* own = reinterpret_cast<int*>(cl_smem + Ly.o_own);
+    int* pre = reinterpret_cast<int*>(cl_smem + Ly.o_pre);
     uint8_t* pat = cl_smem + Ly.o_pat;
     const int r = (int)cluster.block_rank();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const int lo = r * S, hi = min(lo + S, W);             // slots owned here: [lo, hi)
+    // Slot s belongs to CTA s mod C at local index s / C (interleaved, so the
+    // heavy targets just below the pivot spread over the cluster). s < 449
+    // and C <= 8: (s * mC) >> 16 with mC = ceil(65536 / C) is s / C exactly.
+    const int mC = (65536 + C - 1) / C;
+    auto divC = [mC](int v) { return (v * mC) >> 16; };
 
     // Initial front: columns 0 .. min(W, n) - 1 sit in slots 0 .. W - 1.
     for (int q = threadIdx.x; q < S * Wp; q += blockDim.x) {
@@ -335,8 +345,8 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
         pat[q] = 0;
     }
     __syncthreads();
-    for (int ls = warp; lo + ls < hi; ls += nw) {
-        const int64_t c = lo + ls;
+    for (int ls = warp; r + ls * C < W; ls += nw) {
+        const int64_t c = r + ls * C;
         if (c >= n) continue;
         for (int64_t k = Ap[c] + lane; k < Ap[c + 1]; k += 32) {
             const int64_t i = Ar[k];
@@ -372,7 +382,7 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
 
     for (int64_t j = 0; j < n; ++j) {
         if (warp == 0) {
-            const int f = slot / S, lsj = slot - f * S;
+            const int lsj = divC(slot), f = slot - lsj * C;
             const double rs = rs_next;
             if (j + 1 < n) rs_next = rsum[j + 1];
             const double* Fj = cluster.map_shared_rank(F, f) + lsj * Wp;
@@ -403,72 +413,88 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
             else if (nnz + 1 + cn > max_nnz || nnz + 1 + cn > cap) fail = -2;   // ichol.py:82-83
             const bool owner = f == r;
             const int64_t nnz0 = nnz + 1;
+            // Candidates in ascending rows: value and offset, compacted.
+            int cpos = 0;
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) {
+                if (flag[k]) {
+                    const int q = cpos + __popc(fm[k] & lt);
+                    cL[q] = a[k];
+                    ci[q] = 1 + lane + 32 * k;
+                }
+                cpos += __popc(fm[k]);
+            }
+            __syncwarp();
             int kept = 0, nown = 0;
             if (!fail) {
                 const double sj = sqrt(dj);
                 const double rel = rel_discard * rs;
-                if (owner && lane == 0) {
-                    Lv[nnz] = sj;
-                    Lr[nnz] = j;
-                    level[j] = levj;
-                }
-                bool keep[NCH], mine[NCH];
-#pragma unroll
-                for (int k = 0; k < NCH; ++k) {
-                    // Lanes without a candidate divide 1.0: a zero numerator
-                    // would take the division's slow path on every lane.
-                    const double q = (flag[k] ? a[k] : 1.0) / sj;
-                    const double L = flag[k] ? q : 0.0;
-                    keep[k] = flag[k] && fabs(L) > discard && fabs(a[k]) > rel;
-                    a[k] = L;
-                    int sl = slot + 1 + lane + 32 * k;
-                    if (sl >= W) sl -= W;
-                    mine[k] = keep[k] && sl >= lo && sl < hi;
-                }
-                int cpos = 0;
-#pragma unroll
-                for (int k = 0; k < NCH; ++k) {
-                    const int o = 1 + lane + 32 * k;
-                    const unsigned km = __ballot_sync(0xffffffffu, keep[k]);
-                    const unsigned om = __ballot_sync(0xffffffffu, mine[k]);
-                    if (flag[k]) {
-                        const int q = cpos + __popc(fm[k] & lt);
-                        cL[q] = a[k];
-                        ci[q] = keep[k] ? o : -o;
+                if (lane == 0) s_sj = sj;
+                // One quotient per candidate, lane-strided (the candidates
+                // of a column are a quarter of its offsets or fewer).
+                for (int t0 = 0; t0 < cn; t0 += 32) {
+                    const int t = t0 + lane;
+                    double L = 0.0;
+                    bool keep = false, mine = false;
+                    int o = 0;
+                    if (t < cn) {
+                        const double av = cL[t];
+                        o = ci[t];
+                        L = av / sj;
+                        keep = fabs(L) > discard && fabs(av) > rel;
+                        int sl = slot + o;
+                        if (sl >= W) sl -= W;
+                        mine = keep && sl - divC(sl) * C == r;
+                        cL[t] = L;
+                        ci[t] = keep ? o : -o;
                     }
-                    if (keep[k]) {
+                    const unsigned km = __ballot_sync(0xffffffffu, keep);
+                    const unsigned om = __ballot_sync(0xffffffffu, mine);
+                    if (keep) {
                         const int pos = kept + __popc(km & lt);
-                        kv[pos] = a[k];
+                        kv[pos] = L;
                         ki[pos] = o;
-                        if (owner) {
-                            Lv[nnz0 + pos] = a[k];
-                            Lr[nnz0 + pos] = j + o;
-                        }
-                        if (mine[k]) own[nown + __popc(om & lt)] = pos;
+                        if (mine) own[nown + __popc(om & lt)] = pos;
                     }
-                    cpos += __popc(fm[k]);
                     kept += __popc(km);
                     nown += __popc(om);
                 }
             }
+            // Exclusive prefix of the owned targets' pair counts (kept - 1 -
+            // pb pairs for the target at kept index pb).
+            int np = 0;
+            for (int t0 = 0; t0 < nown; t0 += 32) {
+                const int t = t0 + lane;
+                const int cnt = t < nown ? kept - 1 - own[t] : 0;
+                int incl = cnt;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                if (t < nown) pre[t] = np + incl - cnt;
+                np += __shfl_sync(0xffffffffu, incl, 31);
+            }
             if (lane == 0) {
                 s_fail = fail;
                 if (!fail) {
-                    s_m = kept;
                     s_cn = cn;
                     s_nown = nown;
+                    s_np = np;
                     s_levj = levj;
+                    s_kept = kept;
+                    s_owner = owner;
                     s_nnz = nnz0 + kept;
-                    if (owner) Lp[j + 1] = nnz0 + kept;
                 }
             }
         } else if (warp == nw - 1) {
             // Recycle slot (j - 1) % W for column c = j - 1 + W (its readers
             // all passed the barrier of column j - 1).
             const int64_t c = j - 1 + W;
-            if (j >= 1 && c < n && pslot >= lo && pslot < hi) {
-                double* Fc = F + (pslot - lo) * Wp;
-                uint8_t* Pc = pat + (pslot - lo) * Wp;
+            const int pls = divC(pslot);
+            if (j >= 1 && c < n && pslot - pls * C == r) {
+                double* Fc = F + pls * Wp;
+                uint8_t* Pc = pat + pls * Wp;
                 for (int o = lane; o < W; o += 32) {
                     Fc[o] = 0.0;
                     Pc[o] = 0;
@@ -491,8 +517,8 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
                     }
                 }
                 if (lane == 0) {
-                    dl[pslot - lo] = ed0;
-                    lev[pslot - lo] = 0;
+                    dl[pls] = ed0;
+                    lev[pls] = 0;
                 }
             }
             // Entries of column j + W for the next column's recycle.
@@ -516,32 +542,58 @@ k_ichol_factor_cluster(int64_t n, int W, int C, const int64_t* __restrict__ Ap,
         __syncthreads();
         if (s_fail) break;
         // Phase P: CTA-local updates of the rows and front columns owned here.
-        const int m = s_m, nown = s_nown, cn = s_cn, lj = s_levj + 1;
-        for (int t = warp; t < nown; t += nw) {
-            const int pb = own[t];
+        // Pairs are spread evenly over the threads (target found by binary
+        // search of the prefix); the diagonal and level updates go to the
+        // threads with the fewest pairs.
+        const int nown = s_nown, cn = s_cn, np = s_np, lj = s_levj + 1;
+        // The owner of slot j writes column j of L from the kept list
+        // (threads 128.., which have the fewest pairs besides the diagonal
+        // and level updates).
+        if (s_owner) {
+            const int kept = s_kept;
+            const int64_t end = s_nnz, nnz = end - kept - 1;
+            for (int q = (int)((threadIdx.x + blockDim.x - 128) % blockDim.x); q <= kept;
+                 q += blockDim.x) {
+                if (q == 0) {
+                    Lv[nnz] = s_sj;
+                    Lr[nnz] = j;
+                    level[j] = s_levj;
+                    Lp[j + 1] = end;
+                } else {
+                    Lv[nnz + q] = kv[q - 1];
+                    Lr[nnz + q] = j + ki[q - 1];
+                }
+            }
+        }
+        for (int p = threadIdx.x; p < np; p += blockDim.x) {
+            int tl = 0, th = nown - 1;
+            while (tl < th) {
+                const int mid = (tl + th + 1) >> 1;
+                if (pre[mid] <= p) tl = mid;
+                else th = mid - 1;
+            }
+            const int pb = own[tl];
+            const int q = pb + 1 + (p - pre[tl]);
             const int ob = ki[pb];
             int sl = slot + ob;
             if (sl >= W) sl -= W;
-            double* Fb = F + (sl - lo) * Wp;
-            uint8_t* Pb = pat + (sl - lo) * Wp;
-            const double Lb = kv[pb];
-            for (int q = pb + 1 + lane; q < m; q += 32) {
-                const int o = ki[q] - ob;
-                Fb[o] -= kv[q] * Lb;
-                Pb[o] = 1;
-            }
+            const int o = ki[q] - ob;
+            F[divC(sl) * Wp + o] -= kv[q] * kv[pb];
+            pat[divC(sl) * Wp + o] = 1;
         }
-        for (int q = threadIdx.x; q < cn; q += blockDim.x) {
+        for (int q = (int)blockDim.x - 1 - (int)threadIdx.x; q < cn; q += blockDim.x) {
             const int code = ci[q];
             int sl = slot + (code < 0 ? -code : code);
             if (sl >= W) sl -= W;
-            if (sl < lo || sl >= hi || (!diag_keep && code < 0)) continue;
-            dl[sl - lo] -= cL[q] * cL[q];
+            const int ls = divC(sl);
+            if (sl - ls * C != r || (!diag_keep && code < 0)) continue;
+            dl[ls] -= cL[q] * cL[q];
         }
-        for (int t = threadIdx.x; t < nown; t += blockDim.x) {
+        for (int t = (int)(threadIdx.x ^ (blockDim.x >> 1)); t < nown; t += blockDim.x) {
             int sl = slot + ki[own[t]];
             if (sl >= W) sl -= W;
-            if (lev[sl - lo] < lj) lev[sl - lo] = lj;
+            const int ls = divC(sl);
+            if (lev[ls] < lj) lev[ls] = lj;
         }
         pslot = slot;
         slot = slot + 1 == W ? 0 : slot + 1;
@@ -613,9 +665,56 @@ __global__ void k_row_fill(int64_t n, const int64_t* __restrict__ Lp, const int6
     }
 }
 
+// Rows of up to kRowSortMax entries: one warp per row, entries in registers
+// (8 a lane); each entry's place is the number of smaller column indices in
+// its row (the indices of a row are distinct), counted by broadcasting every
+// key through the warp.
+constexpr int kRowSortMax = 256;
+
+__global__ void k_row_sort_warp(int64_t n, const int64_t* __restrict__ Rp, int64_t* Rc, double* Rv) {
+    const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int64_t b = Rp[i];
+    const int64_t len = Rp[i + 1] - b;
+    if (len <= 1 || len > kRowSortMax) return;
+    int64_t c[8];
+    double v[8];
+    int rank[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int k = lane + 32 * u;
+        c[u] = k < len ? Rc[b + k] : INT64_MAX;
+        v[u] = k < len ? Rv[b + k] : 0.0;
+        rank[u] = 0;
+    }
+    const int U = (int)((len + 31) >> 5);
+#pragma unroll
+    for (int u2 = 0; u2 < 8; ++u2) {
+        if (u2 < U) {
+            for (int src = 0; src < 32; ++src) {
+                const int64_t key = __shfl_sync(0xffffffffu, c[u2], src);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) rank[u] += key < c[u] ? 1 : 0;
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int k = lane + 32 * u;
+        if (k < len) {
+            Rc[b + rank[u]] = c[u];
+            Rv[b + rank[u]] = v[u];
+        }
+    }
+}
+
+// Longer rows: insertion sort by one thread.
 __global__ void k_row_sort(int64_t n, const int64_t* __restrict__ Rp, int64_t* Rc, double* Rv) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (Rp[i + 1] - Rp[i] <= kRowSortMax) return;
     for (int64_t k = Rp[i] + 1; k < Rp[i + 1]; ++k) {
         const int64_t c = Rc[k];
         const double v = Rv[k];
@@ -813,9 +912,18 @@ k_ichol_solve_stream(int64_t n, int total, StreamFirst first, const unsigned cha
             const int* col = reinterpret_cast<const int*>(val + ents);
             for (int k = warp; k < rows; k += nw) {
                 const StreamRow rw = rec[k];
+                const double* rv = val + rw.start;
+                const int* rc = col + rw.start;
                 double acc = 0.0;
-                for (int e = lane; e < rw.count; e += 32)
-                    acc += val[rw.start + e] * sx[col[rw.start + e]];
+                int e = lane;
+                for (; e + 32 < rw.count; e += 64) {     // two terms' loads in flight
+                    const double v0 = rv[e], v1 = rv[e + 32];
+                    const int c0 = rc[e], c1 = rc[e + 32];
+                    const double x0 = sx[c0], x1 = sx[c1];
+                    acc += v0 * x0;
+                    acc += v1 * x1;
+                }
+                if (e < rw.count) acc += rv[e] * sx[rc[e]];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
                 if (lane == 0) sx[rw.row] = (sx[rw.row] - acc) / rw.diag;
@@ -993,6 +1101,7 @@ void ichol_launch_row_fill(int64_t n, const int64_t* Lp, const int64_t* Lr, cons
                            cudaStream_t s) {
     if (n > 0) {
         k_row_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Lp, Lr, Lv, rfill, Rc, Rv);
+        k_row_sort_warp<<<(unsigned)((n * 32 + 255) / 256), 256, 0, s>>>(n, Rp, Rc, Rv);
         k_row_sort<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, Rp, Rc, Rv);
     }
 }

@@ -266,6 +266,10 @@ class IcholFactor:
     def levels(self):
         return int(_ffi.lib().pmb_ichol_levels(self._h))
 
+    def factor_ms(self):
+        """Device time of the last factorisation kernel (ms)."""
+        return float(_ffi.lib().pmb_ichol_factor_ms(self._h))
+
     def cluster(self):
         """CTAs that held the band front on chip in the last factorisation
         (0: the front was in global memory)."""

@@ -26,7 +26,7 @@ def cluster_size(W):
     for C in range(1, 9):
         Wp = (W + 7) & ~7
         S = (W + C - 1) // C
-        size = S * Wp * 8 + S * 8 + 2 * W * 8 + S * 4 + 3 * W * 4 + S * Wp
+        size = S * Wp * 8 + S * 8 + 2 * W * 8 + S * 4 + 4 * W * 4 + S * Wp
         if (size + 15) & ~15 <= 227 * 1024 - 256:
             return C
     return 0

@@ -328,16 +328,17 @@ def test_foreground_cf_neighbour_sets():
         pm.estimate_foreground_cf(np.zeros((4, 4, 3)), np.zeros((4, 4)), neighbors=[(1, 1)])
 
 
-def test_bench_reference_arm_foreground_line():
-    """bench.py --impl reference --workload foreground runs the oracle on the
-    host and prints one JSON line with the contract's keys."""
+@pytest.mark.parametrize("workload", ["foreground", "hard320"])
+def test_bench_reference_arm_line(workload):
+    """bench.py --impl reference --workload foreground / hard320 runs the
+    oracle on the host and prints one JSON line with the contract's keys."""
     import json
     import subprocess
     import sys
     import os
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
-                          "--workload", "foreground", "--steps", "1", "--warmup", "0"],
+                          "--workload", workload, "--steps", "1", "--warmup", "0"],
                          capture_output=True, text=True, timeout=600, cwd=root)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
