@@ -218,3 +218,7 @@ def test_soft_1080p_fp64_and_mixed(pm):
     batch = AlphaBatch([img], [tri], precision="mixed")
     xm = batch.solve().cpu().numpy()
     assert np.linalg.norm(b - A.dot(xm)) / np.linalg.norm(b) <= 1e-7
+    # The last FP32 phase stops at the FP64 tolerance, so FP32 arithmetic
+    # costs no extra iterations here.
+    sm = batch.stats()[0]
+    assert sm.iters <= s64.iters + 1, (sm.iters, s64.iters)
