@@ -932,7 +932,8 @@ static void cg_iteration(Stencil& S, int reorth) {
                        v.p0, v.p1, v.ap, st, S.partials(), S.err(), s);
     prof_mark(S, kPkApply);
     const bool mixed = S.precision == 1;
-    launch_cg_update<T>(S.precond, LaunchCfg{persistent_grid(S.flat0)}, S.flat0.wl, v.P, v.x, v.r,
+    const int upd_grid = std::min(persistent_grid(S.flat0), 148 * resident_cg_update<T>(S.precond));
+    launch_cg_update<T>(S.precond, LaunchCfg{upd_grid}, S.flat0.wl, v.P, v.x, v.r,
                         v.z, v.p0, v.p1, v.ap, v.dr, reorth, mixed ? 1 : 0, S.err() + kPendingSlot, st,
                         S.partials(), s);
     prof_mark(S, kPkUpdate);

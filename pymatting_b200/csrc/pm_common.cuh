@@ -29,7 +29,10 @@ constexpr int kTX = 64;      // fine tile width
 constexpr int kTY = 8;       // fine tile height
 constexpr int kThreads = 256;      // element-wise kernels
 constexpr int kTileThreads = 512;  // tiled stencil kernels: one pixel per thread
-constexpr int kFlat = 4096;  // elements per tile of the element-wise kernels
+// Elements per tile of the element-wise kernels. 8192 halves the per-chunk
+// barriers and directory lookups of the flat loops against 4096 (the FP32 CG
+// update: 0.38 -> 0.31 ms per iteration of the 64-image batch).
+constexpr int kFlat = 8192;
 
 // Shared-memory boxes loaded by TMA around a fine tile at (x0, y0): origin
 // (x0 - kBOX, y0 - 2), kBW x kBH elements. x0 - kBOX keeps the box start

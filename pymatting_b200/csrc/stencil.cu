@@ -7,7 +7,7 @@
 // operator planes (72 x 12 x 13), 2D boxes hold the vector operands; the
 // hardware zero-fills everything outside the image, which supplies the
 // stencil's border terms. The kernels then read operators and operands from
-// shared memory only. Element-wise kernels stream 1024-element chunks.
+// shared memory only. Element-wise kernels stream kFlat-element chunks.
 //
 // Every kernel walks a WorkList of tiles over a batch of grids (images of
 // different sizes, or the same multigrid level of several images) with a
@@ -573,7 +573,7 @@ k_cg_apply(WorkList wl, const CUtensorMap* maps, int zslot, T* p0, T* p1, T* Ap,
     tile_loop<kTY, kTX>(wl, st, pipe, s_m, s_g, issue, body, flush);
 }
 
-// Element-wise loop over a flat work list (1024-element chunks) with the same
+// Element-wise loop over a flat work list (kFlat-element chunks) with the same
 // per-CTA, per-image flush as the tiled kernels. Chunks cover the pitched
 // rows; padding columns are skipped.
 template <int GATE = kGateRunning, typename Body, typename Flush>
@@ -2498,6 +2498,19 @@ template <typename T> int resident_cg_apply(int vec, int stages) {
     return ns == 1 ? occupancy_of(k_cg_apply_v<T, 2, 1>, tile_threads_v<2>(), sm)
                    : occupancy_of(k_cg_apply_v<T, 2, 2>, tile_threads_v<2>(), sm);
 }
+// Resident CTAs per SM of k_cg_update (a register limit, below the flat
+// lists' default of 8: a persistent grid beyond it would run a second, thin
+// wave of CTAs after the first).
+template <typename T> int resident_cg_update(int prec) {
+    static int cached[3] = {0, 0, 0};
+    const int k = prec == kPrecNone ? 0 : (prec == kPrecJacobi ? 1 : 2);
+    if (!cached[k]) {
+        cached[k] = k == 0 ? occupancy_of(k_cg_update<T, kPrecNone>, kThreads, 0)
+                  : k == 1 ? occupancy_of(k_cg_update<T, kPrecJacobi>, kThreads, 0)
+                           : occupancy_of(k_cg_update<T, kPrecVcycle>, kThreads, 0);
+    }
+    return cached[k];
+}
 template <typename T> int resident_down(int stages) {
     stencil_prepare();
     constexpr int V = kVSolve<T>;
@@ -2562,6 +2575,7 @@ void stencil_prepare() {
     template size_t smem_apply_v<T>(int);                                                         \
     template int resident_cg_apply<T>(int, int);                                                  \
     template int resident_down<T>(int);                                                           \
+    template int resident_cg_update<T>(int);                                                      \
     template int resident_up<T>(int, int);                                                        \
     template size_t smem_down_v<T>(int);                                                          \
     template size_t smem_up_v<T>(int);                                                            \

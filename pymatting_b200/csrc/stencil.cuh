@@ -61,6 +61,7 @@ template <typename T> size_t smem_up_v(int nst);
 // prolongation kernels for a vector width and buffer count (occupancy API).
 template <typename T> int resident_cg_apply(int vec, int stages);
 template <typename T> int resident_down(int stages);
+template <typename T> int resident_cg_update(int prec);
 template <typename T> int resident_up(int vec, int stages);
 // Width of the register-blocked restriction box (its TMA maps).
 template <typename T> int down_box_width();
