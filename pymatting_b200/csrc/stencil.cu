@@ -1291,31 +1291,59 @@ __global__ void k_convert_f32(const double* __restrict__ src, float* dst, int64_
 // Packing between user layout (contiguous h*w per image) and pitched grids
 // --------------------------------------------------------------------------
 
+// Grid g of element idx of the user layout (the last g with off[g] <= idx;
+// every grid has at least one element) and idx's position in that grid.
+// The offsets come from shared memory when the list has at most kDirGrids
+// grids; positions within one image fit 32 bits.
+struct PackLoc {
+    int g, y, x;
+};
+__device__ __forceinline__ PackLoc pack_locate(const GridDesc* grids, int ngrids,
+                                               const int64_t* off, int64_t idx) {
+    int lo = 0, hi = ngrids - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= idx) lo = mid;
+        else hi = mid - 1;
+    }
+    const int w = grids[lo].w;
+    const int local = (int)(idx - off[lo]);
+    const int y = local / w;
+    return PackLoc{lo, y, local - y * w};
+}
+
+__device__ __forceinline__ const int64_t* pack_offsets(int64_t* s_off, const int64_t* user_off,
+                                                       int ngrids) {
+    const bool fits = ngrids <= kDirGrids;
+    if (fits)
+        for (int i = threadIdx.x; i < ngrids; i += blockDim.x) s_off[i] = user_off[i];
+    __syncthreads();
+    return fits ? s_off : user_off;
+}
+
 template <typename TS, typename TD>
 __global__ void k_pack(const GridDesc* grids, int ngrids, const int64_t* user_off,
                        const TS* __restrict__ src, TD* dst, int64_t total) {
+    __shared__ int64_t s_off[kDirGrids];
+    const int64_t* off = pack_offsets(s_off, user_off, ngrids);
     int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     for (; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
-        int g = 0;
-        while (g + 1 < ngrids && user_off[g + 1] <= idx) ++g;
-        const GridDesc d = grids[g];
-        const int64_t local = idx - user_off[g];
-        const int y = (int)(local / d.w), x = (int)(local % d.w);
-        dst[d.voff + (int64_t)y * d.pitch + x] = (TD)src[idx];
+        const PackLoc q = pack_locate(grids, ngrids, off, idx);
+        const GridDesc& d = grids[q.g];
+        dst[d.voff + (int64_t)q.y * d.pitch + q.x] = (TD)src[idx];
     }
 }
 
 template <typename TS, typename TD>
 __global__ void k_unpack(const GridDesc* grids, int ngrids, const int64_t* user_off,
                          const TS* __restrict__ src, TD* dst, int64_t total) {
+    __shared__ int64_t s_off[kDirGrids];
+    const int64_t* off = pack_offsets(s_off, user_off, ngrids);
     int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     for (; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
-        int g = 0;
-        while (g + 1 < ngrids && user_off[g + 1] <= idx) ++g;
-        const GridDesc d = grids[g];
-        const int64_t local = idx - user_off[g];
-        const int y = (int)(local / d.w), x = (int)(local % d.w);
-        dst[idx] = (TD)src[d.voff + (int64_t)y * d.pitch + x];
+        const PackLoc q = pack_locate(grids, ngrids, off, idx);
+        const GridDesc& d = grids[q.g];
+        dst[idx] = (TD)src[d.voff + (int64_t)q.y * d.pitch + q.x];
     }
 }
 
