@@ -259,6 +259,16 @@ def gen_c1(pm):
                         alpha_unknown=alpha[unknown], frac=np.array([frac]))
 
 
+def gen_alpha_r2(pm):
+    """estimate_alpha_cf with laplacian_kwargs={"radius": 2} (default ichol),
+    on the 48x64 synthetic image of the device test of that option."""
+    from pymatting_b200.synthetic import make_matting_problem
+    img, tri, _, _ = make_matting_problem(48, 64, 9, sigma=2.0, band=4, unknown_fraction=0.2)
+    alpha = pm.estimate_alpha_cf(img, tri, laplacian_kwargs={"radius": 2})
+    np.savez_compressed(os.path.join(HERE, "alpha_cf_radius2.npz"),
+                        image_sum=np.array([img.sum(), tri.sum()]), alpha=alpha)
+
+
 def _fg_case(rng, h, w, depth=3, kind="random"):
     img = rng.random((h, w, depth)).astype(np.float32)
     if kind == "random":
@@ -471,6 +481,7 @@ def main():
     for name, fn in [("cf", lambda: gen_cf(pm, rng)), ("cg", lambda: gen_cg(pm)),
                      ("ichol", lambda: gen_ichol(pm, rng)), ("soft", lambda: gen_soft(pm)),
                      ("lemur", lambda: gen_lemur(pm, root)), ("c1", lambda: gen_c1(pm)),
+                     ("alpha_r2", lambda: gen_alpha_r2(pm)),
                      ("lkm", lambda: gen_lkm(pm, root, np.random.default_rng(77))),
                      ("foreground", lambda: gen_foreground(pm, root, np.random.default_rng(91))),
                      ("cutout", lambda: gen_cutout(pm, root)),

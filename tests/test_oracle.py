@@ -132,6 +132,20 @@ def test_synthetic_320x240_estimate_alpha_cf():
     np.testing.assert_allclose(alpha[unknown], g["alpha_unknown"], rtol=0, atol=1e-9)
 
 
+def test_estimate_alpha_cf_radius2_matches_reference():
+    """estimate_alpha_cf with laplacian_kwargs={"radius": 2}: the oracle's
+    composition (radius-2 Laplacian, L_U slicing, ichol, cg) against the
+    reference's own result on the image the device test of that option uses."""
+    from pymatting_b200.synthetic import make_matting_problem
+    g = golden("alpha_cf_radius2.npz")
+    img, tri, _, _ = make_matting_problem(48, 64, 9, sigma=2.0, band=4, unknown_fraction=0.2)
+    np.testing.assert_allclose([img.sum(), tri.sum()], g["image_sum"], rtol=1e-12)
+    alpha = oracle.estimate_alpha_cf(img, tri, laplacian_kwargs={"radius": 2})
+    np.testing.assert_allclose(alpha, g["alpha"], rtol=0, atol=1e-9)
+    r1 = oracle.estimate_alpha_cf(img, tri)
+    assert np.abs(g["alpha"] - r1).max() > 1e-6     # radius 2 is a different system
+
+
 def test_oracle_laplacian_vjp_matches_finite_differences():
     """The FP64 restatement of d(mu' L(I) x)/dI that the adjoint kernels are
     checked against, pinned by central differences of the oracle Laplacian."""
